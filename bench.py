@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Throughput of the SPH hot path on B200 (particle-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl uph|reference]
+
+Workload (the hydrostatic-tank configuration): still water 2.0 m wide x 1.0 m
+deep at dx = 0.002 m -- 500,000 fluid particles on a lattice, density set
+hydrostatically -- in an open tank with 3 wall layers, h = 1.3 dx,
+rho0 = 1000, gamma = 7, c0 = 10 sqrt(2 g), dt = 0.2 h / c0.  Synthetic data
+built from those numbers; no dataset is involved.
+
+A step is one leapfrog step of the hot path (neighbour search, the rate pass,
+kick-drift) over all particles, advanced on the device through the C ABI.
+The headline is the reference's own formulation (the drop-in "REF"
+profile) in FP64; `variants` adds the textbook WCSPH profile of the same
+configuration (cubic spline, algebraic Tait, Monaghan viscosity) in FP64 and
+with FP32 pair arithmetic.
+
+One process per GPU; with N > 1 every rank advances its own tank (replicas,
+no collective on the data path) and value = all ranks' particle-steps / the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200: plain SPH vs batched+surrogate at ≤1% ρ error"
+UNIT = "particle-steps/s"
+WORKLOAD = ("hydrostatic tank 2.0 x 1.0 m, dx=0.002 m (500,000 fluid particles) + 3 wall layers, h=1.3dx, "
+            "rho0=1000, gamma=7, c0=10*sqrt(2g), dt=0.2h/c0; REF (drop-in) physics, FP64")
+
+# Algorithmic bytes of one rate pass (the dominant kernel): every
+# interacting particle's 13 FP64 fields (x y u v ut vt rho rhot p pt m
+# 1/rho 1/rhot) + orig index + itype + its cell-list entry read once
+# (120 B), every fluid particle's 12 rates + Tait pressure written once and
+# its sponge factor read (112 B).  Neighbour re-reads are served on chip.
+PASS_BYTES_PER_SLOT = 13 * 8 + 4 + 4 + 8
+PASS_BYTES_PER_FLUID = 13 * 8 + 8
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_deck():
+    from uph_b200 import deck as D
+    return D.hydrostatic_tank(width=2.0, depth=1.0, dx=0.002, layers=3)
+
+
+# ---------------------------------------------------------------- clocks ----
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                if self.uuid and parts[1] != self.uuid:
+                    continue
+                rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower().startswith("active")})
+        pw = [float(r[4]) for r in rows if r[4].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+# ------------------------------------------------------------ CPU baseline ---
+
+def cpu_reference_run(deck, budget_s: float, max_steps: int, warmup: int = 1):
+    """The reference's own solver (oracle/_ref, compiled from its sources) on
+    the host cores: returns (particle-steps/s, steps timed, threads, kind)."""
+    from oracle import oracle as O
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    with tempfile.TemporaryDirectory() as tmp:
+        deck.write(tmp)
+        if os.path.exists(os.path.join(O.REF_DIR, "libuph_ref.so")):
+            run = O.RefRun(tmp, eta_override=deck.eta_override, fluid_capacity_pct=16)
+            kind = "reference"
+            step = run.step
+        else:
+            o = O.Oracle(deck.uph_params(), deck.initial_state())
+            kind = "port"
+            threads = 1
+            step = o.step
+        for _ in range(warmup):
+            step(1)
+        t0 = time.perf_counter()
+        step(1)
+        first = time.perf_counter() - t0
+        n = int(max(1, min(max_steps - 1, budget_s / max(first, 1e-9) - 1)))
+        t1 = time.perf_counter()
+        step(n)
+        total = first + (time.perf_counter() - t1)
+        if kind == "reference":
+            run.close()
+    steps = n + 1
+    return deck.n_fluid * steps / total, steps, threads, kind
+
+
+# ---------------------------------------------------------------- GPU arm ---
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from uph_b200._capi import PREC_FP32_PAIR, PROFILE_REF, PROFILE_WCSPH
+    from uph_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    deck = workload_deck()
+    nf, n_all = deck.n_fluid, deck.n_all
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(sim, k, sampler=None):
+        barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = sim.launch_count()
+        e0.record(stream)
+        sim.step(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        return e0.elapsed_time(e1), sim.launch_count() - l0, clocks
+
+    # --- headline: REF profile, FP64
+    sim = Simulation.from_deck(deck, profile=PROFILE_REF)
+    sim.set_stream(stream.cuda_stream)
+    sim.step(args.warmup)
+    sim.profile(True)
+    try:
+        uuid = torch.cuda.get_device_properties(dev).uuid
+        uuid = "GPU-" + str(uuid) if uuid else None
+    except Exception:
+        uuid = None
+    ms, launches, clocks = timed_steps(sim, args.steps, ClockSampler(uuid) if rank == 0 else None)
+    ktimes = sim.kernel_times()
+    stats = sim.stats()
+    sim.profile(False)
+    ms_max = max_over_ranks(ms)
+    value = world * nf * args.steps / (ms_max / 1e3)
+
+    pass_ms, pass_n = ktimes.get("rate_pass", (0.0, 0))
+    pass_avg_s = pass_ms / max(pass_n, 1) / 1e3
+    pass_bytes = n_all * PASS_BYTES_PER_SLOT + nf * PASS_BYTES_PER_FLUID
+    peak, peak_kind = load_peaks()
+    achieved = pass_bytes / pass_avg_s / 1e9 if pass_avg_s > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "rate_pass_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("ref_fp64_bytes_per_launch")
+
+    # --- e2e: every step through the C ABI with pinned host buffers:
+    # upload the full state, one step, download the full state
+    from uph_b200._capi import empty_state
+    st_host = {}
+    for name, a in deck.initial_state().items():
+        t = torch.empty(a.shape, dtype=torch.int32 if a.dtype == np.int32 else torch.float64, pin_memory=True)
+        arr = t.numpy()
+        arr[...] = a
+        st_host[name] = arr
+    out_host = {}
+    for name, a in empty_state(nf, n_all).items():
+        t = torch.empty(a.shape, dtype=torch.int32 if a.dtype == np.int32 else torch.float64, pin_memory=True)
+        out_host[name] = t.numpy()
+    h2d = sum(a.nbytes for a in st_host.values())
+    d2h = sum(a.nbytes for a in out_host.values())
+    k_e2e = max(1, min(args.steps, args.e2e_steps))
+    sim.upload(st_host, 0)
+    sim.step(1)
+    sim.download(out_host)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    itime = 1
+    for _ in range(k_e2e):
+        sim.upload(out_host if itime > 1 else st_host, itime)
+        sim.step(1)
+        sim.download(out_host)
+        itime += 1
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * nf * k_e2e / e2e_s
+    sim.close()
+
+    # --- variants: the WCSPH profile of the same configuration
+    variants = {}
+    k_var = max(1, min(args.steps, args.variant_steps))
+    for label, prof, prec in [("wcsph_fp64", PROFILE_WCSPH, 0), ("wcsph_fp32_pair", PROFILE_WCSPH, PREC_FP32_PAIR)]:
+        v = Simulation.from_deck(deck, profile=prof, precision=prec)
+        v.set_stream(stream.cuda_stream)
+        v.step(args.warmup)
+        v.profile(True)
+        vms, _, _ = timed_steps(v, k_var)
+        kt = v.kernel_times()
+        v.close()
+        vms = max_over_ranks(vms)
+        p_ms, p_n = kt.get("rate_pass", (0.0, 0))
+        variants[label] = {"value": world * nf * k_var / (vms / 1e3), "steps": k_var,
+                           "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1)}
+
+    return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
+                pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
+                traffic=traffic, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
+                deck=deck)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["uph", "reference"], default="uph")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--variant-steps", type=int, default=500)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "uph":
+        args.warmup = 3
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference's own CPU solver on rank 0's host cores; other ranks idle
+        if rank != 0:
+            return
+        deck = workload_deck()
+        value, steps, threads, kind = cpu_reference_run(deck, budget_s=60.0, max_steps=max(2, args.steps),
+                                                        warmup=min(args.warmup, 1))
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": deck.n_fluid / value * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host OpenMP"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                                 "sample": f"{steps} leapfrog steps of the full 500k-particle tank (bounded to ~60 s)"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    try:
+        r = gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, steps, threads, kind = cpu_reference_run(r["deck"], budget_s=args.cpu_budget, max_steps=1000)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{steps} leapfrog steps of the same 500k-particle tank on the host "
+                         f"(reference solver compiled from its sources; search stand-in for libnabo)"}
+    kt = {k: {"ms_total": round(v[0], 4), "launches": v[1]} for k, v in r["ktimes"].items() if v[1]}
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_fluid": r["deck"].n_fluid, "n_particles": r["deck"].n_all,
+                   "l2": "state 0.2 GB per GPU > 126 MB L2; no flush between steps",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
+                     "frac": r["achieved"] / r["peak"], "traffic": r["traffic"],
+                     "kernel": "rate pass (k_ref_pass)", "bytes_per_launch": r["pass_bytes"],
+                     "avg_launch_ms": r["pass_avg_s"] * 1e3, "peak_source": r["peak_kind"]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": r["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "steps": r["k_e2e"],
+                "how": "per step: uph_sim_upload of the full state from pinned host memory, uph_sim_step(1), "
+                       "uph_sim_download of the full state"},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+        "kernel_ms": kt,
+        "variants": r["variants"],
+        "stats": {"niac": r["stats"]["niac"], "max_neighbors": r["stats"]["max_neighbors"]},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

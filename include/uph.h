@@ -1,0 +1,234 @@
+/*
+ * uph.h -- C ABI of the B200 SPH hot path.
+ *
+ * The library advances the reference solver's per-timestep hot path on one
+ * GPU: neighbour search (cell list in place of the kd-tree), the smoothing
+ * kernel, the continuity and Tait-EOS update, pressure / viscous / wall forces
+ * and the leapfrog kick-drift.  Every entry point takes plain pointers and
+ * sizes, returns a uph_status and never exits the process.
+ *
+ * Particle order and layout follow the reference's System struct
+ * (src/lib/System.h:13-153): index ranges
+ *     [0, n_fluid)                          fluid
+ *     [n_fluid, +n_solid)                   solid
+ *     [.., +n_fixed)                        fixed boundary
+ *     [.., +n_moving)                       moving boundary
+ * and vectors are row-major [n][2] doubles, exactly the memory behind the
+ * reference's double** matrices (System.c:10-18, CreateMatrix), so a caller
+ * can pass sys->Position[0] and friends directly.
+ *
+ * Reference interfaces each group replaces:
+ *   uph_search_neighbors  <- SearchNeighbors       src/lib/Search.cc:5
+ *   uph_sim_derivatives   <- derivatives           src/lib/derivatives.h:12 (derivatives.c:3137)
+ *   uph_sim_step          <- the time loop         src/bin/sph.cc:90-168
+ *   uph_params_from_deck  <- CreateSystem params   src/lib/System.c:38-345
+ *   uph_deck_read         <- input + inputbp read  src/lib/input.c:22-164, src/lib/inputbp.c:12-191
+ * The layout-compatible System drop-in (derivatives / SearchNeighbors with
+ * the reference's own signatures) is declared in uph_system.h.
+ */
+#ifndef UPH_H
+#define UPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UPH_ABI_VERSION 1
+
+typedef enum uph_status {
+  UPH_OK = 0,
+  UPH_BAD_ARG = 1,           /* a pointer, size or parameter is invalid */
+  UPH_OUT_OF_DOMAIN = 2,     /* a particle left the cell grid's domain */
+  UPH_NEIGHBOR_OVERFLOW = 3, /* a pair or cell capacity was exceeded */
+  UPH_NAN = 4,               /* a non-finite value appeared in the state */
+  UPH_TIMEOUT = 5,           /* a bounded device-side wait gave up */
+  UPH_CUDA_ERROR = 6,        /* a CUDA runtime call failed */
+  UPH_NO_DEVICE = 7,         /* no CUDA device is visible */
+  UPH_UNSUPPORTED = 8,       /* a reference mode this library does not implement */
+  UPH_OUT_OF_MEMORY = 9,
+  UPH_IO_ERROR = 10          /* a deck file is missing or malformed */
+} uph_status;
+
+/* Physics profiles.
+ *   REF   : the reference's active formulation, derivatives.c:4196-4326 with
+ *           flagInitSimul == 1 -- poly-7 convolution / deconvolution kernel
+ *           pair, predictor rates, local fluctuations, rate-form Tait with
+ *           pressure / density diffusion, single-step deviatoric viscosity,
+ *           gravity, sponge layer and the selected wall force.
+ *   WCSPH : textbook weakly-compressible SPH on the same particles: the
+ *           reference's cubic spline Kernel() (derivatives.c:44-66),
+ *           continuity, algebraic Tait EOS (derivatives.c:1674-1682) feeding
+ *           the pressure force, Monaghan artificial viscosity (Monaghan 1992,
+ *           ARA&A 30:543, beta = 0) and the reference's wall forces, advanced
+ *           with the same leapfrog structure as sph.cc:90-168. */
+enum { UPH_PROFILE_REF = 0, UPH_PROFILE_WCSPH = 1 };
+
+/* Pair arithmetic: FP64 everywhere, or (WCSPH only) FP32 pair forces and
+ * density rates with FP64 positions, velocities and integration. */
+enum { UPH_PREC_FP64 = 0, UPH_PREC_FP32_PAIR = 1 };
+
+typedef struct uph_params {
+  int32_t profile;   /* UPH_PROFILE_* */
+  int32_t precision; /* UPH_PREC_* */
+  int32_t n_fluid, n_solid, n_fixed, n_moving;
+
+  /* parameters.dat fields, in file order (System.c:60-94) */
+  double stroke, wave_period, local_depth, flat_bottom_length;
+  double density0, adiabatic_constant, gravity, dx, dy;
+  int32_t dim;
+  double viscosity0, mach_number, peclet_number, epsilon, alpha;
+  int32_t virtual_type, print_step, screen_step;
+  double time_step, lid_velocity;
+  int32_t near_neighbor, select_boundary_force;
+  double lennard_select, spring_constant0, damping_constant0;
+  int32_t flag_init_simul, gravity_flag;
+  double thermal_diffusivity0;
+  int32_t moving_boundary, number_of_initialization_steps;
+  double pressure_probe_x, pressure_probe_y;
+  int32_t stress_type, dissipation_control_volume;
+
+  /* derived values (System.c:292-335, input.c:107) */
+  double speed_of_sound;     /* c0 */
+  double compression_factor; /* B = rho0 c0^2 / gamma */
+  double omega;              /* 2 pi / wave_period */
+  double eta;                /* h = eta * dx */
+  double h;                  /* smoothing length of every particle */
+  double lennard_coefficient;
+  double sponge_factor0, sponge_position0;
+  int32_t wave_absorption;
+
+  /* WCSPH only: Monaghan viscosity coefficient (beta = 0) */
+  double av_alpha;
+
+  /* Neighbour search.  knn_cap = 0 keeps every pair inside the radius.  The
+   * reference keeps only each fluid query's 40 nearest points
+   * (derivatives.c:1085); both agree whenever no query has more than 39
+   * in-radius neighbours, which uph_sim_stats reports. */
+  int32_t knn_cap;
+
+  /* Cell-grid domain: every interacting particle must stay inside
+   * [lo, hi] or the step fails with UPH_OUT_OF_DOMAIN. */
+  double domain_lo[2], domain_hi[2];
+} uph_params;
+
+/* Host particle arrays in the reference's layout.  "all" arrays hold
+ * n = n_fluid + n_solid + n_fixed + n_moving entries, "fluid" arrays n_fluid.
+ * Field names are the reference's System names.  A NULL pointer is allowed
+ * where noted. */
+typedef struct uph_state {
+  double *Position;            /* all  [n][2] */
+  double *Velocity;            /* all  [n][2] */
+  double *localVelocity;       /* all  [n][2] */
+  double *density;             /* all */
+  double *localDensity;        /* all */
+  double *DynamicPressure;     /* all */
+  double *localPressure;       /* all */
+  double *mass;                /* all */
+  int32_t *itype;              /* all */
+  double *Velocity_min;        /* fluid [n_fluid][2] */
+  double *density_min;         /* fluid */
+  double *DynamicPressure_min; /* fluid */
+  double *spongeFactor;        /* fluid, may be NULL (zero) */
+  /* rates of the last derivatives() evaluation (fluid) */
+  double *ddensitydt, *dpdt, *dvdt;                      /* dvdt [n_fluid][2] */
+  double *ddensitydt_approx, *dpdt_approx, *dvdt_approx; /* dvdt_approx [n_fluid][2] */
+  double *densityFluctuation, *pressureFluctuation;      /* fluid */
+  double *velocityFluctuation;                           /* fluid [n_fluid][2] */
+  double *Pressure;                                      /* all, algebraic Tait (diagnostic) */
+} uph_state;
+
+typedef struct uph_stats {
+  int64_t niac;            /* interaction pairs (i < j) of the last evaluation */
+  int32_t max_neighbors;   /* largest in-radius neighbour count of a fluid particle */
+  int32_t itime;           /* completed leapfrog steps */
+  double kinetic_energy;   /* sum 0.5 m |v|^2 over fluid (derivatives.c:2254-2264) */
+  double potential_energy; /* sum m g y over fluid */
+  double total_mass;       /* sum m over fluid */
+  double max_abs_density_error; /* max |rho - rho0| / rho0 over fluid */
+} uph_stats;
+
+typedef struct uph_sim uph_sim;
+
+/* ---- set-up -------------------------------------------------------------- */
+
+/* Fills `out` from the 34-field parameters.dat (System.c:60-94) and applies the
+ * derivations of System.c:292-335.  Counts are left to the caller (or
+ * uph_deck_read).  eta_override > 0 replaces eta = sqrt(nearNeighbor / 4 pi). */
+uph_status uph_params_from_file(const char *parameters_dat, double eta_override, uph_params *out);
+
+/* Recomputes the derived fields of `p` from its parameters.dat fields. */
+uph_status uph_params_derive(uph_params *p, double eta_override);
+
+/* Reads a deck directory (parameters.dat + the particle files of
+ * input.c:57-72 / inputbp.c:88-150) into caller-owned arrays.  Call once with
+ * st == NULL to get the counts in *p, allocate, then again to fill. */
+uph_status uph_deck_read(const char *deck_dir, double eta_override, uph_params *p, uph_state *st);
+
+/* ---- resident simulation -------------------------------------------------- */
+
+/* Allocates device state for p's particle counts on the current CUDA device. */
+uph_status uph_sim_create(const uph_params *p, uph_sim **out);
+uph_status uph_sim_destroy(uph_sim *sim);
+
+/* Issues all later work of `sim` on this cudaStream_t (NULL: the sim's own). */
+uph_status uph_sim_set_stream(uph_sim *sim, void *cuda_stream);
+
+/* Host -> device.  `itime` is the number of leapfrog steps already taken by
+ * this state (0 for a fresh deck: the next step is the reference's itime==1
+ * branch).  Rates are read too: the next step's predictor needs them. */
+uph_status uph_sim_upload(uph_sim *sim, const uph_state *st, int32_t itime);
+
+/* Device -> host, reference order.  NULL fields are skipped. */
+uph_status uph_sim_download(uph_sim *sim, uph_state *st);
+
+/* Advances `nsteps` leapfrog steps (sph.cc:90-168) on the device. */
+uph_status uph_sim_step(uph_sim *sim, int32_t nsteps);
+
+/* One rate evaluation at time t on the uploaded state, no integration: what
+ * the reference's derivatives() computes for the hot path. */
+uph_status uph_sim_derivatives(uph_sim *sim, double t);
+
+/* Pairs (i < j, reference indices) of the last evaluation, ordered by i then
+ * j, with rij2, the convolution kernel w and the gradient dwcdx [niac][2]
+ * (derivatives.c:1088-1105).  *niac gets the pair count even when it is
+ * larger than `cap` (then UPH_NEIGHBOR_OVERFLOW and nothing is written).
+ * Any output pointer may be NULL. */
+uph_status uph_sim_pairs(uph_sim *sim, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
+                         double *w, double *dwcdx, int64_t *niac);
+
+uph_status uph_sim_stats(uph_sim *sim, uph_stats *out);
+
+/* Device time per kernel family since the last reset, measured with CUDA
+ * events when profiling is on.  names: comma-separated list written to
+ * `names` (size `names_len`); ms / launches: arrays of `n` entries. */
+uph_status uph_sim_profile(uph_sim *sim, int32_t enable);
+uph_status uph_sim_kernel_times(uph_sim *sim, int32_t n, double *ms, int64_t *launches, char *names,
+                                size_t names_len, int32_t *n_written);
+/* Kernels this sim has launched since creation. */
+int64_t uph_sim_launch_count(const uph_sim *sim);
+
+/* ---- one-shot neighbour search -------------------------------------------- */
+
+/* SearchNeighbors semantics (Search.cc:5-44): pairs (s, j) with s <
+ * n_fluid, j > s, rij2 < dist, j < particle_boundary, DBL_EPSILON < rij2
+ * (no self matches), ordered by s then j.  knn (the reference passes 40)
+ * caps each query's neighbour list; queries where the cap removes in-radius
+ * points return UPH_UNSUPPORTED.  Host arrays in, host arrays out. */
+uph_status uph_search_neighbors(const double *position, int32_t n_fluid, int32_t n_all,
+                                int32_t particle_boundary, int32_t knn, double dist, int64_t cap,
+                                int32_t *i_pair, int32_t *j_pair, double *rij2, int64_t *niac);
+
+/* ---- errors ---------------------------------------------------------------- */
+
+const char *uph_status_string(uph_status s);
+/* Last error message of the calling thread ("" when none). */
+const char *uph_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UPH_H */

@@ -1,0 +1,247 @@
+"""Test infrastructure (oracle only): Python access to the CPU checkers.
+
+* ``Oracle`` wraps the CPU restatement oracle/uph_oracle.c
+  (oracle/_ref/libuph_oracle.so).
+* ``RefRun`` wraps the reference's own solver compiled from its sources
+  (oracle/_ref/libuph_ref.so; oracle/ref_harness.c drives it).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  The product (uph_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from uph_b200._capi import (STATE_FIELDS, UphParams, empty_state, state_struct)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REFERENCE_TREE = "/root/reference"
+
+
+def build(reference: bool = True) -> None:
+    """make -C oracle (the compiled reference only when its sources exist)."""
+    target = "all" if reference else "port"
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+
+
+def _load(name: str) -> C.CDLL:
+    path = os.path.join(REF_DIR, name)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (make -C oracle)")
+    return C.CDLL(path)
+
+
+_oracle_lib = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _oracle_lib
+    if _oracle_lib is None:
+        lib = _load("libuph_oracle.so")
+        lib.uph_oracle_create.restype = C.c_void_p
+        lib.uph_oracle_create.argtypes = [C.POINTER(UphParams)]
+        lib.uph_oracle_destroy.argtypes = [C.c_void_p]
+        lib.uph_oracle_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        lib.uph_oracle_get_state.argtypes = [C.c_void_p, C.c_void_p]
+        lib.uph_oracle_derivatives.argtypes = [C.c_void_p, C.c_double]
+        lib.uph_oracle_step.argtypes = [C.c_void_p, C.c_int]
+        lib.uph_oracle_pairs.restype = C.c_int64
+        lib.uph_oracle_pairs.argtypes = [C.c_void_p, C.c_int64] + [C.c_void_p] * 5
+        lib.uph_oracle_max_neighbors.argtypes = [C.c_void_p]
+        lib.uph_oracle_energies.argtypes = [C.c_void_p, C.c_void_p]
+        lib.uph_oracle_search.restype = C.c_int64
+        lib.uph_oracle_search.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _oracle_lib = lib
+    return _oracle_lib
+
+
+class Oracle:
+    """The CPU restatement holding one simulation."""
+
+    def __init__(self, params: dict, state: dict, itime: int = 0):
+        self.lib = oracle_lib()
+        self.params = UphParams.from_dict(params)
+        self.nf = params["n_fluid"]
+        self.n = params["n_fluid"] + params["n_solid"] + params["n_fixed"] + params["n_moving"]
+        self.h = self.lib.uph_oracle_create(C.byref(self.params))
+        keep = []
+        st = state_struct({k: np.ascontiguousarray(v) for k, v in state.items()}, keep)
+        self.lib.uph_oracle_set_state(self.h, C.byref(st), itime)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.uph_oracle_destroy(self.h)
+            self.h = None
+
+    def step(self, nsteps: int = 1) -> None:
+        self.lib.uph_oracle_step(self.h, nsteps)
+
+    def derivatives(self, t: float) -> None:
+        self.lib.uph_oracle_derivatives(self.h, t)
+
+    def state(self) -> dict:
+        out = empty_state(self.nf, self.n)
+        keep = []
+        st = state_struct(out, keep)
+        self.lib.uph_oracle_get_state(self.h, C.byref(st))
+        return out
+
+    def pairs(self):
+        n = self.lib.uph_oracle_pairs(self.h, 0, None, None, None, None, None)
+        i = np.zeros(n, np.int32)
+        j = np.zeros(n, np.int32)
+        r2 = np.zeros(n)
+        w = np.zeros(n)
+        dw = np.zeros((n, 2))
+        self.lib.uph_oracle_pairs(self.h, n, i.ctypes.data, j.ctypes.data, r2.ctypes.data, w.ctypes.data,
+                                  dw.ctypes.data)
+        return i, j, r2, w, dw
+
+    def max_neighbors(self) -> int:
+        return self.lib.uph_oracle_max_neighbors(self.h)
+
+    def energies(self):
+        out = np.zeros(3)
+        self.lib.uph_oracle_energies(self.h, out.ctypes.data)
+        return out
+
+
+def search(pos: np.ndarray, n_fluid: int, particle_boundary: int, dist: float):
+    """Radius search with SearchNeighbors' filter; returns (i, j, rij2, max_inradius)."""
+    lib = oracle_lib()
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n_all = pos.shape[0]
+    mx = C.c_int(0)
+    n = lib.uph_oracle_search(pos.ctypes.data, n_fluid, n_all, particle_boundary, dist, 0, None, None, None,
+                              C.byref(mx))
+    i = np.zeros(n, np.int32)
+    j = np.zeros(n, np.int32)
+    r2 = np.zeros(n)
+    lib.uph_oracle_search(pos.ctypes.data, n_fluid, n_all, particle_boundary, dist, n, i.ctypes.data,
+                          j.ctypes.data, r2.ctypes.data, C.byref(mx))
+    return i, j, r2, mx.value
+
+
+# --------------------------------------------------------- compiled reference
+
+_ref_lib = None
+
+
+def ref_lib() -> C.CDLL:
+    global _ref_lib
+    if _ref_lib is None:
+        lib = _load("libuph_ref.so")
+        lib.ref_open.restype = C.c_void_p
+        lib.ref_open.argtypes = [C.c_char_p, C.c_double, C.c_int]
+        lib.ref_close.argtypes = [C.c_void_p]
+        lib.ref_step.argtypes = [C.c_void_p, C.c_int]
+        lib.ref_derivatives.argtypes = [C.c_void_p, C.c_double]
+        lib.ref_counts.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_scalars.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_get.restype = C.c_long
+        lib.ref_get.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p]
+        lib.ref_set.restype = C.c_long
+        lib.ref_set.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p]
+        lib.ref_get_itype.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        lib.ref_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.uph_standin_reset_stats.argtypes = []
+        lib.uph_standin_truncated_queries.restype = C.c_long
+        lib.uph_standin_max_inradius.restype = C.c_int
+        _ref_lib = lib
+    return _ref_lib
+
+
+VECTOR_FIELDS = {"Position", "Velocity", "localVelocity", "Velocity_min", "dvdt", "dvdt_approx",
+                 "velocityFluctuation", "dwcdx"}
+
+
+class RefRun:
+    """The reference solver (CreateSystem + input + sph.cc's loop) on a deck
+    directory.  fluid_capacity_pct > 0 shrinks the reference's 100 Nf
+    particle capacity (see oracle/ref_harness.c)."""
+
+    def __init__(self, deck_dir: str, eta_override: float = 0.0, fluid_capacity_pct: int = 0):
+        self.lib = ref_lib()
+        self.lib.uph_standin_reset_stats()
+        self.h = self.lib.ref_open(os.fsencode(deck_dir), eta_override, fluid_capacity_pct)
+        if not self.h:
+            raise FileNotFoundError(f"reference could not open deck {deck_dir}")
+
+    def close(self):
+        if self.h:
+            self.lib.ref_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def counts(self) -> dict:
+        c = np.zeros(8, np.int32)
+        self.lib.ref_counts(self.h, c.ctypes.data)
+        keys = ["n_fluid", "n_solid", "n_fixed", "n_moving", "n_boundary", "niac", "max_n", "itime"]
+        return dict(zip(keys, (int(v) for v in c)))
+
+    def scalars(self) -> dict:
+        s = np.zeros(16)
+        self.lib.ref_scalars(self.h, s.ctypes.data)
+        keys = ["dt", "c0", "B", "eta", "h", "rho0", "gamma", "g", "k_spring", "c_damp", "kappa", "mu",
+                "epsilon", "dx", "omega", "stroke"]
+        return dict(zip(keys, (float(v) for v in s)))
+
+    def step(self, nsteps: int = 1) -> None:
+        self.lib.ref_step(self.h, nsteps)
+
+    def derivatives(self, t: float) -> None:
+        self.lib.ref_derivatives(self.h, t)
+
+    def get(self, name: str, first: int = 0, n: int = None) -> np.ndarray:
+        c = self.counts()
+        if n is None:
+            n = c["niac"] if name in ("rij2", "w", "dwcdx") else c["n_fluid"]
+        vec = name in VECTOR_FIELDS
+        out = np.zeros((n, 2) if vec else n)
+        got = self.lib.ref_get(self.h, name.encode(), first, n, out.ctypes.data)
+        if got < 0:
+            raise KeyError(name)
+        return out
+
+    def set(self, name: str, values: np.ndarray, first: int = 0) -> None:
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        n = values.shape[0]
+        if self.lib.ref_set(self.h, name.encode(), first, n, values.ctypes.data) < 0:
+            raise KeyError(name)
+
+    def itype(self, first: int = 0, n: int = None) -> np.ndarray:
+        if n is None:
+            c = self.counts()
+            n = c["n_fluid"] + c["n_solid"] + c["n_boundary"]
+        out = np.zeros(n, np.int32)
+        self.lib.ref_get_itype(self.h, first, n, out.ctypes.data)
+        return out
+
+    def pairs(self):
+        n = self.counts()["niac"]
+        i = np.zeros(n, np.int32)
+        j = np.zeros(n, np.int32)
+        self.lib.ref_pairs(self.h, i.ctypes.data, j.ctypes.data)
+        return i, j
+
+    def truncated_queries(self) -> int:
+        return int(self.lib.uph_standin_truncated_queries())
+
+    def max_inradius(self) -> int:
+        return int(self.lib.uph_standin_max_inradius())
+
+
+# fields compared after a step (reference name -> uph_state name is the same)
+FLUID_FIELDS = ["Position", "Velocity", "localVelocity", "density", "localDensity", "DynamicPressure",
+                "localPressure", "ddensitydt", "dpdt", "dvdt", "ddensitydt_approx", "dpdt_approx", "dvdt_approx",
+                "densityFluctuation", "pressureFluctuation", "velocityFluctuation", "Pressure"]
+
+STATE_NAMES = [name for name, _, _ in STATE_FIELDS]

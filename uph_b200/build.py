@@ -1,0 +1,89 @@
+"""Builds the CUDA library in-tree for sm_100a.
+
+    python -m uph_b200.build          # libuph.so and libuph_sph.so next to this file
+
+libuph.so      the C ABI of include/uph.h (kernels + host code)
+libuph_sph.so  derivatives() / SearchNeighbors() with the reference's own
+               signatures (include/uph_system.h), linked against libuph.so
+
+Objects are rebuilt only when a source or header is newer than the object.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(HERE, "_build")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
+          "-ccbin", "g++"]
+
+# (source, extra flags).  The leapfrog is compiled without multiply-add
+# contraction so its arithmetic rounds exactly like the reference's.
+CORE_SOURCES = [
+    ("host.cpp", []),
+    ("celllist.cu", []),
+    ("ref_pass.cu", []),
+    ("wcsph_pass.cu", []),
+    ("integrate.cu", ["--fmad=false"]),
+    ("sim.cu", []),
+]
+DROPIN_SOURCES = [("dropin.cpp", [])]
+
+LIB = os.path.join(HERE, "libuph.so")
+LIB_SPH = os.path.join(HERE, "libuph_sph.so")
+
+
+def _headers():
+    out = []
+    for d in (CSRC, INCLUDE):
+        for f in os.listdir(d):
+            if f.endswith((".h", ".cuh")):
+                out.append(os.path.join(d, f))
+    return out
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _compile(src, flags, verbose):
+    os.makedirs(BUILD, exist_ok=True)
+    path = os.path.join(CSRC, src)
+    obj = os.path.join(BUILD, src + ".o")
+    if _newer(obj, [path] + _headers() + [__file__]):
+        _run([NVCC] + ARCH + COMMON + flags + ["-c", path, "-o", obj], verbose)
+    return obj
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile both libraries; returns the path of libuph.so."""
+    extra = ["-Xptxas", "-v"] if ptxas_info else []
+    objs = [_compile(s, f + extra, verbose) for s, f in CORE_SOURCES]
+    if _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+    dobjs = [_compile(s, f, verbose) for s, f in DROPIN_SOURCES]
+    if _newer(LIB_SPH, dobjs + [LIB]):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB_SPH] + dobjs +
+             ["-L" + HERE, "-luph", "-Xlinker", "-rpath,$ORIGIN", "-lcudart"], verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="--ptxas" in sys.argv)

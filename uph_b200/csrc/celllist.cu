@@ -1,0 +1,178 @@
+// Cell list: the GPU replacement of the reference's kd-tree search
+// (src/lib/Search.cc:5-44).  Every step the interacting particles are binned
+// into square cells no smaller than the search radius by a counting sort:
+//   1. cell key per slot + histogram (atomic add per cell),
+//   2. exclusive scan of the histogram -> first entry of every cell,
+//   3. scatter of slot ids into their cell's range,
+//   4. sort of every cell's (short) range by slot id, so the order in which
+//      the pair pass visits neighbours -- and with it every floating-point
+//      sum -- does not depend on atomic arrival order.
+// A particle's neighbours then lie in the 3 x 3 block of cells around it.
+#include "uph_internal.cuh"
+
+namespace uph {
+
+__global__ void k_cell_keys(DevParams P, const double *__restrict__ x, const double *__restrict__ y, int first,
+                            int count, int *__restrict__ cell_of, int *__restrict__ cnt, unsigned *err)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int s = first + k;
+  const double fx = (x[s] - P.lo_x) * P.inv_cell;
+  const double fy = (y[s] - P.lo_y) * P.inv_cell;
+  int cx = (int)floor(fx), cy = (int)floor(fy);
+  // NaN positions fail both comparisons below and are treated as outside
+  if (!(fx >= 0.0 && fy >= 0.0 && cx < P.ncx && cy < P.ncy)) {
+    atomicOr(err, ERR_OUT_OF_DOMAIN);
+    cx = (fx >= 0.0) ? min(cx, P.ncx - 1) : 0;
+    cy = (fy >= 0.0) ? min(cy, P.ncy - 1) : 0;
+    if (cx < 0) cx = 0;
+    if (cy < 0) cy = 0;
+  }
+  const int c = cy * P.ncx + cx;
+  cell_of[s] = c;
+  atomicAdd(&cnt[c], 1);
+}
+
+void launch_cell_keys(const DevParams &P, const double *x, const double *y, int first, int count, CellGrid &G,
+                      unsigned *err, cudaStream_t s)
+{
+  if (count <= 0) return;
+  k_cell_keys<<<(count + 255) / 256, 256, 0, s>>>(P, x, y, first, count, G.cell_of, G.count, err);
+}
+
+// ---- exclusive scan ----------------------------------------------------------
+// Three passes over chunks of SCAN_CHUNK ints: chunk sums, a scan of the
+// chunk sums in one block, then the chunk-local scans plus their offsets.
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_PER_THREAD;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_tot, int &total)
+{
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int wv = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
+    int wi = wv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    warp_tot[lane] = wi - wv;  // exclusive prefix of warp totals
+    if (lane == 31) warp_tot[32] = wi;
+  }
+  __syncthreads();
+  const int out = incl - v + warp_tot[wid];
+  total = warp_tot[32];
+  __syncthreads();
+  return out;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunk_sums(const int *__restrict__ in, int n,
+                                                                  int *__restrict__ sums)
+{
+  __shared__ int wt[33];
+  const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER_THREAD;
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++)
+    if (base + k < n) v += in[base + k];
+  int total;
+  block_exclusive_scan(v, wt, total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int *sums, int nsums)
+{
+  __shared__ int wt[33];
+  int carry = 0;
+  for (int base = 0; base < nsums; base += SCAN_THREADS) {
+    const int i = base + threadIdx.x;
+    const int v = (i < nsums) ? sums[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, wt, total);
+    if (i < nsums) sums[i] = ex + carry;
+    carry += total;
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunks(const int *__restrict__ in, int *__restrict__ out,
+                                                              int n, const int *__restrict__ sums)
+{
+  __shared__ int wt[33];
+  const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER_THREAD;
+  int v[SCAN_PER_THREAD];
+  int tsum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    tsum += v[k];
+  }
+  int total;
+  int run = block_exclusive_scan(tsum, wt, total) + sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  // out[n] = grand total, written by the thread that owns element n-1
+  if (base <= n - 1 && n - 1 < base + SCAN_PER_THREAD) out[n] = run;
+}
+
+int scan_block_sums_needed(int n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
+
+void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s)
+{
+  const int nb = scan_block_sums_needed(n);
+  k_scan_chunk_sums<<<nb, SCAN_THREADS, 0, s>>>(in, n, block_sums);
+  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(block_sums, nb);
+  k_scan_chunks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, block_sums);
+}
+
+__global__ void k_cell_scatter(const int *__restrict__ cell_of, const int *__restrict__ start, int *fill,
+                               int *__restrict__ list, int first, int count)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int s = first + k;
+  const int c = cell_of[s];
+  list[start[c] + atomicAdd(&fill[c], 1)] = s;
+}
+
+void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s)
+{
+  if (count <= 0) return;
+  k_cell_scatter<<<(count + 255) / 256, 256, 0, s>>>(G.cell_of, G.start, G.fill, G.list, first, count);
+}
+
+__global__ void k_cell_sort_segments(const int *__restrict__ start, int *__restrict__ list, int ncell)
+{
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int a = start[c], b = start[c + 1];
+  for (int i = a + 1; i < b; i++) {
+    const int v = list[i];
+    int j = i - 1;
+    while (j >= a && list[j] > v) {
+      list[j + 1] = list[j];
+      j--;
+    }
+    list[j + 1] = v;
+  }
+}
+
+void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s)
+{
+  k_cell_sort_segments<<<(G.ncell + 255) / 256, 256, 0, s>>>(G.start, G.list, G.ncell);
+}
+
+}  // namespace uph

@@ -1,0 +1,236 @@
+// libuph_sph: derivatives() and SearchNeighbors() with the reference's own
+// signatures, on top of the C ABI in uph.h.  The caller keeps the rest of
+// its libSPH (inputbp.c, inoutflow.c, ...) and its driver; see uph_system.h.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "uph.h"
+#include "uph_system.h"
+
+extern "C" {
+// the caller's own libSPH provides these (inputbp.c:12, inoutflow.c:14)
+void inputbp(System *sys, double t);
+void inoutflow(System *sys);
+}
+
+namespace {
+
+struct DropIn {
+  uph_sim *sim = nullptr;
+  uph_params p;
+};
+
+DropIn g;
+
+[[noreturn]] void die(const char *where, uph_status s)
+{
+  // the reference reports errors with printf + exit(1) (System.c:55-59)
+  printf("%s: %s: %s\n", where, uph_status_string(s), uph_last_error());
+  fflush(stdout);
+  exit(1);
+}
+
+// System -> uph_params (the fields CreateSystem filled, System.c:60-335)
+void params_from_system(const System *sys, uph_params *p)
+{
+  memset(p, 0, sizeof *p);
+  p->profile = UPH_PROFILE_REF;
+  p->precision = UPH_PREC_FP64;
+  p->n_fluid = sys->NumberOfFluidParticles;
+  p->n_solid = sys->NumberOfSolidParticles;
+  p->n_fixed = sys->NumberOfFixedBoundaryParticles;
+  p->n_moving = sys->NumberOfMovingBoundaryParticles;
+  p->stroke = sys->stroke;
+  p->wave_period = sys->wavePeriod;
+  p->local_depth = sys->LocalDepth;
+  p->flat_bottom_length = sys->FlatBottomLength;
+  p->density0 = sys->density0;
+  p->adiabatic_constant = sys->AdiabaticConstant;
+  p->gravity = sys->Gravity;
+  p->dx = sys->dx;
+  p->dy = sys->dy;
+  p->dim = sys->dim;
+  p->viscosity0 = sys->viscosity0;
+  p->mach_number = sys->machNumber;
+  p->peclet_number = sys->pecletNumber;
+  p->epsilon = sys->epsilon;
+  p->alpha = sys->alpha;
+  p->virtual_type = sys->virtualType;
+  p->print_step = sys->printStep;
+  p->screen_step = sys->screenStep;
+  p->time_step = sys->timeStep;
+  p->lid_velocity = sys->lidVelocity;
+  p->near_neighbor = sys->nearNeighbor;
+  p->select_boundary_force = sys->selectBoundaryForce;
+  p->lennard_select = sys->lennardSelect;
+  p->spring_constant0 = sys->springConstant0;
+  p->damping_constant0 = sys->dampingConstant0;
+  p->flag_init_simul = sys->flagInitSimul;
+  p->gravity_flag = sys->gravityFlag;
+  p->thermal_diffusivity0 = sys->thermalDiffusivity0;
+  p->moving_boundary = sys->movingBoundary;
+  p->number_of_initialization_steps = sys->NumberOfInitializationSteps;
+  p->pressure_probe_x = sys->pressureProbeX;
+  p->pressure_probe_y = sys->pressureProbeY;
+  p->stress_type = sys->stressType;
+  p->dissipation_control_volume = sys->disspationControlVolume;
+  p->speed_of_sound = sys->SpeedOfSound;
+  p->compression_factor = sys->CompressionFactor;
+  p->omega = sys->omega;
+  p->eta = sys->eta;
+  p->h = sys->hsml[0];
+  p->lennard_coefficient = sys->LennardCoefficient;
+  p->sponge_factor0 = sys->spongeFactor0;
+  p->sponge_position0 = sys->spongePosition0;
+  p->wave_absorption = sys->waveAbsorption;
+  p->av_alpha = sys->alpha;
+  p->knn_cap = 0;
+}
+
+// The library uses one smoothing length, one viscosity and one diffusivity;
+// input.c:105-119 and inputbp.c:285-299 give every particle the same values.
+void check_uniform(const System *sys, int n)
+{
+  const double h = sys->hsml[0], mu = sys->viscosity[0], k = sys->thermalDiffusivity[0];
+  for (int i = 0; i < n; i++)
+    if (sys->hsml[i] != h || sys->viscosity[i] != mu || sys->thermalDiffusivity[i] != k) {
+      printf("derivatives: particle %d has its own hsml/viscosity/thermalDiffusivity; "
+             "the GPU path needs the uniform values input() assigns\n", i);
+      exit(1);
+    }
+  if (mu != sys->viscosity0 || k != sys->thermalDiffusivity0) {
+    printf("derivatives: per-particle viscosity/thermalDiffusivity differ from viscosity0/thermalDiffusivity0\n");
+    exit(1);
+  }
+}
+
+void ensure_sim(const System *sys, int n)
+{
+  uph_params p;
+  params_from_system(sys, &p);
+  // cell-grid domain: the particles' bounding box with room to move
+  double lo[2] = {sys->Position[0][0], sys->Position[0][1]}, hi[2] = {lo[0], lo[1]};
+  for (int i = 1; i < n; i++)
+    for (int d = 0; d < 2; d++) {
+      lo[d] = fmin(lo[d], sys->Position[i][d]);
+      hi[d] = fmax(hi[d], sys->Position[i][d]);
+    }
+  bool inside = g.sim != nullptr;
+  if (inside) {
+    const uph_params &q = g.p;
+    inside = q.n_fluid == p.n_fluid && q.n_solid == p.n_solid && q.n_fixed == p.n_fixed &&
+             q.n_moving == p.n_moving && q.h == p.h && q.time_step == p.time_step &&
+             lo[0] >= q.domain_lo[0] && lo[1] >= q.domain_lo[1] && hi[0] <= q.domain_hi[0] &&
+             hi[1] <= q.domain_hi[1] && memcmp(&q.stroke, &p.stroke, offsetof(uph_params, domain_lo) -
+                                                                          offsetof(uph_params, stroke)) == 0;
+  }
+  if (inside) return;
+  if (g.sim) uph_sim_destroy(g.sim);
+  g.sim = nullptr;
+  for (int d = 0; d < 2; d++) {
+    const double ext = hi[d] - lo[d];
+    p.domain_lo[d] = lo[d] - 0.5 * ext - 8.0 * p.h;
+    p.domain_hi[d] = hi[d] + 0.5 * ext + 8.0 * p.h;
+  }
+  uph_status s = uph_sim_create(&p, &g.sim);
+  if (s != UPH_OK) die("derivatives", s);
+  g.p = p;
+}
+
+}  // namespace
+
+extern "C" void derivatives(System *sys, double t)
+{
+  const int nf = sys->NumberOfFluidParticles;
+  // derivatives.c:3147-3157 (the stress arrays feed stressType 2 only)
+  memset(sys->ddensitydt, 0, sizeof(double) * sys->MaxNumberOfParticles);
+  memset(sys->dpdt, 0, sizeof(double) * sys->MaxNumberOfParticles);
+  memset(sys->dvdt[0], 0, sizeof(double) * sys->MaxNumberOfParticles * 2);
+  memset(sys->ddensitydt_approx, 0, sizeof(double) * sys->MaxNumberOfParticles);
+  memset(sys->dpdt_approx, 0, sizeof(double) * sys->MaxNumberOfParticles);
+  memset(sys->dvdt_approx[0], 0, sizeof(double) * sys->MaxNumberOfParticles * 2);
+  if (t > 0) inoutflow(sys);  // derivatives.c:3162-3164
+  inputbp(sys, t);            // derivatives.c:3168: re-reads the boundary decks, moves walls
+  // derivatives.c:3171-3182 only feeds inoutflow's inflow branch, whose
+  // threshold (x > 5000.1, inoutflow.c:26) no deck reaches; it is not repeated.
+  sys->inflowParticles = 0;
+  const int nb = sys->NumberOfBoundaryParticles, ns = sys->NumberOfSolidParticles;
+  for (int i = 0; i < nb; i++)  // derivatives.c:3187-3191
+    for (int d = 0; d < 2; d++) sys->Velocity_xsph[nf + ns + i][d] = sys->Velocity[nf + ns + i][d];
+  sys->NumberOfVirtualParticles = 0;
+  const int n = nf + ns + nb;
+  check_uniform(sys, n);
+  ensure_sim(sys, n);
+
+  uph_state in;
+  memset(&in, 0, sizeof in);
+  in.Position = sys->Position[0];
+  in.Velocity = sys->Velocity[0];
+  in.localVelocity = sys->localVelocity[0];
+  in.density = sys->density;
+  in.localDensity = sys->localDensity;
+  in.DynamicPressure = sys->DynamicPressure;
+  in.localPressure = sys->localPressure;
+  in.mass = sys->mass;
+  in.itype = sys->itype;
+  in.spongeFactor = sys->spongeFactor;
+  uph_status s = uph_sim_upload(g.sim, &in, 0);
+  if (s != UPH_OK) die("derivatives", s);
+  s = uph_sim_derivatives(g.sim, t);
+  if (s != UPH_OK) die("derivatives", s);
+  uph_state out;
+  memset(&out, 0, sizeof out);
+  out.ddensitydt = sys->ddensitydt;
+  out.dpdt = sys->dpdt;
+  out.dvdt = sys->dvdt[0];
+  out.ddensitydt_approx = sys->ddensitydt_approx;
+  out.dpdt_approx = sys->dpdt_approx;
+  out.dvdt_approx = sys->dvdt_approx[0];
+  out.densityFluctuation = sys->densityFluctuation;
+  out.pressureFluctuation = sys->pressureFluctuation;
+  out.velocityFluctuation = sys->velocityFluctuation[0];
+  out.Pressure = sys->Pressure;
+  s = uph_sim_download(g.sim, &out);
+  if (s != UPH_OK) die("derivatives", s);
+  // LocalDensity/Pressure/VelocityFluctuation zero the boundary entries (derivatives.c:2062-2066, 2103-2106, 2140-2143)
+  for (int i = nf; i < nf + nb; i++) {
+    sys->densityFluctuation[i] = 0.0;
+    sys->pressureFluctuation[i] = 0.0;
+    sys->velocityFluctuation[i][0] = 0.0;
+    sys->velocityFluctuation[i][1] = 0.0;
+  }
+  // pair list (CalculateKernel's outputs, derivatives.c:1076-1105)
+  int64_t niac = 0;
+  s = uph_sim_pairs(g.sim, sys->MaxNumberOfParticles, sys->i_pair, sys->j_pair, sys->rij2, sys->w, sys->dwcdx[0],
+                    &niac);
+  if (s != UPH_OK) die("derivatives", s);
+  sys->NumberOfInteractingParticles = (int)niac;
+  // TotalKineticEnergy, derivatives.c:2254-2264
+  double ke = 0.0, pe = 0.0;
+  for (int i = 0; i < nf; i++) {
+    ke += 0.5 * sys->mass[i] * (sys->Velocity[i][0] * sys->Velocity[i][0] + sys->Velocity[i][1] * sys->Velocity[i][1]);
+    pe += sys->mass[i] * sys->Gravity * sys->Position[i][1];
+  }
+  sys->totalKineticEnergy = ke;
+  sys->potentialEnergy = pe;
+}
+
+extern "C" int SearchNeighbors(const double **Position, int *i_pair, int *j_pair, double *rij2,
+                               const int NumberOfFluidParticles, const int NumberOfParticles, int ParticleBoundary,
+                               const int NumberOfNeighbors, const double dist)
+{
+  int64_t niac = 0;
+  // the caller sizes the pair arrays by MaxNumberOfParticles; it is not passed, so
+  // ask for the count first and then fill
+  uph_status s = uph_search_neighbors(Position[0], NumberOfFluidParticles, NumberOfParticles, ParticleBoundary,
+                                      NumberOfNeighbors, dist, 0, nullptr, nullptr, nullptr, &niac);
+  if (s != UPH_OK && s != UPH_NEIGHBOR_OVERFLOW) die("SearchNeighbors", s);
+  s = uph_search_neighbors(Position[0], NumberOfFluidParticles, NumberOfParticles, ParticleBoundary,
+                           NumberOfNeighbors, dist, niac, i_pair, j_pair, rij2, &niac);
+  if (s != UPH_OK) die("SearchNeighbors", s);
+  return (int)niac;
+}

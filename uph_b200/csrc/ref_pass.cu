@@ -1,0 +1,298 @@
+// The fused rate pass of the REF profile: one thread per fluid particle
+// gathers every pair term of the reference's derivatives() from the 3 x 3
+// cells around it, in FP64.
+//
+// The reference evaluates each term as a scatter loop over pairs (i < j)
+// that adds one formula to i and another to j.  Here particle a sees every
+// neighbour b; a plays the reference's i when orig(a) < orig(b) and its j
+// otherwise.  With g = F(r) (x_a - x_b) (= the reference's dwcdx for the
+// pair when a is i, and its negation when a is j), the per-a contributions
+// are (V = m / rho, P = rho0 c0^2 + gamma p, ms = m_b if a is i else m_a):
+//
+//   ddensitydt_approx  (PredictingDensityEquation, derivatives.c:1217-1252)
+//       i: m_b (v_a - vt_b).g        j: m_a (vt_a - v_b).g
+//   dpdt_approx        (PredictingDynamicPressureEquation, :1254-1331)
+//       m_b/rho_a P_a (v_a - v_b).g + gamma kappa ms/rho_b (p_a - p_b) nu 4P_a/(P_a+P_b)
+//       - kappa P_a ms/rho_b (rho_a - rho_b)(1/rho_a + 1/rho_b) nu
+//   dvdt_approx        (PredictingPressureGradientForce, :1333-1377)
+//       -m_b (p_a/rho_a^2 + p_b/rho_b^2) g
+//   densityFluctuation / pressureFluctuation (:2100-2172)
+//       -V_b (f_a - f_b) W
+//   velocityFluctuation (:2060-2097), i side only
+//       (v_a - v_b) W (m_a/rhot_b - m_b/rhot_a)
+//   ddensitydt         (DensityEquation, :1520-1567)
+//       V_b rhot_b (v_a - vt_b).g
+//   dpdt               (DynamicPressureEquation, :1569-1672)
+//       V_b rhot_b/rho_a P_a (v_a - vt_b).g + gamma kappa V_b (p_a - pt_b) nu 4P_a/(P_a+P_b)
+//       - kappa P_a V_b (rho_a - rhot_b)(1/rho_a + 1/rho_b) nu
+//   dvdt               (PressureGradientForce, :1109-1163)
+//       -m_b (p_a rhot_b/(rho_a^2 rho_b) + p_b rhot_a/(rho_b^2 rho_a)) g
+//   dvdt viscous       (ViscousForcesSingleStep, :1770-1839)
+//       s m_b mu_ab/(r^2 + 0.01h^2) (rhot_b/(rho_a^2 rho_b) - rhot_a/(rho_b^2 rho_a)) S.g,
+//       s = +1 on the i side and -1 on the j side (the reference's jSigma is
+//       -iSigma, so the pair force is a difference, not a sum)
+//   dvdt_approx viscous (PredictingViscousForcesSingleStep, :1448-1515)
+//       m_b mu_ab/(r^2 + 0.01h^2) (1/rho_a^2 + 1/rho_b^2) S.g
+//   with nu = (x_a - x_b).g / (r^2 + 0.01 h^2), mu_ab = 2 mu rho_a rho_b/(rho_a + rho_b),
+//   S = [[s00, s01], [s01, -s00]], s00 = dx' du - dy' dv, s01 = dx' dv + dy' du,
+//   (dx', dy') = x_b - x_a, (du, dv) = v_a - v_b.
+// Wall forces (derivatives.c:2396-2449, 1392-1446 and the other modes),
+// gravity (:1167-1178, 1379-1390), the sponge layer (:2827-2838) and the
+// algebraic Tait pressure (:1674-1682) are added in the same pass.
+//
+// A pair exists iff it would be in the reference's list: both particles
+// interacting, max(orig a, orig b) < ParticleBoundary (Search.cc:33 with
+// derivatives.c:1082-1084), DBL_EPSILON < r^2 < (h h) 4 where r^2 is
+// dx*dx + dy*dy rounded exactly like the reference (no fused multiply-add).
+#include <float.h>
+
+#include "uph_internal.cuh"
+
+namespace uph {
+
+__device__ __forceinline__ double exact_r2(double dx, double dy)
+{
+  return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+struct RefAcc {
+  double drho, dp, ax, ay;
+  double drho_a, dp_a, ax_a, ay_a;
+  double frho, fp, fu, fv;
+};
+
+__device__ __forceinline__ void wall_pair_force(const DevParams &P, bool isI, int ita, int itb, double r, double dxa,
+                                                double dya, double dua, double dva, double ma, double &fx,
+                                                double &fy, double &fx_spring, double &fy_spring)
+{
+  fx = fy = fx_spring = fy_spring = 0.0;
+  if (!isI || ita != 1) return;
+  // SpringBoundaryForces / PredictingSpringBoundaryForces (derivatives.c:2396-2449, 1392-1446)
+  if (itb == 2 || itb == 3 || itb == 5) {
+    const double r0 = 3.0 * P.dx;
+    if (r < r0) {
+      const double rv = dxa * dua + dya * dva;
+      const double c1 = P.k_spring * (r0 - r) / (r * ma);
+      const double c2 = P.c_damp * rv / (r * r * ma);
+      fx_spring = -c1 * dxa - c2 * dxa;
+      fy_spring = -c1 * dya - c2 * dya;
+    }
+  }
+  if (P.boundary_force == 4 && (itb == 2 || itb == 3) && r < P.dx) {
+    // ImprovedMonaghan, derivatives.c:1955-2012
+    const double hh = P.h;
+    const double norm = 7.0 / (64.0 * 3.142 * hh * hh);
+    const double q = r / hh;
+    double phi = 0.0;
+    if (q < 2.0) {
+      const double t = 2.0 - q;
+      phi = norm * (1.0 + 2.0 * q) * (t * t) * (t * t);
+    }
+    const double rd = r - P.dx / 5.0;
+    const double vmax = P.mach_c * P.mach_c / 5.0;
+    const double c = vmax * phi / (rd * r);
+    fx = c * dxa;
+    fy = c * dya;
+  } else if (P.boundary_force == 5 && itb == 2 && r < P.dx) {
+    // SerialSpringBoundaryForces, derivatives.c:2452-2479
+    fx = -(P.k_spring * dxa + P.c_damp * dua) / ma;
+    fy = -(P.k_spring * dya + P.c_damp * dva) / ma;
+  }
+}
+
+// LeonnardJonesBoundaryForces (mode 1, derivatives.c:1184-1211) and
+// MonaghanBoundaryForce (default mode, :1919-1953): every fluid particle
+// against every boundary particle, no pair-list filter.
+__device__ __forceinline__ void brute_wall_force(const DevParams &P, double r2, double dxa, double dya, double mb,
+                                                 double &fx, double &fy)
+{
+  if (P.boundary_force == 1) {
+    const double r0 = P.dx;
+    if (r2 < r0 * r0) {
+      double rr = r0 / sqrt(r2);
+      rr *= rr;
+      rr *= rr;
+      const double pb = P.lj_coeff * rr * (rr * rr - 1.) / r2;
+      fx += pb * dxa;
+      fy += pb * dya;
+    }
+  } else {
+    const double r = sqrt(r2);
+    const double q = r / P.h;
+    double phi = 0.0;
+    if (q >= 0.0 && q < 2.0) {
+      const double t = 2.0 - q;
+      phi = 0.125 * (1.0 + 1.5 * q) * t * t * t;
+    }
+    const double gama = P.mach_c * P.mach_c / (P.rho0 * P.dx * P.dy);
+    const double c = gama * phi * mb / r2;
+    fx += c * dxa;
+    fy += c * dya;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                  PassStats st)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = a < P.nf;
+  unsigned long long my_pairs = 0;
+  int my_nb = 0;
+  if (active) {
+    const double xa = S.x[a], ya = S.y[a];
+    const double ua = S.u[a], va = S.v[a], uta = S.ut[a], vta = S.vt[a];
+    const double rhoa = S.rho[a], rhota = S.rhot[a], pa = S.p[a], ma = S.m[a];
+    const double ira = S.inv_rho[a], irta = S.inv_rhot[a];
+    const int oa = S.orig[a], ita = S.itype[a];
+    const double Pa = P.rho0c2 + P.gamma * pa;
+    const double ira2 = ira * ira;
+    const bool brute_walls = (P.boundary_force == 1) || (P.boundary_force != 3 && P.boundary_force != 4 &&
+                                                         P.boundary_force != 5);
+    RefAcc A = {};
+    double bx = 0.0, by = 0.0;  // mode-1 / default wall force (dvdt only)
+    const int c = G.cell_of[a];
+    const int cx = c % P.ncx, cy = c / P.ncx;
+    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++) {
+      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
+        const int cc = yy * P.ncx + xx;
+        const int k1 = G.start[cc + 1];
+        for (int k = G.start[cc]; k < k1; k++) {
+          const int b = G.list[k];
+          if (b == a) continue;
+          const double dxa = xa - S.x[b], dya = ya - S.y[b];
+          const double r2 = exact_r2(dxa, dya);
+          if (!(r2 < P.r2cut)) continue;
+          const int ob = S.orig[b];
+          if (brute_walls && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
+          if (r2 <= DBL_EPSILON) continue;
+          my_nb++;
+          const bool isI = ob > oa;
+          if (max(oa, ob) >= P.pb) continue;
+          if (isI) my_pairs++;
+
+          const double ub = S.u[b], vb = S.v[b], utb = S.ut[b], vtb = S.vt[b];
+          const double rhob = S.rho[b], rhotb = S.rhot[b], pb = S.p[b], ptb = S.pt[b], mb = S.m[b];
+          const double irb = S.inv_rho[b], irtb = S.inv_rhot[b];
+
+          // PolyOrderSeven convolution W and deconvolution dW/dr factor
+          const double r = sqrt(r2);
+          const double q = r * P.inv_h;
+          const double q2 = q * q;
+          const double t = 1.0 - 0.25 * q2;
+          const double t2 = t * t, t4 = t2 * t2;
+          const double t7 = t4 * t2 * t, t8 = t4 * t4;
+          const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
+          const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
+          const double W = P.w_alpha * t8 * pp;
+          const double F = P.dw_alpha * t7 * pp7 * P.inv_h2;
+          const double gx = F * dxa, gy = F * dya;
+
+          const double Pb = P.rho0c2 + P.gamma * pb;
+          const double Vb = mb * irb;
+          const double ms = isI ? mb : ma;
+          const double rhosum = ira + irb;
+          const double inv_r2e = 1.0 / (r2 + P.eta2);
+          const double nu = (dxa * gx + dya * gy) * inv_r2e;
+          const double ep = 4.0 * Pa / (Pa + Pb);
+          const double gk = P.gamma * P.kappa;
+
+          // predictor density
+          const double pdx = isI ? (ua - utb) : (uta - ub);
+          const double pdy = isI ? (va - vtb) : (vta - vb);
+          A.drho_a += ms * (pdx * gx + pdy * gy);
+          // predictor pressure
+          const double dux = ua - ub, duy = va - vb;
+          const double vdw = dux * gx + duy * gy;
+          const double msb = ms * irb;
+          A.dp_a += (mb * ira) * Pa * vdw + gk * msb * (pa - pb) * nu * ep - P.kappa * Pa * msb * (rhoa - rhob) * rhosum * nu;
+          // predictor pressure gradient
+          const double pij_p = pa * ira2 + pb * irb * irb;
+          A.ax_a -= mb * pij_p * gx;
+          A.ay_a -= mb * pij_p * gy;
+          // fluctuations
+          A.frho -= Vb * (rhoa - rhob) * W;
+          A.fp -= Vb * (pa - pb) * W;
+          const double cfv = isI ? (ma * irtb - mb * irta) * W : 0.0;
+          A.fu += dux * cfv;
+          A.fv += duy * cfv;
+          // continuity
+          const double vdwt = (ua - utb) * gx + (va - vtb) * gy;
+          const double Vr = Vb * rhotb;
+          A.drho += Vr * vdwt;
+          // rate-form Tait with diffusion
+          A.dp += Vr * ira * Pa * vdwt + gk * Vb * (pa - ptb) * nu * ep - P.kappa * Pa * Vb * (rhoa - rhotb) * rhosum * nu;
+          // pressure gradient
+          const double pij = pa * rhotb * ira2 * irb + pb * rhota * irb * irb * ira;
+          A.ax -= mb * pij * gx;
+          A.ay -= mb * pij * gy;
+          // deviatoric viscous stress
+          if (P.stress_type == 1) {
+            const double meff = 2.0 * P.mu0 / rhosum;
+            const double s00 = (-dxa) * dux - (-dya) * duy;
+            const double s01 = (-dxa) * duy + (-dya) * dux;
+            const double sgx = s00 * gx + s01 * gy;
+            const double sgy = s01 * gx - s00 * gy;
+            const double base = mb * meff * inv_r2e;
+            const double D = rhotb * ira2 * irb - rhota * irb * irb * ira;
+            const double sD = (isI ? base : -base) * D;
+            A.ax += sD * sgx;
+            A.ay += sD * sgy;
+            const double Dp = base * (ira2 + irb * irb);
+            A.ax_a += Dp * sgx;
+            A.ay_a += Dp * sgy;
+          }
+          // wall forces
+          if (isI && ita == 1) {
+            const int itb = S.itype[b];
+            double fx, fy, sx, sy;
+            wall_pair_force(P, isI, ita, itb, r, dxa, dya, dux, duy, ma, fx, fy, sx, sy);
+            A.ax_a += sx;
+            A.ay_a += sy;
+            if (P.boundary_force == 3) {
+              A.ax += sx;
+              A.ay += sy;
+            } else {
+              A.ax += fx;
+              A.ay += fy;
+            }
+          }
+        }
+      }
+    }
+    A.ax += bx;
+    A.ay += by;
+    if (P.gravity_flag == 1) {
+      A.ay -= P.g;
+      A.ay_a -= P.g;
+    }
+    if (P.moving_boundary == 1 && P.wave_absorption == 1) A.ax -= S.sponge[a] * ua;
+    S.drho[a] = A.drho;
+    S.dp[a] = A.dp;
+    S.ax[a] = A.ax;
+    S.ay[a] = A.ay;
+    S.drho_a[a] = A.drho_a;
+    S.dp_a[a] = A.dp_a;
+    S.ax_a[a] = A.ax_a;
+    S.ay_a[a] = A.ay_a;
+    S.frho[a] = A.frho;
+    S.fp[a] = A.fp;
+    S.fu[a] = A.fu;
+    S.fv[a] = A.fv;
+    S.pressure[a] = P.B * (pow(rhoa / P.rho0, P.gamma) - 1.0);
+  }
+  // pass statistics: one atomic per warp
+  const unsigned long long wp = __reduce_add_sync(0xffffffffu, (unsigned)my_pairs);
+  const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
+  if ((threadIdx.x & 31) == 0) {
+    if (wp) atomicAdd(st.niac, wp);
+    if (wn) atomicMax(st.max_nb, wn);
+  }
+}
+
+void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+{
+  if (P.nf <= 0) return;
+  k_ref_pass<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G, st);
+}
+
+}  // namespace uph

@@ -1,0 +1,1019 @@
+// uph_sim: resident device state and the step loop behind the C ABI.
+//
+// Device layout (all SoA doubles unless noted), "slot" order:
+//   slots [0, nf)  fluid particles, spatially sorted by cell,
+//   slots [nf, n)  solid / fixed / moving boundary particles, sorted by cell.
+// S.orig[slot] is the particle's reference index; uploads and downloads
+// permute through it, so callers only ever see reference order.  Every
+// `reorder_interval` steps the fluid slots are re-sorted by their current
+// cell so that a warp's particles keep sharing neighbour cells.
+#include <float.h>
+#include <math.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "uph_internal.cuh"
+
+using namespace uph;
+
+namespace uph {
+int scan_block_sums_needed(int n);
+}
+
+namespace {
+
+constexpr int kReorderInterval = 16;
+
+enum KernelFamily { KF_PREDICT, KF_WALLS, KF_REFRESH, KF_CELLS, KF_PASS, KF_CORRECT, KF_REORDER, KF_COUNT };
+const char *kFamilyNames[KF_COUNT] = {"predict", "wall_motion", "refresh", "cell_list", "rate_pass", "correct",
+                                      "reorder"};
+
+// staging buffers in reference order (the caller's layout)
+struct Staging {
+  double *pos, *vel, *lvel;  // [n][2]
+  double *rho, *lrho, *p, *lp, *mass, *pressure;
+  int32_t *itype;
+  double *vmin;  // [nf][2]
+  double *rhomin, *pmin, *sponge, *drho, *dp, *drho_a, *dp_a, *frho, *fp;
+  double *acc, *acc_a, *fvel;  // [nf][2]
+  double *tmp_x, *tmp_y;       // positions split for the key kernel
+};
+
+}  // namespace
+
+struct uph_sim {
+  uph_params hp;
+  DevParams P;
+  SlotArrays S, S2;
+  CellGrid G;
+  Staging T;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  unsigned *d_err = nullptr;
+  unsigned long long *d_niac = nullptr;
+  int *d_max_nb = nullptr;
+  int *d_perm = nullptr;  // scratch for uploads and reorders
+  int itime = 0;
+  int steps_since_reorder = 0;
+  bool have_rates = false;
+  int64_t launches = 0;
+  bool profiling = false;
+  // profiling: event pairs recorded around every kernel family without
+  // synchronising; read back after the call's own final synchronisation
+  static constexpr int kEventPool = 2048;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_family;
+  int ev_used = 0;
+  double fam_ms[KF_COUNT] = {0};
+  int64_t fam_launch[KF_COUNT] = {0};
+  std::vector<void *> allocations;
+  double *d_partials = nullptr;
+  int n_partials = 0;
+};
+
+namespace {
+
+template <typename T>
+cudaError_t dalloc(uph_sim *s, T **p, size_t count)
+{
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+  if (e == cudaSuccess) s->allocations.push_back((void *)*p);
+  return e;
+}
+
+cudaError_t alloc_slots(uph_sim *s, SlotArrays &A, int n, int nf)
+{
+  cudaError_t e = cudaSuccess;
+  double **all[] = {&A.x, &A.y, &A.u, &A.v, &A.ut, &A.vt, &A.rho, &A.rhot, &A.p, &A.pt, &A.m, &A.inv_rho,
+                    &A.inv_rhot, &A.pressure};
+  for (double **p : all)
+    if ((e = dalloc(s, p, (size_t)n)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &A.itype, (size_t)n)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &A.orig, (size_t)n)) != cudaSuccess) return e;
+  double **fl[] = {&A.rho_min, &A.p_min, &A.u_min, &A.v_min, &A.sponge, &A.drho, &A.dp, &A.ax, &A.ay,
+                   &A.drho_a, &A.dp_a, &A.ax_a, &A.ay_a, &A.frho, &A.fp, &A.fu, &A.fv};
+  for (double **p : fl)
+    if ((e = dalloc(s, p, (size_t)nf)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// adds the recorded event pairs to the per-family totals; the caller has
+// synchronised the stream (or this waits for the last event)
+void flush_profile(uph_sim *s)
+{
+  for (int k = 0; k < s->ev_used; k++) {
+    cudaEvent_t a = s->ev_pool[2 * k], b = s->ev_pool[2 * k + 1];
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) {
+      s->fam_ms[s->ev_family[k]] += ms;
+      s->fam_launch[s->ev_family[k]]++;
+    }
+  }
+  s->ev_used = 0;
+}
+
+struct Timer {
+  uph_sim *s;
+  int fam;
+  int slot = -1;
+  Timer(uph_sim *s_, int f) : s(s_), fam(f)
+  {
+    if (!s->profiling || s->ev_pool.empty()) return;
+    if (s->ev_used == uph_sim::kEventPool) flush_profile(s);
+    slot = s->ev_used++;
+    s->ev_family[slot] = fam;
+    cudaEventRecord(s->ev_pool[2 * slot], s->stream);
+  }
+  ~Timer()
+  {
+    if (slot >= 0) cudaEventRecord(s->ev_pool[2 * slot + 1], s->stream);
+  }
+};
+
+// ---- permutation kernels ------------------------------------------------------
+
+__global__ void k_split_xy(const double *__restrict__ pos, double *__restrict__ x, double *__restrict__ y, int n)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    x[k] = pos[2 * k];
+    y[k] = pos[2 * k + 1];
+  }
+}
+
+// slots <- staging (reference order) through perm[slot] = reference index
+__global__ void k_gather_upload(SlotArrays S, Staging T, const int *__restrict__ perm, int n, int nf, double rho0)
+{
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = perm[s];
+  S.orig[s] = o;
+  S.x[s] = T.pos[2 * o];
+  S.y[s] = T.pos[2 * o + 1];
+  S.u[s] = T.vel[2 * o];
+  S.v[s] = T.vel[2 * o + 1];
+  S.ut[s] = T.lvel[2 * o];
+  S.vt[s] = T.lvel[2 * o + 1];
+  S.rho[s] = T.rho[o];
+  S.rhot[s] = T.lrho[o];
+  S.p[s] = T.p[o];
+  S.pt[s] = T.lp[o];
+  S.m[s] = T.mass[o];
+  S.itype[s] = T.itype[o];
+  S.pressure[s] = T.pressure[o];
+  if (s < nf) {
+    S.rho_min[s] = T.rhomin[o];
+    S.p_min[s] = T.pmin[o];
+    S.u_min[s] = T.vmin[2 * o];
+    S.v_min[s] = T.vmin[2 * o + 1];
+    S.sponge[s] = T.sponge[o];
+    S.drho[s] = T.drho[o];
+    S.dp[s] = T.dp[o];
+    S.ax[s] = T.acc[2 * o];
+    S.ay[s] = T.acc[2 * o + 1];
+    S.drho_a[s] = T.drho_a[o];
+    S.dp_a[s] = T.dp_a[o];
+    S.ax_a[s] = T.acc_a[2 * o];
+    S.ay_a[s] = T.acc_a[2 * o + 1];
+    S.frho[s] = T.frho[o];
+    S.fp[s] = T.fp[o];
+    S.fu[s] = T.fvel[2 * o];
+    S.fv[s] = T.fvel[2 * o + 1];
+  }
+}
+
+// staging (reference order) <- slots
+__global__ void k_scatter_download(SlotArrays S, Staging T, int n, int nf)
+{
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = S.orig[s];
+  T.pos[2 * o] = S.x[s];
+  T.pos[2 * o + 1] = S.y[s];
+  T.vel[2 * o] = S.u[s];
+  T.vel[2 * o + 1] = S.v[s];
+  T.lvel[2 * o] = S.ut[s];
+  T.lvel[2 * o + 1] = S.vt[s];
+  T.rho[o] = S.rho[s];
+  T.lrho[o] = S.rhot[s];
+  T.p[o] = S.p[s];
+  T.lp[o] = S.pt[s];
+  T.mass[o] = S.m[s];
+  T.itype[o] = S.itype[s];
+  T.pressure[o] = S.pressure[s];
+  if (s < nf) {
+    T.rhomin[o] = S.rho_min[s];
+    T.pmin[o] = S.p_min[s];
+    T.vmin[2 * o] = S.u_min[s];
+    T.vmin[2 * o + 1] = S.v_min[s];
+    T.sponge[o] = S.sponge[s];
+    T.drho[o] = S.drho[s];
+    T.dp[o] = S.dp[s];
+    T.acc[2 * o] = S.ax[s];
+    T.acc[2 * o + 1] = S.ay[s];
+    T.drho_a[o] = S.drho_a[s];
+    T.dp_a[o] = S.dp_a[s];
+    T.acc_a[2 * o] = S.ax_a[s];
+    T.acc_a[2 * o + 1] = S.ay_a[s];
+    T.frho[o] = S.frho[s];
+    T.fp[o] = S.fp[s];
+    T.fvel[2 * o] = S.fu[s];
+    T.fvel[2 * o + 1] = S.fv[s];
+  }
+}
+
+// D <- S through perm[new slot] = old slot, for slots [0, count)
+__global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ perm, int count, int nf)
+{
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  const int o = perm[s];
+  D.x[s] = S.x[o]; D.y[s] = S.y[o]; D.u[s] = S.u[o]; D.v[s] = S.v[o];
+  D.ut[s] = S.ut[o]; D.vt[s] = S.vt[o]; D.rho[s] = S.rho[o]; D.rhot[s] = S.rhot[o];
+  D.p[s] = S.p[o]; D.pt[s] = S.pt[o]; D.m[s] = S.m[o]; D.inv_rho[s] = S.inv_rho[o];
+  D.inv_rhot[s] = S.inv_rhot[o]; D.pressure[s] = S.pressure[o]; D.itype[s] = S.itype[o]; D.orig[s] = S.orig[o];
+  if (s < nf) {
+    D.rho_min[s] = S.rho_min[o]; D.p_min[s] = S.p_min[o]; D.u_min[s] = S.u_min[o]; D.v_min[s] = S.v_min[o];
+    D.sponge[s] = S.sponge[o]; D.drho[s] = S.drho[o]; D.dp[s] = S.dp[o]; D.ax[s] = S.ax[o]; D.ay[s] = S.ay[o];
+    D.drho_a[s] = S.drho_a[o]; D.dp_a[s] = S.dp_a[o]; D.ax_a[s] = S.ax_a[o]; D.ay_a[s] = S.ay_a[o];
+    D.frho[s] = S.frho[o]; D.fp[s] = S.fp[o]; D.fu[s] = S.fu[o]; D.fv[s] = S.fv[o];
+  }
+}
+
+__global__ void k_iota(int *p, int first, int count)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count) p[first + k] = first + k;
+}
+
+// fluid-only (or wall-only) counting sort of [first, first+count) by cell,
+// result: G.list[0, count) = ids in cell order, ties by id
+uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count)
+{
+  CellGrid &G = s->G;
+  cudaStream_t st = s->stream;
+  UPH_CUDA(cudaMemsetAsync(G.count, 0, sizeof(int) * G.ncell, st));
+  UPH_CUDA(cudaMemsetAsync(G.fill, 0, sizeof(int) * G.ncell, st));
+  launch_cell_keys(s->P, x, y, first, count, G, s->d_err, st);
+  launch_exclusive_scan(G.count, G.start, G.ncell, G.block_sums, st);
+  // scatter ids; list is indexed from 0 because start[] only counted this range
+  launch_cell_scatter(G, first, count, st);
+  launch_cell_sort_segments(G, st);
+  s->launches += 6;
+  return UPH_OK;
+}
+
+uph_status build_cell_list(uph_sim *s)
+{
+  Timer t(s, KF_CELLS);
+  return sort_range(s, s->S.x, s->S.y, 0, s->P.n);
+}
+
+uph_status reorder_fluid(uph_sim *s)
+{
+  Timer t(s, KF_REORDER);
+  const int nf = s->P.nf, n = s->P.n;
+  uph_status r = sort_range(s, s->S.x, s->S.y, 0, nf);
+  if (r != UPH_OK) return r;
+  UPH_CUDA(cudaMemcpyAsync(s->d_perm, s->G.list, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
+  if (n > nf) k_iota<<<(n - nf + 255) / 256, 256, 0, s->stream>>>(s->d_perm, nf, n - nf);
+  k_reorder<<<(n + 255) / 256, 256, 0, s->stream>>>(s->S2, s->S, s->d_perm, n, nf);
+  s->launches += 2;
+  SlotArrays tmp = s->S;
+  s->S = s->S2;
+  s->S2 = tmp;
+  s->steps_since_reorder = 0;
+  return UPH_OK;
+}
+
+uph_status check_error_word(uph_sim *s)
+{
+  unsigned err = 0;
+  UPH_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  UPH_CUDA(cudaGetLastError());
+  if (err & ERR_NAN) return fail(UPH_NAN, "a non-finite value appeared in the particle state");
+  if (err & ERR_OUT_OF_DOMAIN) return fail(UPH_OUT_OF_DOMAIN, "a particle left the cell-grid domain");
+  if (err & ERR_NEIGHBOR_OVERFLOW) return fail(UPH_NEIGHBOR_OVERFLOW, "neighbour capacity exceeded");
+  if (err & ERR_TIMEOUT) return fail(UPH_TIMEOUT, "a device-side wait timed out");
+  return UPH_OK;
+}
+
+uph_status rate_pass(uph_sim *s)
+{
+  UPH_CUDA(cudaMemsetAsync(s->d_niac, 0, sizeof(unsigned long long), s->stream));
+  UPH_CUDA(cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), s->stream));
+  {
+    Timer t(s, KF_REFRESH);
+    launch_refresh_inverse(s->P, s->S, 0, s->P.nf, s->stream);
+    s->launches++;
+  }
+  uph_status r = build_cell_list(s);
+  if (r != UPH_OK) return r;
+  Timer t(s, KF_PASS);
+  PassStats st{s->d_niac, s->d_max_nb};
+  if (s->P.profile == UPH_PROFILE_REF)
+    launch_ref_pass(s->P, s->S, s->G, st, s->stream);
+  else
+    launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
+  s->launches++;
+  s->have_rates = true;
+  return UPH_OK;
+}
+
+uph_status validate(const uph_params *p)
+{
+  if (p->n_fluid < 0 || p->n_solid < 0 || p->n_fixed < 0 || p->n_moving < 0)
+    return fail(UPH_BAD_ARG, "negative particle count");
+  const long long n = (long long)p->n_fluid + p->n_solid + p->n_fixed + p->n_moving;
+  if (n <= 0 || n > (1LL << 30)) return fail(UPH_BAD_ARG, "particle count out of range");
+  if (p->profile != UPH_PROFILE_REF && p->profile != UPH_PROFILE_WCSPH) return fail(UPH_BAD_ARG, "unknown profile");
+  if (p->precision != UPH_PREC_FP64 && p->precision != UPH_PREC_FP32_PAIR)
+    return fail(UPH_BAD_ARG, "unknown precision");
+  if (p->precision == UPH_PREC_FP32_PAIR && p->profile != UPH_PROFILE_WCSPH)
+    return fail(UPH_UNSUPPORTED, "FP32 pair arithmetic is implemented for the WCSPH profile only");
+  if (!(p->h > 0) || !(p->dx > 0)) return fail(UPH_BAD_ARG, "smoothing length and dx must be positive");
+  if (p->dim != 2) return fail(UPH_UNSUPPORTED, "only dim = 2 exists in the reference");
+  if (p->flag_init_simul != 1)
+    return fail(UPH_UNSUPPORTED, "flagInitSimul != 1 (particle-packing initialisation) is not implemented");
+  const int vt = p->virtual_type;
+  if (vt == 1 || vt == 3 || vt == 4 || vt == 5 || vt == 7 || vt == 8)
+    return fail(UPH_UNSUPPORTED, "virtual mirror particles (virtualType 1,3,4,5,7,8) are not implemented");
+  if (p->stress_type == 2) return fail(UPH_UNSUPPORTED, "stressType 2 (two-step viscous stress) is not implemented");
+  if (p->knn_cap != 0) return fail(UPH_UNSUPPORTED, "the k-NN cap is not implemented; use knn_cap = 0");
+  if (!(p->domain_hi[0] > p->domain_lo[0]) || !(p->domain_hi[1] > p->domain_lo[1]))
+    return fail(UPH_BAD_ARG, "empty cell-grid domain");
+  return UPH_OK;
+}
+
+DevParams make_dev_params(const uph_params *p)
+{
+  DevParams P;
+  memset(&P, 0, sizeof P);
+  P.nf = p->n_fluid;
+  P.n = p->n_fluid + p->n_solid + p->n_fixed + p->n_moving;
+  P.pb = P.n - 1;
+  P.b0 = p->n_fluid + p->n_solid;
+  P.b1 = P.n;
+  P.m0 = p->n_fluid + p->n_solid + p->n_fixed;
+  P.profile = p->profile;
+  P.precision = p->precision;
+  const double h = p->h;
+  P.h = h;
+  P.inv_h = 1.0 / h;
+  P.inv_h2 = 1.0 / (h * h);
+  P.r2cut = h * h * 4;                                  // derivatives.c:1086
+  P.eta2 = 0.01 * h * h;
+  P.w_alpha = 2145.0 / (1347584.0 * M_PI * h * h);      // derivatives.c:769
+  P.dw_alpha = -1.0 * (2145.0 / (192512.0 * M_PI * h * h));  // derivatives.c:788, 817
+  P.cs_alpha = 10.0 / (7. * M_PI * h * h);              // derivatives.c:46
+  P.rho0 = p->density0;
+  P.gamma = p->adiabatic_constant;
+  P.c0 = p->speed_of_sound;
+  P.B = p->compression_factor;
+  P.rho0c2 = p->density0 * p->speed_of_sound * p->speed_of_sound;
+  P.g = p->gravity;
+  P.gravity_flag = p->gravity_flag;
+  P.mu0 = p->viscosity0;
+  P.kappa = p->thermal_diffusivity0;
+  P.eps = p->epsilon;
+  P.stress_type = p->stress_type;
+  P.boundary_force = p->select_boundary_force;
+  P.k_spring = p->spring_constant0;
+  P.c_damp = p->damping_constant0;
+  P.dx = p->dx;
+  P.dy = p->dy;
+  P.lj_coeff = p->lennard_coefficient;
+  P.mach_c = p->mach_number * p->speed_of_sound;
+  P.moving_boundary = p->moving_boundary;
+  P.flag_init_simul = p->flag_init_simul;
+  P.wave_absorption = p->wave_absorption;
+  P.stroke = p->stroke;
+  P.omega = p->omega;
+  P.av_alpha_c0 = p->av_alpha * p->speed_of_sound;
+  P.dt = p->time_step;
+  const double cell = sqrt(P.r2cut) * (1.0 + 1e-9);
+  P.lo_x = p->domain_lo[0];
+  P.lo_y = p->domain_lo[1];
+  P.cell = cell;
+  P.inv_cell = 1.0 / cell;
+  P.ncx = (int)ceil((p->domain_hi[0] - p->domain_lo[0]) / cell);
+  P.ncy = (int)ceil((p->domain_hi[1] - p->domain_lo[1]) / cell);
+  if (P.ncx < 1) P.ncx = 1;
+  if (P.ncy < 1) P.ncy = 1;
+  return P;
+}
+
+}  // namespace
+
+// ---- C ABI ---------------------------------------------------------------------
+
+extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
+{
+  if (!p || !out) return fail(UPH_BAD_ARG, "uph_sim_create: NULL argument");
+  *out = nullptr;
+  uph_status v = validate(p);
+  if (v != UPH_OK) return v;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(UPH_NO_DEVICE, "no CUDA device is visible");
+  uph_sim *s = new uph_sim();
+  s->hp = *p;
+  s->P = make_dev_params(p);
+  const long long ncell = (long long)s->P.ncx * s->P.ncy;
+  if (ncell > (1LL << 28)) {
+    delete s;
+    return fail(UPH_BAD_ARG, "cell grid larger than 2^28 cells; shrink the domain");
+  }
+  const int n = s->P.n, nf = s->P.nf;
+#define TRY(x)                       \
+  do {                               \
+    cudaError_t e_ = (x);            \
+    if (e_ != cudaSuccess) {         \
+      uph_sim_destroy(s);            \
+      return cuda_fail(e_, #x);      \
+    }                                \
+  } while (0)
+  TRY(alloc_slots(s, s->S, n, nf));
+  TRY(alloc_slots(s, s->S2, n, nf));
+  CellGrid &G = s->G;
+  G.ncell = (int)ncell;
+  TRY(dalloc(s, &G.count, (size_t)ncell));
+  TRY(dalloc(s, &G.start, (size_t)ncell + 1));
+  TRY(dalloc(s, &G.fill, (size_t)ncell));
+  TRY(dalloc(s, &G.list, (size_t)n));
+  TRY(dalloc(s, &G.cell_of, (size_t)n));
+  G.nblock_sums = scan_block_sums_needed((int)ncell);
+  TRY(dalloc(s, &G.block_sums, (size_t)G.nblock_sums));
+  Staging &T = s->T;
+  double **tall[] = {&T.rho, &T.lrho, &T.p, &T.lp, &T.mass, &T.pressure, &T.tmp_x, &T.tmp_y};
+  for (double **q : tall) TRY(dalloc(s, q, (size_t)n));
+  double **tall2[] = {&T.pos, &T.vel, &T.lvel};
+  for (double **q : tall2) TRY(dalloc(s, q, 2 * (size_t)n));
+  TRY(dalloc(s, &T.itype, (size_t)n));
+  double **tfl[] = {&T.rhomin, &T.pmin, &T.sponge, &T.drho, &T.dp, &T.drho_a, &T.dp_a, &T.frho, &T.fp};
+  for (double **q : tfl) TRY(dalloc(s, q, (size_t)nf));
+  double **tfl2[] = {&T.vmin, &T.acc, &T.acc_a, &T.fvel};
+  for (double **q : tfl2) TRY(dalloc(s, q, 2 * (size_t)nf));
+  TRY(dalloc(s, &s->d_err, 1));
+  TRY(dalloc(s, &s->d_niac, 1));
+  TRY(dalloc(s, &s->d_max_nb, 1));
+  TRY(dalloc(s, &s->d_perm, (size_t)n));
+  s->n_partials = 1024;
+  TRY(dalloc(s, &s->d_partials, (size_t)s->n_partials * 4));
+  TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  s->own_stream = true;
+  TRY(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream));
+#undef TRY
+  *out = s;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_destroy(uph_sim *s)
+{
+  if (!s) return UPH_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void *p : s->allocations) cudaFree(p);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  for (cudaEvent_t e : s->ev_pool)
+    if (e) cudaEventDestroy(e);
+  delete s;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_set_stream(uph_sim *s, void *stream)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else {
+    UPH_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
+  return UPH_OK;
+}
+
+namespace {
+
+template <typename T>
+cudaError_t h2d(T *dst, const T *src, size_t count, cudaStream_t st)
+{
+  if (!src) return cudaMemsetAsync(dst, 0, sizeof(T) * count, st);
+  return cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+}
+
+template <typename T>
+cudaError_t d2h(T *dst, const T *src, size_t count, cudaStream_t st)
+{
+  if (!dst) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyDeviceToHost, st);
+}
+
+}  // namespace
+
+extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t itime)
+{
+  if (!s || !st) return fail(UPH_BAD_ARG, "uph_sim_upload: NULL argument");
+  if (!st->Position || !st->Velocity || !st->density || !st->DynamicPressure || !st->mass || !st->itype)
+    return fail(UPH_BAD_ARG, "uph_sim_upload: Position, Velocity, density, DynamicPressure, mass and itype are required");
+  if (itime < 0) return fail(UPH_BAD_ARG, "uph_sim_upload: negative itime");
+  const int n = s->P.n, nf = s->P.nf;
+  cudaStream_t q = s->stream;
+  Staging &T = s->T;
+  UPH_CUDA(h2d(T.pos, st->Position, 2 * (size_t)n, q));
+  UPH_CUDA(h2d(T.vel, st->Velocity, 2 * (size_t)n, q));
+  UPH_CUDA(h2d(T.lvel, st->localVelocity ? st->localVelocity : st->Velocity, 2 * (size_t)n, q));
+  UPH_CUDA(h2d(T.rho, st->density, (size_t)n, q));
+  UPH_CUDA(h2d(T.lrho, st->localDensity ? st->localDensity : st->density, (size_t)n, q));
+  UPH_CUDA(h2d(T.p, st->DynamicPressure, (size_t)n, q));
+  UPH_CUDA(h2d(T.lp, st->localPressure, (size_t)n, q));
+  UPH_CUDA(h2d(T.mass, st->mass, (size_t)n, q));
+  UPH_CUDA(h2d(T.itype, st->itype, (size_t)n, q));
+  UPH_CUDA(h2d(T.pressure, st->Pressure, (size_t)n, q));
+  UPH_CUDA(h2d(T.vmin, st->Velocity_min, 2 * (size_t)nf, q));
+  UPH_CUDA(h2d(T.rhomin, st->density_min, (size_t)nf, q));
+  UPH_CUDA(h2d(T.pmin, st->DynamicPressure_min, (size_t)nf, q));
+  UPH_CUDA(h2d(T.sponge, st->spongeFactor, (size_t)nf, q));
+  UPH_CUDA(h2d(T.drho, st->ddensitydt, (size_t)nf, q));
+  UPH_CUDA(h2d(T.dp, st->dpdt, (size_t)nf, q));
+  UPH_CUDA(h2d(T.acc, st->dvdt, 2 * (size_t)nf, q));
+  UPH_CUDA(h2d(T.drho_a, st->ddensitydt_approx, (size_t)nf, q));
+  UPH_CUDA(h2d(T.dp_a, st->dpdt_approx, (size_t)nf, q));
+  UPH_CUDA(h2d(T.acc_a, st->dvdt_approx, 2 * (size_t)nf, q));
+  UPH_CUDA(h2d(T.frho, st->densityFluctuation, (size_t)nf, q));
+  UPH_CUDA(h2d(T.fp, st->pressureFluctuation, (size_t)nf, q));
+  UPH_CUDA(h2d(T.fvel, st->velocityFluctuation, 2 * (size_t)nf, q));
+  UPH_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), q));
+  // spatial order: fluid and walls sorted by cell separately
+  k_split_xy<<<(n + 255) / 256, 256, 0, q>>>(T.pos, T.tmp_x, T.tmp_y, n);
+  s->launches++;
+  uph_status r = sort_range(s, T.tmp_x, T.tmp_y, 0, nf);
+  if (r != UPH_OK) return r;
+  UPH_CUDA(cudaMemcpyAsync(s->d_perm, s->G.list, sizeof(int) * nf, cudaMemcpyDeviceToDevice, q));
+  if (n > nf) {
+    r = sort_range(s, T.tmp_x, T.tmp_y, nf, n - nf);
+    if (r != UPH_OK) return r;
+    UPH_CUDA(cudaMemcpyAsync(s->d_perm + nf, s->G.list, sizeof(int) * (n - nf), cudaMemcpyDeviceToDevice, q));
+  }
+  k_gather_upload<<<(n + 255) / 256, 256, 0, q>>>(s->S, T, s->d_perm, n, nf, s->P.rho0);
+  launch_refresh_inverse(s->P, s->S, 0, n, q);
+  launch_wall_pressure(s->P, s->S, q);
+  s->launches += 3;
+  s->itime = itime;
+  s->steps_since_reorder = 0;
+  s->have_rates = false;
+  return check_error_word(s);
+}
+
+extern "C" uph_status uph_sim_download(uph_sim *s, uph_state *st)
+{
+  if (!s || !st) return fail(UPH_BAD_ARG, "uph_sim_download: NULL argument");
+  const int n = s->P.n, nf = s->P.nf;
+  cudaStream_t q = s->stream;
+  Staging &T = s->T;
+  k_scatter_download<<<(n + 255) / 256, 256, 0, q>>>(s->S, T, n, nf);
+  s->launches++;
+  UPH_CUDA(d2h(st->Position, T.pos, 2 * (size_t)n, q));
+  UPH_CUDA(d2h(st->Velocity, T.vel, 2 * (size_t)n, q));
+  UPH_CUDA(d2h(st->localVelocity, T.lvel, 2 * (size_t)n, q));
+  UPH_CUDA(d2h(st->density, T.rho, (size_t)n, q));
+  UPH_CUDA(d2h(st->localDensity, T.lrho, (size_t)n, q));
+  UPH_CUDA(d2h(st->DynamicPressure, T.p, (size_t)n, q));
+  UPH_CUDA(d2h(st->localPressure, T.lp, (size_t)n, q));
+  UPH_CUDA(d2h(st->mass, T.mass, (size_t)n, q));
+  UPH_CUDA(d2h(st->itype, T.itype, (size_t)n, q));
+  UPH_CUDA(d2h(st->Pressure, T.pressure, (size_t)n, q));
+  UPH_CUDA(d2h(st->Velocity_min, T.vmin, 2 * (size_t)nf, q));
+  UPH_CUDA(d2h(st->density_min, T.rhomin, (size_t)nf, q));
+  UPH_CUDA(d2h(st->DynamicPressure_min, T.pmin, (size_t)nf, q));
+  UPH_CUDA(d2h(st->spongeFactor, T.sponge, (size_t)nf, q));
+  UPH_CUDA(d2h(st->ddensitydt, T.drho, (size_t)nf, q));
+  UPH_CUDA(d2h(st->dpdt, T.dp, (size_t)nf, q));
+  UPH_CUDA(d2h(st->dvdt, T.acc, 2 * (size_t)nf, q));
+  UPH_CUDA(d2h(st->ddensitydt_approx, T.drho_a, (size_t)nf, q));
+  UPH_CUDA(d2h(st->dpdt_approx, T.dp_a, (size_t)nf, q));
+  UPH_CUDA(d2h(st->dvdt_approx, T.acc_a, 2 * (size_t)nf, q));
+  UPH_CUDA(d2h(st->densityFluctuation, T.frho, (size_t)nf, q));
+  UPH_CUDA(d2h(st->pressureFluctuation, T.fp, (size_t)nf, q));
+  UPH_CUDA(d2h(st->velocityFluctuation, T.fvel, 2 * (size_t)nf, q));
+  UPH_CUDA(cudaStreamSynchronize(q));
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  if (nsteps < 0) return fail(UPH_BAD_ARG, "negative step count");
+  const bool walls_move = s->P.moving_boundary == 1 && s->P.flag_init_simul == 1 && s->hp.n_moving > 0;
+  for (int k = 0; k < nsteps; k++) {
+    const int itime = ++s->itime;
+    const double t = itime * s->P.dt;
+    if (itime != 1) {
+      Timer tm(s, KF_PREDICT);
+      launch_predict(s->P, s->S, s->stream);
+      s->launches++;
+    }
+    if (walls_move) {
+      Timer tm(s, KF_WALLS);
+      launch_wall_motion(s->P, s->S, t, s->stream);
+      s->launches++;
+    }
+    uph_status r = rate_pass(s);
+    if (r != UPH_OK) return r;
+    {
+      Timer tm(s, KF_CORRECT);
+      launch_correct(s->P, s->S, itime == 1, s->d_err, s->stream);
+      s->launches++;
+    }
+    if (++s->steps_since_reorder >= kReorderInterval) {
+      r = reorder_fluid(s);
+      if (r != UPH_OK) return r;
+    }
+  }
+  UPH_CUDA(cudaGetLastError());
+  return check_error_word(s);
+}
+
+extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  // the piston position is a closed form of t, so applying it again after the
+  // caller's own inputbp() changes nothing
+  if (s->P.moving_boundary == 1 && s->P.flag_init_simul == 1 && s->hp.n_moving > 0) {
+    launch_wall_motion(s->P, s->S, t, s->stream);
+    s->launches++;
+  }
+  uph_status r = rate_pass(s);
+  if (r != UPH_OK) return r;
+  UPH_CUDA(cudaGetLastError());
+  return check_error_word(s);
+}
+
+// ---- pair export ---------------------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ double pr2(double dx, double dy) { return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)); }
+
+// count pairs whose i (smaller reference index) is the fluid particle in slot a
+__global__ void k_pair_count(DevParams P, SlotArrays S, CellGrid G, int *__restrict__ cnt_by_orig)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const double xa = S.x[a], ya = S.y[a];
+  const int oa = S.orig[a];
+  const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
+  int cnt = 0;
+  for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
+    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
+      const int cc = yy * P.ncx + xx;
+      for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
+        const int b = G.list[k];
+        const int ob = S.orig[b];
+        if (ob <= oa || ob >= P.pb) continue;
+        const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
+        if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
+      }
+    }
+  cnt_by_orig[oa] = cnt;
+}
+
+__global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *__restrict__ off, int32_t *ip,
+                             int32_t *jp, double *rij2, double *w, double *dw)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const double xa = S.x[a], ya = S.y[a];
+  const int oa = S.orig[a];
+  const int base = off[oa];
+  int cnt = 0;
+  const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
+  for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
+    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
+      const int cc = yy * P.ncx + xx;
+      for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
+        const int b = G.list[k];
+        const int ob = S.orig[b];
+        if (ob <= oa || ob >= P.pb) continue;
+        const double dx = xa - S.x[b], dy = ya - S.y[b];
+        const double r2 = pr2(dx, dy);
+        if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
+        const double r = sqrt(r2), q = r * P.inv_h;
+        double W, F;
+        if (P.profile == UPH_PROFILE_REF) {
+          const double q2 = q * q, t = 1.0 - 0.25 * q2, t2 = t * t, t4 = t2 * t2;
+          const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
+          const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
+          W = P.w_alpha * (t4 * t4) * pp;
+          F = P.dw_alpha * (t4 * t2 * t) * pp7 * P.inv_h2;
+        } else if (q < 1.0) {
+          W = P.cs_alpha * (1 - 1.5 * q * q + 0.75 * q * q * q);
+          F = P.cs_alpha * (-3 + 2.25 * q) * P.inv_h2;
+        } else {
+          const double t = 2 - q;
+          W = P.cs_alpha * 0.25 * t * t * t;
+          F = -P.cs_alpha * 0.75 * t * t / (P.h * r);
+        }
+        const int o = base + cnt++;
+        if (ip) ip[o] = oa;
+        if (jp) jp[o] = ob;
+        if (rij2) rij2[o] = r2;
+        if (w) w[o] = W;
+        if (dw) {
+          dw[2 * o] = F * dx;
+          dw[2 * o + 1] = F * dy;
+        }
+      }
+    }
+  // order the segment by j (insertion sort; segments are short)
+  if (jp) {
+    for (int i = base + 1; i < base + cnt; i++) {
+      const int vj = jp[i];
+      const double vr = rij2 ? rij2[i] : 0, vw = w ? w[i] : 0, vx = dw ? dw[2 * i] : 0, vy = dw ? dw[2 * i + 1] : 0;
+      int j = i - 1;
+      while (j >= base && jp[j] > vj) {
+        jp[j + 1] = jp[j];
+        if (rij2) rij2[j + 1] = rij2[j];
+        if (w) w[j + 1] = w[j];
+        if (dw) { dw[2 * (j + 1)] = dw[2 * j]; dw[2 * (j + 1) + 1] = dw[2 * j + 1]; }
+        j--;
+      }
+      jp[j + 1] = vj;
+      if (rij2) rij2[j + 1] = vr;
+      if (w) w[j + 1] = vw;
+      if (dw) { dw[2 * (j + 1)] = vx; dw[2 * (j + 1) + 1] = vy; }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
+                                    double *w, double *dwcdx, int64_t *niac)
+{
+  if (!s || !niac) return fail(UPH_BAD_ARG, "uph_sim_pairs: NULL argument");
+  const int nf = s->P.nf;
+  cudaStream_t q = s->stream;
+  // the cell list of the last evaluation is still valid unless a reorder moved slots since
+  uph_status r = build_cell_list(s);
+  if (r != UPH_OK) return r;
+  int *cnt = nullptr, *off = nullptr, *bsum = nullptr;
+  const int nb = scan_block_sums_needed(nf > 0 ? nf : 1);
+  UPH_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * (nf + 1), q));
+  UPH_CUDA(cudaMallocAsync((void **)&off, sizeof(int) * (nf + 1), q));
+  UPH_CUDA(cudaMallocAsync((void **)&bsum, sizeof(int) * nb, q));
+  uph_status result = UPH_OK;
+  int total = 0;
+  if (nf > 0) {
+    k_pair_count<<<(nf + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, cnt);
+    launch_exclusive_scan(cnt, off, nf, bsum, q);
+    s->launches += 4;
+    cudaMemcpyAsync(&total, off + nf, sizeof(int), cudaMemcpyDeviceToHost, q);
+    cudaStreamSynchronize(q);
+  }
+  *niac = total;
+  if (total > cap) {
+    result = fail(UPH_NEIGHBOR_OVERFLOW, "pair buffer too small: " + std::to_string(total) + " pairs");
+  } else if (total > 0) {
+    int32_t *dip = nullptr, *djp = nullptr;
+    double *dr = nullptr, *dww = nullptr, *ddw = nullptr;
+    cudaMallocAsync((void **)&dip, sizeof(int32_t) * total, q);
+    cudaMallocAsync((void **)&djp, sizeof(int32_t) * total, q);
+    cudaMallocAsync((void **)&dr, sizeof(double) * total, q);
+    cudaMallocAsync((void **)&dww, sizeof(double) * total, q);
+    cudaMallocAsync((void **)&ddw, sizeof(double) * 2 * total, q);
+    k_pair_write<<<(nf + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, off, dip, djp, dr, dww, ddw);
+    s->launches++;
+    if (i_pair) cudaMemcpyAsync(i_pair, dip, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, q);
+    if (j_pair) cudaMemcpyAsync(j_pair, djp, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, q);
+    if (rij2) cudaMemcpyAsync(rij2, dr, sizeof(double) * total, cudaMemcpyDeviceToHost, q);
+    if (w) cudaMemcpyAsync(w, dww, sizeof(double) * total, cudaMemcpyDeviceToHost, q);
+    if (dwcdx) cudaMemcpyAsync(dwcdx, ddw, sizeof(double) * 2 * total, cudaMemcpyDeviceToHost, q);
+    cudaFreeAsync(dip, q);
+    cudaFreeAsync(djp, q);
+    cudaFreeAsync(dr, q);
+    cudaFreeAsync(dww, q);
+    cudaFreeAsync(ddw, q);
+  }
+  cudaFreeAsync(cnt, q);
+  cudaFreeAsync(off, q);
+  cudaFreeAsync(bsum, q);
+  UPH_CUDA(cudaStreamSynchronize(q));
+  UPH_CUDA(cudaGetLastError());
+  return result;
+}
+
+// ---- statistics -----------------------------------------------------------------
+
+namespace {
+
+// per-block partial sums (KE, PE, mass) and max |rho - rho0| / rho0; the host
+// adds the partials in block order, so the result is deterministic
+__global__ void k_stats(DevParams P, SlotArrays S, double *partials, int nblocks_total)
+{
+  __shared__ double sh[4][256];
+  double ke = 0, pe = 0, m = 0, de = 0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.nf; a += gridDim.x * blockDim.x) {
+    const double ma = S.m[a], u = S.u[a], v = S.v[a];
+    ke += 0.5 * ma * (u * u + v * v);
+    pe += ma * P.g * S.y[a];
+    m += ma;
+    de = fmax(de, fabs(S.rho[a] - P.rho0) / P.rho0);
+  }
+  sh[0][threadIdx.x] = ke;
+  sh[1][threadIdx.x] = pe;
+  sh[2][threadIdx.x] = m;
+  sh[3][threadIdx.x] = de;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + o];
+      sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) partials[k * nblocks_total + blockIdx.x] = sh[k][0];
+}
+
+}  // namespace
+
+extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
+{
+  if (!s || !out) return fail(UPH_BAD_ARG, "uph_sim_stats: NULL argument");
+  memset(out, 0, sizeof *out);
+  const int nb = s->n_partials;
+  k_stats<<<nb, 256, 0, s->stream>>>(s->P, s->S, s->d_partials, nb);
+  s->launches++;
+  std::vector<double> part(4 * (size_t)nb);
+  unsigned long long niac = 0;
+  int mx = 0;
+  UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(&niac, s->d_niac, sizeof niac, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  for (int b = 0; b < nb; b++) {
+    out->kinetic_energy += part[b];
+    out->potential_energy += part[nb + b];
+    out->total_mass += part[2 * nb + b];
+    out->max_abs_density_error = fmax(out->max_abs_density_error, part[3 * nb + b]);
+  }
+  out->niac = s->have_rates ? (int64_t)niac : 0;
+  out->max_neighbors = s->have_rates ? mx : 0;
+  out->itime = s->itime;
+  return UPH_OK;
+}
+
+// ---- profiling --------------------------------------------------------------------
+
+extern "C" uph_status uph_sim_profile(uph_sim *s, int32_t enable)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  if (enable && s->ev_pool.empty()) {
+    s->ev_pool.resize(2 * uph_sim::kEventPool, nullptr);
+    s->ev_family.resize(uph_sim::kEventPool, 0);
+    for (cudaEvent_t &e : s->ev_pool) UPH_CUDA(cudaEventCreate(&e));
+  }
+  flush_profile(s);
+  s->profiling = enable != 0;
+  for (int k = 0; k < KF_COUNT; k++) {
+    s->fam_ms[k] = 0;
+    s->fam_launch[k] = 0;
+  }
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_kernel_times(uph_sim *s, int32_t n, double *ms, int64_t *launches, char *names,
+                                           size_t names_len, int32_t *n_written)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  flush_profile(s);
+  const int m = n < KF_COUNT ? n : KF_COUNT;
+  std::string all;
+  for (int k = 0; k < m; k++) {
+    if (ms) ms[k] = s->fam_ms[k];
+    if (launches) launches[k] = s->fam_launch[k];
+    if (k) all += ",";
+    all += kFamilyNames[k];
+  }
+  if (names && names_len) {
+    strncpy(names, all.c_str(), names_len - 1);
+    names[names_len - 1] = 0;
+  }
+  if (n_written) *n_written = m;
+  return UPH_OK;
+}
+
+extern "C" int64_t uph_sim_launch_count(const uph_sim *s) { return s ? s->launches : 0; }
+
+// ---- one-shot neighbour search ------------------------------------------------------
+
+namespace {
+
+__global__ void k_load_positions(SlotArrays S, const double *__restrict__ pos, int n)
+{
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  S.x[k] = pos[2 * k];
+  S.y[k] = pos[2 * k + 1];
+  S.orig[k] = k;
+}
+
+// largest in-radius candidate count (any index, no self matches) of a query
+__global__ void k_inradius_max(DevParams P, SlotArrays S, CellGrid G, int *mx)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt = 0;
+  if (a < P.nf) {
+    const double xa = S.x[a], ya = S.y[a];
+    const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
+    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
+      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
+        const int cc = yy * P.ncx + xx;
+        for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
+          const int b = G.list[k];
+          const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
+          if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
+        }
+      }
+  }
+  const int w = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+  if ((threadIdx.x & 31) == 0 && w) atomicMax(mx, w);
+}
+
+}  // namespace
+
+extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_fluid, int32_t n_all,
+                                           int32_t particle_boundary, int32_t knn, double dist, int64_t cap,
+                                           int32_t *i_pair, int32_t *j_pair, double *rij2, int64_t *niac)
+{
+  if (!position || !niac || n_fluid < 0 || n_all < n_fluid || n_all <= 0)
+    return fail(UPH_BAD_ARG, "uph_search_neighbors: bad arguments");
+  *niac = 0;
+  if (n_fluid == 0 || !(dist > 0.0)) return UPH_OK;
+  double lo[2] = {position[0], position[1]}, hi[2] = {position[0], position[1]};
+  for (int k = 1; k < n_all; k++)
+    for (int d = 0; d < 2; d++) {
+      const double v = position[2 * k + d];
+      if (!(v == v)) return fail(UPH_NAN, "uph_search_neighbors: non-finite position");
+      lo[d] = fmin(lo[d], v);
+      hi[d] = fmax(hi[d], v);
+    }
+  uph_params p;
+  memset(&p, 0, sizeof p);
+  p.n_fluid = n_fluid;
+  p.n_fixed = n_all - n_fluid;
+  p.dim = 2;
+  p.flag_init_simul = 1;
+  p.dx = 1.0;
+  p.h = 0.5 * sqrt(dist);
+  p.density0 = 1.0;
+  const double pad = sqrt(dist);
+  p.domain_lo[0] = lo[0] - pad;
+  p.domain_lo[1] = lo[1] - pad;
+  p.domain_hi[0] = hi[0] + pad;
+  p.domain_hi[1] = hi[1] + pad;
+  uph_sim *s = nullptr;
+  uph_status r = uph_sim_create(&p, &s);
+  if (r != UPH_OK) return r;
+  // the reference's own threshold and boundary index, not ones derived from h
+  s->P.r2cut = dist;
+  s->P.pb = particle_boundary;
+  cudaStream_t q = s->stream;
+  double *dpos = s->T.pos;
+  r = UPH_OK;
+  if (cudaMemcpyAsync(dpos, position, sizeof(double) * 2 * n_all, cudaMemcpyHostToDevice, q) != cudaSuccess) {
+    uph_sim_destroy(s);
+    return fail(UPH_CUDA_ERROR, "uph_search_neighbors: upload failed");
+  }
+  k_load_positions<<<(n_all + 255) / 256, 256, 0, q>>>(s->S, dpos, n_all);
+  r = build_cell_list(s);
+  if (r == UPH_OK && knn > 0) {
+    int mx = 0;
+    cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), q);
+    k_inradius_max<<<(n_fluid + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, s->d_max_nb);
+    cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, q);
+    cudaStreamSynchronize(q);
+    if (mx > knn - 1)
+      r = fail(UPH_UNSUPPORTED, "a query has " + std::to_string(mx) + " in-radius neighbours; the reference's " +
+                                    std::to_string(knn) + "-NN cap would bind and its tie order is not reproduced");
+  }
+  if (r == UPH_OK) r = check_error_word(s);
+  if (r == UPH_OK) {
+    s->have_rates = true;
+    // uph_sim_pairs without the cell-list rebuild side effects on positions
+    r = uph_sim_pairs(s, cap, i_pair, j_pair, rij2, nullptr, nullptr, niac);
+  }
+  uph_sim_destroy(s);
+  return r;
+}

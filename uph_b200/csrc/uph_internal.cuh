@@ -1,0 +1,116 @@
+// Internal definitions shared by the CUDA translation units of libuph.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "uph.h"
+
+namespace uph {
+
+// ---- device error word bits (set by kernels, read by the host) -------------
+enum : unsigned {
+  ERR_OUT_OF_DOMAIN = 1u,
+  ERR_NAN = 2u,
+  ERR_NEIGHBOR_OVERFLOW = 4u,
+  ERR_TIMEOUT = 8u,
+};
+
+// Particle data in storage ("slot") order.  Fluid particles occupy slots
+// [0, nf), the other interacting particles [nf, n).  Storage order is
+// spatially sorted (cell order) so that a warp's particles share neighbours.
+struct SlotArrays {
+  double *x, *y, *u, *v;  // Position, Velocity
+  double *ut, *vt;        // localVelocity
+  double *rho, *rhot;     // density, localDensity
+  double *p, *pt;         // DynamicPressure, localPressure
+  double *m;              // mass
+  double *inv_rho;        // 1 / density (refreshed before every rate evaluation)
+  double *inv_rhot;       // 1 / localDensity
+  int32_t *itype;
+  int32_t *orig;          // reference index of the particle in this slot
+  // fluid-only (first nf slots)
+  double *rho_min, *p_min, *u_min, *v_min;
+  double *sponge;
+  double *drho, *dp, *ax, *ay;              // ddensitydt, dpdt, dvdt
+  double *drho_a, *dp_a, *ax_a, *ay_a;      // *_approx
+  double *frho, *fp, *fu, *fv;              // density/pressure/velocity fluctuation
+  double *pressure;                         // algebraic Tait (all slots)
+};
+
+// Constants of one simulation as the kernels see them.
+struct DevParams {
+  int nf, n;        // fluid slots, all slots
+  int pb;           // ParticleBoundary = Nf + Ns + Nb - 1 (reference indices)
+  int b0, b1;       // boundary reference index range [Nf+Ns, Nf+Ns+Nb)
+  int m0;           // first moving-boundary reference index
+  int profile, precision;
+  double h, inv_h, inv_h2;
+  double r2cut;     // (h*h)*4, the reference's search radius squared
+  double eta2;      // 0.01 h^2
+  double w_alpha;   // poly-7 convolution normalisation (derivatives.c:769)
+  double dw_alpha;  // -alpha_0 of the poly-7 deconvolution (derivatives.c:788)
+  double cs_alpha;  // cubic spline sigma = 10 / (7 pi h^2) (derivatives.c:46)
+  double rho0, gamma, c0, B, rho0c2, g;
+  int gravity_flag;
+  double mu0, kappa, eps;
+  int stress_type;
+  int boundary_force;
+  double k_spring, c_damp, dx, dy;
+  double lj_coeff, mach_c;  // LennardCoefficient, machNumber * SpeedOfSound
+  int moving_boundary, flag_init_simul, wave_absorption;
+  double stroke, omega;
+  double av_alpha_c0;       // WCSPH: alpha * c0
+  double dt;
+  // cell grid
+  double lo_x, lo_y, cell, inv_cell;
+  int ncx, ncy;
+};
+
+struct CellGrid {
+  int ncell;
+  int *count;    // [ncell]
+  int *start;    // [ncell + 1]
+  int *fill;     // [ncell]
+  int *list;     // [n] slots in cell order
+  int *cell_of;  // [n]
+  int *block_sums;
+  int nblock_sums;
+};
+
+std::string &last_error();
+uph_status fail(uph_status s, const std::string &msg);
+uph_status cuda_fail(cudaError_t e, const char *what);
+
+#define UPH_CUDA(call)                                  \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return ::uph::cuda_fail(e_, #call); \
+  } while (0)
+
+// ---- launches implemented in the .cu files ---------------------------------
+// cell list
+void launch_cell_keys(const DevParams &P, const double *x, const double *y, int first, int count,
+                      CellGrid &G, unsigned *err, cudaStream_t s);
+void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s);
+void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s);
+void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s);
+
+// REF / WCSPH rate pass over the fluid slots
+struct PassStats {
+  unsigned long long *niac;  // pairs (i < j) counted from the i side
+  int *max_nb;               // largest in-radius neighbour count of a fluid particle
+};
+void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+
+// leapfrog
+void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);
+void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, unsigned *err, cudaStream_t s);
+void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s);
+void launch_wall_motion(const DevParams &P, const SlotArrays &S, double t, cudaStream_t s);
+void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t s);
+
+}  // namespace uph

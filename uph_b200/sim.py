@@ -1,0 +1,145 @@
+"""Python host mirror of the reference's hot-path interface.
+
+The reference drives its solver as
+
+    sys = CreateSystem(...); input(sys)                 # System.c:38, input.c:22
+    for itime in 1..N: ...; derivatives(sys, t); ...    # sph.cc:90-168
+    SearchNeighbors(Position, i_pair, j_pair, rij2, Nf, N, PB, 40, dist)   # Search.cc:5
+
+`Simulation` holds one case resident on the GPU and offers the same
+operations -- `derivatives(t)` (one rate evaluation, derivatives.c:3137),
+`step(n)` (the sph.cc leapfrog), `search_neighbors` (SearchNeighbors) --
+through libuph.so.  Arrays are numpy, in the reference's particle order and
+layout ([n][2] vectors).  Errors raise UphError with the library's status
+instead of the reference's printf + exit(1).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _lib
+from ._capi import (PREC_FP64, PROFILE_REF, STATE_FIELDS, UphParams, UphStats, empty_state, state_struct)
+from .deck import Deck
+
+
+class Simulation:
+    def __init__(self, params: dict):
+        self.lib = _lib.lib()
+        self.params = UphParams.from_dict(params)
+        self.n_fluid = int(params["n_fluid"])
+        self.n_all = int(params["n_fluid"] + params["n_solid"] + params["n_fixed"] + params["n_moving"])
+        h = C.c_void_p()
+        _lib.check(self.lib.uph_sim_create(C.byref(self.params), C.byref(h)), "uph_sim_create")
+        self.handle = h
+
+    @classmethod
+    def from_deck(cls, deck: Deck, profile: int = PROFILE_REF, precision: int = PREC_FP64,
+                  av_alpha: Optional[float] = None) -> "Simulation":
+        sim = cls(deck.uph_params(profile, precision, av_alpha))
+        sim.upload(deck.initial_state(), 0)
+        return sim
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.uph_sim_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ----------------------------------------------------------------
+    def upload(self, state: Dict[str, np.ndarray], itime: int = 0) -> None:
+        keep = []
+        st = state_struct(state, keep)
+        _lib.check(self.lib.uph_sim_upload(self.handle, C.byref(st), itime), "uph_sim_upload")
+
+    def download(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        if out is None:
+            out = empty_state(self.n_fluid, self.n_all)
+        keep = []
+        st = state_struct(out, keep)
+        _lib.check(self.lib.uph_sim_download(self.handle, C.byref(st)), "uph_sim_download")
+        return out
+
+    state = download
+
+    # -- the hot path ----------------------------------------------------------
+    def step(self, nsteps: int = 1) -> None:
+        _lib.check(self.lib.uph_sim_step(self.handle, nsteps), "uph_sim_step")
+
+    def derivatives(self, t: float) -> None:
+        _lib.check(self.lib.uph_sim_derivatives(self.handle, t), "uph_sim_derivatives")
+
+    def pairs(self):
+        """(i_pair, j_pair, rij2, w, dwcdx) of the current positions."""
+        n = C.c_int64(0)
+        st = self.lib.uph_sim_pairs(self.handle, 0, None, None, None, None, None, C.byref(n))
+        if st not in (0, 3):
+            _lib.check(st, "uph_sim_pairs")
+        k = n.value
+        i = np.zeros(k, np.int32)
+        j = np.zeros(k, np.int32)
+        r2 = np.zeros(k)
+        w = np.zeros(k)
+        dw = np.zeros((k, 2))
+        _lib.check(self.lib.uph_sim_pairs(self.handle, k, i.ctypes.data, j.ctypes.data, r2.ctypes.data,
+                                          w.ctypes.data, dw.ctypes.data, C.byref(n)), "uph_sim_pairs")
+        return i, j, r2, w, dw
+
+    def stats(self) -> dict:
+        s = UphStats()
+        _lib.check(self.lib.uph_sim_stats(self.handle, C.byref(s)), "uph_sim_stats")
+        return {name: getattr(s, name) for name, _ in UphStats._fields_}
+
+    # -- measurement -----------------------------------------------------------
+    def set_stream(self, cuda_stream: int) -> None:
+        _lib.check(self.lib.uph_sim_set_stream(self.handle, C.c_void_p(cuda_stream)), "uph_sim_set_stream")
+
+    def profile(self, enable: bool) -> None:
+        _lib.check(self.lib.uph_sim_profile(self.handle, 1 if enable else 0), "uph_sim_profile")
+
+    def kernel_times(self) -> Dict[str, tuple]:
+        ms = np.zeros(16)
+        cnt = np.zeros(16, np.int64)
+        names = C.create_string_buffer(512)
+        nw = C.c_int32(0)
+        _lib.check(self.lib.uph_sim_kernel_times(self.handle, 16, ms.ctypes.data, cnt.ctypes.data, names, 512,
+                                                 C.byref(nw)), "uph_sim_kernel_times")
+        keys = names.value.decode().split(",")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(keys[:nw.value])}
+
+    def launch_count(self) -> int:
+        return int(self.lib.uph_sim_launch_count(self.handle))
+
+
+def search_neighbors(position: np.ndarray, n_fluid: int, particle_boundary: int, dist: float,
+                     number_of_neighbors: int = 40):
+    """SearchNeighbors (Search.cc:5): pairs (s, j), s < n_fluid < ..., j > s,
+    DBL_EPSILON < rij2 < dist, j < particle_boundary; returns (i, j, rij2)."""
+    l = _lib.lib()
+    pos = np.ascontiguousarray(position, dtype=np.float64).reshape(-1, 2)
+    n = C.c_int64(0)
+    st = l.uph_search_neighbors(pos.ctypes.data, n_fluid, pos.shape[0], particle_boundary, number_of_neighbors,
+                                dist, 0, None, None, None, C.byref(n))
+    if st not in (0, 3):
+        _lib.check(st, "uph_search_neighbors")
+    k = n.value
+    i = np.zeros(k, np.int32)
+    j = np.zeros(k, np.int32)
+    r2 = np.zeros(k)
+    _lib.check(l.uph_search_neighbors(pos.ctypes.data, n_fluid, pos.shape[0], particle_boundary,
+                                      number_of_neighbors, dist, k, i.ctypes.data, j.ctypes.data, r2.ctypes.data,
+                                      C.byref(n)), "uph_search_neighbors")
+    return i, j, r2
+
+
+__all__ = ["Simulation", "search_neighbors", "STATE_FIELDS"]
