@@ -872,6 +872,12 @@ int uph_oracle_step(uph_oracle *o, int nsteps)
           o->pos[2 * i + d] += dt * o->vel[2 * i + d];
         }
     }
+    if (o->p.profile == UPH_PROFILE_WCSPH)
+      for (int i = 0; i < nf; i++) { /* the WCSPH pressure is Tait's law of the new density */
+        const double density = o->rho[i] / o->p.density0;
+        o->pr[i] = o->p.compression_factor * (pow(density, o->p.adiabatic_constant) - 1.0);
+        o->pressure[i] = o->pr[i];
+      }
   }
   return 0;
 }

@@ -43,23 +43,25 @@ def _perturb(deck: D.Deck, seed: int, vel: float = 0.05) -> D.Deck:
 def cases():
     """name -> Deck"""
     out = {}
+    K = dict(thermal_diffusivity0=0.015)  # the reference hydrostatic deck's value
     out["dambreak_h13"] = _perturb(D.dam_break(tank=(1.0, 1.0), column=(0.4, 0.6), dx=0.02, layers=2,
-                                               hydrostatic=True), seed=1)
+                                               hydrostatic=True, **K), seed=1)
     # the reference decks' own smoothing length eta = sqrt(19 / 4 pi)
-    d = D.dam_break(tank=(0.8, 0.6), column=(0.5, 0.3), dx=0.02, layers=2, eta=0.0, hydrostatic=True)
+    d = D.dam_break(tank=(0.8, 0.6), column=(0.5, 0.3), dx=0.02, layers=2, eta=0.0, hydrostatic=True, **K)
     d.params["near_neighbor"] = 19
     out["tank_nn19"] = _perturb(d, seed=2)
     out["flume_piston_sponge"] = _perturb(D.wave_flume(length=7.6, depth=0.2, dx=0.04, layers=2, amplitude=0.02,
-                                                       period=1.2), seed=3, vel=0.02)
+                                                       period=1.2, **K), seed=3, vel=0.02)
     for mode in (1, 4, 5, 0):
         out[f"wallforce_mode{mode}"] = _perturb(D.dam_break(tank=(0.5, 0.5), column=(0.3, 0.3), dx=0.02, layers=2,
-                                                            hydrostatic=True, select_boundary_force=mode), seed=10 + mode)
+                                                            hydrostatic=True, select_boundary_force=mode, **K),
+                                                seed=10 + mode)
     # no walls: ParticleBoundary = Nf - 1 excludes the last fluid particle as a partner
-    d = D.dam_break(tank=(0.4, 0.4), column=(0.2, 0.2), dx=0.02, layers=2, hydrostatic=True)
+    d = D.dam_break(tank=(0.4, 0.4), column=(0.2, 0.2), dx=0.02, layers=2, hydrostatic=True, **K)
     d.fixed = np.zeros((0, 12))
     out["fluid_only"] = _perturb(d, seed=20)
     # ragged: irregular fluid positions, gravity off, a solid block
-    d = D.dam_break(tank=(0.6, 0.6), column=(0.4, 0.4), dx=0.02, layers=2, hydrostatic=True, gravity_flag=0)
+    d = D.dam_break(tank=(0.6, 0.6), column=(0.4, 0.4), dx=0.02, layers=2, hydrostatic=True, gravity_flag=0, **K)
     rng = np.random.default_rng(21)
     d.fluid[:, 0:2] += rng.uniform(-0.2, 0.2, size=(d.fluid.shape[0], 2)) * 0.02
     solid = d.fluid[-40:].copy()

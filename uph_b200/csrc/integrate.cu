@@ -68,6 +68,11 @@ __global__ void k_correct(const DevParams P, const SlotArrays S, int first_step,
     u = umin + dt * ax;
     v = vmin + dt * ay;
   }
+  if (P.profile == UPH_PROFILE_WCSPH) {
+    // the WCSPH pressure is the algebraic Tait law of the new density
+    p = P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
+    S.pressure[a] = p;
+  }
   S.rho[a] = rho;
   S.p[a] = p;
   S.u[a] = u;

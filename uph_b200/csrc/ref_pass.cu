@@ -44,16 +44,16 @@
 // interacting, max(orig a, orig b) < ParticleBoundary (Search.cc:33 with
 // derivatives.c:1082-1084), DBL_EPSILON < r^2 < (h h) 4 where r^2 is
 // dx*dx + dy*dy rounded exactly like the reference (no fused multiply-add).
-#include <float.h>
-
-#include "uph_internal.cuh"
+//
+// Execution: one thread per fluid slot.  Each thread first walks its 3 x 3
+// cells with only the exact distance test and lists the in-radius partners in
+// shared memory (kNbChunk at a time); then the warp runs the heavy FP64 pair
+// arithmetic over those lists.  The lists have nearly equal lengths, so the
+// lanes of a warp stay converged in the expensive loop instead of idling while
+// their neighbours reject out-of-radius candidates.
+#include "pass_common.cuh"
 
 namespace uph {
-
-__device__ __forceinline__ double exact_r2(double dx, double dy)
-{
-  return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-}
 
 struct RefAcc {
   double drho, dp, ax, ay;
@@ -61,12 +61,12 @@ struct RefAcc {
   double frho, fp, fu, fv;
 };
 
-__device__ __forceinline__ void wall_pair_force(const DevParams &P, bool isI, int ita, int itb, double r, double dxa,
-                                                double dya, double dua, double dva, double ma, double &fx,
-                                                double &fy, double &fx_spring, double &fy_spring)
+// wall forces of a listed pair whose i side is this fluid particle
+__device__ __forceinline__ void wall_pair_force(const DevParams &P, int itb, double r2, double dxa, double dya,
+                                                double dua, double dva, double ma, RefAcc &A)
 {
-  fx = fy = fx_spring = fy_spring = 0.0;
-  if (!isI || ita != 1) return;
+  const double r = sqrt(r2);
+  double sx = 0.0, sy = 0.0;
   // SpringBoundaryForces / PredictingSpringBoundaryForces (derivatives.c:2396-2449, 1392-1446)
   if (itb == 2 || itb == 3 || itb == 5) {
     const double r0 = 3.0 * P.dx;
@@ -74,11 +74,16 @@ __device__ __forceinline__ void wall_pair_force(const DevParams &P, bool isI, in
       const double rv = dxa * dua + dya * dva;
       const double c1 = P.k_spring * (r0 - r) / (r * ma);
       const double c2 = P.c_damp * rv / (r * r * ma);
-      fx_spring = -c1 * dxa - c2 * dxa;
-      fy_spring = -c1 * dya - c2 * dya;
+      sx = -c1 * dxa - c2 * dxa;
+      sy = -c1 * dya - c2 * dya;
     }
   }
-  if (P.boundary_force == 4 && (itb == 2 || itb == 3) && r < P.dx) {
+  A.ax_a += sx;
+  A.ay_a += sy;
+  if (P.boundary_force == 3) {
+    A.ax += sx;
+    A.ay += sy;
+  } else if (P.boundary_force == 4 && (itb == 2 || itb == 3) && r < P.dx) {
     // ImprovedMonaghan, derivatives.c:1955-2012
     const double hh = P.h;
     const double norm = 7.0 / (64.0 * 3.142 * hh * hh);
@@ -91,12 +96,12 @@ __device__ __forceinline__ void wall_pair_force(const DevParams &P, bool isI, in
     const double rd = r - P.dx / 5.0;
     const double vmax = P.mach_c * P.mach_c / 5.0;
     const double c = vmax * phi / (rd * r);
-    fx = c * dxa;
-    fy = c * dya;
+    A.ax += c * dxa;
+    A.ay += c * dya;
   } else if (P.boundary_force == 5 && itb == 2 && r < P.dx) {
     // SerialSpringBoundaryForces, derivatives.c:2452-2479
-    fx = -(P.k_spring * dxa + P.c_damp * dua) / ma;
-    fy = -(P.k_spring * dya + P.c_damp * dva) / ma;
+    A.ax -= (P.k_spring * dxa + P.c_damp * dua) / ma;
+    A.ay -= (P.k_spring * dya + P.c_damp * dva) / ma;
   }
 }
 
@@ -131,134 +136,139 @@ __device__ __forceinline__ void brute_wall_force(const DevParams &P, double r2, 
   }
 }
 
-__global__ void __launch_bounds__(128) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                  PassStats st)
+__global__ void __launch_bounds__(kPassThreads) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                           PassStats st)
 {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ unsigned s_nb[kNbChunk][kPassThreads];
+  const int tid = threadIdx.x;
+  const int a = blockIdx.x * blockDim.x + tid;
   const bool active = a < P.nf;
-  unsigned long long my_pairs = 0;
+  unsigned my_pairs = 0;
   int my_nb = 0;
-  if (active) {
-    const double xa = S.x[a], ya = S.y[a];
-    const double ua = S.u[a], va = S.v[a], uta = S.ut[a], vta = S.vt[a];
-    const double rhoa = S.rho[a], rhota = S.rhot[a], pa = S.p[a], ma = S.m[a];
-    const double ira = S.inv_rho[a], irta = S.inv_rhot[a];
-    const int oa = S.orig[a], ita = S.itype[a];
-    const double Pa = P.rho0c2 + P.gamma * pa;
-    const double ira2 = ira * ira;
-    const bool brute_walls = (P.boundary_force == 1) || (P.boundary_force != 3 && P.boundary_force != 4 &&
-                                                         P.boundary_force != 5);
-    RefAcc A = {};
-    double bx = 0.0, by = 0.0;  // mode-1 / default wall force (dvdt only)
-    const int c = G.cell_of[a];
-    const int cx = c % P.ncx, cy = c / P.ncx;
-    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++) {
-      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
-        const int cc = yy * P.ncx + xx;
-        const int k1 = G.start[cc + 1];
-        for (int k = G.start[cc]; k < k1; k++) {
-          const int b = G.list[k];
-          if (b == a) continue;
-          const double dxa = xa - S.x[b], dya = ya - S.y[b];
-          const double r2 = exact_r2(dxa, dya);
-          if (!(r2 < P.r2cut)) continue;
-          const int ob = S.orig[b];
-          if (brute_walls && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
-          if (r2 <= DBL_EPSILON) continue;
-          my_nb++;
-          const bool isI = ob > oa;
-          if (max(oa, ob) >= P.pb) continue;
-          if (isI) my_pairs++;
+  const int as = active ? a : 0;
+  const double xa = S.x[as], ya = S.y[as];
+  const double ua = S.u[as], va = S.v[as], uta = S.ut[as], vta = S.vt[as];
+  const double rhoa = S.rho[as], rhota = S.rhot[as], pa = S.p[as], ma = S.m[as];
+  const double ira = S.inv_rho[as], irta = S.inv_rhot[as];
+  const int oa = S.orig[as], ita = S.itype[as];
+  const double Pa = P.rho0c2 + P.gamma * pa;
+  const double ira2 = ira * ira;
+  const double gk = P.gamma * P.kappa;
+  const bool brute_walls = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
+  RefAcc A = {};
+  double bx = 0.0, by = 0.0;  // mode-1 / default wall force (dvdt only)
 
-          const double ub = S.u[b], vb = S.v[b], utb = S.ut[b], vtb = S.vt[b];
-          const double rhob = S.rho[b], rhotb = S.rhot[b], pb = S.p[b], ptb = S.pt[b], mb = S.m[b];
-          const double irb = S.inv_rho[b], irtb = S.inv_rhot[b];
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[as]);
+  bool more = active;
+  while (__any_sync(0xffffffffu, more)) {
+    // phase 1: list up to kNbChunk partners (distance test and pair filter only)
+    int cnt = 0;
+    int pos;
+    while (more && cnt < kNbChunk) {
+      if (!cur.next(pos)) {
+        more = false;
+        break;
+      }
+      const int b = G.list[pos];
+      if (b == a) continue;
+      const double dxa = xa - S.x[b], dya = ya - S.y[b];
+      const double r2 = exact_r2(dxa, dya);
+      if (!(r2 < P.r2cut)) continue;
+      const int ob = S.orig[b];
+      if (brute_walls && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
+      if (r2 <= DBL_EPSILON) continue;
+      my_nb++;
+      if (max(oa, ob) >= P.pb) continue;
+      const bool isI = ob > oa;
+      my_pairs += isI;
+      s_nb[cnt++][tid] = (unsigned)b | (isI ? kRoleI : 0u);
+    }
+    __syncwarp();
+    // phase 2: the pair terms
+    for (int e = 0; e < cnt; e++) {
+      const unsigned ent = s_nb[e][tid];
+      const int b = (int)(ent & ~kRoleI);
+      const bool isI = (ent & kRoleI) != 0;
+      const double dxa = xa - S.x[b], dya = ya - S.y[b];
+      const double r2 = exact_r2(dxa, dya);
+      const double ub = S.u[b], vb = S.v[b], utb = S.ut[b], vtb = S.vt[b];
+      const double rhob = S.rho[b], rhotb = S.rhot[b], pb = S.p[b], ptb = S.pt[b], mb = S.m[b];
+      const double irb = S.inv_rho[b], irtb = S.inv_rhot[b];
 
-          // PolyOrderSeven convolution W and deconvolution dW/dr factor
-          const double r = sqrt(r2);
-          const double q = r * P.inv_h;
-          const double q2 = q * q;
-          const double t = 1.0 - 0.25 * q2;
-          const double t2 = t * t, t4 = t2 * t2;
-          const double t7 = t4 * t2 * t, t8 = t4 * t4;
-          const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
-          const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
-          const double W = P.w_alpha * t8 * pp;
-          const double F = P.dw_alpha * t7 * pp7 * P.inv_h2;
-          const double gx = F * dxa, gy = F * dya;
+      // poly-7 convolution W and deconvolution gradient factor: functions of q^2 only
+      const double q2 = r2 * P.inv_h2;
+      const double t = fma(-0.25, q2, 1.0);
+      const double t2 = t * t, t4 = t2 * t2;
+      const double t7 = t4 * t2 * t, t8 = t4 * t4;
+      const double pp = fma(fma(fma(fma(fma(fma(305.0, q2, -628.0), q2, 1184.0), q2, -1984.0), q2, 2816.0), q2, -3072.0), q2, 2048.0);
+      const double pp7 = fma(fma(fma(fma(fma(fma(305.0, q2, -1106.0), q2, 1912.0), q2, -2912.0), q2, 3712.0), q2, -3584.0), q2, 2048.0);
+      const double W = P.w_alpha * t8 * pp;
+      const double F = P.dw_alpha * P.inv_h2 * t7 * pp7;
+      const double gx = F * dxa, gy = F * dya;
 
-          const double Pb = P.rho0c2 + P.gamma * pb;
-          const double Vb = mb * irb;
-          const double ms = isI ? mb : ma;
-          const double rhosum = ira + irb;
-          const double inv_r2e = 1.0 / (r2 + P.eta2);
-          const double nu = (dxa * gx + dya * gy) * inv_r2e;
-          const double ep = 4.0 * Pa / (Pa + Pb);
-          const double gk = P.gamma * P.kappa;
+      const double Pb = fma(P.gamma, pb, P.rho0c2);
+      const double Vb = mb * irb;
+      const double ms = isI ? mb : ma;
+      const double rhosum = ira + irb;
+      const double inv_r2e = rcp_nr(r2 + P.eta2);
+      const double nu = (dxa * gx + dya * gy) * inv_r2e;
+      const double ep = 4.0 * Pa * rcp_nr(Pa + Pb);
 
-          // predictor density
-          const double pdx = isI ? (ua - utb) : (uta - ub);
-          const double pdy = isI ? (va - vtb) : (vta - vb);
-          A.drho_a += ms * (pdx * gx + pdy * gy);
-          // predictor pressure
-          const double dux = ua - ub, duy = va - vb;
-          const double vdw = dux * gx + duy * gy;
-          const double msb = ms * irb;
-          A.dp_a += (mb * ira) * Pa * vdw + gk * msb * (pa - pb) * nu * ep - P.kappa * Pa * msb * (rhoa - rhob) * rhosum * nu;
-          // predictor pressure gradient
-          const double pij_p = pa * ira2 + pb * irb * irb;
-          A.ax_a -= mb * pij_p * gx;
-          A.ay_a -= mb * pij_p * gy;
-          // fluctuations
-          A.frho -= Vb * (rhoa - rhob) * W;
-          A.fp -= Vb * (pa - pb) * W;
-          const double cfv = isI ? (ma * irtb - mb * irta) * W : 0.0;
-          A.fu += dux * cfv;
-          A.fv += duy * cfv;
-          // continuity
-          const double vdwt = (ua - utb) * gx + (va - vtb) * gy;
-          const double Vr = Vb * rhotb;
-          A.drho += Vr * vdwt;
-          // rate-form Tait with diffusion
-          A.dp += Vr * ira * Pa * vdwt + gk * Vb * (pa - ptb) * nu * ep - P.kappa * Pa * Vb * (rhoa - rhotb) * rhosum * nu;
-          // pressure gradient
-          const double pij = pa * rhotb * ira2 * irb + pb * rhota * irb * irb * ira;
-          A.ax -= mb * pij * gx;
-          A.ay -= mb * pij * gy;
-          // deviatoric viscous stress
-          if (P.stress_type == 1) {
-            const double meff = 2.0 * P.mu0 / rhosum;
-            const double s00 = (-dxa) * dux - (-dya) * duy;
-            const double s01 = (-dxa) * duy + (-dya) * dux;
-            const double sgx = s00 * gx + s01 * gy;
-            const double sgy = s01 * gx - s00 * gy;
-            const double base = mb * meff * inv_r2e;
-            const double D = rhotb * ira2 * irb - rhota * irb * irb * ira;
-            const double sD = (isI ? base : -base) * D;
-            A.ax += sD * sgx;
-            A.ay += sD * sgy;
-            const double Dp = base * (ira2 + irb * irb);
-            A.ax_a += Dp * sgx;
-            A.ay_a += Dp * sgy;
-          }
-          // wall forces
-          if (isI && ita == 1) {
-            const int itb = S.itype[b];
-            double fx, fy, sx, sy;
-            wall_pair_force(P, isI, ita, itb, r, dxa, dya, dux, duy, ma, fx, fy, sx, sy);
-            A.ax_a += sx;
-            A.ay_a += sy;
-            if (P.boundary_force == 3) {
-              A.ax += sx;
-              A.ay += sy;
-            } else {
-              A.ax += fx;
-              A.ay += fy;
-            }
-          }
-        }
+      // predictor density
+      const double pdx = isI ? (ua - utb) : (uta - ub);
+      const double pdy = isI ? (va - vtb) : (vta - vb);
+      A.drho_a += ms * (pdx * gx + pdy * gy);
+      // predictor pressure
+      const double dux = ua - ub, duy = va - vb;
+      const double vdw = dux * gx + duy * gy;
+      const double msb = ms * irb;
+      A.dp_a += (mb * ira) * Pa * vdw + gk * msb * (pa - pb) * nu * ep - P.kappa * Pa * msb * (rhoa - rhob) * rhosum * nu;
+      // predictor pressure gradient
+      const double pij_p = pa * ira2 + pb * irb * irb;
+      A.ax_a -= mb * pij_p * gx;
+      A.ay_a -= mb * pij_p * gy;
+      // fluctuations
+      A.frho -= Vb * (rhoa - rhob) * W;
+      A.fp -= Vb * (pa - pb) * W;
+      const double cfv = isI ? (ma * irtb - mb * irta) * W : 0.0;
+      A.fu += dux * cfv;
+      A.fv += duy * cfv;
+      // continuity
+      const double vdwt = (ua - utb) * gx + (va - vtb) * gy;
+      const double Vr = Vb * rhotb;
+      A.drho += Vr * vdwt;
+      // rate-form Tait with diffusion
+      A.dp += Vr * ira * Pa * vdwt + gk * Vb * (pa - ptb) * nu * ep - P.kappa * Pa * Vb * (rhoa - rhotb) * rhosum * nu;
+      // pressure gradient
+      const double pij = pa * rhotb * ira2 * irb + pb * rhota * irb * irb * ira;
+      A.ax -= mb * pij * gx;
+      A.ay -= mb * pij * gy;
+      // deviatoric viscous stress
+      if (P.stress_type == 1) {
+        const double meff = 2.0 * P.mu0 * rcp_nr(rhosum);
+        const double s00 = (-dxa) * dux - (-dya) * duy;
+        const double s01 = (-dxa) * duy + (-dya) * dux;
+        const double sgx = s00 * gx + s01 * gy;
+        const double sgy = s01 * gx - s00 * gy;
+        const double base = mb * meff * inv_r2e;
+        const double D = rhotb * ira2 * irb - rhota * irb * irb * ira;
+        const double sD = (isI ? base : -base) * D;
+        A.ax += sD * sgx;
+        A.ay += sD * sgy;
+        const double Dp = base * (ira2 + irb * irb);
+        A.ax_a += Dp * sgx;
+        A.ay_a += Dp * sgy;
+      }
+      // wall forces: only pairs whose i is this fluid particle
+      if (isI && ita == 1) {
+        const int itb = S.itype[b];
+        if (itb >= 2) wall_pair_force(P, itb, r2, dxa, dya, dux, duy, ma, A);
       }
     }
+    __syncwarp();
+  }
+  if (active) {
     A.ax += bx;
     A.ay += by;
     if (P.gravity_flag == 1) {
@@ -281,10 +291,10 @@ __global__ void __launch_bounds__(128) k_ref_pass(const DevParams P, const SlotA
     S.pressure[a] = P.B * (pow(rhoa / P.rho0, P.gamma) - 1.0);
   }
   // pass statistics: one atomic per warp
-  const unsigned long long wp = __reduce_add_sync(0xffffffffu, (unsigned)my_pairs);
+  const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
   const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
   if ((threadIdx.x & 31) == 0) {
-    if (wp) atomicAdd(st.niac, wp);
+    if (wp) atomicAdd(st.niac, (unsigned long long)wp);
     if (wn) atomicMax(st.max_nb, wn);
   }
 }
@@ -292,7 +302,7 @@ __global__ void __launch_bounds__(128) k_ref_pass(const DevParams P, const SlotA
 void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
   if (P.nf <= 0) return;
-  k_ref_pass<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G, st);
+  k_ref_pass<<<(P.nf + kPassThreads - 1) / kPassThreads, kPassThreads, 0, s>>>(P, S, G, st);
 }
 
 }  // namespace uph

@@ -25,6 +25,7 @@ int scan_block_sums_needed(int n);
 namespace {
 
 constexpr int kReorderInterval = 16;
+constexpr int kErrorCheckInterval = 64;
 
 enum KernelFamily { KF_PREDICT, KF_WALLS, KF_REFRESH, KF_CELLS, KF_PASS, KF_CORRECT, KF_REORDER, KF_COUNT };
 const char *kFamilyNames[KF_COUNT] = {"predict", "wall_motion", "refresh", "cell_list", "rate_pass", "correct",
@@ -635,6 +636,12 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
     }
     if (++s->steps_since_reorder >= kReorderInterval) {
       r = reorder_fluid(s);
+      if (r != UPH_OK) return r;
+    }
+    // a particle that left the grid is clamped into a border cell, which can
+    // make that cell arbitrarily crowded: stop early rather than run on
+    if ((k + 1) % kErrorCheckInterval == 0 && k + 1 < nsteps) {
+      r = check_error_word(s);
       if (r != UPH_OK) return r;
     }
   }

@@ -209,10 +209,17 @@ def base_params(dx: float, local_depth: float = 2.0, dt: Optional[float] = None,
         pressure_probe_y=0.0, stress_type=1, dissipation_control_volume=1,
     )
     p.update(over)
+    d = derive_params(p, eta)
     if dt is None:
-        d = derive_params(p, eta)
         dt = 0.2 * d["h"] / d["speed_of_sound"]
     p["time_step"] = dt
+    if "thermal_diffusivity0" not in over:
+        # The REF profile's pressure / density diffusion (derivatives.c:1569-1672)
+        # is explicit with coefficient gamma * kappa; the reference deck's
+        # kappa = 0.015 m^2/s belongs to dx = 0.01 m, dt = 1e-5 s.  At the
+        # workloads' finer spacings it would break the explicit diffusion
+        # limit, so kappa keeps the diffusion number gamma kappa dt / h^2 at 0.02.
+        p["thermal_diffusivity0"] = 0.02 * d["h"] ** 2 / (p["adiabatic_constant"] * dt)
     return p
 
 
