@@ -12,33 +12,40 @@
 
 namespace uph {
 
+// storage_order = false: row-major cell ids for the cell list;
+// storage_order = true: tile-major keys for sorting the particle storage.
 __global__ void k_cell_keys(DevParams P, const double *__restrict__ x, const double *__restrict__ y, int first,
-                            int count, int *__restrict__ cell_of, int *__restrict__ cnt, unsigned *err)
+                            int count, int *__restrict__ cell_of, int *__restrict__ cnt, unsigned *err,
+                            bool storage_order)
 {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
   const int s = first + k;
-  const double fx = (x[s] - P.lo_x) * P.inv_cell;
-  const double fy = (y[s] - P.lo_y) * P.inv_cell;
-  int cx = (int)floor(fx), cy = (int)floor(fy);
-  // NaN positions fail both comparisons below and are treated as outside
-  if (!(fx >= 0.0 && fy >= 0.0 && cx < P.ncx && cy < P.ncy)) {
+  const double px = x[s], py = y[s];
+  const double fx = (px - P.lo_x) * P.inv_cell;
+  const double fy = (py - P.lo_y) * P.inv_cell;
+  // the declared domain [lo, hi]; NaN positions fail the comparisons too
+  const bool inside = px >= P.lo_x && py >= P.lo_y && px <= P.hi_x && py <= P.hi_y;
+  int cx = 0, cy = 0;
+  if (inside) {
+    cx = min((int)floor(fx), P.ncx - 1);
+    cy = min((int)floor(fy), P.ncy - 1);
+  } else {
     atomicOr(err, ERR_OUT_OF_DOMAIN);
-    cx = (fx >= 0.0) ? min(cx, P.ncx - 1) : 0;
-    cy = (fy >= 0.0) ? min(cy, P.ncy - 1) : 0;
-    if (cx < 0) cx = 0;
-    if (cy < 0) cy = 0;
+    // clamp into the grid so the cell list stays well formed
+    if (fx > 0.0) cx = (int)fmin(fx, (double)(P.ncx - 1));
+    if (fy > 0.0) cy = (int)fmin(fy, (double)(P.ncy - 1));
   }
-  const int c = cy * P.ncx + cx;
+  const int c = storage_order ? storage_key(cx, cy, P.ntx) : cy * P.ncx + cx;
   cell_of[s] = c;
   atomicAdd(&cnt[c], 1);
 }
 
 void launch_cell_keys(const DevParams &P, const double *x, const double *y, int first, int count, CellGrid &G,
-                      unsigned *err, cudaStream_t s)
+                      unsigned *err, bool storage_order, cudaStream_t s)
 {
   if (count <= 0) return;
-  k_cell_keys<<<(count + 255) / 256, 256, 0, s>>>(P, x, y, first, count, G.cell_of, G.count, err);
+  k_cell_keys<<<(count + 255) / 256, 256, 0, s>>>(P, x, y, first, count, G.cell_of, G.count, err, storage_order);
 }
 
 // ---- exclusive scan ----------------------------------------------------------

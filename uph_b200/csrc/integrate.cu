@@ -2,25 +2,35 @@
 // with the reference's operation order so the state matches it bit for bit
 // whenever the rates do.  Also the wall motion of inputbp.c:194-207 and the
 // per-particle quantities the rate pass reads.
+//
+// Inside a multi-step call the corrector of step n and the predictor of step
+// n + 1 run in one kernel (they touch the same per-particle state and the
+// predictor needs nothing the corrector does not already hold); the first
+// step of a call uses the stand-alone predictor.
 #include "uph_internal.cuh"
 
 namespace uph {
 
-// sph.cc:93-125 (itime != 1): *_min <- current, local* <- current, then the
-// half kick with the predictor rates and the fluctuations of the previous
-// rate evaluation.
-__global__ void k_predict(const DevParams P, const SlotArrays S)
+// WCSPH pressure is the algebraic Tait law of the density (derivatives.c:1674-1682)
+__device__ __forceinline__ double tait(const DevParams &P, double rho)
 {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= P.nf) return;
+  return P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
+}
+
+// sph.cc:93-125 (itime != 1) for one particle whose post-step state is
+// (rho, p, u, v): *_min <- current, local* <- current, then the half kick
+// with the predictor rates and the fluctuations of the last rate
+// evaluation.  Also refreshes 1/rho and 1/rhot for the next rate pass.
+__device__ __forceinline__ void predict_one(const DevParams &P, const SlotArrays &S, int a, double rho, double p,
+                                            double u, double v)
+{
   const double dt = P.dt;
-  const double rho = S.rho[a], p = S.p[a], u = S.u[a], v = S.v[a];
   const double drho_a = S.drho_a[a], dp_a = S.dp_a[a];
   S.rho_min[a] = rho;
   S.p_min[a] = p;
-  S.rho[a] = rho + 0.5 * dt * drho_a;
-  S.rhot[a] = rho + 0.5 * dt * drho_a + S.frho[a];
-  S.p[a] = p + 0.5 * dt * dp_a;
+  const double rn = rho + 0.5 * dt * drho_a;
+  const double rt = rho + 0.5 * dt * drho_a + S.frho[a];
+  double pn = p + 0.5 * dt * dp_a;
   S.pt[a] = p + 0.5 * dt * dp_a + S.fp[a];
   S.u_min[a] = u;
   S.v_min[a] = v;
@@ -30,6 +40,22 @@ __global__ void k_predict(const DevParams P, const SlotArrays S)
   S.v[a] = vn;
   S.ut[a] = un + 0.5 * dt * ax_a + P.eps * S.fu[a];
   S.vt[a] = vn + 0.5 * dt * ay_a + P.eps * S.fv[a];
+  if (P.profile == UPH_PROFILE_WCSPH) {
+    pn = tait(P, rn);
+    S.pressure[a] = pn;
+  }
+  S.rho[a] = rn;
+  S.rhot[a] = rt;
+  S.p[a] = pn;
+  S.inv_rho[a] = 1.0 / rn;
+  S.inv_rhot[a] = 1.0 / rt;
+}
+
+__global__ void k_predict(const DevParams P, const SlotArrays S)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  predict_one(P, S, a, S.rho[a], S.p[a], S.u[a], S.v[a]);
 }
 
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s)
@@ -38,60 +64,68 @@ void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s)
 }
 
 // sph.cc:137-168: the corrector with the rates just evaluated, then the
-// drift x += dt v.  Flags non-finite results.
-__global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, unsigned *err)
+// drift x += dt v.  With predict_next the predictor of the following step
+// runs right after.  Flags non-finite results.
+__global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, int predict_next, unsigned *err)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.nf) return;
   const double dt = P.dt;
   const double drho = S.drho[a], dp = S.dp[a], ax = S.ax[a], ay = S.ay[a];
   const double frho = S.frho[a], fp = S.fp[a], fu = P.eps * S.fu[a], fv = P.eps * S.fv[a];
-  double rho, p, u, v;
+  double rho, p, u, v, rt, pt, ut, vt;
   if (first_step) {
     const double rho0 = S.rho[a], p0 = S.p[a], u0 = S.u[a], v0 = S.v[a];
-    S.rhot[a] = rho0 + 0.5 * dt * drho + frho;
+    rt = rho0 + 0.5 * dt * drho + frho;
     rho = rho0 + 0.5 * dt * drho;
-    S.pt[a] = p0 + 0.5 * dt * dp + fp;
+    pt = p0 + 0.5 * dt * dp + fp;
     p = p0 + 0.5 * dt * dp;
-    S.ut[a] = u0 + 0.5 * dt * ax + fu;
-    S.vt[a] = v0 + 0.5 * dt * ay + fv;
+    ut = u0 + 0.5 * dt * ax + fu;
+    vt = v0 + 0.5 * dt * ay + fv;
     u = u0 + 0.5 * dt * ax;
     v = v0 + 0.5 * dt * ay;
   } else {
     const double rmin = S.rho_min[a], pmin = S.p_min[a], umin = S.u_min[a], vmin = S.v_min[a];
-    S.rhot[a] = rmin + dt * drho + frho;
+    rt = rmin + dt * drho + frho;
     rho = rmin + dt * drho;
-    S.pt[a] = pmin + dt * dp + fp;
+    pt = pmin + dt * dp + fp;
     p = pmin + dt * dp;
-    S.ut[a] = umin + dt * ax + fu;
-    S.vt[a] = vmin + dt * ay + fv;
+    ut = umin + dt * ax + fu;
+    vt = vmin + dt * ay + fv;
     u = umin + dt * ax;
     v = vmin + dt * ay;
   }
   if (P.profile == UPH_PROFILE_WCSPH) {
-    // the WCSPH pressure is the algebraic Tait law of the new density
-    p = P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
+    p = tait(P, rho);
     S.pressure[a] = p;
   }
-  S.rho[a] = rho;
-  S.p[a] = p;
-  S.u[a] = u;
-  S.v[a] = v;
   const double x = S.x[a] + dt * u, y = S.y[a] + dt * v;
   S.x[a] = x;
   S.y[a] = y;
   if (!isfinite(rho) || !isfinite(p) || !isfinite(x) || !isfinite(y) || !isfinite(u) || !isfinite(v))
     atomicOr(err, ERR_NAN);
+  if (predict_next) {
+    predict_one(P, S, a, rho, p, u, v);
+  } else {
+    S.rho[a] = rho;
+    S.p[a] = p;
+    S.u[a] = u;
+    S.v[a] = v;
+    S.rhot[a] = rt;
+    S.pt[a] = pt;
+    S.ut[a] = ut;
+    S.vt[a] = vt;
+  }
 }
 
-void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, unsigned *err, cudaStream_t s)
+void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
+                    cudaStream_t s)
 {
-  if (P.nf > 0) k_correct<<<(P.nf + 255) / 256, 256, 0, s>>>(P, S, first_step, err);
+  if (P.nf > 0) k_correct<<<(P.nf + 255) / 256, 256, 0, s>>>(P, S, first_step, predict_next, err);
 }
 
-// 1/rho and 1/rhot for the rate pass; for WCSPH also p = B((rho/rho0)^g - 1)
-// (derivatives.c:1674-1682) since that profile's pressure is a function of
-// the density.
+// 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure.
+// Needed where no predictor ran: a fresh upload and the first step.
 __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int count)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,7 +135,7 @@ __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int 
   S.inv_rho[a] = 1.0 / rho;
   S.inv_rhot[a] = 1.0 / S.rhot[a];
   if (P.profile == UPH_PROFILE_WCSPH) {
-    const double pr = P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
+    const double pr = tait(P, rho);
     S.p[a] = pr;
     S.pressure[a] = pr;
   }

@@ -33,8 +33,10 @@ __device__ __forceinline__ double rcp_nr(double x)
   return fma(y, e, y);
 }
 
-// Walks the 3 x 3 cells around a particle in a fixed order: rows bottom to
-// top, cells left to right, each cell's slots in ascending order.
+// Walks the (2 reach + 1)^2 cells around a particle in a fixed order: rows
+// bottom to top, cells left to right, each cell's slots in ascending order.
+// The cells of one row are consecutive in the cell list, so a row is a single
+// range of list positions.
 struct NeighbourCursor {
   int cx0, cx1, cy, cy1, ncx, k, kend;
   const int *start;
@@ -42,27 +44,90 @@ struct NeighbourCursor {
   __device__ __forceinline__ void init(const DevParams &P, const CellGrid &G, int cell)
   {
     const int cx = cell % P.ncx, cyy = cell / P.ncx;
-    cx0 = max(cx - 1, 0);
-    cx1 = min(cx + 1, P.ncx - 1);
-    cy = max(cyy - 1, 0);
-    cy1 = min(cyy + 1, P.ncy - 1);
+    cx0 = max(cx - P.reach, 0);
+    cx1 = min(cx + P.reach, P.ncx - 1);
+    cy = max(cyy - P.reach, 0);
+    cy1 = min(cyy + P.reach, P.ncy - 1);
     ncx = P.ncx;
     start = G.start;
-    // one row of adjacent cells is one contiguous range of the cell list
     k = start[cy * ncx + cx0];
     kend = start[cy * ncx + cx1 + 1];
   }
-  // advances to the next candidate list position; false when exhausted
-  __device__ __forceinline__ bool next(int &pos)
+  // moves to the next non-empty row range; false when the stencil is exhausted
+  __device__ __forceinline__ bool advance()
   {
     while (k >= kend) {
       if (++cy > cy1) return false;
       k = start[cy * ncx + cx0];
       kend = start[cy * ncx + cx1 + 1];
     }
+    return true;
+  }
+  // advances to the next candidate list position; false when exhausted
+  __device__ __forceinline__ bool next(int &pos)
+  {
+    if (!advance()) return false;
     pos = k++;
     return true;
   }
+  // up to kBatch candidates of the current range; returns how many, 0 when exhausted
+  template <int kBatch>
+  __device__ __forceinline__ int next_batch(int &pos)
+  {
+    if (!advance()) return 0;
+    pos = k;
+    const int n = min(kBatch, kend - k);
+    k += n;
+    return n;
+  }
 };
+
+// Lists the in-radius partners of particle `a` (position xa, ya, reference
+// index oa) that form a pair of the reference's list, kNbChunk at a time,
+// into column `tid` of `s_nb`.  `on_candidate(b, ob, r2, dx, dy)` sees every
+// candidate inside the radius first (for the brute-force wall modes).
+// Candidates are tested four at a time so their loads overlap.
+template <typename OnCandidate>
+__device__ __forceinline__ int list_partners(const DevParams &P, const SlotArrays &S, const CellGrid &G,
+                                             NeighbourCursor &cur, bool &more, int a, int oa, double xa, double ya,
+                                             unsigned (*s_nb)[kPassThreads], int tid, unsigned &my_pairs,
+                                             int &my_nb, OnCandidate on_candidate)
+{
+  constexpr int kB = 4;
+  int cnt = 0;
+  while (more && cnt <= kNbChunk - kB) {
+    int pos;
+    const int n = cur.next_batch<kB>(pos);
+    if (n == 0) {
+      more = false;
+      break;
+    }
+    int b[kB];
+    double bx[kB], by[kB];
+#pragma unroll
+    for (int u = 0; u < kB; u++) b[u] = (u < n) ? G.list[pos + u] : a;
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      bx[u] = S.x[b[u]];
+      by[u] = S.y[b[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      if (b[u] == a) continue;
+      const double dxa = xa - bx[u], dya = ya - by[u];
+      const double r2 = exact_r2(dxa, dya);
+      if (!(r2 < P.r2cut)) continue;
+      const int ob = S.orig[b[u]];
+      on_candidate(b[u], ob, r2, dxa, dya);
+      if (r2 <= DBL_EPSILON) continue;
+      my_nb++;
+      if (max(oa, ob) >= P.pb) continue;
+      const bool isI = ob > oa;
+      my_pairs += isI;
+      s_nb[cnt++][tid] = (unsigned)b[u] | (isI ? kRoleI : 0u);
+    }
+  }
+  return cnt;
+}
 
 }  // namespace uph

@@ -45,9 +45,9 @@
 // derivatives.c:1082-1084), DBL_EPSILON < r^2 < (h h) 4 where r^2 is
 // dx*dx + dy*dy rounded exactly like the reference (no fused multiply-add).
 //
-// Execution: one thread per fluid slot.  Each thread first walks its 3 x 3
-// cells with only the exact distance test and lists the in-radius partners in
-// shared memory (kNbChunk at a time); then the warp runs the heavy FP64 pair
+// Execution: one thread per fluid slot.  Each thread first walks its 5 x 5
+// block of half-radius cells with only the exact distance test and lists the
+// in-radius partners in shared memory (kNbChunk at a time); then the warp runs the heavy FP64 pair
 // arithmetic over those lists.  The lists have nearly equal lengths, so the
 // lanes of a warp stay converged in the expensive loop instead of idling while
 // their neighbours reject out-of-radius candidates.
@@ -136,7 +136,7 @@ __device__ __forceinline__ void brute_wall_force(const DevParams &P, double r2, 
   }
 }
 
-__global__ void __launch_bounds__(kPassThreads) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+__global__ void __launch_bounds__(kPassThreads, 4) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
                                                            PassStats st)
 {
   __shared__ unsigned s_nb[kNbChunk][kPassThreads];
@@ -163,27 +163,11 @@ __global__ void __launch_bounds__(kPassThreads) k_ref_pass(const DevParams P, co
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
     // phase 1: list up to kNbChunk partners (distance test and pair filter only)
-    int cnt = 0;
-    int pos;
-    while (more && cnt < kNbChunk) {
-      if (!cur.next(pos)) {
-        more = false;
-        break;
-      }
-      const int b = G.list[pos];
-      if (b == a) continue;
-      const double dxa = xa - S.x[b], dya = ya - S.y[b];
-      const double r2 = exact_r2(dxa, dya);
-      if (!(r2 < P.r2cut)) continue;
-      const int ob = S.orig[b];
-      if (brute_walls && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
-      if (r2 <= DBL_EPSILON) continue;
-      my_nb++;
-      if (max(oa, ob) >= P.pb) continue;
-      const bool isI = ob > oa;
-      my_pairs += isI;
-      s_nb[cnt++][tid] = (unsigned)b | (isI ? kRoleI : 0u);
-    }
+    const int cnt = list_partners(P, S, G, cur, more, a, oa, xa, ya, s_nb, tid, my_pairs, my_nb,
+                                  [&](int b, int ob, double r2, double dxa, double dya) {
+                                    if (brute_walls && ob >= P.b0 && ob < P.b1)
+                                      brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
+                                  });
     __syncwarp();
     // phase 2: the pair terms
     for (int e = 0; e < cnt; e++) {

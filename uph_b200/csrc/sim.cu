@@ -14,7 +14,7 @@
 #include <string>
 #include <vector>
 
-#include "uph_internal.cuh"
+#include "pass_common.cuh"
 
 using namespace uph;
 
@@ -26,6 +26,7 @@ namespace {
 
 constexpr int kReorderInterval = 16;
 constexpr int kErrorCheckInterval = 64;
+constexpr int kCellReach = 2;
 
 enum KernelFamily { KF_PREDICT, KF_WALLS, KF_REFRESH, KF_CELLS, KF_PASS, KF_CORRECT, KF_REORDER, KF_COUNT };
 const char *kFamilyNames[KF_COUNT] = {"predict", "wall_motion", "refresh", "cell_list", "rate_pass", "correct",
@@ -252,15 +253,16 @@ __global__ void k_iota(int *p, int first, int count)
   if (k < count) p[first + k] = first + k;
 }
 
-// fluid-only (or wall-only) counting sort of [first, first+count) by cell,
-// result: G.list[0, count) = ids in cell order, ties by id
-uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count)
+// counting sort of ids [first, first+count) by cell, result: G.list[0, count)
+// = ids in key order, ties by id.  storage_order selects the tile-major
+// storage key instead of the row-major cell-list id.
+uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order)
 {
   CellGrid &G = s->G;
   cudaStream_t st = s->stream;
   UPH_CUDA(cudaMemsetAsync(G.count, 0, sizeof(int) * G.ncell, st));
   UPH_CUDA(cudaMemsetAsync(G.fill, 0, sizeof(int) * G.ncell, st));
-  launch_cell_keys(s->P, x, y, first, count, G, s->d_err, st);
+  launch_cell_keys(s->P, x, y, first, count, G, s->d_err, storage_order, st);
   launch_exclusive_scan(G.count, G.start, G.ncell, G.block_sums, st);
   // scatter ids; list is indexed from 0 because start[] only counted this range
   launch_cell_scatter(G, first, count, st);
@@ -272,14 +274,14 @@ uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, i
 uph_status build_cell_list(uph_sim *s)
 {
   Timer t(s, KF_CELLS);
-  return sort_range(s, s->S.x, s->S.y, 0, s->P.n);
+  return sort_range(s, s->S.x, s->S.y, 0, s->P.n, false);
 }
 
 uph_status reorder_fluid(uph_sim *s)
 {
   Timer t(s, KF_REORDER);
   const int nf = s->P.nf, n = s->P.n;
-  uph_status r = sort_range(s, s->S.x, s->S.y, 0, nf);
+  uph_status r = sort_range(s, s->S.x, s->S.y, 0, nf, true);
   if (r != UPH_OK) return r;
   UPH_CUDA(cudaMemcpyAsync(s->d_perm, s->G.list, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
   if (n > nf) k_iota<<<(n - nf + 255) / 256, 256, 0, s->stream>>>(s->d_perm, nf, n - nf);
@@ -305,11 +307,13 @@ uph_status check_error_word(uph_sim *s)
   return UPH_OK;
 }
 
-uph_status rate_pass(uph_sim *s)
+// refresh: recompute 1/rho, 1/rhot (and the WCSPH pressure) first; a
+// predictor that ran since the last state change has done it already
+uph_status rate_pass(uph_sim *s, bool refresh)
 {
   UPH_CUDA(cudaMemsetAsync(s->d_niac, 0, sizeof(unsigned long long), s->stream));
   UPH_CUDA(cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), s->stream));
-  {
+  if (refresh) {
     Timer t(s, KF_REFRESH);
     launch_refresh_inverse(s->P, s->S, 0, s->P.nf, s->stream);
     s->launches++;
@@ -398,15 +402,24 @@ DevParams make_dev_params(const uph_params *p)
   P.omega = p->omega;
   P.av_alpha_c0 = p->av_alpha * p->speed_of_sound;
   P.dt = p->time_step;
-  const double cell = sqrt(P.r2cut) * (1.0 + 1e-9);
+  // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
+  // against 36 h^2 for a 3 x 3 block of radius-wide cells
+  P.reach = kCellReach;
+  const double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
   P.lo_x = p->domain_lo[0];
   P.lo_y = p->domain_lo[1];
+  P.hi_x = p->domain_hi[0];
+  P.hi_y = p->domain_hi[1];
   P.cell = cell;
   P.inv_cell = 1.0 / cell;
-  P.ncx = (int)ceil((p->domain_hi[0] - p->domain_lo[0]) / cell);
-  P.ncy = (int)ceil((p->domain_hi[1] - p->domain_lo[1]) / cell);
-  if (P.ncx < 1) P.ncx = 1;
-  if (P.ncy < 1) P.ncy = 1;
+  // whole tiles: the cell count per axis is rounded up to a multiple of the tile
+  const double nx = ceil((p->domain_hi[0] - p->domain_lo[0]) / cell);
+  const double ny = ceil((p->domain_hi[1] - p->domain_lo[1]) / cell);
+  const double tiles_x = ceil(fmax(nx, 1.0) / kCellTile), tiles_y = ceil(fmax(ny, 1.0) / kCellTile);
+  // clamp before converting; uph_sim_create rejects grids this large
+  P.ntx = (int)fmin(tiles_x, 1 << 20);
+  P.ncx = P.ntx * kCellTile;
+  P.ncy = (int)fmin(tiles_y, 1 << 20) * kCellTile;
   return P;
 }
 
@@ -556,11 +569,11 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
   // spatial order: fluid and walls sorted by cell separately
   k_split_xy<<<(n + 255) / 256, 256, 0, q>>>(T.pos, T.tmp_x, T.tmp_y, n);
   s->launches++;
-  uph_status r = sort_range(s, T.tmp_x, T.tmp_y, 0, nf);
+  uph_status r = sort_range(s, T.tmp_x, T.tmp_y, 0, nf, true);
   if (r != UPH_OK) return r;
   UPH_CUDA(cudaMemcpyAsync(s->d_perm, s->G.list, sizeof(int) * nf, cudaMemcpyDeviceToDevice, q));
   if (n > nf) {
-    r = sort_range(s, T.tmp_x, T.tmp_y, nf, n - nf);
+    r = sort_range(s, T.tmp_x, T.tmp_y, nf, n - nf, true);
     if (r != UPH_OK) return r;
     UPH_CUDA(cudaMemcpyAsync(s->d_perm + nf, s->G.list, sizeof(int) * (n - nf), cudaMemcpyDeviceToDevice, q));
   }
@@ -617,7 +630,9 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
   for (int k = 0; k < nsteps; k++) {
     const int itime = ++s->itime;
     const double t = itime * s->P.dt;
-    if (itime != 1) {
+    // the predictor of steps after the first of this call ran inside the
+    // previous step's corrector
+    if (itime != 1 && k == 0) {
       Timer tm(s, KF_PREDICT);
       launch_predict(s->P, s->S, s->stream);
       s->launches++;
@@ -627,11 +642,11 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
       launch_wall_motion(s->P, s->S, t, s->stream);
       s->launches++;
     }
-    uph_status r = rate_pass(s);
+    uph_status r = rate_pass(s, itime == 1);
     if (r != UPH_OK) return r;
     {
       Timer tm(s, KF_CORRECT);
-      launch_correct(s->P, s->S, itime == 1, s->d_err, s->stream);
+      launch_correct(s->P, s->S, itime == 1, k + 1 < nsteps, s->d_err, s->stream);
       s->launches++;
     }
     if (++s->steps_since_reorder >= kReorderInterval) {
@@ -658,7 +673,7 @@ extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
     launch_wall_motion(s->P, s->S, t, s->stream);
     s->launches++;
   }
-  uph_status r = rate_pass(s);
+  uph_status r = rate_pass(s, true);
   if (r != UPH_OK) return r;
   UPH_CUDA(cudaGetLastError());
   return check_error_word(s);
@@ -677,19 +692,16 @@ __global__ void k_pair_count(DevParams P, SlotArrays S, CellGrid G, int *__restr
   if (a >= P.nf) return;
   const double xa = S.x[a], ya = S.y[a];
   const int oa = S.orig[a];
-  const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
-  int cnt = 0;
-  for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
-    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
-      const int cc = yy * P.ncx + xx;
-      for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
-        const int b = G.list[k];
-        const int ob = S.orig[b];
-        if (ob <= oa || ob >= P.pb) continue;
-        const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
-        if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
-      }
-    }
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[a]);
+  int cnt = 0, k;
+  while (cur.next(k)) {
+    const int b = G.list[k];
+    const int ob = S.orig[b];
+    if (ob <= oa || ob >= P.pb) continue;
+    const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
+    if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
+  }
   cnt_by_orig[oa] = cnt;
 }
 
@@ -701,45 +713,42 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
   const double xa = S.x[a], ya = S.y[a];
   const int oa = S.orig[a];
   const int base = off[oa];
-  int cnt = 0;
-  const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
-  for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
-    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
-      const int cc = yy * P.ncx + xx;
-      for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
-        const int b = G.list[k];
-        const int ob = S.orig[b];
-        if (ob <= oa || ob >= P.pb) continue;
-        const double dx = xa - S.x[b], dy = ya - S.y[b];
-        const double r2 = pr2(dx, dy);
-        if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
-        const double r = sqrt(r2), q = r * P.inv_h;
-        double W, F;
-        if (P.profile == UPH_PROFILE_REF) {
-          const double q2 = q * q, t = 1.0 - 0.25 * q2, t2 = t * t, t4 = t2 * t2;
-          const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
-          const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
-          W = P.w_alpha * (t4 * t4) * pp;
-          F = P.dw_alpha * (t4 * t2 * t) * pp7 * P.inv_h2;
-        } else if (q < 1.0) {
-          W = P.cs_alpha * (1 - 1.5 * q * q + 0.75 * q * q * q);
-          F = P.cs_alpha * (-3 + 2.25 * q) * P.inv_h2;
-        } else {
-          const double t = 2 - q;
-          W = P.cs_alpha * 0.25 * t * t * t;
-          F = -P.cs_alpha * 0.75 * t * t / (P.h * r);
-        }
-        const int o = base + cnt++;
-        if (ip) ip[o] = oa;
-        if (jp) jp[o] = ob;
-        if (rij2) rij2[o] = r2;
-        if (w) w[o] = W;
-        if (dw) {
-          dw[2 * o] = F * dx;
-          dw[2 * o + 1] = F * dy;
-        }
-      }
+  int cnt = 0, k;
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[a]);
+  while (cur.next(k)) {
+    const int b = G.list[k];
+    const int ob = S.orig[b];
+    if (ob <= oa || ob >= P.pb) continue;
+    const double dx = xa - S.x[b], dy = ya - S.y[b];
+    const double r2 = pr2(dx, dy);
+    if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
+    const double r = sqrt(r2), q = r * P.inv_h;
+    double W, F;
+    if (P.profile == UPH_PROFILE_REF) {
+      const double q2 = q * q, t = 1.0 - 0.25 * q2, t2 = t * t, t4 = t2 * t2;
+      const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
+      const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
+      W = P.w_alpha * (t4 * t4) * pp;
+      F = P.dw_alpha * (t4 * t2 * t) * pp7 * P.inv_h2;
+    } else if (q < 1.0) {
+      W = P.cs_alpha * (1 - 1.5 * q * q + 0.75 * q * q * q);
+      F = P.cs_alpha * (-3 + 2.25 * q) * P.inv_h2;
+    } else {
+      const double t = 2 - q;
+      W = P.cs_alpha * 0.25 * t * t * t;
+      F = -P.cs_alpha * 0.75 * t * t / (P.h * r);
     }
+    const int o = base + cnt++;
+    if (ip) ip[o] = oa;
+    if (jp) jp[o] = ob;
+    if (rij2) rij2[o] = r2;
+    if (w) w[o] = W;
+    if (dw) {
+      dw[2 * o] = F * dx;
+      dw[2 * o + 1] = F * dy;
+    }
+  }
   // order the segment by j (insertion sort; segments are short)
   if (jp) {
     for (int i = base + 1; i < base + cnt; i++) {
@@ -943,16 +952,14 @@ __global__ void k_inradius_max(DevParams P, SlotArrays S, CellGrid G, int *mx)
   int cnt = 0;
   if (a < P.nf) {
     const double xa = S.x[a], ya = S.y[a];
-    const int c = G.cell_of[a], cx = c % P.ncx, cy = c / P.ncx;
-    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, P.ncy - 1); yy++)
-      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, P.ncx - 1); xx++) {
-        const int cc = yy * P.ncx + xx;
-        for (int k = G.start[cc]; k < G.start[cc + 1]; k++) {
-          const int b = G.list[k];
-          const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
-          if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
-        }
-      }
+    NeighbourCursor cur;
+    cur.init(P, G, G.cell_of[a]);
+    int k;
+    while (cur.next(k)) {
+      const int b = G.list[k];
+      const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
+      if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
+    }
   }
   const int w = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
   if ((threadIdx.x & 31) == 0 && w) atomicMax(mx, w);

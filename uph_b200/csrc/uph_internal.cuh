@@ -66,8 +66,25 @@ struct DevParams {
   double dt;
   // cell grid
   double lo_x, lo_y, cell, inv_cell;
-  int ncx, ncy;
+  double hi_x, hi_y;  // declared domain; the grid itself is rounded up to whole tiles
+  int ncx, ncy;  // cells per axis, multiples of kCellTile
+  int ntx;       // tiles per row
+  int reach;     // cells are >= radius / reach wide; partners lie within `reach` cells
 };
+
+// The cell list numbers cells row-major (cy * ncx + cx), so the cells of one
+// stencil row are one contiguous range of the list.  Particle *storage* is
+// sorted by a tile-major key instead: kCellTile x kCellTile cells form a
+// tile, tiles row-major, cells inside a tile row-major.  A block's 128
+// consecutive slots then cover a compact 2-D patch whose neighbours stay in
+// the SM's L1, rather than a long strip of one cell row.
+constexpr int kCellTile = 8;
+
+__host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx)
+{
+  const int tx = cx / kCellTile, lx = cx % kCellTile, ty = cy / kCellTile, ly = cy % kCellTile;
+  return ((ty * ntx + tx) * kCellTile + ly) * kCellTile + lx;
+}
 
 struct CellGrid {
   int ncell;
@@ -93,7 +110,7 @@ uph_status cuda_fail(cudaError_t e, const char *what);
 // ---- launches implemented in the .cu files ---------------------------------
 // cell list
 void launch_cell_keys(const DevParams &P, const double *x, const double *y, int first, int count,
-                      CellGrid &G, unsigned *err, cudaStream_t s);
+                      CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s);
 void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s);
 void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s);
 void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s);
@@ -108,7 +125,8 @@ void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &
 
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);
-void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, unsigned *err, cudaStream_t s);
+void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
+                    cudaStream_t s);
 void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s);
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, double t, cudaStream_t s);
 void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t s);

@@ -95,7 +95,7 @@ __device__ __forceinline__ void wcsph_wall_brute(const DevParams &P, double r2d,
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(kPassThreads) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+__global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
                                                              PassStats st)
 {
   __shared__ unsigned s_nb[kNbChunk][kPassThreads];
@@ -122,27 +122,11 @@ __global__ void __launch_bounds__(kPassThreads) k_wcsph_pass(const DevParams P, 
   cur.init(P, G, G.cell_of[as]);
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
-    int cnt = 0;
-    int pos;
-    while (more && cnt < kNbChunk) {
-      if (!cur.next(pos)) {
-        more = false;
-        break;
-      }
-      const int b = G.list[pos];
-      if (b == a) continue;
-      const double dxd = xa - S.x[b], dyd = ya - S.y[b];
-      const double r2d = exact_r2(dxd, dyd);
-      if (!(r2d < P.r2cut)) continue;
-      const int ob = S.orig[b];
-      if (brute_walls && ob >= P.b0 && ob < P.b1) wcsph_wall_brute(P, r2d, dxd, dyd, S.m[b], wx, wy);
-      if (r2d <= DBL_EPSILON) continue;
-      my_nb++;
-      if (max(oa, ob) >= P.pb) continue;
-      const bool isI = ob > oa;
-      my_pairs += isI;
-      s_nb[cnt++][tid] = (unsigned)b | (isI ? kRoleI : 0u);
-    }
+    const int cnt = list_partners(P, S, G, cur, more, a, oa, xa, ya, s_nb, tid, my_pairs, my_nb,
+                                  [&](int b, int ob, double r2d, double dxd, double dyd) {
+                                    if (brute_walls && ob >= P.b0 && ob < P.b1)
+                                      wcsph_wall_brute(P, r2d, dxd, dyd, S.m[b], wx, wy);
+                                  });
     __syncwarp();
     for (int e = 0; e < cnt; e++) {
       const unsigned ent = s_nb[e][tid];
