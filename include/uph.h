@@ -221,6 +221,25 @@ uph_status uph_search_neighbors(const double *position, int32_t n_fluid, int32_t
                                 int32_t particle_boundary, int32_t knn, double dist, int64_t cap,
                                 int32_t *i_pair, int32_t *j_pair, double *rij2, int64_t *niac);
 
+/* The same search for callers that must not allocate GPU memory: code that
+ * runs inside a host application's own memory pool, a real-time loop where
+ * an allocation could stall, or a plugin host that forbids cudaMalloc after
+ * start-up.  No counterpart in the reference.
+ * position, i_pair, j_pair and rij2 are DEVICE buffers owned by the caller;
+ * the grid box [lo, hi] must contain every position.  Scratch lives in one
+ * statically sized __device__ array of the library (about 10 MiB, held by
+ * every GPU that loads the library until exit); no call allocates.
+ * Limits: n_all <= 262,144 particles and at most 524,288 search cells of width
+ * sqrt(dist) over [lo, hi]; larger inputs return UPH_BAD_ARG.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array, so calls that
+ * overlap on the GPU race.  The call synchronises `stream` (a cudaStream_t,
+ * NULL for the default stream) to return *niac and the status. */
+uph_status uph_search_neighbors_noalloc(const double *position, int32_t n_fluid, int32_t n_all,
+                                        int32_t particle_boundary, double dist, const double lo[2],
+                                        const double hi[2], int64_t cap, int32_t *i_pair, int32_t *j_pair,
+                                        double *rij2, int64_t *niac, void *stream);
+
 /* ---- errors ---------------------------------------------------------------- */
 
 const char *uph_status_string(uph_status s);

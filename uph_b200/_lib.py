@@ -36,6 +36,10 @@ SIGNATURES = {
     "uph_sim_launch_count": (C.c_int64, [C.c_void_p]),
     "uph_search_neighbors": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                        C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
+    "uph_search_neighbors_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                               C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2), C.c_int64,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
+                                               C.c_void_p]),
     "uph_status_string": (C.c_char_p, [C.c_int]),
     "uph_last_error": (C.c_char_p, []),
 }

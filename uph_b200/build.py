@@ -34,6 +34,7 @@ CORE_SOURCES = [
     ("wcsph_pass.cu", []),
     ("integrate.cu", ["--fmad=false"]),
     ("sim.cu", []),
+    ("search_noalloc.cu", []),
 ]
 DROPIN_SOURCES = [("dropin.cpp", [])]
 
