@@ -211,11 +211,16 @@ def gpu_arm(args, rank, world, local_rank):
     pass_bytes = n_all * PASS_BYTES_PER_SLOT + nf * PASS_BYTES_PER_FLUID
     peak, peak_kind = load_peaks()
     achieved = pass_bytes / pass_avg_s / 1e9 if pass_avg_s > 0 else 0.0
+    # DRAM read + write bytes of one launch from the committed ncu capture
+    # (profiles/rate_pass_ref_fp64_hydrostatic500k.md)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "rate_pass_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "rate_pass_traffic.txt")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("ref_fp64_bytes_per_launch")
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2 and parts[0] == "ref_fp64_bytes_per_launch":
+                    traffic = int(parts[1])
 
     # --- e2e: every step through the C ABI with pinned host buffers:
     # upload the full state, one step, download the full state

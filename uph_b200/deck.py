@@ -298,8 +298,14 @@ def hydrostatic_tank(width=2.0, depth=1.0, dx=0.002, layers=3, eta=1.3, tank_hei
     """Config 1: still water filling the tank width, density set
     hydrostatically; the analytic answer is p = rho0 g (H - y)."""
     th = depth * 1.2 if tank_height is None else tank_height
-    return dam_break(tank=(width, th), column=(width, depth), dx=dx, layers=layers, eta=eta,
+    deck = dam_break(tank=(width, th), column=(width, depth), dx=dx, layers=layers, eta=eta,
                      hydrostatic=True, **over)
+    # wall particles carry the hydrostatic state of their depth (zero gauge
+    # pressure above the surface), so the walls push back as hard as the
+    # water next to them
+    yw = np.minimum(deck.fixed[:, 1], depth)
+    deck.fixed[:, 4], deck.fixed[:, 5] = hydrostatic_fields(yw, depth, deck.params)
+    return deck
 
 
 def wave_flume(length=10.0, depth=0.5, dx=0.005, layers=3, eta=1.3, amplitude=0.04, period=1.3,
