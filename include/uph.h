@@ -187,6 +187,35 @@ uph_status uph_sim_download(uph_sim *sim, uph_state *st);
 /* Advances `nsteps` leapfrog steps (sph.cc:90-168) on the device. */
 uph_status uph_sim_step(uph_sim *sim, int32_t nsteps);
 
+/* Records the kernel sequence of a `steps_per_graph`-step call into a CUDA
+ * graph on the first such call (after the simulation's first step) and
+ * replays it on later calls of the same length: one host launch per call
+ * instead of ~10 per step.  0 turns graphs off.  (The reference has no
+ * counterpart; its loop is sph.cc:90-168.) */
+uph_status uph_sim_set_graph(uph_sim *sim, int32_t steps_per_graph);
+
+/* Execution tuning (no counterpart in the reference): cell width = search
+ * radius / reach (reach 1-3), particle-storage tile edge in cells (power of
+ * two <= 32) and the storage re-sort interval in steps.  Defaults 2, 8, 16. */
+uph_status uph_sim_set_tuning(uph_sim *sim, int32_t reach, int32_t tile, int32_t reorder_interval);
+
+/* Picks the tuning by timing `trial_steps` steps per candidate on this
+ * simulation (a coordinate search over reach, tile and interval; it advances
+ * the simulation by about 9 (trial_steps + 2) steps) and applies the fastest.
+ * Results are cached per size class, so later sims of the same class are
+ * tuned without trials.  choice[3] receives (reach, tile, interval);
+ * *ms_per_step the best trial's time (0 when taken from the cache). */
+uph_status uph_sim_autotune(uph_sim *sim, int32_t trial_steps, int32_t choice[3], double *ms_per_step);
+
+/* Shakes the moving-boundary block horizontally, one entry per moving
+ * particle (reference order): x = x0 + half_stroke (1 - cos(omega t)),
+ * u = half_stroke omega sin(omega t).  This generalises the reference's
+ * piston and sloshing walls (inputbp.c:194-207, 244-276) to tanks that move
+ * rigidly with their own amplitude and period.  NULL pointers switch back to
+ * the movingBoundary mode of the parameters. */
+uph_status uph_sim_set_wall_motion(uph_sim *sim, const double *x0, const double *half_stroke,
+                                   const double *omega);
+
 /* One rate evaluation at time t on the uploaded state, no integration: what
  * the reference's derivatives() computes for the hot path. */
 uph_status uph_sim_derivatives(uph_sim *sim, double t);

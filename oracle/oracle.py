@@ -53,6 +53,7 @@ def oracle_lib() -> C.CDLL:
         lib.uph_oracle_pairs.restype = C.c_int64
         lib.uph_oracle_pairs.argtypes = [C.c_void_p, C.c_int64] + [C.c_void_p] * 5
         lib.uph_oracle_max_neighbors.argtypes = [C.c_void_p]
+        lib.uph_oracle_set_wall_motion.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.uph_oracle_energies.argtypes = [C.c_void_p, C.c_void_p]
         lib.uph_oracle_search.restype = C.c_int64
         lib.uph_oracle_search.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64,
@@ -105,6 +106,10 @@ class Oracle:
 
     def max_neighbors(self) -> int:
         return self.lib.uph_oracle_max_neighbors(self.h)
+
+    def set_wall_motion(self, x0, half_stroke, omega) -> None:
+        self._wall = [np.ascontiguousarray(a, dtype=np.float64) for a in (x0, half_stroke, omega)]
+        self.lib.uph_oracle_set_wall_motion(self.h, *(a.ctypes.data for a in self._wall))
 
     def energies(self):
         out = np.zeros(3)

@@ -43,6 +43,7 @@ struct uph_oracle {
   double *rij2, *w, *dw;
   int max_nb;
   double *tmp; /* 2n scratch, the reference's per-thread tmp row */
+  double *wall_tab; /* optional shaking table of the moving block: x0, hs, om */
 };
 
 static void *xcalloc(size_t n, size_t s)
@@ -83,7 +84,7 @@ void uph_oracle_destroy(uph_oracle *o)
   if (!o) return;
   void *ptrs[] = {o->pos, o->vel, o->lvel, o->rho, o->lrho, o->pr, o->lpr, o->mass, o->pressure, o->itype,
                   o->vmin, o->rhomin, o->prmin, o->sponge, o->drho, o->dp, o->acc, o->drho_a, o->dp_a, o->acc_a,
-                  o->frho, o->fp, o->fvel, o->wall_x0, o->tmp, o->ip, o->jp, o->rij2, o->w, o->dw};
+                  o->frho, o->fp, o->fvel, o->wall_x0, o->tmp, o->ip, o->jp, o->rij2, o->w, o->dw, o->wall_tab};
   for (size_t k = 0; k < sizeof ptrs / sizeof ptrs[0]; k++) free(ptrs[k]);
   free(o);
 }
@@ -692,9 +693,32 @@ static void monaghan_boundary(uph_oracle *o)
     }
 }
 
-/* inputbp.c:194-207: piston wavemaker (movingBoundary 1) */
+/* per-particle shaking of the moving block: x = x0 + hs (1 - cos(om t)) */
+void uph_oracle_set_wall_motion(uph_oracle *o, const double *x0, const double *hs, const double *om)
+{
+  const int nm = o->p.n_moving;
+  free(o->wall_tab);
+  o->wall_tab = NULL;
+  if (!x0 || nm <= 0) return;
+  o->wall_tab = (double *)xcalloc(3 * (size_t)nm, 8);
+  memcpy(o->wall_tab, x0, 8 * (size_t)nm);
+  memcpy(o->wall_tab + nm, hs, 8 * (size_t)nm);
+  memcpy(o->wall_tab + 2 * nm, om, 8 * (size_t)nm);
+}
+
+/* inputbp.c:194-207: piston wavemaker (movingBoundary 1), or the table above */
 static void wall_motion(uph_oracle *o, double t)
 {
+  const int m0 = o->nf + o->p.n_solid + o->p.n_fixed, nm = o->p.n_moving;
+  if (o->wall_tab) {
+    for (int k = 0; k < nm; k++) {
+      const double hs = o->wall_tab[nm + k], om = o->wall_tab[2 * nm + k];
+      o->pos[2 * (m0 + k)] = o->wall_tab[k] + hs * (1.0 - cos(om * t));
+      o->vel[2 * (m0 + k)] = hs * om * sin(om * t);
+      o->lvel[2 * (m0 + k)] = o->vel[2 * (m0 + k)];
+    }
+    return;
+  }
   if (o->p.moving_boundary == 1 && o->p.flag_init_simul == 1) {
     const double lbp = 0.5 * o->p.stroke * (1.0 - cos(o->p.omega * t));
     const double lbv = 0.5 * o->p.stroke * o->p.omega * sin(o->p.omega * t);

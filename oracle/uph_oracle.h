@@ -27,6 +27,8 @@ int uph_oracle_step(uph_oracle *o, int nsteps);
 int64_t uph_oracle_pairs(const uph_oracle *o, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
                          double *w, double *dwcdx);
 int uph_oracle_max_neighbors(const uph_oracle *o);
+/* per-particle shaking of the moving block (NULL: the movingBoundary mode) */
+void uph_oracle_set_wall_motion(uph_oracle *o, const double *x0, const double *hs, const double *om);
 void uph_oracle_energies(const uph_oracle *o, double out[3]);
 
 /* stand-alone radius search with SearchNeighbors' filter (Search.cc:31-40) */

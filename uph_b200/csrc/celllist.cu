@@ -36,7 +36,7 @@ __global__ void k_cell_keys(DevParams P, const double *__restrict__ x, const dou
     if (fx > 0.0) cx = (int)fmin(fx, (double)(P.ncx - 1));
     if (fy > 0.0) cy = (int)fmin(fy, (double)(P.ncy - 1));
   }
-  const int c = storage_order ? storage_key(cx, cy, P.ntx) : cy * P.ncx + cx;
+  const int c = storage_order ? storage_key(cx, cy, P.ntx, P.tile) : cy * P.ncx + cx;
   cell_of[s] = c;
   atomicAdd(&cnt[c], 1);
 }

@@ -66,9 +66,11 @@ void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s)
 // sph.cc:137-168: the corrector with the rates just evaluated, then the
 // drift x += dt v.  With predict_next the predictor of the following step
 // runs right after.  Flags non-finite results.
-__global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, int predict_next, unsigned *err)
+__global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, int predict_next, unsigned *err,
+                          int *d_itime)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0 && d_itime) *d_itime += 1;  // steps completed, read by the next step's wall motion
   if (a >= P.nf) return;
   const double dt = P.dt;
   const double drho = S.drho[a], dp = S.dp[a], ax = S.ax[a], ay = S.ay[a];
@@ -119,9 +121,10 @@ __global__ void k_correct(const DevParams P, const SlotArrays S, int first_step,
 }
 
 void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
-                    cudaStream_t s)
+                    int *d_itime, cudaStream_t s)
 {
-  if (P.nf > 0) k_correct<<<(P.nf + 255) / 256, 256, 0, s>>>(P, S, first_step, predict_next, err);
+  const int n = P.nf > 0 ? P.nf : 1;
+  k_correct<<<(n + 255) / 256, 256, 0, s>>>(P, S, first_step, predict_next, err, d_itime);
 }
 
 // 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure.
@@ -146,27 +149,42 @@ void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, 
   if (count > 0) k_refresh<<<(count + 255) / 256, 256, 0, s>>>(P, S, first, count);
 }
 
-// inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
-// x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt.  Slots of moving
-// particles are found through their reference index.
-__global__ void k_wall_motion(const DevParams P, const SlotArrays S, double t)
+// Moving boundary particles (reference indices [m0, b1)), found through
+// their slot's reference index.
+//  - inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
+//    x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt;
+//  - a WallTable shakes each particle about its own rest position with its
+//    own half stroke and frequency (one entry per particle, e.g. every wall
+//    of a sloshing tank moving rigidly).
+__global__ void k_wall_motion(const DevParams P, const SlotArrays S, const WallTable W, double t_host,
+                              const int *d_itime)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = P.nf + k;
   if (s >= P.n) return;
   const int o = S.orig[s];
   if (o < P.m0 || o >= P.b1) return;
-  const double lbp = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
-  const double lbv = 0.5 * P.stroke * P.omega * sin(P.omega * t);
-  S.x[s] = lbp;
-  S.u[s] = lbv;
-  S.ut[s] = lbv;
+  const double t = d_itime ? (*d_itime + 1) * P.dt : t_host;
+  double x, u;
+  if (W.enabled) {
+    const int m = o - P.m0;
+    const double hs = W.hs[m], om = W.om[m];
+    x = W.x0[m] + hs * (1.0 - cos(om * t));
+    u = hs * om * sin(om * t);
+  } else {
+    x = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
+    u = 0.5 * P.stroke * P.omega * sin(P.omega * t);
+  }
+  S.x[s] = x;
+  S.u[s] = u;
+  S.ut[s] = u;
 }
 
-void launch_wall_motion(const DevParams &P, const SlotArrays &S, double t, cudaStream_t s)
+void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
+                        const int *d_itime, cudaStream_t s)
 {
   const int n = P.n - P.nf;
-  if (n > 0) k_wall_motion<<<(n + 255) / 256, 256, 0, s>>>(P, S, t);
+  if (n > 0) k_wall_motion<<<(n + 255) / 256, 256, 0, s>>>(P, S, W, t_host, d_itime);
 }
 
 // EquationOfState for the non-fluid slots (derivatives.c:1674-1682); their

@@ -11,6 +11,9 @@
 #include <math.h>
 #include <string.h>
 
+#include <array>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -73,6 +76,21 @@ struct uph_sim {
   std::vector<void *> allocations;
   double *d_partials = nullptr;
   int n_partials = 0;
+  // device step counter (steps completed) and moving-wall table
+  int *d_itime = nullptr;
+  double *d_wall_tab = nullptr;
+  WallTable W = {nullptr, nullptr, nullptr, 0};
+  // CUDA graph of `graph_steps` steps, recorded on the first eligible call
+  int graph_steps = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  const double *graph_buffer = nullptr;  // S.x when recorded: the buffer parity it needs
+  int graph_since_after = 0;
+  int64_t graph_launches = 0;
+  int64_t graph_replays = 0;
+  // tuning: storage re-sort interval and the grid arrays' capacity in cells
+  int reorder_interval = kReorderInterval;
+  long long grid_capacity = 0;
 };
 
 namespace {
@@ -356,6 +374,46 @@ uph_status validate(const uph_params *p)
   return UPH_OK;
 }
 
+// (Re)allocates the per-cell arrays for the current grid geometry; they grow
+// only, so a smaller grid after re-tuning keeps the old allocation.
+cudaError_t alloc_grid(uph_sim *s)
+{
+  CellGrid &G = s->G;
+  const long long ncell = (long long)s->P.ncx * s->P.ncy;
+  if (ncell > (1LL << 28)) return cudaErrorInvalidValue;
+  G.ncell = (int)ncell;
+  G.nblock_sums = scan_block_sums_needed((int)ncell);
+  if (ncell <= s->grid_capacity) return cudaSuccess;
+  for (int **p : {&G.count, &G.start, &G.fill, &G.block_sums}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  cudaError_t e;
+  if ((e = cudaMalloc((void **)&G.count, sizeof(int) * ncell)) != cudaSuccess) return e;
+  if ((e = cudaMalloc((void **)&G.start, sizeof(int) * (ncell + 1))) != cudaSuccess) return e;
+  if ((e = cudaMalloc((void **)&G.fill, sizeof(int) * ncell)) != cudaSuccess) return e;
+  if ((e = cudaMalloc((void **)&G.block_sums, sizeof(int) * (G.nblock_sums + 1))) != cudaSuccess) return e;
+  s->grid_capacity = ncell;
+  return cudaSuccess;
+}
+
+// Cell width radius / reach; cells per axis rounded up to whole tiles.
+void set_grid_geometry(DevParams &P, int reach, int tile)
+{
+  P.reach = reach;
+  P.tile = tile;
+  const double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
+  P.cell = cell;
+  P.inv_cell = 1.0 / cell;
+  const double nx = ceil((P.hi_x - P.lo_x) / cell);
+  const double ny = ceil((P.hi_y - P.lo_y) / cell);
+  const double tiles_x = ceil(fmax(nx, 1.0) / tile), tiles_y = ceil(fmax(ny, 1.0) / tile);
+  // clamp before converting; callers reject grids this large
+  P.ntx = (int)fmin(tiles_x, 1 << 20);
+  P.ncx = P.ntx * tile;
+  P.ncy = (int)fmin(tiles_y, 1 << 20) * tile;
+}
+
 DevParams make_dev_params(const uph_params *p)
 {
   DevParams P;
@@ -402,24 +460,13 @@ DevParams make_dev_params(const uph_params *p)
   P.omega = p->omega;
   P.av_alpha_c0 = p->av_alpha * p->speed_of_sound;
   P.dt = p->time_step;
-  // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
-  // against 36 h^2 for a 3 x 3 block of radius-wide cells
-  P.reach = kCellReach;
-  const double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
   P.lo_x = p->domain_lo[0];
   P.lo_y = p->domain_lo[1];
   P.hi_x = p->domain_hi[0];
   P.hi_y = p->domain_hi[1];
-  P.cell = cell;
-  P.inv_cell = 1.0 / cell;
-  // whole tiles: the cell count per axis is rounded up to a multiple of the tile
-  const double nx = ceil((p->domain_hi[0] - p->domain_lo[0]) / cell);
-  const double ny = ceil((p->domain_hi[1] - p->domain_lo[1]) / cell);
-  const double tiles_x = ceil(fmax(nx, 1.0) / kCellTile), tiles_y = ceil(fmax(ny, 1.0) / kCellTile);
-  // clamp before converting; uph_sim_create rejects grids this large
-  P.ntx = (int)fmin(tiles_x, 1 << 20);
-  P.ncx = P.ntx * kCellTile;
-  P.ncy = (int)fmin(tiles_y, 1 << 20) * kCellTile;
+  // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
+  // against 36 h^2 for a 3 x 3 block of radius-wide cells
+  set_grid_geometry(P, kCellReach, kCellTile);
   return P;
 }
 
@@ -456,14 +503,9 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(alloc_slots(s, s->S, n, nf));
   TRY(alloc_slots(s, s->S2, n, nf));
   CellGrid &G = s->G;
-  G.ncell = (int)ncell;
-  TRY(dalloc(s, &G.count, (size_t)ncell));
-  TRY(dalloc(s, &G.start, (size_t)ncell + 1));
-  TRY(dalloc(s, &G.fill, (size_t)ncell));
   TRY(dalloc(s, &G.list, (size_t)n));
   TRY(dalloc(s, &G.cell_of, (size_t)n));
-  G.nblock_sums = scan_block_sums_needed((int)ncell);
-  TRY(dalloc(s, &G.block_sums, (size_t)G.nblock_sums));
+  TRY(alloc_grid(s));
   Staging &T = s->T;
   double **tall[] = {&T.rho, &T.lrho, &T.p, &T.lp, &T.mass, &T.pressure, &T.tmp_x, &T.tmp_y};
   for (double **q : tall) TRY(dalloc(s, q, (size_t)n));
@@ -478,6 +520,8 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &s->d_niac, 1));
   TRY(dalloc(s, &s->d_max_nb, 1));
   TRY(dalloc(s, &s->d_perm, (size_t)n));
+  TRY(dalloc(s, &s->d_itime, 1));
+  TRY(dalloc(s, &s->d_wall_tab, 3 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
   s->n_partials = 1024;
   TRY(dalloc(s, &s->d_partials, (size_t)s->n_partials * 4));
   TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -488,11 +532,18 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   return UPH_OK;
 }
 
+namespace {
+void drop_graph(uph_sim *s);
+}
+
 extern "C" uph_status uph_sim_destroy(uph_sim *s)
 {
   if (!s) return UPH_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
   for (void *p : s->allocations) cudaFree(p);
+  for (void *p : {(void *)s->G.count, (void *)s->G.start, (void *)s->G.fill, (void *)s->G.block_sums})
+    if (p) cudaFree(p);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   for (cudaEvent_t e : s->ev_pool)
     if (e) cudaEventDestroy(e);
@@ -582,6 +633,7 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
   launch_wall_pressure(s->P, s->S, q);
   s->launches += 3;
   s->itime = itime;
+  UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, q));
   s->steps_since_reorder = 0;
   s->have_rates = false;
   return check_error_word(s);
@@ -622,14 +674,23 @@ extern "C" uph_status uph_sim_download(uph_sim *s, uph_state *st)
   return UPH_OK;
 }
 
-extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
+namespace {
+
+bool walls_move(const uph_sim *s)
 {
-  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
-  if (nsteps < 0) return fail(UPH_BAD_ARG, "negative step count");
-  const bool walls_move = s->P.moving_boundary == 1 && s->P.flag_init_simul == 1 && s->hp.n_moving > 0;
+  return s->hp.n_moving > 0 && (s->W.enabled || (s->P.moving_boundary == 1 && s->P.flag_init_simul == 1));
+}
+
+// Enqueues `nsteps` leapfrog steps on the sim's stream.  With `capturing`
+// the sequence is being recorded into a CUDA graph: no host synchronisation,
+// no profiling events, and an even number of storage re-sorts so the graph
+// ends on the buffer it started on.
+uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
+{
+  const bool moving = walls_move(s);
+  int swaps = 0;
   for (int k = 0; k < nsteps; k++) {
     const int itime = ++s->itime;
-    const double t = itime * s->P.dt;
     // the predictor of steps after the first of this call ran inside the
     // previous step's corrector
     if (itime != 1 && k == 0) {
@@ -637,31 +698,131 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
       launch_predict(s->P, s->S, s->stream);
       s->launches++;
     }
-    if (walls_move) {
+    if (moving) {
       Timer tm(s, KF_WALLS);
-      launch_wall_motion(s->P, s->S, t, s->stream);
+      launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->stream);
       s->launches++;
     }
     uph_status r = rate_pass(s, itime == 1);
     if (r != UPH_OK) return r;
     {
       Timer tm(s, KF_CORRECT);
-      launch_correct(s->P, s->S, itime == 1, k + 1 < nsteps, s->d_err, s->stream);
+      launch_correct(s->P, s->S, itime == 1, k + 1 < nsteps, s->d_err, s->d_itime, s->stream);
       s->launches++;
     }
-    if (++s->steps_since_reorder >= kReorderInterval) {
+    if (++s->steps_since_reorder >= s->reorder_interval) {
       r = reorder_fluid(s);
       if (r != UPH_OK) return r;
+      swaps++;
     }
     // a particle that left the grid is clamped into a border cell, which can
     // make that cell arbitrarily crowded: stop early rather than run on
-    if ((k + 1) % kErrorCheckInterval == 0 && k + 1 < nsteps) {
+    if (!capturing && (k + 1) % kErrorCheckInterval == 0 && k + 1 < nsteps) {
       r = check_error_word(s);
       if (r != UPH_OK) return r;
     }
   }
+  if (capturing && (swaps & 1)) {
+    uph_status r = reorder_fluid(s);
+    if (r != UPH_OK) return r;
+  }
+  return UPH_OK;
+}
+
+void drop_graph(uph_sim *s)
+{
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graph_exec = nullptr;
+  s->graph = nullptr;
+}
+
+}  // namespace
+
+extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  if (nsteps < 0) return fail(UPH_BAD_ARG, "negative step count");
+  // graph replay: a call of exactly graph_steps steps that is not the
+  // simulation's first step and starts on the buffer the graph was recorded on
+  if (s->graph_steps > 0 && nsteps == s->graph_steps && s->itime >= 1 && !s->profiling) {
+    if (s->graph_exec && s->graph_buffer != s->S.x) drop_graph(s);
+    if (!s->graph_exec) {
+      const int itime0 = s->itime, since0 = s->steps_since_reorder;
+      const int64_t launches0 = s->launches;
+      const double *buffer0 = s->S.x;
+      s->steps_since_reorder = 0;
+      UPH_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      uph_status r = enqueue_steps(s, nsteps, true);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+      // the recording ran nothing: restore the host-side counters
+      s->itime = itime0;
+      s->steps_since_reorder = since0;
+      s->graph_launches = s->launches - launches0;
+      s->launches = launches0;
+      if (r != UPH_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+      s->graph = g;
+      UPH_CUDA(cudaGraphInstantiate(&s->graph_exec, g, 0));
+      s->graph_buffer = buffer0;
+      s->graph_since_after = 0;
+      // replaying leaves the re-sort counter where the recording left it
+      int since = 0, swaps = 0;
+      for (int k = 0; k < nsteps; k++)
+        if (++since >= s->reorder_interval) {
+          since = 0;
+          swaps++;
+        }
+      s->graph_since_after = (swaps & 1) ? 0 : since;
+    }
+    UPH_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
+    s->itime += nsteps;
+    s->steps_since_reorder = s->graph_since_after;
+    s->launches += s->graph_launches;
+    s->graph_replays++;
+    UPH_CUDA(cudaGetLastError());
+    return check_error_word(s);
+  }
+  uph_status r = enqueue_steps(s, nsteps, false);
+  if (r != UPH_OK) return r;
   UPH_CUDA(cudaGetLastError());
   return check_error_word(s);
+}
+
+extern "C" uph_status uph_sim_set_graph(uph_sim *s, int32_t steps_per_graph)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  if (steps_per_graph < 0) return fail(UPH_BAD_ARG, "negative graph length");
+  drop_graph(s);
+  s->graph_steps = steps_per_graph;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_set_wall_motion(uph_sim *s, const double *x0, const double *half_stroke,
+                                              const double *omega)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  const int nm = s->hp.n_moving;
+  if (!x0 || !half_stroke || !omega) {
+    s->W.enabled = 0;
+    drop_graph(s);
+    return UPH_OK;
+  }
+  if (nm <= 0) return fail(UPH_BAD_ARG, "uph_sim_set_wall_motion: the sim has no moving boundary particles");
+  UPH_CUDA(cudaMemcpyAsync(s->d_wall_tab, x0, sizeof(double) * nm, cudaMemcpyHostToDevice, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(s->d_wall_tab + nm, half_stroke, sizeof(double) * nm, cudaMemcpyHostToDevice, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(s->d_wall_tab + 2 * nm, omega, sizeof(double) * nm, cudaMemcpyHostToDevice, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  s->W.x0 = s->d_wall_tab;
+  s->W.hs = s->d_wall_tab + nm;
+  s->W.om = s->d_wall_tab + 2 * nm;
+  s->W.enabled = 1;
+  drop_graph(s);
+  return UPH_OK;
 }
 
 extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
@@ -669,8 +830,8 @@ extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
   if (!s) return fail(UPH_BAD_ARG, "NULL sim");
   // the piston position is a closed form of t, so applying it again after the
   // caller's own inputbp() changes nothing
-  if (s->P.moving_boundary == 1 && s->P.flag_init_simul == 1 && s->hp.n_moving > 0) {
-    launch_wall_motion(s->P, s->S, t, s->stream);
+  if (walls_move(s)) {
+    launch_wall_motion(s->P, s->S, s->W, t, nullptr, s->stream);
     s->launches++;
   }
   uph_status r = rate_pass(s, true);
@@ -887,6 +1048,126 @@ extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
   out->niac = s->have_rates ? (int64_t)niac : 0;
   out->max_neighbors = s->have_rates ? mx : 0;
   out->itime = s->itime;
+  return UPH_OK;
+}
+
+// ---- tuning -----------------------------------------------------------------------
+
+extern "C" uph_status uph_sim_set_tuning(uph_sim *s, int32_t reach, int32_t tile, int32_t reorder_interval)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  if (reach < 1 || reach > 3) return fail(UPH_BAD_ARG, "cell reach must be 1, 2 or 3");
+  if (tile < 1 || tile > 32 || (tile & (tile - 1))) return fail(UPH_BAD_ARG, "tile must be a power of two <= 32");
+  if (reorder_interval < 1 || reorder_interval > 4096) return fail(UPH_BAD_ARG, "reorder interval out of range");
+  DevParams P2 = s->P;
+  set_grid_geometry(P2, reach, tile);
+  if ((long long)P2.ncx * P2.ncy > (1LL << 28)) return fail(UPH_BAD_ARG, "tuned cell grid larger than 2^28 cells");
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  s->P = P2;
+  UPH_CUDA(alloc_grid(s));
+  s->reorder_interval = reorder_interval;
+  drop_graph(s);
+  // storage order follows the new tile from now on
+  return reorder_fluid(s);
+}
+
+namespace {
+
+struct TuneKey {
+  int profile, precision, nf_class, cell_class;
+  bool operator<(const TuneKey &o) const
+  {
+    if (profile != o.profile) return profile < o.profile;
+    if (precision != o.precision) return precision < o.precision;
+    if (nf_class != o.nf_class) return nf_class < o.nf_class;
+    return cell_class < o.cell_class;
+  }
+};
+
+std::mutex g_tune_mutex;
+std::map<TuneKey, std::array<int, 3>> g_tune_cache;
+
+int log2_class(double v) { return v < 1.0 ? 0 : (int)floor(log2(v)); }
+
+// ms per step of `steps` steps (after two warm-up steps) with the current tuning
+uph_status time_steps(uph_sim *s, int steps, double *ms)
+{
+  uph_status r = enqueue_steps(s, 2, false);
+  if (r != UPH_OK) return r;
+  cudaEvent_t a, b;
+  UPH_CUDA(cudaEventCreate(&a));
+  UPH_CUDA(cudaEventCreate(&b));
+  cudaEventRecord(a, s->stream);
+  r = enqueue_steps(s, steps, false);
+  cudaEventRecord(b, s->stream);
+  cudaEventSynchronize(b);
+  float f = 0.f;
+  cudaEventElapsedTime(&f, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (r != UPH_OK) return r;
+  *ms = f / steps;
+  return check_error_word(s);
+}
+
+}  // namespace
+
+// Coordinate search over (cell reach, storage tile, re-sort interval): the
+// reach first with tile 8 and interval 16, then the tile at the best reach,
+// then the interval.  Each trial times `trial_steps` steps of this very
+// simulation, so tuning advances it by about 9 (trial_steps + 2) steps.
+// Results are cached per size class (profile, precision, log2 of the fluid
+// count, log2 of the radius-wide cell count); a sim of a cached class is set
+// without trials.
+extern "C" uph_status uph_sim_autotune(uph_sim *s, int32_t trial_steps, int32_t choice[3], double *ms_per_step)
+{
+  if (!s || !choice) return fail(UPH_BAD_ARG, "uph_sim_autotune: NULL argument");
+  if (trial_steps < 1) return fail(UPH_BAD_ARG, "uph_sim_autotune: trial_steps must be positive");
+  DevParams P1 = s->P;
+  set_grid_geometry(P1, 1, 1);
+  const TuneKey key{s->P.profile, s->P.precision, log2_class(s->P.nf), log2_class((double)P1.ncx * P1.ncy)};
+  std::array<int, 3> best{kCellReach, kCellTile, kReorderInterval};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      best = it->second;
+      cached = true;
+    }
+  }
+  double best_ms = 0.0;
+  if (!cached) {
+    auto trial = [&](std::array<int, 3> c, double *ms) -> uph_status {
+      uph_status r = uph_sim_set_tuning(s, c[0], c[1], c[2]);
+      if (r != UPH_OK) return r;
+      return time_steps(s, trial_steps, ms);
+    };
+    best_ms = 1e300;
+    for (int axis = 0; axis < 3; axis++) {
+      static const int options[3][3] = {{1, 2, 3}, {4, 8, 16}, {8, 16, 32}};
+      std::array<int, 3> axis_best = best;
+      for (int v : options[axis]) {
+        std::array<int, 3> c = best;
+        c[axis] = v;
+        double ms = 0.0;
+        uph_status r = trial(c, &ms);
+        if (r == UPH_BAD_ARG) continue;  // e.g. a grid too large for this reach
+        if (r != UPH_OK) return r;
+        if (ms < best_ms) {
+          best_ms = ms;
+          axis_best = c;
+        }
+      }
+      best = axis_best;
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+  }
+  uph_status r = uph_sim_set_tuning(s, best[0], best[1], best[2]);
+  if (r != UPH_OK) return r;
+  for (int k = 0; k < 3; k++) choice[k] = best[k];
+  if (ms_per_step) *ms_per_step = best_ms;
   return UPH_OK;
 }
 

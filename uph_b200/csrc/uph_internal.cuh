@@ -67,7 +67,8 @@ struct DevParams {
   // cell grid
   double lo_x, lo_y, cell, inv_cell;
   double hi_x, hi_y;  // declared domain; the grid itself is rounded up to whole tiles
-  int ncx, ncy;  // cells per axis, multiples of kCellTile
+  int ncx, ncy;  // cells per axis, multiples of `tile`
+  int tile;      // storage-order tile edge in cells
   int ntx;       // tiles per row
   int reach;     // cells are >= radius / reach wide; partners lie within `reach` cells
 };
@@ -78,13 +79,22 @@ struct DevParams {
 // tile, tiles row-major, cells inside a tile row-major.  A block's 128
 // consecutive slots then cover a compact 2-D patch whose neighbours stay in
 // the SM's L1, rather than a long strip of one cell row.
+// The tile edge is a tuning parameter (DevParams::tile, default 8).
 constexpr int kCellTile = 8;
 
-__host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx)
+__host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx, int tile)
 {
-  const int tx = cx / kCellTile, lx = cx % kCellTile, ty = cy / kCellTile, ly = cy % kCellTile;
-  return ((ty * ntx + tx) * kCellTile + ly) * kCellTile + lx;
+  const int tx = cx / tile, lx = cx % tile, ty = cy / tile, ly = cy % tile;
+  return ((ty * ntx + tx) * tile + ly) * tile + lx;
 }
+
+// Per-particle horizontal shaking of the moving boundary block (reference
+// indices [m0, b1)): x = x0 + hs (1 - cos w t), u = ut = hs w sin w t.
+// Indexed by reference index - m0, so it does not move with re-sorts.
+struct WallTable {
+  const double *x0, *hs, *om;
+  int enabled;
+};
 
 struct CellGrid {
   int ncell;
@@ -126,9 +136,13 @@ void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);
 void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
-                    cudaStream_t s);
+                    int *d_itime, cudaStream_t s);
 void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s);
-void launch_wall_motion(const DevParams &P, const SlotArrays &S, double t, cudaStream_t s);
+// t = (*d_itime + 1) dt when d_itime is given (the step being computed; the
+// counter lives on the device so CUDA-graph replays see the right time),
+// else t = t_host
+void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
+                        const int *d_itime, cudaStream_t s);
 void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t s);
 
 }  // namespace uph

@@ -76,6 +76,27 @@ class Simulation:
     def step(self, nsteps: int = 1) -> None:
         _lib.check(self.lib.uph_sim_step(self.handle, nsteps), "uph_sim_step")
 
+    def set_graph(self, steps_per_graph: int) -> None:
+        """Record / replay `steps_per_graph`-step calls of step() as a CUDA graph."""
+        _lib.check(self.lib.uph_sim_set_graph(self.handle, steps_per_graph), "uph_sim_set_graph")
+
+    def set_tuning(self, reach: int, tile: int, reorder_interval: int) -> None:
+        _lib.check(self.lib.uph_sim_set_tuning(self.handle, reach, tile, reorder_interval), "uph_sim_set_tuning")
+
+    def autotune(self, trial_steps: int = 10):
+        """Native autotuner; returns ((reach, tile, interval), best ms/step or 0 if cached)."""
+        choice = (C.c_int32 * 3)()
+        ms = C.c_double(0.0)
+        _lib.check(self.lib.uph_sim_autotune(self.handle, trial_steps, C.byref(choice), C.byref(ms)),
+                   "uph_sim_autotune")
+        return tuple(choice), ms.value
+
+    def set_wall_motion(self, x0, half_stroke, omega) -> None:
+        """Shake each moving-boundary particle: x = x0 + hs (1 - cos(omega t))."""
+        self._wall = [np.ascontiguousarray(a, dtype=np.float64) for a in (x0, half_stroke, omega)]
+        _lib.check(self.lib.uph_sim_set_wall_motion(self.handle, *(a.ctypes.data for a in self._wall)),
+                   "uph_sim_set_wall_motion")
+
     def derivatives(self, t: float) -> None:
         _lib.check(self.lib.uph_sim_derivatives(self.handle, t), "uph_sim_derivatives")
 
