@@ -270,11 +270,100 @@ def gpu_arm(args, rank, world, local_rank):
         p_ms, p_n = kt.get("rate_pass", (0.0, 0))
         variants[label] = {"value": world * nf * k_var / (vms / 1e3), "steps": k_var,
                            "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1)}
+    if not args.no_batched:
+        variants["batched_tanks"] = batched_arm(args, stream.cuda_stream)
 
     return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
                 pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
                 traffic=traffic, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
                 deck=deck)
+
+
+def batched_arm(args, stream_ptr):
+    """The batched-tank configuration: 256 dam-break and sloshing tanks from
+    seed 0 (1.5k-30k particles each, ~2.9 M in all), WCSPH physics.
+    - plain: every tank its own simulation in FP64, advanced one after the
+      other, 1 + graph_steps steps each (the plain GPU path);
+    - batched: all tanks as one simulation, FP32 pair arithmetic with FP64
+      integration, autotuned, graph_steps steps per CUDA-graph replay.
+    Errors compare the batched state with the plain one after the same
+    1 + graph_steps steps: density relative to rho0, free-surface height
+    relative to the tank's column height."""
+    import torch
+    from uph_b200 import batch as B
+    from uph_b200.sim import Simulation
+
+    gsteps = args.graph_steps
+    tanks = B.draw_tanks(seed=0, count=args.tanks)
+    batch = B.build_batch(tanks)
+    nf_total = batch.deck.n_fluid
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    # plain: one FP64 simulation per tank
+    sims = []
+    for k in range(len(tanks)):
+        d, table = B.tank_deck(batch, k)
+        s = Simulation.from_deck(d, profile=1, precision=0)
+        s.set_stream(stream.cuda_stream)
+        if table is not None:
+            s.set_wall_motion(*table)
+        sims.append((d, s))
+    plain_s = timed(lambda: [s.step(1 + gsteps) for _, s in sims])
+    plain_value = nf_total * (1 + gsteps) / plain_s
+    plain_states = []
+    for d, s in sims:
+        plain_states.append((d.n_fluid, s.download()))
+        s.close()
+
+    # tuning for this size class (trials on a throw-away copy)
+    tuner = Simulation.from_deck(batch.deck, profile=1, precision=1)
+    tuner.set_wall_motion(batch.wall_x0, batch.wall_hs, batch.wall_om)
+    choice, _ = tuner.autotune(trial_steps=5)
+    tuner.close()
+
+    sim = Simulation.from_deck(batch.deck, profile=1, precision=1)
+    sim.set_stream(stream.cuda_stream)
+    sim.set_wall_motion(batch.wall_x0, batch.wall_hs, batch.wall_om)
+    sim.set_tuning(*choice)
+    sim.set_graph(gsteps)
+    sim.step(1)
+    sim.step(gsteps)  # records the graph and runs it once
+    st = sim.download()
+    rho0, dx = batch.deck.params["density0"], batch.deck.params["dx"]
+    max_drho = max_fs = 0.0
+    for k, spec in enumerate(tanks):
+        f0, f1 = batch.fluid_ranges[k]
+        n, pst = plain_states[k]
+        max_drho = max(max_drho, float(np.abs(st["density"][f0:f1] - pst["density"][:n]).max() / rho0))
+        length = 2.5 * spec.width if spec.kind == "dambreak" else spec.width
+        x0 = batch.offsets[k][0]
+        hb = B.free_surface_heights(st["Position"][f0:f1], x0, length, dx)
+        hp = B.free_surface_heights(pst["Position"][:n], x0, length, dx)
+        max_fs = max(max_fs, float(np.abs(hb - hp).max() / spec.height))
+    reps = args.graph_replays
+    l0 = sim.launch_count()
+    batched_s = timed(lambda: [sim.step(gsteps) for _ in range(reps)])
+    launches = sim.launch_count() - l0
+    sim.close()
+    batched_value = nf_total * gsteps * reps / batched_s
+    return {
+        "tanks": len(tanks), "n_fluid": nf_total, "steps_per_graph": gsteps,
+        "batched_fp32_graph": {"value": batched_value, "ms_per_step": batched_s / (gsteps * reps) * 1e3,
+                               "replays": reps, "kernels_per_replay": launches // max(reps, 1),
+                               "tuning": {"cell_reach": choice[0], "tile": choice[1], "resort_interval": choice[2]}},
+        "plain_per_tank_fp64": {"value": plain_value, "steps": 1 + gsteps},
+        "speedup": batched_value / plain_value,
+        "max_density_error": max_drho, "max_free_surface_error": max_fs,
+    }
 
 
 def main():
@@ -287,6 +376,10 @@ def main():
     ap.add_argument("--variant-steps", type=int, default=500)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tanks", type=int, default=256, help="batched-tank configuration: number of tanks")
+    ap.add_argument("--graph-steps", type=int, default=200, help="steps per CUDA-graph replay of the batch")
+    ap.add_argument("--graph-replays", type=int, default=3)
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "uph":
         args.warmup = 3
