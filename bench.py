@@ -272,11 +272,61 @@ def gpu_arm(args, rank, world, local_rank):
                            "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1)}
     if not args.no_batched:
         variants["batched_tanks"] = batched_arm(args, stream.cuda_stream)
+    if not args.no_dambreak:
+        variants.update(dambreak_arm(args, stream))
 
     return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
                 pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
                 traffic=traffic, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
                 deck=deck)
+
+
+def dambreak_arm(args, stream):
+    """The dam-break configurations, WCSPH physics (cubic spline, Tait,
+    Monaghan alpha = 0.01), hydrostatic initial pressure in the column:
+    - dambreak_5k: tank 4.0 x 3.0 m, column 1.0 x 2.0 m, dx = 0.02 m, 2 wall
+      layers, FP64, 1,000 steps as one CUDA-graph replay (the case is small
+      enough that launches, not kernels, would otherwise dominate);
+    - dambreak_2M: tank 8.0 x 4.0 m, column 2.0 x 4.0 m, dx = 0.002 m,
+      FP32 pair arithmetic with FP64 integration, 500 steps."""
+    import torch
+    from uph_b200 import deck as D
+    from uph_b200.sim import Simulation
+
+    out = {}
+    cases = [("dambreak_5k_fp64_graph", D.dam_break(tank=(4.0, 3.0), column=(1.0, 2.0), dx=0.02, layers=2,
+                                                    hydrostatic=True), 0, 1000, True),
+             # c0 = 10 sqrt(g H) with H = 4 m, the column height (the 5k case's
+             # 10 sqrt(2 g) belongs to its own 2 m column)
+             ("dambreak_2M_fp32_pair", D.dam_break(tank=(8.0, 4.0), column=(2.0, 4.0), dx=0.002, layers=2,
+                                                   hydrostatic=True, local_depth=4.0), 1, 500, False)]
+    for label, deck, prec, steps, graph in cases:
+        s = Simulation.from_deck(deck, profile=1, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        s.step(1)
+        if graph:
+            s.set_graph(steps)
+            s.step(steps)  # records the graph and runs it once
+        else:
+            s.step(args.warmup)
+        s.profile(not graph)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        entry = {"value": deck.n_fluid * steps / sec, "n_fluid": deck.n_fluid, "steps": steps,
+                 "ms_per_step": sec / steps * 1e3}
+        if not graph:
+            ms, n = s.kernel_times().get("rate_pass", (0.0, 0))
+            entry["rate_pass_ms"] = ms / max(n, 1)
+        st = s.stats()
+        entry["max_abs_density_error"] = st["max_abs_density_error"]
+        s.close()
+        out[label] = entry
+    return out
 
 
 def batched_arm(args, stream_ptr):
@@ -380,6 +430,7 @@ def main():
     ap.add_argument("--graph-steps", type=int, default=200, help="steps per CUDA-graph replay of the batch")
     ap.add_argument("--graph-replays", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-dambreak", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "uph":
         args.warmup = 3
