@@ -35,6 +35,7 @@ CORE_SOURCES = [
     ("integrate.cu", ["--fmad=false"]),
     ("sim.cu", []),
     ("search_noalloc.cu", []),
+    ("tc_gemm.cu", ["@cutlass"]),
 ]
 DROPIN_SOURCES = [("dropin.cpp", [])]
 
@@ -64,7 +65,22 @@ def _run(cmd, verbose):
     subprocess.run(cmd, check=True)
 
 
+def cutlass_include() -> str:
+    """CUTLASS / CuTe headers (only the UMMA descriptor types are used): the
+    copy vendored by the installed flashinfer or tilelang package."""
+    import importlib.util
+    for pkg, sub in (("flashinfer", ("data", "cutlass", "include")),
+                     ("tilelang", ("3rdparty", "cutlass", "include"))):
+        spec = importlib.util.find_spec(pkg)
+        if spec and spec.submodule_search_locations:
+            path = os.path.join(list(spec.submodule_search_locations)[0], *sub)
+            if os.path.exists(os.path.join(path, "cute", "arch", "mma_sm100_desc.hpp")):
+                return path
+    raise RuntimeError("CUTLASS headers with sm100 UMMA descriptors not found")
+
+
 def _compile(src, flags, verbose):
+    flags = [("-I" + cutlass_include()) if f == "@cutlass" else f for f in flags]
     os.makedirs(BUILD, exist_ok=True)
     path = os.path.join(CSRC, src)
     obj = os.path.join(BUILD, src + ".o")

@@ -1,0 +1,303 @@
+// BF16 tensor-core GEMM on sm_100a (tcgen05), FP32 accumulation in TMEM.
+//
+//   C[M x N] = A[M x K] . B[N x K]^T  (+ bias[N], optional ReLU)
+//
+// A and B are row-major with K contiguous ("K-major"), K a multiple of 64,
+// N a multiple of 128.  One CTA of 128 threads computes a 128 x 128 tile of
+// C over a K range (the whole K, or one split of it):
+//   - the 128 threads copy a 128 x 64 slice of A and of B into shared memory
+//     in the 128-byte-swizzled K-major layout that UMMA descriptors describe
+//     (16-byte chunk c of row r at r*128 + ((c ^ (r % 8)) * 16) inside a
+//     1024-byte-aligned tile), two stages so the next copy overlaps the MMAs;
+//   - one thread issues four tcgen05.mma (M = 128, N = 128, K = 16 each,
+//     kind::f16 with BF16 inputs) into a 128-column FP32 accumulator in TMEM
+//     and commits them to an mbarrier;
+//   - after the last slice, each warp reads its 32 TMEM lanes (one output row
+//     per thread) with tcgen05.ld and applies the epilogue.
+// Split-K launches write FP32 partial tiles that k_splitk_reduce sums in a
+// fixed order (deterministic).
+//
+// Every mbarrier wait is bounded; a wait that gives up sets ERR_TIMEOUT in the
+// error word, and the CTA still frees its TMEM before returning.
+#include <cuda_bf16.h>
+
+#include <cute/arch/mma_sm100_desc.hpp>
+#include <cute/numeric/numeric_types.hpp>
+
+#include "uph_internal.cuh"
+#include "uph_surrogate.h"
+
+namespace uph {
+
+constexpr int kTcM = 128;       // rows of C per CTA (UMMA M)
+constexpr int kTcN = 128;       // columns of C per CTA (UMMA N)
+constexpr int kTcBK = 64;       // K per shared-memory slice: one 128-byte swizzle atom row
+constexpr int kTcUmmaK = 16;    // K of one tcgen05.mma of kind::f16
+constexpr int kTcStages = 2;
+constexpr int kTcTileBytes = kTcM * kTcBK * 2;  // 16 KiB, same for the B slice (kTcN rows)
+constexpr int kTcSmemBytes = kTcStages * 2 * kTcTileBytes + 1024 + 64;
+constexpr long long kWaitLimit = 1LL << 26;     // ~1 s of polling
+
+struct TcGemmArgs {
+  const __nv_bfloat16 *A;
+  const __nv_bfloat16 *B;
+  int lda, ldb;              // elements
+  int M, N, K;               // K multiple of 64, N multiple of 128
+  int k_per_split;           // multiple of 64
+  const float *bias;         // [N] or null
+  int relu;
+  float *c_f32;              // [M x ldc] or null
+  __nv_bfloat16 *c_bf16;     // [M x ldc] or null
+  int ldc;
+  float *partials;           // split-K: [splits][M][N] FP32
+  unsigned *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr)
+{
+  // K-major, 128-byte swizzle: 8-row groups 1024 bytes apart (SBO), unit
+  // leading offset, Blackwell descriptor version
+  cute::UMMA::SmemDescriptor d;
+  d.desc_ = 0;
+  d.start_address_ = static_cast<uint16_t>(smem_addr >> 4);
+  d.leading_byte_offset_ = 1;
+  d.stride_byte_offset_ = 1024 >> 4;
+  d.version_ = 1;
+  d.base_offset_ = 0;
+  d.lbo_mode_ = 0;
+  d.layout_type_ = static_cast<uint8_t>(cute::UMMA::LayoutType::SWIZZLE_128B);
+  return d.desc_;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+  for (long long i = 0; i < kWaitLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// copies rows [r0, r0 + 128) x cols [k0, k0 + 64) of a row-major BF16 matrix
+// into the swizzled tile at `tile`; rows beyond `rows` read as zero
+__device__ __forceinline__ void load_tile(uint8_t *tile, const __nv_bfloat16 *src, int ld, int r0, int rows, int k0)
+{
+  const int t = threadIdx.x;
+  const int c = t & 7;  // 16-byte chunk of the row
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int r = (t >> 3) + 16 * i;
+    const int gr = r0 + r;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gr < rows) v = *reinterpret_cast<const uint4 *>(src + (size_t)gr * ld + k0 + c * 8);
+    *reinterpret_cast<uint4 *>(tile + r * 128 + ((c ^ (r & 7)) << 4)) = v;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
+{
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t mbar[kTcStages];
+  __shared__ uint32_t tmem_base_slot;
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int m0 = blockIdx.x * kTcM, n0 = blockIdx.y * kTcN;
+  const int kbeg = blockIdx.z * g.k_per_split;
+  const int kend = min(g.K, kbeg + g.k_per_split);
+  const int nslices = max(0, (kend - kbeg) / kTcBK);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (warp == 0) {  // TMEM: 128 FP32 columns for the 128 x 128 accumulator
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_slot)),
+                 "r"(kTcN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0)
+    for (int s = 0; s < kTcStages; s++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])));
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_slot;
+
+  const uint32_t idesc = static_cast<uint32_t>(cute::UMMA::make_instr_desc<cute::bfloat16_t, cute::bfloat16_t, float, kTcM, kTcN,
+                                                                            cute::UMMA::Major::K, cute::UMMA::Major::K>());
+  bool ok = true;
+  uint32_t phase[kTcStages] = {0u, 0u};
+  for (int s = 0; s < nslices && ok; s++) {
+    const int st = s % kTcStages;
+    uint8_t *ta = smem + st * 2 * kTcTileBytes;
+    uint8_t *tb = ta + kTcTileBytes;
+    // the stage's previous MMAs must be done before its tiles are overwritten
+    if (s >= kTcStages) {
+      ok = mbar_wait(smem_u32(&mbar[st]), phase[st]);
+      phase[st] ^= 1u;
+      if (!ok) break;
+    }
+    const int k0 = kbeg + s * kTcBK;
+    load_tile(ta, g.A, g.lda, m0, g.M, k0);
+    load_tile(tb, g.B, g.ldb, n0, g.N, k0);
+    // generic-proxy shared stores -> visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+      const uint32_t a_addr = smem_u32(ta), b_addr = smem_u32(tb);
+#pragma unroll
+      for (int kk = 0; kk < kTcBK / kTcUmmaK; kk++) {
+        // advancing K inside the 128-byte swizzle atom moves the start address
+        const uint64_t da = umma_desc_sw128(a_addr + kk * kTcUmmaK * 2);
+        const uint64_t db = umma_desc_sw128(b_addr + kk * kTcUmmaK * 2);
+        const uint32_t accumulate = (s > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            :
+            : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[st]))
+                   : "memory");
+    }
+  }
+  // wait for the MMAs still in flight: every stage that was used has exactly
+  // one commit the loop has not waited for (its last one)
+  for (int st = 0; st < kTcStages && ok; st++) {
+    if (nslices > st) {
+      if (!mbar_wait(smem_u32(&mbar[st]), phase[st])) ok = false;
+      phase[st] ^= 1u;
+    }
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(g.err, ERR_TIMEOUT);
+  } else {
+    // epilogue: warp w owns TMEM lanes [32w, 32w + 32) = rows m0 + 32w + lane
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    for (int c0 = 0; c0 < kTcN; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(lane_addr + c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < g.M && nslices > 0) {
+        const int col = n0 + c0;
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+        if (g.partials) {
+          float *dst = g.partials + ((size_t)blockIdx.z * g.M + row) * g.N + col;
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            if (g.bias) v[j] += g.bias[col + j];
+            if (g.relu) v[j] = fmaxf(v[j], 0.0f);
+          }
+          if (g.c_f32) {
+            float *dst = g.c_f32 + (size_t)row * g.ldc + col;
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+              *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+          }
+          if (g.c_bf16) {
+            __nv_bfloat16 *dst = g.c_bf16 + (size_t)row * g.ldc + col;
+            __align__(16) __nv_bfloat162 h[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<uint4 *>(&h[0]);
+            *reinterpret_cast<uint4 *>(dst + 8) = *reinterpret_cast<uint4 *>(&h[4]);
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN));
+}
+
+// out[m][n] (+)= sum over splits of partials[s][m][n], in split order
+__global__ void k_splitk_reduce(const float *__restrict__ partials, int splits, int M, int N, float *out,
+                                int accumulate)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M * N) return;
+  float acc = accumulate ? out[i] : 0.0f;
+  for (int s = 0; s < splits; s++) acc += partials[(size_t)s * M * N + i];
+  out[i] = acc;
+}
+
+}  // namespace uph
+
+using namespace uph;
+
+// Host launcher (C ABI for tests and the surrogate code): device pointers.
+// splits > 1 requires `partials` of splits * M * N floats and writes the sum
+// into c_f32 (accumulated onto its contents when accumulate != 0).
+extern "C" uph_status uph_tc_gemm_bf16(const void *A, int32_t lda, const void *B, int32_t ldb, int32_t M, int32_t N,
+                                       int32_t K, const float *bias, int32_t relu, float *c_f32, void *c_bf16,
+                                       int32_t ldc, int32_t splits, float *partials, int32_t accumulate,
+                                       unsigned *err, void *stream)
+{
+  if (!A || !B || !err || M <= 0 || N <= 0 || K <= 0) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: bad arguments");
+  if (K % kTcBK || N % kTcN) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: K must be a multiple of 64, N of 128");
+  if (lda % 8 || ldb % 8 || ldc % 8) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: leading dimensions must be multiples of 8");
+  if (splits < 1) splits = 1;
+  if (splits > 1 && (!partials || !c_f32 || bias || relu || c_bf16))
+    return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: split-K writes FP32 only, without bias or ReLU");
+  if (splits == 1 && !c_f32 && !c_bf16) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: no output");
+  cudaStream_t s = (cudaStream_t)stream;
+  static bool configured = false;
+  if (!configured) {
+    UPH_CUDA(cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
+    configured = true;
+  }
+  TcGemmArgs g;
+  g.A = (const __nv_bfloat16 *)A;
+  g.B = (const __nv_bfloat16 *)B;
+  g.lda = lda;
+  g.ldb = ldb;
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  int kps = K;
+  if (splits > 1) kps = ((K / kTcBK + splits - 1) / splits) * kTcBK;
+  g.k_per_split = kps;
+  splits = (K + kps - 1) / kps;
+  g.bias = bias;
+  g.relu = relu;
+  g.c_f32 = splits > 1 ? nullptr : c_f32;
+  g.c_bf16 = (__nv_bfloat16 *)c_bf16;
+  g.ldc = ldc;
+  g.partials = splits > 1 ? partials : nullptr;
+  g.err = err;
+  dim3 grid((M + kTcM - 1) / kTcM, N / kTcN, splits);
+  k_tc_gemm<<<grid, 128, kTcSmemBytes, s>>>(g);
+  if (splits > 1) {
+    if (ldc != N) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: split-K output must be dense (ldc == N)");
+    k_splitk_reduce<<<(M * N + 255) / 256, 256, 0, s>>>(partials, splits, M, N, c_f32, accumulate);
+  }
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
