@@ -30,14 +30,15 @@ def _exported(path):
 
 
 def test_libuph_exports_every_declared_symbol():
-    names = _declared("uph.h")
-    assert len(names) >= 18
+    names = _declared("uph.h") + _declared("uph_surrogate.h")
+    assert len(names) >= 30
     exported = _exported(_lib.LIB_PATH)
     missing = [n for n in names if n not in exported]
     assert not missing, missing
     l = _lib.lib()  # loads and binds every signature
     for n in names:
         assert hasattr(l, n)
+        assert n in _lib.SIGNATURES, n
 
 
 def test_libuph_sph_exports_dropin_symbols():

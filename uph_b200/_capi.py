@@ -146,3 +146,31 @@ def state_struct(arrays: dict, keepalive: list) -> UphState:
         keepalive.append(a)
         setattr(st, name, a.ctypes.data_as(IP if name == "itype" else DP))
     return st
+
+
+# ---- include/uph_surrogate.h -------------------------------------------------
+class SurConfig(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("macro_steps", C.c_int32), ("radius", C.c_double), ("dt", C.c_double),
+                ("rho0", C.c_double), ("vel_scale", C.c_double), ("rho_scale", C.c_double),
+                ("out_scale", C.c_double * 5)]
+
+
+class SurNodes(C.Structure):
+    _fields_ = [("n", C.c_int32), ("n_fluid", C.c_int32)] + \
+               [(k, C.c_void_p) for k in ("x", "y", "u", "v", "rho", "itype")] + \
+               [(k, C.c_double) for k in ("lo_x", "lo_y", "hi_x", "hi_y")]
+
+
+class SurJudge(C.Structure):
+    _fields_ = [("judge_every", C.c_int32), ("fallback_macro", C.c_int32), ("max_rho_err", C.c_double),
+                ("max_surface_err", C.c_double), ("depth", C.c_double), ("surface_x0", C.c_double),
+                ("surface_x1", C.c_double), ("surface_bins", C.c_int32)]
+
+
+class SurReport(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("macro_steps", "network_steps", "judged_steps", "failed_checks",
+                                         "plain_steps")] + \
+               [(k, C.c_double) for k in ("last_rho_err", "last_surface_err", "max_rho_err", "max_surface_err")]
+
+    def to_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}

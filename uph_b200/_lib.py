@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from ._capi import UphParams, UphStats
+from ._capi import SurConfig, SurJudge, SurNodes, SurReport, UphParams, UphStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libuph.so")
@@ -44,6 +44,22 @@ SIGNATURES = {
                                                C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2), C.c_int64,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
                                                C.c_void_p]),
+    # include/uph_surrogate.h
+    "uph_tc_gemm_bf16": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                   C.c_int32, C.c_void_p, C.c_void_p]),
+    "uph_sur_create": (C.c_int, [C.POINTER(SurConfig), C.c_int32, C.POINTER(C.c_void_p)]),
+    "uph_sur_destroy": (C.c_int, [C.c_void_p]),
+    "uph_sur_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "uph_sur_param_count": (C.c_int64, [C.c_int32]),
+    "uph_sur_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "uph_sur_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "uph_sur_reset_optimizer": (C.c_int, [C.c_void_p]),
+    "uph_sur_forward": (C.c_int, [C.c_void_p, C.POINTER(SurNodes), C.c_void_p]),
+    "uph_sur_gradients": (C.c_int, [C.c_void_p, C.POINTER(SurNodes), C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_double)]),
+    "uph_sur_adam": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "uph_sur_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(SurJudge), C.POINTER(SurReport)]),
     "uph_status_string": (C.c_char_p, [C.c_int]),
     "uph_last_error": (C.c_char_p, []),
 }

@@ -18,11 +18,11 @@
 #include <vector>
 
 #include "pass_common.cuh"
+#include "sim_access.cuh"
 
 using namespace uph;
 
 namespace uph {
-int scan_block_sums_needed(int n);
 }
 
 namespace {
@@ -91,6 +91,9 @@ struct uph_sim {
   // tuning: storage re-sort interval and the grid arrays' capacity in cells
   int reorder_interval = kReorderInterval;
   long long grid_capacity = 0;
+  // the fluid state was replaced from outside (the learned surrogate): the
+  // next step starts the leapfrog afresh with the first-step half kick
+  bool restart = false;
 };
 
 namespace {
@@ -636,6 +639,7 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
   UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, q));
   s->steps_since_reorder = 0;
   s->have_rates = false;
+  s->restart = false;
   return check_error_word(s);
 }
 
@@ -691,9 +695,10 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
   int swaps = 0;
   for (int k = 0; k < nsteps; k++) {
     const int itime = ++s->itime;
+    const bool first = itime == 1 || (k == 0 && s->restart);
     // the predictor of steps after the first of this call ran inside the
     // previous step's corrector
-    if (itime != 1 && k == 0) {
+    if (!first && k == 0) {
       Timer tm(s, KF_PREDICT);
       launch_predict(s->P, s->S, s->stream);
       s->launches++;
@@ -703,11 +708,12 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
       launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->stream);
       s->launches++;
     }
-    uph_status r = rate_pass(s, itime == 1);
+    uph_status r = rate_pass(s, first);
     if (r != UPH_OK) return r;
+    if (k == 0) s->restart = false;
     {
       Timer tm(s, KF_CORRECT);
-      launch_correct(s->P, s->S, itime == 1, k + 1 < nsteps, s->d_err, s->d_itime, s->stream);
+      launch_correct(s->P, s->S, first, k + 1 < nsteps, s->d_err, s->d_itime, s->stream);
       s->launches++;
     }
     if (++s->steps_since_reorder >= s->reorder_interval) {
@@ -745,7 +751,7 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
   if (nsteps < 0) return fail(UPH_BAD_ARG, "negative step count");
   // graph replay: a call of exactly graph_steps steps that is not the
   // simulation's first step and starts on the buffer the graph was recorded on
-  if (s->graph_steps > 0 && nsteps == s->graph_steps && s->itime >= 1 && !s->profiling) {
+  if (s->graph_steps > 0 && nsteps == s->graph_steps && s->itime >= 1 && !s->profiling && !s->restart) {
     if (s->graph_exec && s->graph_buffer != s->S.x) drop_graph(s);
     if (!s->graph_exec) {
       const int itime0 = s->itime, since0 = s->steps_since_reorder;
@@ -1312,3 +1318,44 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
   uph_sim_destroy(s);
   return r;
 }
+
+// ---- access for the learned surrogate (sim_access.cuh) ----------------------
+namespace uph {
+
+SimView sim_view(uph_sim *s)
+{
+  SimView v;
+  v.P = s->P;
+  v.S = s->S;
+  v.W = s->W;
+  v.stream = s->stream;
+  v.err = s->d_err;
+  v.itime = s->itime;
+  v.walls_move = walls_move(s);
+  return v;
+}
+
+uph_status sim_jump(uph_sim *s, int nsteps)
+{
+  s->itime += nsteps;
+  UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+  // the moving walls at the new time, as after a step that ended there
+  if (walls_move(s)) {
+    launch_wall_motion(s->P, s->S, s->W, s->itime * s->P.dt, nullptr, s->stream);
+    s->launches++;
+  }
+  s->restart = true;
+  s->steps_since_reorder += nsteps;
+  if (s->steps_since_reorder >= s->reorder_interval) {
+    uph_status r = reorder_fluid(s);
+    if (r != UPH_OK) return r;
+  }
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+uph_status sim_check(uph_sim *s) { return check_error_word(s); }
+
+void sim_count_launches(uph_sim *s, int n) { s->launches += n; }
+
+}  // namespace uph

@@ -1,0 +1,32 @@
+// What the learned surrogate needs of a simulation: its slot arrays and
+// constants, and a way to hand the simulation back a fluid state it did not
+// compute itself.
+#pragma once
+
+#include "uph_internal.cuh"
+
+struct uph_sim;
+
+namespace uph {
+
+struct SimView {
+  DevParams P;
+  SlotArrays S;   // current storage buffers (they swap at every re-sort)
+  WallTable W;
+  cudaStream_t stream;
+  unsigned *err;
+  int itime;      // steps completed
+  bool walls_move;
+};
+
+SimView sim_view(uph_sim *s);
+// The fluid state in the slots now belongs to `nsteps` steps later: advance
+// the step counters, put the moving walls at the new time, restart the
+// leapfrog at the next step (first-step half kick, as after an upload) and
+// keep the storage re-sort schedule.
+uph_status sim_jump(uph_sim *s, int nsteps);
+// the device error word as a status (synchronises the stream; the word is sticky)
+uph_status sim_check(uph_sim *s);
+void sim_count_launches(uph_sim *s, int n);
+
+}  // namespace uph

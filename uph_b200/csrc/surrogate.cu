@@ -1,0 +1,1202 @@
+// Learned surrogate (include/uph_surrogate.h): the message-passing network's
+// forward and backward passes, Adam, and the judged coupling to a simulation.
+//
+// Data layout in HBM, nodes row-major (one row per node, padded to 128
+// columns where a tensor-core K granule needs it):
+//   graph   nbr[n][32] int32 partners (ascending), ef[n][32] float4 (dx, dy, r)/R
+//   F[n][128] BF16 features, a1[n][128] BF16, h[n][128] FP32 (residual stream)
+//   per round: cat[n][256] BF16 = [h | m], PQ[n][256] BF16, S[n][128] BF16,
+//              u[n][128] BF16
+//   out[n][128] FP32 (5 columns used)
+// Node-local layers are BF16 GEMMs on the tcgen05 tensor cores (tc_gemm.cu).
+// The edge layer is a warp per receiving node: lane l owns channels
+// [4l, 4l + 4); partner indices and edge features are loaded by lane k for
+// partner k and broadcast by shuffles; Q_j rows are 256-byte coalesced
+// gathers (the slot order is spatially sorted, so they mostly hit L2).
+// Sums over partners run in ascending partner order and all reductions
+// (bias and W_e gradients, loss) use fixed grids and fixed orders, so a
+// forward/backward pass is bitwise reproducible.
+#include <cuda_bf16.h>
+#include <float.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "sim_access.cuh"
+#include "uph_internal.cuh"
+#include "uph_surrogate.h"
+
+namespace uph {
+namespace {
+
+constexpr int kLat = UPH_SUR_LATENT;
+constexpr int kFeat = 128;
+constexpr int kOutPad = 128;
+constexpr int kNOut = UPH_SUR_OUTPUTS;
+constexpr int kMaxDeg = UPH_SUR_MAX_DEGREE;
+constexpr int kMaxRounds = UPH_SUR_MAX_ROUNDS;
+constexpr int kEdgeThreads = 256;           // 8 warps
+constexpr int kEdgeBlocks = 148 * 4;        // fixed grid: per-warp partials in a fixed order
+constexpr int kEdgeWarps = kEdgeBlocks * (kEdgeThreads / 32);
+constexpr int kColBlocks = 148 * 2;         // bias-gradient partial sums
+constexpr int kSplitMax = 148;              // split-K CTAs of one weight-gradient GEMM tile
+constexpr int kLossBlocks = 148;
+constexpr int kMaxBins = 4096;
+
+typedef __nv_bfloat16 bf16;
+
+// ---- parameter layout --------------------------------------------------------
+struct RoundOff {
+  size_t pq_w, pq_b, we, w2, n1_w, n1_b, n2_w, n2_b;
+};
+struct ParamOff {
+  size_t enc1_w, enc1_b, enc2_w, enc2_b;
+  RoundOff r[kMaxRounds];
+  size_t dec1_w, dec1_b, dec2_w, dec2_b;
+  size_t total;
+};
+
+ParamOff param_layout(int rounds)
+{
+  ParamOff o{};
+  size_t p = 0;
+  auto take = [&](size_t n) {
+    size_t at = p;
+    p += n;
+    return at;
+  };
+  o.enc1_w = take(kLat * kFeat);
+  o.enc1_b = take(kLat);
+  o.enc2_w = take(kLat * kLat);
+  o.enc2_b = take(kLat);
+  for (int r = 0; r < rounds; r++) {
+    o.r[r].pq_w = take(2 * kLat * kLat);
+    o.r[r].pq_b = take(2 * kLat);
+    o.r[r].we = take(kLat * 4);
+    o.r[r].w2 = take(kLat * kLat);
+    o.r[r].n1_w = take(kLat * 2 * kLat);
+    o.r[r].n1_b = take(kLat);
+    o.r[r].n2_w = take(kLat * kLat);
+    o.r[r].n2_b = take(kLat);
+  }
+  o.dec1_w = take(kLat * kLat);
+  o.dec1_b = take(kLat);
+  o.dec2_w = take(kOutPad * kLat);
+  o.dec2_b = take(kOutPad);
+  o.total = p;
+  return o;
+}
+
+// ---- small device helpers ------------------------------------------------------
+__device__ __forceinline__ void load_bf16x4(const bf16 *p, float out[4])
+{
+  const uint2 raw = *reinterpret_cast<const uint2 *>(p);
+  const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162 *>(&raw.x);
+  const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162 *>(&raw.y);
+  const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+  out[0] = fa.x;
+  out[1] = fa.y;
+  out[2] = fb.x;
+  out[3] = fb.y;
+}
+
+__device__ __forceinline__ void store_bf16x4(bf16 *p, const float v[4])
+{
+  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]);
+  __nv_bfloat162 b = __floats2bfloat162_rn(v[2], v[3]);
+  uint2 raw;
+  raw.x = *reinterpret_cast<uint32_t *>(&a);
+  raw.y = *reinterpret_cast<uint32_t *>(&b);
+  *reinterpret_cast<uint2 *>(p) = raw;
+}
+
+// the edge pre-activation, one fixed operation order shared by the forward
+// and backward kernels so both see bit-identical values
+__device__ __forceinline__ float edge_z(float p, float q, const float4 &w, float e0, float e1, float e2)
+{
+  return __fmaf_rn(w.z, e2, __fmaf_rn(w.y, e1, __fmaf_rn(w.x, e0, __fadd_rn(p, q))));
+}
+
+// ---- graph --------------------------------------------------------------------
+// partners of every node within R (DBL_EPSILON < r^2 < R^2), ascending, and
+// their edge features (dx, dy, r) / R in FP32
+__global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const double *__restrict__ y, int n,
+                            const int *__restrict__ cell_of, const int *__restrict__ start,
+                            const int *__restrict__ list, double R, int *__restrict__ nbr,
+                            float4 *__restrict__ ef, int *__restrict__ deg, unsigned *err)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double xi = x[i], yi = y[i];
+  const double r2cut = R * R;
+  const int c = cell_of[i];
+  const int cx = c % G.ncx, cy = c / G.ncx;
+  int cand[kMaxDeg];
+  int cnt = 0;
+  for (int oy = -1; oy <= 1; oy++) {
+    const int yy = cy + oy;
+    if (yy < 0 || yy >= G.ncy) continue;
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, G.ncx - 1);
+    const int a = start[yy * G.ncx + x0], b = start[yy * G.ncx + x1 + 1];
+    for (int k = a; k < b; k++) {
+      const int j = list[k];
+      const double dx = x[j] - xi, dy = y[j] - yi;
+      const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+      if (r2 > DBL_EPSILON && r2 < r2cut) {
+        if (cnt < kMaxDeg) cand[cnt] = j;
+        cnt++;
+      }
+    }
+  }
+  if (cnt > kMaxDeg) {
+    atomicOr(err, ERR_NEIGHBOR_OVERFLOW);
+    cnt = kMaxDeg;
+  }
+  for (int a = 1; a < cnt; a++) {
+    const int v = cand[a];
+    int b = a - 1;
+    while (b >= 0 && cand[b] > v) {
+      cand[b + 1] = cand[b];
+      b--;
+    }
+    cand[b + 1] = v;
+  }
+  for (int k = 0; k < cnt; k++) {
+    const int j = cand[k];
+    const double dx = x[j] - xi, dy = y[j] - yi;
+    const double r = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+    nbr[(size_t)i * kMaxDeg + k] = j;
+    ef[(size_t)i * kMaxDeg + k] = make_float4((float)(dx / R), (float)(dy / R), (float)(r / R), 0.0f);
+  }
+  deg[i] = cnt;
+}
+
+// ---- features -----------------------------------------------------------------
+__global__ void k_sur_features(int n, const double *__restrict__ u, const double *__restrict__ v,
+                               const double *__restrict__ rho, const int32_t *__restrict__ itype, double vel_scale,
+                               double rho0, double rho_scale, bf16 *__restrict__ F, unsigned *err)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int t = itype[i];
+  float f[8];
+  f[0] = (float)(u[i] / vel_scale);
+  f[1] = (float)(v[i] / vel_scale);
+  f[2] = (float)((rho[i] / rho0 - 1.0) / rho_scale);
+  f[3] = t == 1 ? 1.0f : 0.0f;
+  f[4] = (t != 1 && t != 3) ? 1.0f : 0.0f;
+  f[5] = t == 3 ? 1.0f : 0.0f;
+  f[6] = 0.0f;
+  f[7] = 0.0f;
+  if (!isfinite(f[0]) || !isfinite(f[1]) || !isfinite(f[2])) atomicOr(err, ERR_NAN);
+  __align__(16) __nv_bfloat162 h[4];
+  for (int k = 0; k < 4; k++) h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+  uint4 *row = reinterpret_cast<uint4 *>(F + (size_t)i * kFeat);
+  row[0] = *reinterpret_cast<uint4 *>(&h[0]);
+  for (int k = 1; k < kFeat / 8; k++) row[k] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// ---- edge layer -----------------------------------------------------------------
+// S_i = sum_j relu(P_i + Q_j + W_e e_ij), PQ rows = [P | Q]
+__global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16 *__restrict__ PQ,
+                                                                 const float *__restrict__ we,
+                                                                 const int *__restrict__ nbr,
+                                                                 const float4 *__restrict__ ef,
+                                                                 const int *__restrict__ deg, bf16 *__restrict__ S)
+{
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int c0 = lane * 4;
+  float4 w[4];
+  for (int c = 0; c < 4; c++) w[c] = *reinterpret_cast<const float4 *>(we + (c0 + c) * 4);
+  for (int i = gw; i < n; i += nw) {
+    const int d = deg[i];
+    int myj = 0;
+    float4 mye = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane < d) {
+      myj = nbr[(size_t)i * kMaxDeg + lane];
+      mye = ef[(size_t)i * kMaxDeg + lane];
+    }
+    float p[4], acc[4] = {0.f, 0.f, 0.f, 0.f};
+    load_bf16x4(PQ + (size_t)i * 2 * kLat + c0, p);
+    for (int k = 0; k < d; k++) {
+      const int j = __shfl_sync(0xffffffffu, myj, k);
+      const float e0 = __shfl_sync(0xffffffffu, mye.x, k);
+      const float e1 = __shfl_sync(0xffffffffu, mye.y, k);
+      const float e2 = __shfl_sync(0xffffffffu, mye.z, k);
+      float q[4];
+      load_bf16x4(PQ + (size_t)j * 2 * kLat + kLat + c0, q);
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[c] = __fadd_rn(acc[c], fmaxf(edge_z(p[c], q[c], w[c], e0, e1, e2), 0.0f));
+    }
+    store_bf16x4(S + (size_t)i * kLat + c0, acc);
+  }
+}
+
+// gradients of the edge layer, node a as receiver (dP_a, dW_e) and as sender
+// (dQ_a, through every partner b that receives from a: the graph is
+// symmetric and e_ba = (-e_ab.x, -e_ab.y, e_ab.z))
+__global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16 *__restrict__ PQ,
+                                                                 const float *__restrict__ we,
+                                                                 const int *__restrict__ nbr,
+                                                                 const float4 *__restrict__ ef,
+                                                                 const int *__restrict__ deg,
+                                                                 const float *__restrict__ dS, bf16 *__restrict__ dPQ,
+                                                                 float *__restrict__ we_part)
+{
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int c0 = lane * 4;
+  float4 w[4];
+  for (int c = 0; c < 4; c++) w[c] = *reinterpret_cast<const float4 *>(we + (c0 + c) * 4);
+  float g[4][3];
+  for (int c = 0; c < 4; c++) g[c][0] = g[c][1] = g[c][2] = 0.0f;
+  for (int a = gw; a < n; a += nw) {
+    const int d = deg[a];
+    int myj = 0;
+    float4 mye = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane < d) {
+      myj = nbr[(size_t)a * kMaxDeg + lane];
+      mye = ef[(size_t)a * kMaxDeg + lane];
+    }
+    float pa[4], qa[4];
+    load_bf16x4(PQ + (size_t)a * 2 * kLat + c0, pa);
+    load_bf16x4(PQ + (size_t)a * 2 * kLat + kLat + c0, qa);
+    const float4 dsa4 = *reinterpret_cast<const float4 *>(dS + (size_t)a * kLat + c0);
+    const float dsa[4] = {dsa4.x, dsa4.y, dsa4.z, dsa4.w};
+    float dp[4] = {0.f, 0.f, 0.f, 0.f}, dq[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < d; k++) {
+      const int b = __shfl_sync(0xffffffffu, myj, k);
+      const float e0 = __shfl_sync(0xffffffffu, mye.x, k);
+      const float e1 = __shfl_sync(0xffffffffu, mye.y, k);
+      const float e2 = __shfl_sync(0xffffffffu, mye.z, k);
+      float pb[4], qb[4];
+      load_bf16x4(PQ + (size_t)b * 2 * kLat + c0, pb);
+      load_bf16x4(PQ + (size_t)b * 2 * kLat + kLat + c0, qb);
+      const float4 dsb4 = *reinterpret_cast<const float4 *>(dS + (size_t)b * kLat + c0);
+      const float dsb[4] = {dsb4.x, dsb4.y, dsb4.z, dsb4.w};
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        if (edge_z(pa[c], qb[c], w[c], e0, e1, e2) > 0.0f) {
+          dp[c] += dsa[c];
+          g[c][0] = __fmaf_rn(dsa[c], e0, g[c][0]);
+          g[c][1] = __fmaf_rn(dsa[c], e1, g[c][1]);
+          g[c][2] = __fmaf_rn(dsa[c], e2, g[c][2]);
+        }
+        if (edge_z(pb[c], qa[c], w[c], -e0, -e1, e2) > 0.0f) dq[c] += dsb[c];
+      }
+    }
+    store_bf16x4(dPQ + (size_t)a * 2 * kLat + c0, dp);
+    store_bf16x4(dPQ + (size_t)a * 2 * kLat + kLat + c0, dq);
+  }
+  float *dst = we_part + (size_t)gw * kLat * 4;
+  for (int c = 0; c < 4; c++)
+    *reinterpret_cast<float4 *>(dst + (c0 + c) * 4) = make_float4(g[c][0], g[c][1], g[c][2], 0.0f);
+}
+
+// out[c] = sum over rows r (in order) of part[r][c]
+__global__ void k_sum_rows(const float *__restrict__ part, int rows, int cols, float *__restrict__ out)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; r++) s += part[(size_t)r * cols + c];
+  out[c] = s;
+}
+
+// column sums of a BF16 [n x cols] block (ld >= cols): per-block partials
+__global__ void k_colsum_part(const bf16 *__restrict__ src, int ld, int cols, int n, int rows_per_block,
+                              float *__restrict__ part)
+{
+  const int c = threadIdx.x;
+  if (c >= cols) return;
+  const int r0 = blockIdx.x * rows_per_block, r1 = min(n, r0 + rows_per_block);
+  float s = 0.0f;
+  for (int r = r0; r < r1; r++) s += __bfloat162float(src[(size_t)r * ld + c]);
+  part[(size_t)blockIdx.x * cols + c] = s;
+}
+
+// mean squared error over the fluid rows' 5 outputs; dO = dL/dout in BF16
+// (zero outside the fluid rows and the 5 columns)
+__global__ void k_sur_loss(int n, int nf, const float *__restrict__ out, const float *__restrict__ target,
+                           float inv_count, bf16 *__restrict__ dO, float *__restrict__ part)
+{
+  __shared__ float red[256];
+  float s = 0.0f;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    float gr[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (r < nf) {
+      for (int c = 0; c < kNOut; c++) {
+        const float d = out[(size_t)r * kOutPad + c] - target[(size_t)r * kNOut + c];
+        s += d * d;
+        gr[c] = 2.0f * d * inv_count;
+      }
+    }
+    __align__(16) __nv_bfloat162 h[4];
+    for (int k = 0; k < 4; k++) h[k] = __floats2bfloat162_rn(gr[2 * k], gr[2 * k + 1]);
+    uint4 *row = reinterpret_cast<uint4 *>(dO + (size_t)r * kOutPad);
+    row[0] = *reinterpret_cast<uint4 *>(&h[0]);
+    for (int k = 1; k < kOutPad / 8; k++) row[k] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0] * inv_count;
+}
+
+__global__ void k_f32_to_bf16(const float *__restrict__ src, bf16 *__restrict__ dst, size_t count)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+__global__ void k_copy_out(int n, const float *__restrict__ out, float *__restrict__ dst)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * kNOut) return;
+  dst[i] = out[(size_t)(i / kNOut) * kOutPad + i % kNOut];
+}
+
+// sum of squared gradients, per-block partials
+__global__ void k_sumsq_part(const float *__restrict__ g, size_t count, float *__restrict__ part)
+{
+  __shared__ float red[256];
+  float s = 0.0f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    s += g[i] * g[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// Adam (bias-corrected), optional global-norm clipping from *sumsq; writes
+// the FP32 master weights and their BF16 copy
+__global__ void k_adam(size_t count, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, bf16 *__restrict__ wb, float lr, float b1, float b2, float eps,
+                       float c1, float c2, const float *__restrict__ sumsq, float clip)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  float scale = 1.0f;
+  if (clip > 0.0f) {
+    const float norm = sqrtf(*sumsq);
+    if (norm > clip) scale = clip / norm;
+  }
+  const float gi = g[i] * scale;
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  w[i] = wi;
+  wb[i] = __float2bfloat16_rn(wi);
+}
+
+__device__ __forceinline__ double tait_p(const DevParams &P, double rho)
+{
+  return P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
+}
+
+struct OutScale {
+  double T;      // macro_steps * dt
+  double s[kNOut];
+};
+
+// network step of the fluid slots: the new state in place (pred == null) or
+// into pred[orig][5] = (x, y, u, v, rho) for the judge
+__global__ void k_sur_apply(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
+                            double *__restrict__ pred, unsigned *err)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const float *o = out + (size_t)a * kOutPad;
+  const double u = S.u[a], v = S.v[a];
+  const double x = S.x[a] + sc.T * u + sc.s[0] * o[0];
+  const double y = S.y[a] + sc.T * v + sc.s[1] * o[1];
+  const double un = u + sc.s[2] * o[2];
+  const double vn = v + sc.s[3] * o[3];
+  const double rho = S.rho[a] + sc.s[4] * o[4];
+  if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !isfinite(rho) || rho <= 0.0)
+    atomicOr(err, ERR_NAN);
+  if (pred) {
+    double *q = pred + (size_t)S.orig[a] * kNOut;
+    q[0] = x;
+    q[1] = y;
+    q[2] = un;
+    q[3] = vn;
+    q[4] = rho;
+    return;
+  }
+  const double p = tait_p(P, rho);
+  S.x[a] = x;
+  S.y[a] = y;
+  S.u[a] = un;
+  S.v[a] = vn;
+  S.ut[a] = un;
+  S.vt[a] = vn;
+  S.rho[a] = rho;
+  S.rhot[a] = rho;
+  S.p[a] = p;
+  S.pt[a] = p;
+  S.pressure[a] = p;
+}
+
+__device__ __forceinline__ unsigned ordered_bits(float f)
+{
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// the judge: density error of the network's prediction against the plain
+// solver's state (per particle, matched by reference index) and the highest
+// fluid particle of both in every x-bin
+__global__ void k_sur_judge(DevParams P, SlotArrays S, const double *__restrict__ pred, double x0, double inv_bin,
+                            int nbins, unsigned *__restrict__ bins_plain, unsigned *__restrict__ bins_pred,
+                            double *__restrict__ part)
+{
+  __shared__ double red_s[256], red_m[256];
+  double sq = 0.0, mx = 0.0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.nf; a += gridDim.x * blockDim.x) {
+    const double *q = pred + (size_t)S.orig[a] * kNOut;
+    const double rp = S.rho[a];
+    const double rel = (q[4] - rp) / rp;
+    sq += rel * rel;
+    mx = fmax(mx, fabs(rel));
+    const double bp = floor((S.x[a] - x0) * inv_bin), bq = floor((q[0] - x0) * inv_bin);
+    if (bp >= 0.0 && bp < nbins) atomicMax(&bins_plain[(int)bp], ordered_bits((float)S.y[a]));
+    if (bq >= 0.0 && bq < nbins) atomicMax(&bins_pred[(int)bq], ordered_bits((float)q[1]));
+  }
+  red_s[threadIdx.x] = sq;
+  red_m[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      red_s[threadIdx.x] += red_s[threadIdx.x + o];
+      red_m[threadIdx.x] = fmax(red_m[threadIdx.x], red_m[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = red_s[0];
+    part[2 * blockIdx.x + 1] = red_m[0];
+  }
+}
+constexpr int kJudgeBlocks = 296;
+
+struct NodesView {
+  int n, nf;
+  const double *x, *y, *u, *v, *rho;
+  const int32_t *itype;
+  double lo_x, lo_y, hi_x, hi_y;
+};
+
+}  // namespace
+}  // namespace uph
+
+using namespace uph;
+
+struct uph_surrogate {
+  uph_sur_config cfg;
+  ParamOff off;
+  int cap = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocs;
+  unsigned *d_err = nullptr;
+  // parameters: FP32 master, BF16 copy, gradient, Adam moments
+  float *w = nullptr, *g = nullptr, *am = nullptr, *av = nullptr;
+  bf16 *wb = nullptr;
+  int adam_t = 0;
+  // graph
+  CellGrid grid{};
+  long long grid_cap = 0;
+  int *nbr = nullptr, *deg = nullptr;
+  float4 *ef = nullptr;
+  // activations
+  bf16 *F = nullptr, *a1 = nullptr, *d1 = nullptr;
+  float *h = nullptr, *out = nullptr;
+  bf16 *cat[kMaxRounds + 1] = {}, *PQ[kMaxRounds] = {}, *S[kMaxRounds] = {}, *u[kMaxRounds] = {};
+  // backward
+  bf16 *dO = nullptr, *dz = nullptr, *dhb = nullptr, *dm = nullptr, *dPQ = nullptr;
+  float *dh = nullptr, *dS = nullptr;
+  float *partials = nullptr, *colpart = nullptr, *wepart = nullptr, *losspart = nullptr, *lossval = nullptr;
+  float *sqpart = nullptr, *sumsq = nullptr;
+  // judge
+  double *pred = nullptr, *jpart = nullptr;
+  unsigned *bins = nullptr;
+  int n_pred = 0;
+  int n_last = 0, nf_last = 0;
+  bool have_grad = false;
+  // judged coupling: macro steps since the last check, plain macro steps left
+  int since_judge = 0;
+  int fallback_left = 0;
+  const uph_sim *last_sim = nullptr;  // the schedule restarts for another simulation
+};
+
+namespace {
+
+template <typename T>
+cudaError_t salloc(uph_surrogate *s, T **p, size_t count)
+{
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+  if (e == cudaSuccess) s->allocs.push_back((void *)*p);
+  return e;
+}
+
+void free_all(uph_surrogate *s)
+{
+  for (void *p : s->allocs) cudaFree(p);
+  s->allocs.clear();
+}
+
+uph_status ensure_grid(uph_surrogate *s, long long ncell)
+{
+  if (ncell <= s->grid_cap) return UPH_OK;
+  // only the cell-sized arrays grow; list and cell_of are node-sized (create)
+  for (void *p : {(void *)s->grid.count, (void *)s->grid.start, (void *)s->grid.fill, (void *)s->grid.block_sums})
+    if (p) cudaFree(p);
+  s->grid.count = s->grid.start = s->grid.fill = s->grid.block_sums = nullptr;
+  s->grid_cap = 0;
+  const long long cap = ncell + ncell / 4 + 1024;
+  if (cap > (1LL << 30)) return fail(UPH_BAD_ARG, "surrogate: node box too large for the graph grid");
+  UPH_CUDA(cudaMalloc((void **)&s->grid.count, sizeof(int) * cap));
+  UPH_CUDA(cudaMalloc((void **)&s->grid.start, sizeof(int) * (cap + 1)));
+  UPH_CUDA(cudaMalloc((void **)&s->grid.fill, sizeof(int) * cap));
+  const int nb = scan_block_sums_needed((int)cap + 1);
+  UPH_CUDA(cudaMalloc((void **)&s->grid.block_sums, sizeof(int) * (nb + 1)));
+  s->grid.nblock_sums = nb;
+  s->grid_cap = cap;
+  return UPH_OK;
+}
+
+uph_status check_err(uph_surrogate *s)
+{
+  unsigned err = 0;
+  UPH_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  UPH_CUDA(cudaGetLastError());
+  if (err & ERR_NEIGHBOR_OVERFLOW)
+    return fail(UPH_NEIGHBOR_OVERFLOW, "surrogate: a node has more than 32 graph partners");
+  if (err & ERR_NAN) return fail(UPH_NAN, "surrogate: a non-finite value in the node state or prediction");
+  if (err & ERR_OUT_OF_DOMAIN) return fail(UPH_OUT_OF_DOMAIN, "surrogate: a node lies outside the given box");
+  if (err & ERR_TIMEOUT) return fail(UPH_TIMEOUT, "surrogate: a tensor-core wait timed out");
+  return UPH_OK;
+}
+
+// graph + features for `nv`
+uph_status prepare(uph_surrogate *s, const NodesView &nv)
+{
+  if (nv.n <= 0 || nv.n > s->cap || nv.nf < 0 || nv.nf > nv.n)
+    return fail(UPH_BAD_ARG, "surrogate: node count outside [1, capacity]");
+  if (!(nv.hi_x > nv.lo_x) || !(nv.hi_y > nv.lo_y)) return fail(UPH_BAD_ARG, "surrogate: empty node box");
+  cudaStream_t q = s->stream;
+  const double R = s->cfg.radius;
+  DevParams G{};
+  G.lo_x = nv.lo_x;
+  G.lo_y = nv.lo_y;
+  G.hi_x = nv.hi_x;
+  G.hi_y = nv.hi_y;
+  G.cell = R;
+  G.inv_cell = 1.0 / R;
+  G.ncx = (int)ceil((nv.hi_x - nv.lo_x) / R) + 1;
+  G.ncy = (int)ceil((nv.hi_y - nv.lo_y) / R) + 1;
+  G.tile = 1;
+  G.ntx = G.ncx;
+  const long long ncell = (long long)G.ncx * G.ncy;
+  uph_status r = ensure_grid(s, ncell);
+  if (r != UPH_OK) return r;
+  CellGrid &g = s->grid;
+  g.ncell = (int)ncell;
+  UPH_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * ncell, q));
+  UPH_CUDA(cudaMemsetAsync(g.fill, 0, sizeof(int) * ncell, q));
+  launch_cell_keys(G, nv.x, nv.y, 0, nv.n, g, s->d_err, false, q);
+  launch_exclusive_scan(g.count, g.start, (int)ncell, g.block_sums, q);
+  launch_cell_scatter(g, 0, nv.n, q);
+  launch_cell_sort_segments(g, q);
+  k_sur_graph<<<(nv.n + 127) / 128, 128, 0, q>>>(G, nv.x, nv.y, nv.n, g.cell_of, g.start, g.list, R, s->nbr, s->ef,
+                                                 s->deg, s->d_err);
+  k_sur_features<<<(nv.n + 255) / 256, 256, 0, q>>>(nv.n, nv.u, nv.v, nv.rho, nv.itype, s->cfg.vel_scale,
+                                                     s->cfg.rho0, s->cfg.rho_scale, s->F, s->d_err);
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+struct Gemm {
+  GemmCall c;
+  Gemm(const void *A, int lda, const void *B, int ldb, int M, int N, int K)
+  {
+    c.A = A;
+    c.lda = lda;
+    c.B = B;
+    c.ldb = ldb;
+    c.M = M;
+    c.N = N;
+    c.K = K;
+  }
+};
+
+uph_status run(uph_surrogate *s, GemmCall c)
+{
+  c.err = s->d_err;
+  return launch_tc_gemm(c, s->stream);
+}
+
+// weight gradient dW[M x N] = sum over nodes of dY[node][M-index] X[node][N-index]
+uph_status wgrad(uph_surrogate *s, const bf16 *dY, int ldy, int M, const bf16 *X, int ldx, int N, int n, float *dst)
+{
+  GemmCall c;
+  c.A = dY;
+  c.lda = ldy;
+  c.a_trans = 1;
+  c.B = X;
+  c.ldb = ldx;
+  c.b_trans = 1;
+  c.M = M;
+  c.N = N;
+  c.K = (n + 63) / 64 * 64;
+  c.k_valid = n;
+  const int tiles = (M / 128) * (N / 128);
+  c.splits = std::max(1, std::min(kSplitMax / tiles, c.K / 64));
+  c.partials = s->partials;
+  c.c_f32 = dst;
+  c.ldc = N;
+  return run(s, c);
+}
+
+uph_status colsum(uph_surrogate *s, const bf16 *src, int ld, int cols, int n, float *dst)
+{
+  const int rpb = (n + kColBlocks - 1) / kColBlocks;
+  k_colsum_part<<<kColBlocks, cols, 0, s->stream>>>(src, ld, cols, n, rpb, s->colpart);
+  k_sum_rows<<<(cols + 127) / 128, 128, 0, s->stream>>>(s->colpart, kColBlocks, cols, dst);
+  return UPH_OK;
+}
+
+#define TRYS(x)                     \
+  do {                              \
+    uph_status r_ = (x);            \
+    if (r_ != UPH_OK) return r_;    \
+  } while (0)
+
+uph_status forward_net(uph_surrogate *s, int n)
+{
+  const ParamOff &o = s->off;
+  const float *W = s->w;
+  const bf16 *Wb = s->wb;
+  cudaStream_t q = s->stream;
+  {
+    GemmCall c;
+    c.A = s->F; c.lda = kFeat; c.B = Wb + o.enc1_w; c.ldb = kFeat;
+    c.M = n; c.N = kLat; c.K = kFeat;
+    c.bias = W + o.enc1_b; c.relu = 1; c.c_bf16 = s->a1; c.ldc = kLat;
+    TRYS(run(s, c));
+  }
+  {
+    GemmCall c;
+    c.A = s->a1; c.lda = kLat; c.B = Wb + o.enc2_w; c.ldb = kLat;
+    c.M = n; c.N = kLat; c.K = kLat;
+    c.bias = W + o.enc2_b; c.c_f32 = s->h; c.ldc = kLat; c.c_bf16 = s->cat[0]; c.ldc16 = 2 * kLat;
+    TRYS(run(s, c));
+  }
+  const int rounds = s->cfg.rounds;
+  for (int r = 0; r < rounds; r++) {
+    const RoundOff &ro = o.r[r];
+    {
+      GemmCall c;
+      c.A = s->cat[r]; c.lda = 2 * kLat; c.B = Wb + ro.pq_w; c.ldb = kLat;
+      c.M = n; c.N = 2 * kLat; c.K = kLat;
+      c.bias = W + ro.pq_b; c.c_bf16 = s->PQ[r]; c.ldc = 2 * kLat;
+      TRYS(run(s, c));
+    }
+    k_sur_edge_fwd<<<kEdgeBlocks, kEdgeThreads, 0, q>>>(n, s->PQ[r], W + ro.we, s->nbr, s->ef, s->deg, s->S[r]);
+    {
+      GemmCall c;
+      c.A = s->S[r]; c.lda = kLat; c.B = Wb + ro.w2; c.ldb = kLat;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.c_bf16 = s->cat[r] + kLat; c.ldc = 2 * kLat;
+      TRYS(run(s, c));
+    }
+    {
+      GemmCall c;
+      c.A = s->cat[r]; c.lda = 2 * kLat; c.B = Wb + ro.n1_w; c.ldb = 2 * kLat;
+      c.M = n; c.N = kLat; c.K = 2 * kLat;
+      c.bias = W + ro.n1_b; c.relu = 1; c.c_bf16 = s->u[r]; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+    {
+      GemmCall c;
+      c.A = s->u[r]; c.lda = kLat; c.B = Wb + ro.n2_w; c.ldb = kLat;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.bias = W + ro.n2_b; c.accumulate = 1; c.c_f32 = s->h; c.ldc = kLat;
+      c.c_bf16 = s->cat[r + 1]; c.ldc16 = 2 * kLat;
+      TRYS(run(s, c));
+    }
+  }
+  {
+    GemmCall c;
+    c.A = s->cat[rounds]; c.lda = 2 * kLat; c.B = Wb + o.dec1_w; c.ldb = kLat;
+    c.M = n; c.N = kLat; c.K = kLat;
+    c.bias = W + o.dec1_b; c.relu = 1; c.c_bf16 = s->d1; c.ldc = kLat;
+    TRYS(run(s, c));
+  }
+  {
+    GemmCall c;
+    c.A = s->d1; c.lda = kLat; c.B = Wb + o.dec2_w; c.ldb = kLat;
+    c.M = n; c.N = kOutPad; c.K = kLat;
+    c.bias = W + o.dec2_b; c.c_f32 = s->out; c.ldc = kOutPad;
+    TRYS(run(s, c));
+  }
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+// backward from dO (already in s->dO) to s->g
+uph_status backward_net(uph_surrogate *s, int n)
+{
+  const ParamOff &o = s->off;
+  const bf16 *Wb = s->wb;
+  float *G = s->g;
+  cudaStream_t q = s->stream;
+  const int rounds = s->cfg.rounds;
+  UPH_CUDA(cudaMemsetAsync(G, 0, sizeof(float) * o.total, q));
+  // decoder
+  TRYS(wgrad(s, s->dO, kOutPad, kOutPad, s->d1, kLat, kLat, n, G + o.dec2_w));
+  TRYS(colsum(s, s->dO, kOutPad, kOutPad, n, G + o.dec2_b));
+  {
+    GemmCall c;  // dz = (dO . Dec2) masked by d1 > 0
+    c.A = s->dO; c.lda = kOutPad; c.B = Wb + o.dec2_w; c.ldb = kLat; c.b_trans = 1;
+    c.M = n; c.N = kLat; c.K = kOutPad;
+    c.mask = s->d1; c.ldm = kLat; c.c_bf16 = s->dz; c.ldc = kLat;
+    TRYS(run(s, c));
+  }
+  TRYS(wgrad(s, s->dz, kLat, kLat, s->cat[rounds], 2 * kLat, kLat, n, G + o.dec1_w));
+  TRYS(colsum(s, s->dz, kLat, kLat, n, G + o.dec1_b));
+  {
+    GemmCall c;  // dh = dz . Dec1
+    c.A = s->dz; c.lda = kLat; c.B = Wb + o.dec1_w; c.ldb = kLat; c.b_trans = 1;
+    c.M = n; c.N = kLat; c.K = kLat;
+    c.c_f32 = s->dh; c.ldc = kLat;
+    TRYS(run(s, c));
+  }
+  const size_t nl = (size_t)n * kLat;
+  for (int r = rounds - 1; r >= 0; r--) {
+    const RoundOff &ro = o.r[r];
+    k_f32_to_bf16<<<(unsigned)((nl + 255) / 256), 256, 0, q>>>(s->dh, s->dhb, nl);
+    TRYS(wgrad(s, s->dhb, kLat, kLat, s->u[r], kLat, kLat, n, G + ro.n2_w));
+    TRYS(colsum(s, s->dhb, kLat, kLat, n, G + ro.n2_b));
+    {
+      GemmCall c;  // dz = (dh . N2) masked by u > 0
+      c.A = s->dhb; c.lda = kLat; c.B = Wb + ro.n2_w; c.ldb = kLat; c.b_trans = 1;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.mask = s->u[r]; c.ldm = kLat; c.c_bf16 = s->dz; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+    TRYS(wgrad(s, s->dz, kLat, kLat, s->cat[r], 2 * kLat, 2 * kLat, n, G + ro.n1_w));
+    TRYS(colsum(s, s->dz, kLat, kLat, n, G + ro.n1_b));
+    {
+      GemmCall c;  // dh += dz . N1[:, :128]
+      c.A = s->dz; c.lda = kLat; c.B = Wb + ro.n1_w; c.ldb = 2 * kLat; c.b_trans = 1;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.accumulate = 1; c.c_f32 = s->dh; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+    {
+      GemmCall c;  // dm = dz . N1[:, 128:]
+      c.A = s->dz; c.lda = kLat; c.B = Wb + ro.n1_w + kLat; c.ldb = 2 * kLat; c.b_trans = 1;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.c_bf16 = s->dm; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+    TRYS(wgrad(s, s->dm, kLat, kLat, s->S[r], kLat, kLat, n, G + ro.w2));
+    {
+      GemmCall c;  // dS = dm . W2
+      c.A = s->dm; c.lda = kLat; c.B = Wb + ro.w2; c.ldb = kLat; c.b_trans = 1;
+      c.M = n; c.N = kLat; c.K = kLat;
+      c.c_f32 = s->dS; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+    k_sur_edge_bwd<<<kEdgeBlocks, kEdgeThreads, 0, q>>>(n, s->PQ[r], s->w + ro.we, s->nbr, s->ef, s->deg, s->dS,
+                                                        s->dPQ, s->wepart);
+    k_sum_rows<<<(kLat * 4 + 127) / 128, 128, 0, q>>>(s->wepart, kEdgeWarps, kLat * 4, G + ro.we);
+    TRYS(wgrad(s, s->dPQ, 2 * kLat, 2 * kLat, s->cat[r], 2 * kLat, kLat, n, G + ro.pq_w));
+    TRYS(colsum(s, s->dPQ, 2 * kLat, 2 * kLat, n, G + ro.pq_b));
+    {
+      GemmCall c;  // dh += dPQ . W_pq
+      c.A = s->dPQ; c.lda = 2 * kLat; c.B = Wb + ro.pq_w; c.ldb = kLat; c.b_trans = 1;
+      c.M = n; c.N = kLat; c.K = 2 * kLat;
+      c.accumulate = 1; c.c_f32 = s->dh; c.ldc = kLat;
+      TRYS(run(s, c));
+    }
+  }
+  k_f32_to_bf16<<<(unsigned)((nl + 255) / 256), 256, 0, q>>>(s->dh, s->dhb, nl);
+  TRYS(wgrad(s, s->dhb, kLat, kLat, s->a1, kLat, kLat, n, G + o.enc2_w));
+  TRYS(colsum(s, s->dhb, kLat, kLat, n, G + o.enc2_b));
+  {
+    GemmCall c;  // dz = (dh . Enc2) masked by a1 > 0
+    c.A = s->dhb; c.lda = kLat; c.B = Wb + o.enc2_w; c.ldb = kLat; c.b_trans = 1;
+    c.M = n; c.N = kLat; c.K = kLat;
+    c.mask = s->a1; c.ldm = kLat; c.c_bf16 = s->dz; c.ldc = kLat;
+    TRYS(run(s, c));
+  }
+  TRYS(wgrad(s, s->dz, kLat, kLat, s->F, kFeat, kFeat, n, G + o.enc1_w));
+  TRYS(colsum(s, s->dz, kLat, kLat, n, G + o.enc1_b));
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+NodesView view_of(const uph_sur_nodes *nd)
+{
+  NodesView v;
+  v.n = nd->n;
+  v.nf = nd->n_fluid;
+  v.x = nd->x;
+  v.y = nd->y;
+  v.u = nd->u;
+  v.v = nd->v;
+  v.rho = nd->rho;
+  v.itype = nd->itype;
+  v.lo_x = nd->lo_x;
+  v.lo_y = nd->lo_y;
+  v.hi_x = nd->hi_x;
+  v.hi_y = nd->hi_y;
+  return v;
+}
+
+bool nodes_ok(const uph_sur_nodes *nd)
+{
+  return nd && nd->x && nd->y && nd->u && nd->v && nd->rho && nd->itype;
+}
+
+}  // namespace
+
+// ---- C ABI ------------------------------------------------------------------------
+extern "C" int64_t uph_sur_param_count(int32_t rounds)
+{
+  if (rounds < 1 || rounds > kMaxRounds) return -1;
+  return (int64_t)param_layout(rounds).total;
+}
+
+extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_capacity, uph_surrogate **out)
+{
+  if (!cfg || !out) return fail(UPH_BAD_ARG, "uph_sur_create: NULL argument");
+  *out = nullptr;
+  if (cfg->rounds < 1 || cfg->rounds > kMaxRounds) return fail(UPH_BAD_ARG, "uph_sur_create: rounds outside 1..4");
+  if (!(cfg->radius > 0.0) || !(cfg->dt > 0.0) || !(cfg->rho0 > 0.0) || !(cfg->vel_scale > 0.0) ||
+      !(cfg->rho_scale > 0.0) || cfg->macro_steps < 1)
+    return fail(UPH_BAD_ARG, "uph_sur_create: radius, dt, rho0, scales and macro_steps must be positive");
+  if (node_capacity < 1 || node_capacity > (1 << 26)) return fail(UPH_BAD_ARG, "uph_sur_create: bad node capacity");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(UPH_NO_DEVICE, "uph_sur_create: no CUDA device");
+  uph_surrogate *s = new uph_surrogate();
+  s->cfg = *cfg;
+  s->off = param_layout(cfg->rounds);
+  s->cap = (node_capacity + 127) / 128 * 128;
+  const size_t c = (size_t)s->cap;
+  const size_t P = s->off.total;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](auto **p, size_t count) {
+    if (e == cudaSuccess) e = salloc(s, p, count);
+  };
+  A(&s->d_err, 1);
+  A(&s->w, P);
+  A(&s->g, P);
+  A(&s->am, P);
+  A(&s->av, P);
+  A(&s->wb, P);
+  A(&s->nbr, c * kMaxDeg);
+  A(&s->ef, c * kMaxDeg);
+  A(&s->deg, c);
+  A(&s->grid.list, c);
+  A(&s->grid.cell_of, c);
+  A(&s->F, c * kFeat);
+  A(&s->a1, c * kLat);
+  A(&s->d1, c * kLat);
+  A(&s->h, c * kLat);
+  A(&s->out, c * kOutPad);
+  for (int r = 0; r <= cfg->rounds; r++) A(&s->cat[r], c * 2 * kLat);
+  for (int r = 0; r < cfg->rounds; r++) {
+    A(&s->PQ[r], c * 2 * kLat);
+    A(&s->S[r], c * kLat);
+    A(&s->u[r], c * kLat);
+  }
+  A(&s->dO, c * kOutPad);
+  A(&s->dz, c * kLat);
+  A(&s->dhb, c * kLat);
+  A(&s->dm, c * kLat);
+  A(&s->dPQ, c * 2 * kLat);
+  A(&s->dh, c * kLat);
+  A(&s->dS, c * kLat);
+  A(&s->partials, (size_t)kSplitMax * 128 * 128);
+  A(&s->colpart, (size_t)kColBlocks * 2 * kLat);
+  A(&s->wepart, (size_t)kEdgeWarps * kLat * 4);
+  A(&s->losspart, kLossBlocks);
+  A(&s->lossval, 1);
+  A(&s->sqpart, 296);
+  A(&s->sumsq, 1);
+  A(&s->jpart, 2 * kJudgeBlocks);
+  A(&s->bins, 2 * kMaxBins);
+  if (e != cudaSuccess) {
+    free_all(s);
+    delete s;
+    return e == cudaErrorMemoryAllocation ? fail(UPH_OUT_OF_MEMORY, "uph_sur_create: out of device memory")
+                                          : cuda_fail(e, "cudaMalloc");
+  }
+  cudaMemset(s->d_err, 0, sizeof(unsigned));
+  cudaMemset(s->w, 0, sizeof(float) * P);
+  cudaMemset(s->wb, 0, sizeof(bf16) * P);
+  cudaMemset(s->am, 0, sizeof(float) * P);
+  cudaMemset(s->av, 0, sizeof(float) * P);
+  const cudaError_t me = cudaDeviceSynchronize();
+  if (me != cudaSuccess) {
+    free_all(s);
+    delete s;
+    return cuda_fail(me, "uph_sur_create");
+  }
+  *out = s;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_destroy(uph_surrogate *s)
+{
+  if (!s) return UPH_OK;
+  cudaStreamSynchronize(s->stream);
+  for (void *p : {(void *)s->grid.count, (void *)s->grid.start, (void *)s->grid.fill, (void *)s->grid.block_sums,
+                  (void *)s->pred})
+    if (p) cudaFree(p);
+  free_all(s);
+  delete s;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_set_stream(uph_surrogate *s, void *stream)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL surrogate");
+  s->stream = (cudaStream_t)stream;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_set_params(uph_surrogate *s, const float *host, int64_t count)
+{
+  if (!s || !host) return fail(UPH_BAD_ARG, "uph_sur_set_params: NULL argument");
+  if (count != (int64_t)s->off.total) return fail(UPH_BAD_ARG, "uph_sur_set_params: wrong parameter count");
+  UPH_CUDA(cudaMemcpyAsync(s->w, host, sizeof(float) * count, cudaMemcpyHostToDevice, s->stream));
+  k_f32_to_bf16<<<(unsigned)((count + 255) / 256), 256, 0, s->stream>>>(s->w, s->wb, (size_t)count);
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_get_params(uph_surrogate *s, float *host, int64_t count)
+{
+  if (!s || !host) return fail(UPH_BAD_ARG, "uph_sur_get_params: NULL argument");
+  if (count != (int64_t)s->off.total) return fail(UPH_BAD_ARG, "uph_sur_get_params: wrong parameter count");
+  UPH_CUDA(cudaMemcpyAsync(host, s->w, sizeof(float) * count, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_reset_optimizer(uph_surrogate *s)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL surrogate");
+  UPH_CUDA(cudaMemsetAsync(s->am, 0, sizeof(float) * s->off.total, s->stream));
+  UPH_CUDA(cudaMemsetAsync(s->av, 0, sizeof(float) * s->off.total, s->stream));
+  s->adam_t = 0;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_forward(uph_surrogate *s, const uph_sur_nodes *nodes, float *out)
+{
+  if (!s || !nodes_ok(nodes)) return fail(UPH_BAD_ARG, "uph_sur_forward: NULL argument");
+  const NodesView nv = view_of(nodes);
+  TRYS(prepare(s, nv));
+  TRYS(forward_net(s, nv.n));
+  if (out) k_copy_out<<<(nv.n * kNOut + 255) / 256, 256, 0, s->stream>>>(nv.n, s->out, out);
+  s->n_last = nv.n;
+  s->nf_last = nv.nf;
+  TRYS(check_err(s));
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_gradients(uph_surrogate *s, const uph_sur_nodes *nodes, const float *target, float *grad,
+                                        double *loss)
+{
+  if (!s || !nodes_ok(nodes) || !target) return fail(UPH_BAD_ARG, "uph_sur_gradients: NULL argument");
+  const NodesView nv = view_of(nodes);
+  if (nv.nf < 1) return fail(UPH_BAD_ARG, "uph_sur_gradients: no fluid nodes");
+  TRYS(prepare(s, nv));
+  TRYS(forward_net(s, nv.n));
+  const float inv_count = 1.0f / (float)((double)nv.nf * kNOut);
+  k_sur_loss<<<kLossBlocks, 256, 0, s->stream>>>(nv.n, nv.nf, s->out, target, inv_count, s->dO, s->losspart);
+  k_sum_rows<<<1, 32, 0, s->stream>>>(s->losspart, kLossBlocks, 1, s->lossval);
+  TRYS(backward_net(s, nv.n));
+  if (grad)
+    UPH_CUDA(cudaMemcpyAsync(grad, s->g, sizeof(float) * s->off.total, cudaMemcpyDeviceToDevice, s->stream));
+  s->have_grad = true;
+  s->n_last = nv.n;
+  s->nf_last = nv.nf;
+  if (loss) {
+    float l = 0.0f;
+    UPH_CUDA(cudaMemcpyAsync(&l, s->lossval, sizeof l, cudaMemcpyDeviceToHost, s->stream));
+    TRYS(check_err(s));
+    *loss = l;
+  }
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_adam(uph_surrogate *s, double lr, double beta1, double beta2, double eps, double clip)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL surrogate");
+  if (!s->have_grad) return fail(UPH_BAD_ARG, "uph_sur_adam: no gradients computed yet");
+  if (!(lr > 0.0) || !(beta1 >= 0.0 && beta1 < 1.0) || !(beta2 >= 0.0 && beta2 < 1.0) || !(eps > 0.0))
+    return fail(UPH_BAD_ARG, "uph_sur_adam: bad hyper-parameters");
+  const size_t P = s->off.total;
+  s->adam_t++;
+  const double c1 = 1.0 / (1.0 - pow(beta1, s->adam_t)), c2 = 1.0 / (1.0 - pow(beta2, s->adam_t));
+  if (clip > 0.0) {
+    k_sumsq_part<<<296, 256, 0, s->stream>>>(s->g, P, s->sqpart);
+    k_sum_rows<<<1, 32, 0, s->stream>>>(s->sqpart, 296, 1, s->sumsq);
+  }
+  k_adam<<<(unsigned)((P + 255) / 256), 256, 0, s->stream>>>(P, s->w, s->g, s->am, s->av, s->wb, (float)lr,
+                                                              (float)beta1, (float)beta2, (float)eps, (float)c1,
+                                                              (float)c2, s->sumsq, (float)clip);
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+namespace {
+
+uph_status network_step(uph_surrogate *s, uph_sim *sim, double *pred)
+{
+  SimView sv = sim_view(sim);
+  if (s->cap < sv.P.n) return fail(UPH_BAD_ARG, "uph_sur_advance: simulation larger than the node capacity");
+  NodesView nv;
+  nv.n = sv.P.n;
+  nv.nf = sv.P.nf;
+  nv.x = sv.S.x;
+  nv.y = sv.S.y;
+  nv.u = sv.S.u;
+  nv.v = sv.S.v;
+  nv.rho = sv.S.rho;
+  nv.itype = sv.S.itype;
+  nv.lo_x = sv.P.lo_x;
+  nv.lo_y = sv.P.lo_y;
+  nv.hi_x = sv.P.hi_x;
+  nv.hi_y = sv.P.hi_y;
+  TRYS(prepare(s, nv));
+  TRYS(forward_net(s, nv.n));
+  OutScale sc;
+  sc.T = s->cfg.macro_steps * s->cfg.dt;
+  for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
+  if (sv.P.nf > 0)
+    k_sur_apply<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, pred, sv.err);
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+}  // namespace
+
+extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t macro_steps, const uph_sur_judge *judge,
+                                      uph_sur_report *report)
+{
+  if (!s || !sim || !judge || !report) return fail(UPH_BAD_ARG, "uph_sur_advance: NULL argument");
+  if (macro_steps < 0) return fail(UPH_BAD_ARG, "uph_sur_advance: negative step count");
+  if (judge->judge_every < 1 || judge->fallback_macro < 0 || judge->surface_bins < 1 ||
+      judge->surface_bins > kMaxBins || !(judge->surface_x1 > judge->surface_x0) || !(judge->depth > 0.0))
+    return fail(UPH_BAD_ARG, "uph_sur_advance: bad judge settings");
+  SimView sv = sim_view(sim);
+  // the network runs on the simulation's stream for the whole call
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  struct StreamSwap {
+    uph_surrogate *s;
+    cudaStream_t saved;
+    ~StreamSwap() { s->stream = saved; }
+  } swap{s, s->stream};
+  s->stream = sv.stream;
+  if (sv.P.profile != UPH_PROFILE_WCSPH)
+    return fail(UPH_UNSUPPORTED, "uph_sur_advance: the surrogate advances WCSPH simulations only");
+  if (fabs(sv.P.dt - s->cfg.dt) > 1e-12 * s->cfg.dt)
+    return fail(UPH_BAD_ARG, "uph_sur_advance: the simulation's dt differs from the network's");
+  const int K = s->cfg.macro_steps;
+  if (sim != s->last_sim) {
+    s->last_sim = sim;
+    s->since_judge = 0;
+    s->fallback_left = 0;
+  }
+  // the judge's prediction buffer: reference-indexed so it survives re-sorts
+  if (!s->pred || s->n_pred < sv.P.nf) {
+    if (s->pred) cudaFree(s->pred);
+    s->pred = nullptr;
+    s->n_pred = 0;
+    UPH_CUDA(cudaMalloc((void **)&s->pred, sizeof(double) * kNOut * (size_t)std::max(sv.P.nf, 1)));
+    s->n_pred = sv.P.nf;
+  }
+  for (int m = 0; m < macro_steps; m++) {
+    report->macro_steps++;
+    if (s->fallback_left > 0) {
+      s->fallback_left--;
+      TRYS(uph_sim_step(sim, K));
+      report->plain_steps += K;
+      continue;
+    }
+    s->since_judge++;
+    if (s->since_judge < judge->judge_every) {
+      TRYS(network_step(s, sim, nullptr));
+      TRYS(sim_jump(sim, K));
+      report->network_steps++;
+      continue;
+    }
+    // judged macro step: predict, run the plain solver over the same span,
+    // compare, keep the plain state
+    s->since_judge = 0;
+    TRYS(network_step(s, sim, s->pred));
+    TRYS(uph_sim_step(sim, K));
+    report->plain_steps += K;
+    report->judged_steps++;
+    sv = sim_view(sim);
+    const int nb = judge->surface_bins;
+    UPH_CUDA(cudaMemsetAsync(s->bins, 0, sizeof(unsigned) * 2 * nb, s->stream));
+    k_sur_judge<<<kJudgeBlocks, 256, 0, s->stream>>>(sv.P, sv.S, s->pred, judge->surface_x0,
+                                                     nb / (judge->surface_x1 - judge->surface_x0), nb, s->bins,
+                                                     s->bins + nb, s->jpart);
+    std::vector<double> part(2 * kJudgeBlocks);
+    std::vector<unsigned> bins(2 * nb);
+    UPH_CUDA(cudaMemcpyAsync(part.data(), s->jpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
+    UPH_CUDA(cudaMemcpyAsync(bins.data(), s->bins, sizeof(unsigned) * bins.size(), cudaMemcpyDeviceToHost, s->stream));
+    TRYS(check_err(s));
+    double sq = 0.0;
+    for (int b = 0; b < kJudgeBlocks; b++) sq += part[2 * b];
+    const double rho_err = sv.P.nf > 0 ? sqrt(sq / sv.P.nf) : 0.0;
+    double surf = 0.0;
+    for (int b = 0; b < nb; b++) {
+      if (!bins[b] || !bins[nb + b]) continue;  // a bin empty in either state
+      auto val = [](unsigned o) {
+        const unsigned bits = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+        float f;
+        memcpy(&f, &bits, sizeof f);
+        return (double)f;
+      };
+      surf = std::max(surf, fabs(val(bins[nb + b]) - val(bins[b])) / judge->depth);
+    }
+    report->last_rho_err = rho_err;
+    report->last_surface_err = surf;
+    report->max_rho_err = std::max(report->max_rho_err, rho_err);
+    report->max_surface_err = std::max(report->max_surface_err, surf);
+    if (!(rho_err <= judge->max_rho_err) || !(surf <= judge->max_surface_err)) {
+      report->failed_checks++;
+      s->fallback_left = judge->fallback_macro;
+    }
+  }
+  return sim_check(sim);
+}

@@ -42,13 +42,18 @@ struct TcGemmArgs {
   const __nv_bfloat16 *A;
   const __nv_bfloat16 *B;
   int lda, ldb;              // elements
+  int a_trans, b_trans;      // operand stored as [K x rows] (rows contiguous) instead of [rows x K]
   int M, N, K;               // K multiple of 64, N multiple of 128
+  int k_valid;               // transposed operands: K rows >= k_valid read as zero
   int k_per_split;           // multiple of 64
   const float *bias;         // [N] or null
   int relu;
+  const __nv_bfloat16 *mask; // [M x ldm] or null: zero the result where mask <= 0
+  int ldm;
+  int accumulate;            // add the result to c_f32's contents
   float *c_f32;              // [M x ldc] or null
-  __nv_bfloat16 *c_bf16;     // [M x ldc] or null
-  int ldc;
+  __nv_bfloat16 *c_bf16;     // [M x ldc16] or null
+  int ldc, ldc16;
   float *partials;           // split-K: [splits][M][N] FP32
   unsigned *err;
 };
@@ -106,6 +111,34 @@ __device__ __forceinline__ void load_tile(uint8_t *tile, const __nv_bfloat16 *sr
   }
 }
 
+// the same tile from an operand stored transposed, [K x rows] with rows
+// contiguous (e.g. node activations [nodes x features] as the K-major operand
+// of a weight gradient): a lane loads 8 consecutive rows of one K index and
+// stores them one element at a time; the 32 lanes of a warp take 32
+// consecutive K, so their stores fall in one 64-byte span of a tile row.
+// Rows >= `rows` and K >= k_valid read as zero; rows is a multiple of 8.
+__device__ __forceinline__ void load_tile_t(uint8_t *tile, const __nv_bfloat16 *src, int ld, int r0, int rows, int k0,
+                                            int k_valid)
+{
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int q = t + 128 * i;
+    const int kk = q & 63;         // K inside the slice
+    const int rc = (q >> 6) * 8;   // first of 8 rows
+    const int gk = k0 + kk;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gk < k_valid && r0 + rc < rows) v = *reinterpret_cast<const uint4 *>(src + (size_t)gk * ld + r0 + rc);
+    const uint16_t *e = reinterpret_cast<const uint16_t *>(&v);
+    const int chunk = kk >> 3, sub = (kk & 7) * 2;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int r = rc + j;
+      *reinterpret_cast<uint16_t *>(tile + r * 128 + ((chunk ^ (r & 7)) << 4) + sub) = e[j];
+    }
+  }
+}
+
 __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
 {
   extern __shared__ uint8_t smem_raw[];
@@ -146,8 +179,14 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
       if (!ok) break;
     }
     const int k0 = kbeg + s * kTcBK;
-    load_tile(ta, g.A, g.lda, m0, g.M, k0);
-    load_tile(tb, g.B, g.ldb, n0, g.N, k0);
+    if (g.a_trans)
+      load_tile_t(ta, g.A, g.lda, m0, g.M, k0, g.k_valid);
+    else
+      load_tile(ta, g.A, g.lda, m0, g.M, k0);
+    if (g.b_trans)
+      load_tile_t(tb, g.B, g.ldb, n0, g.N, k0, g.k_valid);
+    else
+      load_tile(tb, g.B, g.ldb, n0, g.N, k0);
     // generic-proxy shared stores -> visible to the tensor core's async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -209,10 +248,22 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
 #pragma unroll
           for (int j = 0; j < 16; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
         } else {
+          if (g.bias)
 #pragma unroll
-          for (int j = 0; j < 16; j++) {
-            if (g.bias) v[j] += g.bias[col + j];
-            if (g.relu) v[j] = fmaxf(v[j], 0.0f);
+            for (int j = 0; j < 16; j++) v[j] += g.bias[col + j];
+          if (g.accumulate) {
+            const float *old = g.c_f32 + (size_t)row * g.ldc + col;
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] += old[j];
+          }
+          if (g.relu)
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = fmaxf(v[j], 0.0f);
+          if (g.mask) {
+            const __nv_bfloat16 *mk = g.mask + (size_t)row * g.ldm + col;
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+              if (!(__bfloat162float(mk[j]) > 0.0f)) v[j] = 0.0f;
           }
           if (g.c_f32) {
             float *dst = g.c_f32 + (size_t)row * g.ldc + col;
@@ -221,7 +272,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
               *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
           }
           if (g.c_bf16) {
-            __nv_bfloat16 *dst = g.c_bf16 + (size_t)row * g.ldc + col;
+            __nv_bfloat16 *dst = g.c_bf16 + (size_t)row * g.ldc16 + col;
             __align__(16) __nv_bfloat162 h[8];
 #pragma unroll
             for (int j = 0; j < 8; j++) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
@@ -248,56 +299,90 @@ __global__ void k_splitk_reduce(const float *__restrict__ partials, int splits, 
   out[i] = acc;
 }
 
-}  // namespace uph
 
-using namespace uph;
-
-// Host launcher (C ABI for tests and the surrogate code): device pointers.
-// splits > 1 requires `partials` of splits * M * N floats and writes the sum
-// into c_f32 (accumulated onto its contents when accumulate != 0).
-extern "C" uph_status uph_tc_gemm_bf16(const void *A, int32_t lda, const void *B, int32_t ldb, int32_t M, int32_t N,
-                                       int32_t K, const float *bias, int32_t relu, float *c_f32, void *c_bf16,
-                                       int32_t ldc, int32_t splits, float *partials, int32_t accumulate,
-                                       unsigned *err, void *stream)
+uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s)
 {
-  if (!A || !B || !err || M <= 0 || N <= 0 || K <= 0) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: bad arguments");
-  if (K % kTcBK || N % kTcN) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: K must be a multiple of 64, N of 128");
-  if (lda % 8 || ldb % 8 || ldc % 8) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: leading dimensions must be multiples of 8");
-  if (splits < 1) splits = 1;
-  if (splits > 1 && (!partials || !c_f32 || bias || relu || c_bf16))
-    return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: split-K writes FP32 only, without bias or ReLU");
-  if (splits == 1 && !c_f32 && !c_bf16) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: no output");
-  cudaStream_t s = (cudaStream_t)stream;
+  if (!c.A || !c.B || !c.err || c.M <= 0 || c.N <= 0 || c.K <= 0) return fail(UPH_BAD_ARG, "tc_gemm: bad arguments");
+  if (c.K % kTcBK || c.N % kTcN) return fail(UPH_BAD_ARG, "tc_gemm: K must be a multiple of 64, N of 128");
+  const int ldc16 = c.ldc16 > 0 ? c.ldc16 : c.ldc;
+  if (c.lda % 8 || c.ldb % 8 || c.ldc % 8 || ldc16 % 8 || (c.mask && c.ldm % 8))
+    return fail(UPH_BAD_ARG, "tc_gemm: leading dimensions must be multiples of 8");
+  if ((c.a_trans && c.M % 8) || (c.b_trans && c.N % 8))
+    return fail(UPH_BAD_ARG, "tc_gemm: a transposed operand needs a multiple of 8 rows");
+  int splits = c.splits < 1 ? 1 : c.splits;
+  if (splits > 1 && (!c.partials || !c.c_f32 || c.bias || c.relu || c.c_bf16 || c.mask || c.ldc != c.N))
+    return fail(UPH_BAD_ARG, "tc_gemm: split-K writes a dense FP32 result only, without bias, ReLU or mask");
+  if (splits == 1 && !c.c_f32 && !c.c_bf16) return fail(UPH_BAD_ARG, "tc_gemm: no output");
+  if (splits == 1 && c.accumulate && !c.c_f32) return fail(UPH_BAD_ARG, "tc_gemm: accumulate needs c_f32");
   static bool configured = false;
   if (!configured) {
     UPH_CUDA(cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
     configured = true;
   }
   TcGemmArgs g;
-  g.A = (const __nv_bfloat16 *)A;
-  g.B = (const __nv_bfloat16 *)B;
-  g.lda = lda;
-  g.ldb = ldb;
-  g.M = M;
-  g.N = N;
-  g.K = K;
-  int kps = K;
-  if (splits > 1) kps = ((K / kTcBK + splits - 1) / splits) * kTcBK;
+  g.A = (const __nv_bfloat16 *)c.A;
+  g.B = (const __nv_bfloat16 *)c.B;
+  g.lda = c.lda;
+  g.ldb = c.ldb;
+  g.a_trans = c.a_trans;
+  g.b_trans = c.b_trans;
+  g.M = c.M;
+  g.N = c.N;
+  g.K = c.K;
+  g.k_valid = c.k_valid > 0 ? c.k_valid : c.K;
+  int kps = c.K;
+  if (splits > 1) kps = ((c.K / kTcBK + splits - 1) / splits) * kTcBK;
   g.k_per_split = kps;
-  splits = (K + kps - 1) / kps;
-  g.bias = bias;
-  g.relu = relu;
-  g.c_f32 = splits > 1 ? nullptr : c_f32;
-  g.c_bf16 = (__nv_bfloat16 *)c_bf16;
-  g.ldc = ldc;
-  g.partials = splits > 1 ? partials : nullptr;
-  g.err = err;
-  dim3 grid((M + kTcM - 1) / kTcM, N / kTcN, splits);
+  splits = (c.K + kps - 1) / kps;
+  g.bias = c.bias;
+  g.relu = c.relu;
+  g.mask = (const __nv_bfloat16 *)c.mask;
+  g.ldm = c.ldm;
+  g.accumulate = splits > 1 ? 0 : c.accumulate;
+  g.c_f32 = splits > 1 ? nullptr : c.c_f32;
+  g.c_bf16 = (__nv_bfloat16 *)c.c_bf16;
+  g.ldc = c.ldc;
+  g.ldc16 = ldc16;
+  g.partials = splits > 1 ? c.partials : nullptr;
+  g.err = c.err;
+  dim3 grid((c.M + kTcM - 1) / kTcM, c.N / kTcN, splits);
   k_tc_gemm<<<grid, 128, kTcSmemBytes, s>>>(g);
   if (splits > 1) {
-    if (ldc != N) return fail(UPH_BAD_ARG, "uph_tc_gemm_bf16: split-K output must be dense (ldc == N)");
-    k_splitk_reduce<<<(M * N + 255) / 256, 256, 0, s>>>(partials, splits, M, N, c_f32, accumulate);
+    const int total = c.M * c.N;
+    k_splitk_reduce<<<(total + 255) / 256, 256, 0, s>>>(c.partials, splits, c.M, c.N, c.c_f32, c.accumulate);
   }
   UPH_CUDA(cudaGetLastError());
   return UPH_OK;
+}
+
+}  // namespace uph
+
+using namespace uph;
+
+// C ABI for tests: device pointers, both operands K-major.  splits > 1
+// requires `partials` of splits * M * N floats and writes the sum into c_f32
+// (accumulated onto its contents when accumulate != 0).
+extern "C" uph_status uph_tc_gemm_bf16(const void *A, int32_t lda, const void *B, int32_t ldb, int32_t M, int32_t N,
+                                       int32_t K, const float *bias, int32_t relu, float *c_f32, void *c_bf16,
+                                       int32_t ldc, int32_t splits, float *partials, int32_t accumulate,
+                                       unsigned *err, void *stream)
+{
+  GemmCall c;
+  c.A = A;
+  c.lda = lda;
+  c.B = B;
+  c.ldb = ldb;
+  c.M = M;
+  c.N = N;
+  c.K = K;
+  c.bias = bias;
+  c.relu = relu;
+  c.c_f32 = c_f32;
+  c.c_bf16 = c_bf16;
+  c.ldc = ldc;
+  c.splits = splits;
+  c.partials = partials;
+  c.accumulate = accumulate;
+  c.err = err;
+  return launch_tc_gemm(c, (cudaStream_t)stream);
 }

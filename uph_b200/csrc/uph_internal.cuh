@@ -122,6 +122,7 @@ uph_status cuda_fail(cudaError_t e, const char *what);
 void launch_cell_keys(const DevParams &P, const double *x, const double *y, int first, int count,
                       CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s);
 void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s);
+int scan_block_sums_needed(int n);  // size of launch_exclusive_scan's block_sums
 void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s);
 void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s);
 
@@ -144,5 +145,33 @@ void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, 
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
                         const int *d_itime, cudaStream_t s);
 void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t s);
+
+// BF16 tcgen05 GEMM, C[M x N] = A . B^T with FP32 accumulation.  An operand
+// is K-major ([rows x K], ld >= K) unless its *_trans flag says it is stored
+// [K x rows] (ld >= rows).  Epilogue, in order: + bias[N], + old c_f32
+// (accumulate), ReLU, zero where mask <= 0; then FP32 and/or BF16 stores.
+// splits > 1 splits K over CTAs into `partials` (splits * M * N floats) and
+// sums them in split order into a dense c_f32 (ldc == N).
+struct GemmCall {
+  const void *A = nullptr;
+  int lda = 0, a_trans = 0;
+  const void *B = nullptr;
+  int ldb = 0, b_trans = 0;
+  int M = 0, N = 0, K = 0;
+  int k_valid = 0;  // transposed operands: K rows >= k_valid read as zero (0: K)
+  const float *bias = nullptr;
+  int relu = 0;
+  const void *mask = nullptr;
+  int ldm = 0;
+  int accumulate = 0;
+  float *c_f32 = nullptr;
+  void *c_bf16 = nullptr;
+  int ldc = 0;
+  int ldc16 = 0;  // leading dimension of c_bf16 (0: ldc)
+  int splits = 1;
+  float *partials = nullptr;
+  unsigned *err = nullptr;
+};
+uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s);
 
 }  // namespace uph
