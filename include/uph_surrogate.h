@@ -119,6 +119,9 @@ typedef struct {
   int64_t judged_steps;     /* macro steps checked against the plain solver */
   int64_t failed_checks;    /* checks over a threshold (each starts a fallback) */
   int64_t plain_steps;      /* SPH steps the plain solver ran */
+  int64_t graph_overflows;  /* macro steps handed to the plain solver because a
+                               node had more than UPH_SUR_MAX_DEGREE partners
+                               (each also starts a fallback) */
   double last_rho_err, last_surface_err;
   double max_rho_err, max_surface_err;
 } uph_sur_report;

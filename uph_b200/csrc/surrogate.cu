@@ -39,7 +39,6 @@ constexpr int kMaxDeg = UPH_SUR_MAX_DEGREE;
 constexpr int kMaxRounds = UPH_SUR_MAX_ROUNDS;
 constexpr int kEdgeThreads = 256;           // 8 warps
 constexpr int kEdgeBlocks = 148 * 4;        // fixed grid: per-warp partials in a fixed order
-constexpr int kEdgeWarps = kEdgeBlocks * (kEdgeThreads / 32);
 constexpr int kColBlocks = 148 * 2;         // bias-gradient partial sums
 constexpr int kSplitMax = 148;              // split-K CTAs of one weight-gradient GEMM tile
 constexpr int kLossBlocks = 148;
@@ -293,19 +292,46 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
     store_bf16x4(dPQ + (size_t)a * 2 * kLat + c0, dp);
     store_bf16x4(dPQ + (size_t)a * 2 * kLat + kLat + c0, dq);
   }
-  float *dst = we_part + (size_t)gw * kLat * 4;
-  for (int c = 0; c < 4; c++)
-    *reinterpret_cast<float4 *>(dst + (c0 + c) * 4) = make_float4(g[c][0], g[c][1], g[c][2], 0.0f);
+  // the block's 8 warps summed in warp order: one partial row per block
+  __shared__ float4 red[kEdgeThreads / 32][kLat];
+  const int wib = threadIdx.x >> 5;
+  for (int c = 0; c < 4; c++) red[wib][c0 + c] = make_float4(g[c][0], g[c][1], g[c][2], 0.0f);
+  __syncthreads();
+  if (threadIdx.x < kLat) {
+    float4 t = red[0][threadIdx.x];
+    for (int w = 1; w < kEdgeThreads / 32; w++) {
+      const float4 o = red[w][threadIdx.x];
+      t.x += o.x;
+      t.y += o.y;
+      t.z += o.z;
+    }
+    reinterpret_cast<float4 *>(we_part)[(size_t)blockIdx.x * kLat + threadIdx.x] = t;
+  }
 }
 
-// out[c] = sum over rows r (in order) of part[r][c]
-__global__ void k_sum_rows(const float *__restrict__ part, int rows, int cols, float *__restrict__ out)
+// out[c] = sum over rows of part[r][c] in a fixed order: block = 32 columns
+// x 32 row lanes, lane l sums rows l, l + 32, ... and the lanes are added in
+// lane order (deterministic; 32-way parallel instead of one long chain)
+__global__ void __launch_bounds__(1024) k_sum_rows(const float *__restrict__ part, int rows, int cols,
+                                                    float *__restrict__ out)
 {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cols) return;
+  __shared__ float red[32][33];
+  const int cl = threadIdx.x & 31, l = threadIdx.x >> 5;
+  const int c = blockIdx.x * 32 + cl;
   float s = 0.0f;
-  for (int r = 0; r < rows; r++) s += part[(size_t)r * cols + c];
-  out[c] = s;
+  if (c < cols)
+    for (int r = l; r < rows; r += 32) s += part[(size_t)r * cols + c];
+  red[l][cl] = s;
+  __syncthreads();
+  if (l == 0 && c < cols) {
+    float t = red[0][cl];
+    for (int k = 1; k < 32; k++) t += red[k][cl];
+    out[c] = t;
+  }
+}
+inline void sum_rows(const float *part, int rows, int cols, float *out, cudaStream_t s)
+{
+  k_sum_rows<<<(cols + 31) / 32, 1024, 0, s>>>(part, rows, cols, out);
 }
 
 // column sums of a BF16 [n x cols] block (ld >= cols): per-block partials
@@ -679,7 +705,7 @@ uph_status colsum(uph_surrogate *s, const bf16 *src, int ld, int cols, int n, fl
 {
   const int rpb = (n + kColBlocks - 1) / kColBlocks;
   k_colsum_part<<<kColBlocks, cols, 0, s->stream>>>(src, ld, cols, n, rpb, s->colpart);
-  k_sum_rows<<<(cols + 127) / 128, 128, 0, s->stream>>>(s->colpart, kColBlocks, cols, dst);
+  sum_rows(s->colpart, kColBlocks, cols, dst, s->stream);
   return UPH_OK;
 }
 
@@ -828,7 +854,7 @@ uph_status backward_net(uph_surrogate *s, int n)
     }
     k_sur_edge_bwd<<<kEdgeBlocks, kEdgeThreads, 0, q>>>(n, s->PQ[r], s->w + ro.we, s->nbr, s->ef, s->deg, s->dS,
                                                         s->dPQ, s->wepart);
-    k_sum_rows<<<(kLat * 4 + 127) / 128, 128, 0, q>>>(s->wepart, kEdgeWarps, kLat * 4, G + ro.we);
+    sum_rows(s->wepart, kEdgeBlocks, kLat * 4, G + ro.we, q);
     TRYS(wgrad(s, s->dPQ, 2 * kLat, 2 * kLat, s->cat[r], 2 * kLat, kLat, n, G + ro.pq_w));
     TRYS(colsum(s, s->dPQ, 2 * kLat, 2 * kLat, n, G + ro.pq_b));
     {
@@ -939,7 +965,7 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
   A(&s->dS, c * kLat);
   A(&s->partials, (size_t)kSplitMax * 128 * 128);
   A(&s->colpart, (size_t)kColBlocks * 2 * kLat);
-  A(&s->wepart, (size_t)kEdgeWarps * kLat * 4);
+  A(&s->wepart, (size_t)kEdgeBlocks * kLat * 4);
   A(&s->losspart, kLossBlocks);
   A(&s->lossval, 1);
   A(&s->sqpart, 296);
@@ -1038,7 +1064,7 @@ extern "C" uph_status uph_sur_gradients(uph_surrogate *s, const uph_sur_nodes *n
   TRYS(forward_net(s, nv.n));
   const float inv_count = 1.0f / (float)((double)nv.nf * kNOut);
   k_sur_loss<<<kLossBlocks, 256, 0, s->stream>>>(nv.n, nv.nf, s->out, target, inv_count, s->dO, s->losspart);
-  k_sum_rows<<<1, 32, 0, s->stream>>>(s->losspart, kLossBlocks, 1, s->lossval);
+  sum_rows(s->losspart, kLossBlocks, 1, s->lossval, s->stream);
   TRYS(backward_net(s, nv.n));
   if (grad)
     UPH_CUDA(cudaMemcpyAsync(grad, s->g, sizeof(float) * s->off.total, cudaMemcpyDeviceToDevice, s->stream));
@@ -1066,7 +1092,7 @@ extern "C" uph_status uph_sur_adam(uph_surrogate *s, double lr, double beta1, do
   const double c1 = 1.0 / (1.0 - pow(beta1, s->adam_t)), c2 = 1.0 / (1.0 - pow(beta2, s->adam_t));
   if (clip > 0.0) {
     k_sumsq_part<<<296, 256, 0, s->stream>>>(s->g, P, s->sqpart);
-    k_sum_rows<<<1, 32, 0, s->stream>>>(s->sqpart, 296, 1, s->sumsq);
+    sum_rows(s->sqpart, 296, 1, s->sumsq, s->stream);
   }
   k_adam<<<(unsigned)((P + 255) / 256), 256, 0, s->stream>>>(P, s->w, s->g, s->am, s->av, s->wb, (float)lr,
                                                               (float)beta1, (float)beta2, (float)eps, (float)c1,
@@ -1077,7 +1103,9 @@ extern "C" uph_status uph_sur_adam(uph_surrogate *s, double lr, double beta1, do
 
 namespace {
 
-uph_status network_step(uph_surrogate *s, uph_sim *sim, double *pred)
+// graph and features of the simulation's current state; *fits is false
+// (and the flag cleared) when a node has more partners than the graph holds
+uph_status prepare_sim(uph_surrogate *s, uph_sim *sim, bool *fits)
 {
   SimView sv = sim_view(sim);
   if (s->cap < sv.P.n) return fail(UPH_BAD_ARG, "uph_sur_advance: simulation larger than the node capacity");
@@ -1095,7 +1123,23 @@ uph_status network_step(uph_surrogate *s, uph_sim *sim, double *pred)
   nv.hi_x = sv.P.hi_x;
   nv.hi_y = sv.P.hi_y;
   TRYS(prepare(s, nv));
-  TRYS(forward_net(s, nv.n));
+  unsigned err = 0;
+  UPH_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  *fits = !(err & ERR_NEIGHBOR_OVERFLOW);
+  if (!*fits) {
+    err &= ~ERR_NEIGHBOR_OVERFLOW;
+    UPH_CUDA(cudaMemcpyAsync(s->d_err, &err, sizeof err, cudaMemcpyHostToDevice, s->stream));
+  }
+  return err ? check_err(s) : UPH_OK;
+}
+
+// the prepared graph through the network; the prediction replaces the
+// fluid state, or goes to pred (reference-indexed) for the judge
+uph_status network_step(uph_surrogate *s, uph_sim *sim, double *pred)
+{
+  SimView sv = sim_view(sim);
+  TRYS(forward_net(s, sv.P.n));
   OutScale sc;
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
@@ -1151,6 +1195,18 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
       continue;
     }
     s->since_judge++;
+    bool fits = true;
+    TRYS(prepare_sim(s, sim, &fits));
+    if (!fits) {
+      // a state the network's graph cannot hold: the plain solver takes
+      // this macro step and the fallback after it
+      report->graph_overflows++;
+      s->since_judge = 0;
+      s->fallback_left = judge->fallback_macro;
+      TRYS(uph_sim_step(sim, K));
+      report->plain_steps += K;
+      continue;
+    }
     if (s->since_judge < judge->judge_every) {
       TRYS(network_step(s, sim, nullptr));
       TRYS(sim_jump(sim, K));

@@ -120,6 +120,9 @@ class Deck:
     eta_override: float = 0.0
     domain_lo: tuple = (0.0, 0.0)
     domain_hi: tuple = (0.0, 0.0)
+    # per-particle motion of the moving block (x0, half stroke, omega) for
+    # uph_sim_set_wall_motion, or None for the reference's own wall motion
+    wall_table: Optional[tuple] = None
 
     @property
     def n_fluid(self) -> int:
@@ -309,13 +312,21 @@ def hydrostatic_tank(width=2.0, depth=1.0, dx=0.002, layers=3, eta=1.3, tank_hei
 
 
 def wave_flume(length=10.0, depth=0.5, dx=0.005, layers=3, eta=1.3, amplitude=0.04, period=1.3,
-               **over) -> Deck:
+               piston_layers=1, hydrostatic_walls=False, **over) -> Deck:
     """Config 4 geometry: a flume whose left wall is a piston wavemaker, one
     column of moving particles (itype 3, as in the reference's wave deck) at
     x = S/2 (1 - cos wt) (inputbp.c:194-207, movingBoundary 1, S = 2A).  The
     sponge layer damps u for x >= 7 m (System.c:333-335, input.c:137-144).
     Fluid starts one spacing right of the piston; bottom and right walls have
-    `layers` rows."""
+    `layers` rows.
+
+    For long runs: `piston_layers` > 1 makes the piston that many columns
+    thick (at x = 0, -dx, ...), moved rigidly through `deck.wall_table`
+    (x = x0 + A (1 - cos wt), the same displacement; the reference's own
+    motion would put every column at one x), and `hydrostatic_walls` gives
+    the wall particles the hydrostatic density and pressure of their depth.
+    With one column and walls at rest density the fluid next to the piston
+    leaks through it within a few hundred steps."""
     over = dict(over)
     over.setdefault("local_depth", depth)
     p = base_params(dx, eta=eta, stroke=2.0 * amplitude, wave_period=period, moving_boundary=1, **over)
@@ -336,9 +347,16 @@ def wave_flume(length=10.0, depth=0.5, dx=0.005, layers=3, eta=1.3, amplitude=0.
         xs.append(np.full_like(yside, (nx + 1 + k) * dx))
         ys.append(yside)
     fixed = _rows(np.concatenate(xs), np.concatenate(ys), p["density0"], 0.0, mass, FIXED_WALL_ITYPE)
-    moving = _rows(np.zeros_like(yside), yside, p["density0"], 0.0, mass, 3)
+    xp = np.concatenate([np.full_like(yside, -k * dx) for k in range(piston_layers)])
+    yp = np.tile(yside, piston_layers)
+    moving = _rows(xp, yp, p["density0"], 0.0, mass, 3)
+    if hydrostatic_walls:
+        for blk in (fixed, moving):
+            blk[:, 4], blk[:, 5] = hydrostatic_fields(np.minimum(blk[:, 1], depth), depth, p)
     deck = Deck(p, fluid, np.zeros((0, 12)), fixed, moving, eta_override=eta)
-    pad = 4 * eta * dx + layers * dx + 2 * amplitude
+    if piston_layers > 1:
+        deck.wall_table = (xp.copy(), np.full(xp.size, amplitude), np.full(xp.size, 2.0 * math.pi / period))
+    pad = 4 * eta * dx + max(layers, piston_layers) * dx + 2 * amplitude
     deck.domain_lo = (-pad, -pad)
     deck.domain_hi = (length + pad, depth * 2.0 + pad)
     return deck

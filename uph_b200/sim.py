@@ -40,6 +40,8 @@ class Simulation:
                   av_alpha: Optional[float] = None) -> "Simulation":
         sim = cls(deck.uph_params(profile, precision, av_alpha))
         sim.upload(deck.initial_state(), 0)
+        if deck.wall_table is not None:
+            sim.set_wall_motion(*deck.wall_table)
         return sim
 
     def close(self) -> None:

@@ -252,7 +252,8 @@ def flume_batch(pistons: Sequence[Tuple[float, float]], length: float = 4.0, dep
     piston k = (amplitude A, period T): x = A (1 - cos(2 pi t / T)).  Each
     flume damps u in its last (1 - sponge_fraction) of length, like the
     workload's sponge at x >= 7 m of 10 m (System.c:333-335)."""
-    decks = [D.wave_flume(length, depth, dx, layers, eta, amplitude=a, period=T) for a, T in pistons]
+    decks = [D.wave_flume(length, depth, dx, layers, eta, amplitude=a, period=T, piston_layers=layers,
+                          hydrostatic_walls=True) for a, T in pistons]
     amax = max(a for a, _ in pistons)
     pad = 4 * eta * dx + layers * dx + 2 * amax
     pitch = 2.0 * depth + 2 * pad
@@ -263,9 +264,9 @@ def flume_batch(pistons: Sequence[Tuple[float, float]], length: float = 4.0, dep
             b = blk.copy()
             b[:, 1] += off
             out.append(b)
-        x0.append(d.moving[:, 0].copy())
-        hs.append(np.full(d.moving.shape[0], a))
-        om.append(np.full(d.moving.shape[0], 2.0 * math.pi / T))
+        x0.append(d.wall_table[0])
+        hs.append(d.wall_table[1])
+        om.append(d.wall_table[2])
     p = dict(decks[0].params)
     deck = D.Deck(p, np.concatenate(fl), np.zeros((0, 12)), np.concatenate(fx), np.concatenate(mv), eta_override=eta)
     lo = (-pad, -pad)
@@ -401,3 +402,174 @@ def state_errors(a: Dict[str, np.ndarray], b: Dict[str, np.ndarray], nf: int, de
     ok = ~np.isnan(ha) & ~np.isnan(hb)
     surf = float(np.max(np.abs(ha[ok] - hb[ok])) / depth) if ok.any() else 0.0
     return {"rho_rms": float(np.sqrt(np.mean(rel * rel))), "rho_max": float(np.max(np.abs(rel))), "surface": surf}
+
+
+# ---- the wave-flume surrogate: data, training, evaluation ---------------------------------
+def draw_pistons(seed: int, count: int) -> List[Tuple[float, float]]:
+    """Piston (amplitude, period) pairs of the workload: A ~ U[0.02, 0.06] m,
+    T ~ U[1.0, 1.6] s."""
+    rng = np.random.default_rng(seed)
+    return [(float(rng.uniform(0.02, 0.06)), float(rng.uniform(1.0, 1.6))) for _ in range(count)]
+
+
+def train_flume(out_path: Optional[str] = None, seed: int = 0, n_flumes: int = 6, length: float = 4.0,
+                depth: float = 0.5, dx: float = 0.005, macro_steps: int = 40, warm_time: float = 1.0,
+                windows: int = 16, window_gap_time: float = 0.1, pairs_per_window: int = 10, iters: int = 3000,
+                lr: float = 5e-4, noise_vel: float = 0.0, noise_rho: float = 0.0, log=print) -> dict:
+    """Generates flume trajectories with the plain FP32-pair WCSPH solver,
+    trains a 3-round network on them (the last window held out) and saves
+    it.  Returns the training record (with the trained Surrogate)."""
+    import time
+
+    import torch
+    t0 = time.time()
+    pistons = draw_pistons(seed, n_flumes)
+    batch = flume_batch(pistons, length, depth, dx)
+    p = batch.deck.uph_params(PROFILE_WCSPH, PREC_FP32_PAIR)
+    cfg = NetConfig.for_params(p, macro_steps)
+    dt = cfg.dt
+    frames = generate_frames(batch, cfg, int(round(warm_time / dt)), windows, int(round(window_gap_time / dt)),
+                             pairs_per_window)
+    torch.cuda.synchronize()
+    t_gen = time.time() - t0
+    held = frames[-pairs_per_window:] if windows > 1 else frames[-1:]
+    train_frames = frames[:-pairs_per_window] if windows > 1 else frames
+    cfg.out_scale = fit_output_scales(train_frames)
+    nf = batch.deck.n_fluid
+    u2 = sum(float((f.nodes.u[:nf] ** 2 + f.nodes.v[:nf] ** 2).mean()) for f in train_frames) / len(train_frames)
+    cfg.vel_scale = max(math.sqrt(u2), 1e-3)
+    log(f"frames {len(frames)} ({batch.deck.n_all} nodes each) in {t_gen:.1f} s; scales {cfg.out_scale}, "
+        f"U {cfg.vel_scale:.4f}")
+    sur = Surrogate(cfg, batch.deck.n_all, seed=seed)
+
+    def held_loss():
+        scale = torch.tensor(cfg.out_scale, dtype=torch.float64, device="cuda")
+        tot = 0.0
+        for f in held:
+            l, _ = sur.gradients(f.nodes, (f.raw / scale).to(torch.float32).contiguous(), want_grad=False)
+            tot += l
+        return tot / len(held)
+
+    l0 = held_loss()
+    t1 = time.time()
+    hist = train(sur, train_frames, iters, lr=lr, seed=seed, noise_vel=noise_vel, noise_rho=noise_rho,
+                 log_every=max(1, iters // 20))
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    l1 = held_loss()
+    for it, l in hist:
+        log(f"  iter {it:6d}  loss {l:.5f}")
+    log(f"held-out loss {l0:.4f} -> {l1:.4f}; {iters} iterations in {t_train:.1f} s "
+        f"({1e3 * t_train / max(1, iters):.2f} ms each)")
+    rec = dict(pistons=np.array(pistons), history=np.array(hist), held_loss=np.array([l0, l1]),
+               seconds=np.array([t_gen, t_train]), nodes=np.array(batch.deck.n_all))
+    if out_path:
+        sur.save(out_path, **rec)
+    rec["surrogate"] = sur
+    return rec
+
+
+def evaluate_flume(sur: Surrogate, length: float = 4.0, depth: float = 0.5, dx: float = 0.005,
+                   piston: Tuple[float, float] = (0.04, 1.3), warm_time: float = 0.5, steps: int = 2000,
+                   judge: Optional[Judge] = None, precision: int = PREC_FP32_PAIR, plain_precision: int = None,
+                   baselines: bool = True, log=print) -> dict:
+    """One flume (the workload's geometry, `length` long) warmed up from rest
+    by the plain solver, then advanced `steps` SPH steps (a) by the plain
+    solver in `plain_precision` and (b) by the surrogate with its judge, from
+    the same state.  Returns the errors of (b) against (a), the wall times and
+    the judge's report; with `baselines` also the errors of the network alone
+    (no judge) and of a zero network (x += T u, nothing else changes)."""
+    import time
+
+    import torch
+
+    from ._capi import PREC_FP64
+    from .sim import Simulation
+    plain_precision = PREC_FP64 if plain_precision is None else plain_precision
+    A, T = piston
+    deck = D.wave_flume(length, depth, dx, amplitude=A, period=T, piston_layers=3, hydrostatic_walls=True)
+    K = sur.cfg.macro_steps
+    nmacro = steps // K
+    steps = nmacro * K
+    warm = int(round(warm_time / sur.cfg.dt))
+    w = Simulation.from_deck(deck, PROFILE_WCSPH, precision)
+    w.step(warm)
+    st0 = w.download()
+    w.close()
+    nf = deck.n_fluid
+    judge = judge or Judge(depth=depth, surface_x0=0.0, surface_x1=length, surface_bins=int(length / 0.05))
+    bins = judge.surface_bins
+
+    def new_sim(prec):
+        sim = Simulation(deck.uph_params(PROFILE_WCSPH, prec))
+        sim.upload(st0, warm)
+        sim.set_wall_motion(*deck.wall_table)
+        return sim
+
+    def run_plain(prec):
+        sim = new_sim(prec)
+        sim.step(K)  # untimed: first-call allocations
+        sim.upload(st0, warm)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(nmacro):
+            sim.step(K)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t
+        out = sim.download()
+        sim.close()
+        return out, el
+
+    def run_sur(net, jd):
+        sim = new_sim(precision)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        rep = net.advance(sim, nmacro, jd)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t
+        out = sim.download()
+        sim.close()
+        return out, el, rep
+
+    ref, t_plain = run_plain(plain_precision)
+    res = {"n_fluid": nf, "steps": steps, "macro_steps": K, "t_plain": t_plain}
+    st, t_sur, rep = run_sur(sur, judge)
+    res.update(t_surrogate=t_sur, report=rep.to_dict(), errors=state_errors(st, ref, nf, depth, 0.0, length, bins))
+    res["speedup"] = t_plain / t_sur
+    if baselines:
+        off = dataclasses.replace(judge, judge_every=1 << 30)
+        st_n, t_n, _ = run_sur(sur, off)
+        res["network_only"] = state_errors(st_n, ref, nf, depth, 0.0, length, bins)
+        res["t_network_only"] = t_n
+        zero = Surrogate(sur.cfg, sur.capacity, np.zeros(sur.count, np.float32))
+        st_z, _, _ = run_sur(zero, off)
+        zero.close()
+        res["zero_network"] = state_errors(st_z, ref, nf, depth, 0.0, length, bins)
+        fs, t_fs = run_plain(precision)
+        res["plain_same_precision"] = state_errors(fs, ref, nf, depth, 0.0, length, bins)
+        res["t_plain_same_precision"] = t_fs
+    log(res)
+    return res
+
+
+if __name__ == "__main__":
+    import argparse
+    import os
+    ap = argparse.ArgumentParser(description="train the wave-flume surrogate on the GPU")
+    ap.add_argument("--out", default="uph_b200/weights/flume_mpnn.npz")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--flumes", type=int, default=6)
+    ap.add_argument("--length", type=float, default=4.0)
+    ap.add_argument("--macro-steps", type=int, default=40)
+    ap.add_argument("--warm-time", type=float, default=1.0)
+    ap.add_argument("--windows", type=int, default=16)
+    ap.add_argument("--pairs", type=int, default=10)
+    ap.add_argument("--iters", type=int, default=3000)
+    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--noise-vel", type=float, default=0.0)
+    ap.add_argument("--noise-rho", type=float, default=0.0)
+    a = ap.parse_args()
+    os.makedirs(os.path.dirname(a.out) or ".", exist_ok=True)
+    train_flume(a.out, a.seed, a.flumes, a.length, macro_steps=a.macro_steps, warm_time=a.warm_time,
+                windows=a.windows, pairs_per_window=a.pairs, iters=a.iters, lr=a.lr, noise_vel=a.noise_vel,
+                noise_rho=a.noise_rho)
