@@ -122,17 +122,22 @@ typedef struct {
   int64_t graph_overflows;  /* macro steps handed to the plain solver because a
                                node had more than UPH_SUR_MAX_DEGREE partners
                                (each also starts a fallback) */
+  int64_t rejected_steps;   /* predictions the sanity guard rejected (a value
+                               not finite, or a density beyond rho0 (1 +- 0.05));
+                               the plain solver took the macro step and the
+                               fallback after it */
   double last_rho_err, last_surface_err;
   double max_rho_err, max_surface_err;
 } uph_sur_report;
 
 /* Advances a WCSPH simulation by `macro_steps` macro steps (each
- * cfg.macro_steps SPH steps).  A network step replaces the fluid state in
- * place and restarts the simulation's leapfrog; a judged step runs the plain
- * solver over the macro step instead and compares the network's prediction
- * for it (RMS relative density error, largest free-surface height
- * difference); a failed check hands the next fallback_macro macro steps to
- * the plain solver.  Counts accumulate into *report (host).  The judge
+ * cfg.macro_steps SPH steps).  Every network prediction first passes a
+ * sanity guard; a network step then replaces the fluid state and restarts
+ * the simulation's leapfrog.  A judged step also runs the plain solver over
+ * the same macro step from the same state and compares the prediction with
+ * its result (RMS relative density error, largest free-surface height
+ * difference): a passing prediction is kept, a failing one leaves the plain
+ * state and hands the next fallback_macro macro steps to the plain solver.  Counts accumulate into *report (host).  The judge
  * schedule (macro steps since the last check, fallback steps left) carries
  * over between calls on the same simulation and restarts for another one. */
 uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t macro_steps, const uph_sur_judge *judge,

@@ -148,23 +148,41 @@ def _judge(**kw):
     return SG.Judge(depth=0.2, surface_x0=0.0, surface_x1=1.0, surface_bins=20, **kw)
 
 
-def test_judge_on_every_step_reproduces_the_plain_solver():
-    """judge_every = 1: every macro step is the plain solver's, so the state
-    is bitwise the plain trajectory whatever the network predicts."""
+def _plain_equal(sur, judge, n_macro):
     b = _batch()
-    cfg = _cfg(b, K=5)
-    sur = SG.Surrogate(cfg, b.deck.n_all, _params(7))
     a, p = _sim(b), _sim(b)
     a.step(3)
     p.step(3)
-    rep = sur.advance(a, 4, _judge(judge_every=1))
-    for _ in range(4):
-        p.step(5)
+    rep = sur.advance(a, n_macro, judge)
+    for _ in range(n_macro):
+        p.step(sur.cfg.macro_steps)
     sa, sp = a.download(), p.download()
     for k in ("Position", "Velocity", "density"):
         assert np.array_equal(sa[k], sp[k]), k
-    assert (rep.judged_steps, rep.network_steps, rep.plain_steps) == (4, 0, 20)
+    return rep
+
+
+def test_failing_judge_on_every_step_reproduces_the_plain_solver():
+    """Every macro step judged and every check failed (threshold 1e-12, no
+    extra fallback): the state is bitwise the plain solver's trajectory."""
+    b = _batch()
+    sur = SG.Surrogate(_cfg(b, K=5), b.deck.n_all, _params(7))
+    rep = _plain_equal(sur, _judge(judge_every=1, fallback_macro=0, max_rho_err=1e-12), 4)
+    assert (rep.judged_steps, rep.failed_checks, rep.network_steps, rep.plain_steps) == (4, 4, 0, 20)
     assert rep.max_rho_err > 0
+
+
+def test_sanity_guard_rejects_implausible_predictions():
+    """A network whose density output is far off (+1000 kg/m^3 per macro
+    step) never touches the state: every prediction is rejected and the
+    plain solver takes each macro step."""
+    b = _batch()
+    flat = _params(9)
+    off, _ = SO.offsets(3)
+    flat[off["dec2.b"][0] + 4] = 1000.0
+    sur = SG.Surrogate(_cfg(b, K=5), b.deck.n_all, flat)
+    rep = _plain_equal(sur, _judge(judge_every=3, fallback_macro=0), 4)
+    assert (rep.rejected_steps, rep.network_steps, rep.plain_steps) == (4, 0, 20)
 
 
 def test_failed_check_hands_over_to_the_plain_solver():
@@ -179,10 +197,11 @@ def test_failed_check_hands_over_to_the_plain_solver():
     assert (rep.macro_steps, rep.network_steps, rep.judged_steps, rep.failed_checks) == (7, 2, 2, 2)
     assert rep.plain_steps == 5 * 5
     # generous thresholds: nothing fails, every second macro step is judged
+    # and its prediction kept
     sim2 = _sim(b)
     sim2.step(2)
     rep2 = sur.advance(sim2, 7, _judge(judge_every=2, max_rho_err=1e9, max_surface_err=1e9))
-    assert (rep2.network_steps, rep2.judged_steps, rep2.failed_checks, rep2.plain_steps) == (4, 3, 0, 15)
+    assert (rep2.network_steps, rep2.judged_steps, rep2.failed_checks, rep2.plain_steps) == (7, 3, 0, 15)
     st = sim2.download()
     assert np.all(np.isfinite(st["Position"])) and np.all(np.isfinite(st["density"]))
     sim2.step(10)  # the plain solver carries on from a network-made state

@@ -169,7 +169,7 @@ class SurJudge(C.Structure):
 
 class SurReport(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("macro_steps", "network_steps", "judged_steps", "failed_checks",
-                                         "plain_steps", "graph_overflows")] + \
+                                         "plain_steps", "graph_overflows", "rejected_steps")] + \
                [(k, C.c_double) for k in ("last_rho_err", "last_surface_err", "max_rho_err", "max_surface_err")]
 
     def to_dict(self) -> dict:

@@ -439,10 +439,16 @@ struct OutScale {
   double s[kNOut];
 };
 
-// network step of the fluid slots: the new state in place (pred == null) or
-// into pred[orig][5] = (x, y, u, v, rho) for the judge
-__global__ void k_sur_apply(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
-                            double *__restrict__ pred, unsigned *err)
+// Threshold of the sanity guard: a prediction whose density leaves
+// rho0 (1 +- kMaxRhoDev) is rejected (weakly compressible flow stays within
+// about 1 % of rho0).
+constexpr double kMaxRhoDev = 0.05;
+
+// network prediction of the fluid slots into pred[orig][5] =
+// (x, y, u, v, rho); flags *bad when a value is non-finite or the density
+// leaves the guard band
+__global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
+                              double *__restrict__ pred, unsigned *bad)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.nf) return;
@@ -453,24 +459,32 @@ __global__ void k_sur_apply(DevParams P, SlotArrays S, const float *__restrict__
   const double un = u + sc.s[2] * o[2];
   const double vn = v + sc.s[3] * o[3];
   const double rho = S.rho[a] + sc.s[4] * o[4];
-  if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !isfinite(rho) || rho <= 0.0)
-    atomicOr(err, ERR_NAN);
-  if (pred) {
-    double *q = pred + (size_t)S.orig[a] * kNOut;
-    q[0] = x;
-    q[1] = y;
-    q[2] = un;
-    q[3] = vn;
-    q[4] = rho;
-    return;
-  }
+  if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !(fabs(rho / P.rho0 - 1.0) <= kMaxRhoDev))
+    atomicOr(bad, 1u);
+  double *q = pred + (size_t)S.orig[a] * kNOut;
+  q[0] = x;
+  q[1] = y;
+  q[2] = un;
+  q[3] = vn;
+  q[4] = rho;
+}
+
+// an accepted prediction becomes the fluid state (slots found through their
+// reference index, so it survives re-sorts in between); WCSPH pressure is
+// the Tait law of the density, the local* fields equal the state
+__global__ void k_sur_commit(DevParams P, SlotArrays S, const double *__restrict__ pred)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const double *q = pred + (size_t)S.orig[a] * kNOut;
+  const double rho = q[4];
   const double p = tait_p(P, rho);
-  S.x[a] = x;
-  S.y[a] = y;
-  S.u[a] = un;
-  S.v[a] = vn;
-  S.ut[a] = un;
-  S.vt[a] = vn;
+  S.x[a] = q[0];
+  S.y[a] = q[1];
+  S.u[a] = q[2];
+  S.v[a] = q[3];
+  S.ut[a] = q[2];
+  S.vt[a] = q[3];
   S.rho[a] = rho;
   S.rhot[a] = rho;
   S.p[a] = p;
@@ -539,6 +553,7 @@ struct uph_surrogate {
   cudaStream_t stream = nullptr;
   std::vector<void *> allocs;
   unsigned *d_err = nullptr;
+  unsigned *d_bad = nullptr;  // sanity guard of the last prediction
   // parameters: FP32 master, BF16 copy, gradient, Adam moments
   float *w = nullptr, *g = nullptr, *am = nullptr, *av = nullptr;
   bf16 *wb = nullptr;
@@ -935,6 +950,7 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
     if (e == cudaSuccess) e = salloc(s, p, count);
   };
   A(&s->d_err, 1);
+  A(&s->d_bad, 1);
   A(&s->w, P);
   A(&s->g, P);
   A(&s->am, P);
@@ -1134,19 +1150,33 @@ uph_status prepare_sim(uph_surrogate *s, uph_sim *sim, bool *fits)
   return err ? check_err(s) : UPH_OK;
 }
 
-// the prepared graph through the network; the prediction replaces the
-// fluid state, or goes to pred (reference-indexed) for the judge
-uph_status network_step(uph_surrogate *s, uph_sim *sim, double *pred)
+// the prepared graph through the network into s->pred; *ok is false when
+// the sanity guard rejects the prediction
+uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *ok)
 {
   SimView sv = sim_view(sim);
   TRYS(forward_net(s, sv.P.n));
   OutScale sc;
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
+  UPH_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(unsigned), s->stream));
   if (sv.P.nf > 0)
-    k_sur_apply<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, pred, sv.err);
-  UPH_CUDA(cudaGetLastError());
+    k_sur_predict<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, s->pred, s->d_bad);
+  unsigned bad = 0;
+  UPH_CUDA(cudaMemcpyAsync(&bad, s->d_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream));
+  TRYS(check_err(s));
+  *ok = bad == 0;
   return UPH_OK;
+}
+
+// s->pred becomes the simulation's fluid state, `nsteps` SPH steps after
+// the current time (0 when the plain solver already advanced the clock)
+uph_status network_commit(uph_surrogate *s, uph_sim *sim, int nsteps)
+{
+  SimView sv = sim_view(sim);
+  if (sv.P.nf > 0) k_sur_commit<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->pred);
+  UPH_CUDA(cudaGetLastError());
+  return sim_jump(sim, nsteps);
 }
 
 }  // namespace
@@ -1207,16 +1237,28 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
       report->plain_steps += K;
       continue;
     }
+    bool ok = true;
+    TRYS(network_predict(s, sim, &ok));
+    if (!ok) {
+      // an implausible prediction (non-finite, or density beyond the guard
+      // band) never reaches the state: the plain solver takes over
+      report->rejected_steps++;
+      s->since_judge = 0;
+      s->fallback_left = judge->fallback_macro;
+      TRYS(uph_sim_step(sim, K));
+      report->plain_steps += K;
+      continue;
+    }
     if (s->since_judge < judge->judge_every) {
-      TRYS(network_step(s, sim, nullptr));
-      TRYS(sim_jump(sim, K));
+      TRYS(network_commit(s, sim, K));
       report->network_steps++;
       continue;
     }
-    // judged macro step: predict, run the plain solver over the same span,
-    // compare, keep the plain state
+    // judged macro step: the plain solver runs over the same span from the
+    // same state; a prediction that passes the check is kept (the network's
+    // trajectory goes on undisturbed), a failed one leaves the plain state
+    // and starts the fallback
     s->since_judge = 0;
-    TRYS(network_step(s, sim, s->pred));
     TRYS(uph_sim_step(sim, K));
     report->plain_steps += K;
     report->judged_steps++;
@@ -1252,6 +1294,9 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
     if (!(rho_err <= judge->max_rho_err) || !(surf <= judge->max_surface_err)) {
       report->failed_checks++;
       s->fallback_left = judge->fallback_macro;
+    } else {
+      TRYS(network_commit(s, sim, 0));
+      report->network_steps++;
     }
   }
   return sim_check(sim);
