@@ -89,6 +89,11 @@ uph_status uph_sur_set_stream(uph_surrogate *s, void *stream);
 int64_t uph_sur_param_count(int32_t rounds);
 uph_status uph_sur_set_params(uph_surrogate *s, const float *host, int64_t count);
 uph_status uph_sur_get_params(uph_surrogate *s, float *host, int64_t count);
+/* on != 0 (the default): uph_sur_forward and uph_sur_advance run the
+ * network through the fused node-chain kernels (one per round, every layer
+ * of a round on chip); 0: one GEMM per layer, as the training path does.
+ * Both compute the same network. */
+uph_status uph_sur_set_fused(uph_surrogate *s, int32_t on);
 /* resets the Adam moments and step count */
 uph_status uph_sur_reset_optimizer(uph_surrogate *s);
 

@@ -25,8 +25,9 @@ numpy float64 exactly what the GPU kernels compute:
   backward pass of all of the above.
 
 With ``emulate=True`` every value the GPU stores in BF16 is rounded to BF16
-here at the same place (round to nearest even of the FP32 value); everything
-else is float64.  With ``emulate=False`` the whole network is float64 -- the
+here at the same place (round to nearest even of the FP32 value) -- the
+activations, the residual stream h after every residual add, P, Q, S, m --
+and everything else is float64.  With ``emulate=False`` the whole network is float64 -- the
 form the finite-difference check pins.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
@@ -150,7 +151,7 @@ def forward(flat: np.ndarray, F: np.ndarray, g: Graph, rounds: int = 3, emulate:
     Wm = {k: (rb(v) if (v.ndim == 2 and not k.endswith(".we")) else v) for k, v in W.items()}
     c = {"F": F}
     a1 = rb(np.maximum(F @ Wm["enc1.w"].T + W["enc1.b"], 0.0))
-    h = a1 @ Wm["enc2.w"].T + W["enc2.b"]
+    h = rb(a1 @ Wm["enc2.w"].T + W["enc2.b"])
     c["a1"] = a1
     c["rounds"] = []
     for r in range(rounds):
@@ -163,7 +164,7 @@ def forward(flat: np.ndarray, F: np.ndarray, g: Graph, rounds: int = 3, emulate:
         m = rb(S @ Wm[f"r{r}.w2"].T)
         cat = np.concatenate([hb, m], axis=1)
         u = rb(np.maximum(cat @ Wm[f"r{r}.n1.w"].T + W[f"r{r}.n1.b"], 0.0))
-        h = h + (u @ Wm[f"r{r}.n2.w"].T + W[f"r{r}.n2.b"])
+        h = rb(h + (u @ Wm[f"r{r}.n2.w"].T + W[f"r{r}.n2.b"]))
         c["rounds"].append(dict(hb=hb, PQ=PQ, z=z, S=S, m=m, cat=cat, u=u))
     hb = rb(h)
     d1 = rb(np.maximum(hb @ Wm["dec1.w"].T + W["dec1.b"], 0.0))

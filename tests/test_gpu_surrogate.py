@@ -205,3 +205,33 @@ def test_failed_check_hands_over_to_the_plain_solver():
     st = sim2.download()
     assert np.all(np.isfinite(st["Position"])) and np.all(np.isfinite(st["density"]))
     sim2.step(10)  # the plain solver carries on from a network-made state
+
+
+def test_fused_node_chain_matches_per_layer_gemms():
+    """The fused per-round kernels (every layer of a round on chip) against
+    one GEMM per layer, on 40k nodes so that every persistent CTA runs
+    several tiles: the same network, to FP32-accumulation-order accuracy."""
+    rng = np.random.default_rng(11)
+    nx, ny = 400, 100
+    dx = 0.005
+    xs, ys = np.meshgrid(np.arange(nx) * dx, np.arange(ny) * dx)
+    x = (xs.ravel() + rng.uniform(-0.1, 0.1, xs.size) * dx)
+    y = (ys.ravel() + rng.uniform(-0.1, 0.1, xs.size) * dx)
+    n = x.size
+    itype = np.ones(n, np.int32)
+    itype[-2 * nx:] = 2
+    nf = n - 2 * nx
+    st = {"Position": np.stack([x, y], 1), "Velocity": rng.normal(0, 0.05, (n, 2)),
+          "density": 1000.0 * (1 + rng.normal(0, 0.003, n)), "itype": itype}
+    box = (-0.02, -0.02, nx * dx + 0.02, ny * dx + 0.02)
+    cfg = SG.NetConfig(rounds=3, macro_steps=40, radius=2.6 * dx, dt=5e-5)
+    sur = SG.Surrogate(cfg, n, _params(12))
+    nodes = SG.Nodes.from_state(st, nf, box)
+    fused = sur.forward(nodes).cpu().numpy()
+    sur.set_fused(False)
+    plain = sur.forward(nodes).cpu().numpy()
+    scale = np.abs(plain).max()
+    assert scale > 0
+    err = np.abs(fused - plain).max() / scale
+    print("fused vs per-layer max |diff| / max |out|:", err)
+    assert err <= 1e-5

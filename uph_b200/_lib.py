@@ -55,6 +55,7 @@ SIGNATURES = {
     "uph_sur_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "uph_sur_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "uph_sur_reset_optimizer": (C.c_int, [C.c_void_p]),
+    "uph_sur_set_fused": (C.c_int, [C.c_void_p, C.c_int32]),
     "uph_sur_forward": (C.c_int, [C.c_void_p, C.POINTER(SurNodes), C.c_void_p]),
     "uph_sur_gradients": (C.c_int, [C.c_void_p, C.POINTER(SurNodes), C.c_void_p, C.c_void_p,
                                     C.POINTER(C.c_double)]),

@@ -36,6 +36,7 @@ CORE_SOURCES = [
     ("sim.cu", []),
     ("search_noalloc.cu", []),
     ("tc_gemm.cu", ["@cutlass"]),
+    ("node_chain.cu", ["@cutlass"]),
     ("surrogate.cu", []),
 ]
 DROPIN_SOURCES = [("dropin.cpp", [])]

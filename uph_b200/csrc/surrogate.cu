@@ -4,11 +4,15 @@
 // Data layout in HBM, nodes row-major (one row per node, padded to 128
 // columns where a tensor-core K granule needs it):
 //   graph   nbr[n][32] int32 partners (ascending), ef[n][32] float4 (dx, dy, r)/R
-//   F[n][128] BF16 features, a1[n][128] BF16, h[n][128] FP32 (residual stream)
-//   per round: cat[n][256] BF16 = [h | m], PQ[n][256] BF16, S[n][128] BF16,
+//   F[n][128] BF16 features, a1[n][128] BF16
+//   per round: cat[n][256] BF16 = [h | m] (h, the residual stream, is BF16:
+//              each residual add is FP32, then rounded), PQ[n][256] BF16, S[n][128] BF16,
 //              u[n][128] BF16
 //   out[n][128] FP32 (5 columns used)
-// Node-local layers are BF16 GEMMs on the tcgen05 tensor cores (tc_gemm.cu).
+// Node-local layers are BF16 GEMMs on the tcgen05 tensor cores: for training
+// one GEMM per layer with every activation stored (tc_gemm.cu); for
+// inference fused per round, a tile of nodes going through all of a round's
+// layers on chip (node_chain.cu).
 // The edge layer is a warp per receiving node: lane l owns channels
 // [4l, 4l + 4); partner indices and edge features are loaded by lane k for
 // partner k and broadcast by shuffles; Q_j rows are 256-byte coalesced
@@ -24,6 +28,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "node_chain.cuh"
 #include "sim_access.cuh"
 #include "uph_internal.cuh"
 #include "uph_surrogate.h"
@@ -565,13 +570,20 @@ struct uph_surrogate {
   float4 *ef = nullptr;
   // activations
   bf16 *F = nullptr, *a1 = nullptr, *d1 = nullptr;
-  float *h = nullptr, *out = nullptr;
+  float *out = nullptr;
   bf16 *cat[kMaxRounds + 1] = {}, *PQ[kMaxRounds] = {}, *S[kMaxRounds] = {}, *u[kMaxRounds] = {};
   // backward
   bf16 *dO = nullptr, *dz = nullptr, *dhb = nullptr, *dm = nullptr, *dPQ = nullptr;
   float *dh = nullptr, *dS = nullptr;
   float *partials = nullptr, *colpart = nullptr, *wepart = nullptr, *losspart = nullptr, *lossval = nullptr;
   float *sqpart = nullptr, *sumsq = nullptr;
+  // fused inference path (node_chain.cu): pre-swizzled weight images, the
+  // residual stream ping-pong, TMA tensor maps over F, S[0] and h
+  uint8_t *wimg = nullptr;
+  bool img_dirty = true;
+  bool fused = true;
+  bf16 *hb[2] = {};
+  CUtensorMap tm_F, tm_S, tm_H[2];
   // judge
   double *pred = nullptr, *jpart = nullptr;
   unsigned *bins = nullptr;
@@ -747,7 +759,7 @@ uph_status forward_net(uph_surrogate *s, int n)
     GemmCall c;
     c.A = s->a1; c.lda = kLat; c.B = Wb + o.enc2_w; c.ldb = kLat;
     c.M = n; c.N = kLat; c.K = kLat;
-    c.bias = W + o.enc2_b; c.c_f32 = s->h; c.ldc = kLat; c.c_bf16 = s->cat[0]; c.ldc16 = 2 * kLat;
+    c.bias = W + o.enc2_b; c.c_bf16 = s->cat[0]; c.ldc = 2 * kLat;
     TRYS(run(s, c));
   }
   const int rounds = s->cfg.rounds;
@@ -779,8 +791,8 @@ uph_status forward_net(uph_surrogate *s, int n)
       GemmCall c;
       c.A = s->u[r]; c.lda = kLat; c.B = Wb + ro.n2_w; c.ldb = kLat;
       c.M = n; c.N = kLat; c.K = kLat;
-      c.bias = W + ro.n2_b; c.accumulate = 1; c.c_f32 = s->h; c.ldc = kLat;
-      c.c_bf16 = s->cat[r + 1]; c.ldc16 = 2 * kLat;
+      c.bias = W + ro.n2_b; c.residual = s->cat[r]; c.ldr = 2 * kLat;
+      c.c_bf16 = s->cat[r + 1]; c.ldc = 2 * kLat;
       TRYS(run(s, c));
     }
   }
@@ -801,6 +813,80 @@ uph_status forward_net(uph_surrogate *s, int n)
   UPH_CUDA(cudaGetLastError());
   return UPH_OK;
 }
+
+// the shared-memory images of every weight matrix the fused kernels stream
+void build_images(uph_surrogate *s)
+{
+  const ParamOff &o = s->off;
+  auto img = [&](size_t off, int N, int K) { launch_swizzle_image(s->wb + off, N, K, s->wimg + off * sizeof(bf16), s->stream); };
+  img(o.enc1_w, kLat, kFeat);
+  img(o.enc2_w, kLat, kLat);
+  for (int r = 0; r < s->cfg.rounds; r++) {
+    img(o.r[r].pq_w, 2 * kLat, kLat);
+    img(o.r[r].w2, kLat, kLat);
+    img(o.r[r].n1_w, kLat, 2 * kLat);
+    img(o.r[r].n2_w, kLat, kLat);
+  }
+  img(o.dec1_w, kLat, kLat);
+  img(o.dec2_w, kOutPad, kLat);
+  s->img_dirty = false;
+}
+
+// the same network as forward_net through the fused node-chain kernels:
+// one kernel for the encoder and one per round, with the edge layer
+// between them; outputs land in s->out (columns 0..15)
+uph_status forward_fused(uph_surrogate *s, int n)
+{
+  const ParamOff &o = s->off;
+  const float *W = s->w;
+  if (s->img_dirty) build_images(s);
+  auto layer = [&](size_t w_off, const float *bias) {
+    ChainLayer l;
+    l.img = s->wimg + w_off * sizeof(bf16);
+    l.bias = bias;
+    return l;
+  };
+  ChainArgs a;
+  memset(&a, 0, sizeof a);
+  a.n = n;
+  a.ntiles = (n + 127) / 128;
+  a.err = s->d_err;
+  a.mode = CHAIN_ENCODER;
+  a.tm_a = s->tm_F;
+  a.layer[0] = layer(o.enc1_w, W + o.enc1_b);
+  a.layer[1] = layer(o.enc2_w, W + o.enc2_b);
+  a.layer[2] = layer(o.r[0].pq_w, W + o.r[0].pq_b);
+  a.h_out = s->hb[0];
+  a.pq_out = s->PQ[0];
+  TRYS(launch_node_chain(a, s->stream));
+  const int rounds = s->cfg.rounds;
+  for (int r = 0; r < rounds; r++) {
+    const RoundOff &ro = o.r[r];
+    k_sur_edge_fwd<<<kEdgeBlocks, kEdgeThreads, 0, s->stream>>>(n, s->PQ[0], W + ro.we, s->nbr, s->ef, s->deg,
+                                                                s->S[0]);
+    const bool last = r == rounds - 1;
+    a.mode = last ? CHAIN_LAST : CHAIN_ROUND;
+    a.tm_a = s->tm_S;
+    a.tm_h = s->tm_H[r & 1];
+    a.layer[0] = layer(ro.w2, nullptr);
+    a.layer[1] = layer(ro.n1_w, W + ro.n1_b);
+    a.layer[2] = layer(ro.n2_w, W + ro.n2_b);
+    if (last) {
+      a.layer[3] = layer(o.dec1_w, W + o.dec1_b);
+      a.layer[4] = layer(o.dec2_w, W + o.dec2_b);
+      a.h_out = nullptr;
+      a.out = s->out;
+    } else {
+      a.layer[3] = layer(o.r[r + 1].pq_w, W + o.r[r + 1].pq_b);
+      a.h_out = s->hb[(r + 1) & 1];
+    }
+    TRYS(launch_node_chain(a, s->stream));
+  }
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
+
+uph_status forward_any(uph_surrogate *s, int n) { return s->fused ? forward_fused(s, n) : forward_net(s, n); }
 
 // backward from dO (already in s->dO) to s->g
 uph_status backward_net(uph_surrogate *s, int n)
@@ -964,7 +1050,6 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
   A(&s->F, c * kFeat);
   A(&s->a1, c * kLat);
   A(&s->d1, c * kLat);
-  A(&s->h, c * kLat);
   A(&s->out, c * kOutPad);
   for (int r = 0; r <= cfg->rounds; r++) A(&s->cat[r], c * 2 * kLat);
   for (int r = 0; r < cfg->rounds; r++) {
@@ -987,12 +1072,23 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
   A(&s->sqpart, 296);
   A(&s->sumsq, 1);
   A(&s->jpart, 2 * kJudgeBlocks);
+  A(&s->wimg, P * sizeof(bf16));
+  A(&s->hb[0], c * kLat);
+  A(&s->hb[1], c * kLat);
   A(&s->bins, 2 * kMaxBins);
   if (e != cudaSuccess) {
     free_all(s);
     delete s;
     return e == cudaErrorMemoryAllocation ? fail(UPH_OUT_OF_MEMORY, "uph_sur_create: out of device memory")
                                           : cuda_fail(e, "cudaMalloc");
+  }
+  uph_status tr = make_row_tensor_map(&s->tm_F, s->F, s->cap, kFeat * 2);
+  if (tr == UPH_OK) tr = make_row_tensor_map(&s->tm_S, s->S[0], s->cap, kLat * 2);
+  for (int k = 0; k < 2 && tr == UPH_OK; k++) tr = make_row_tensor_map(&s->tm_H[k], s->hb[k], s->cap, kLat * 2);
+  if (tr != UPH_OK) {
+    free_all(s);
+    delete s;
+    return tr;
   }
   cudaMemset(s->d_err, 0, sizeof(unsigned));
   cudaMemset(s->w, 0, sizeof(float) * P);
@@ -1034,6 +1130,7 @@ extern "C" uph_status uph_sur_set_params(uph_surrogate *s, const float *host, in
   if (count != (int64_t)s->off.total) return fail(UPH_BAD_ARG, "uph_sur_set_params: wrong parameter count");
   UPH_CUDA(cudaMemcpyAsync(s->w, host, sizeof(float) * count, cudaMemcpyHostToDevice, s->stream));
   k_f32_to_bf16<<<(unsigned)((count + 255) / 256), 256, 0, s->stream>>>(s->w, s->wb, (size_t)count);
+  s->img_dirty = true;
   UPH_CUDA(cudaStreamSynchronize(s->stream));
   UPH_CUDA(cudaGetLastError());
   return UPH_OK;
@@ -1045,6 +1142,13 @@ extern "C" uph_status uph_sur_get_params(uph_surrogate *s, float *host, int64_t 
   if (count != (int64_t)s->off.total) return fail(UPH_BAD_ARG, "uph_sur_get_params: wrong parameter count");
   UPH_CUDA(cudaMemcpyAsync(host, s->w, sizeof(float) * count, cudaMemcpyDeviceToHost, s->stream));
   UPH_CUDA(cudaStreamSynchronize(s->stream));
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sur_set_fused(uph_surrogate *s, int32_t on)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL surrogate");
+  s->fused = on != 0;
   return UPH_OK;
 }
 
@@ -1062,7 +1166,7 @@ extern "C" uph_status uph_sur_forward(uph_surrogate *s, const uph_sur_nodes *nod
   if (!s || !nodes_ok(nodes)) return fail(UPH_BAD_ARG, "uph_sur_forward: NULL argument");
   const NodesView nv = view_of(nodes);
   TRYS(prepare(s, nv));
-  TRYS(forward_net(s, nv.n));
+  TRYS(forward_any(s, nv.n));
   if (out) k_copy_out<<<(nv.n * kNOut + 255) / 256, 256, 0, s->stream>>>(nv.n, s->out, out);
   s->n_last = nv.n;
   s->nf_last = nv.nf;
@@ -1113,6 +1217,7 @@ extern "C" uph_status uph_sur_adam(uph_surrogate *s, double lr, double beta1, do
   k_adam<<<(unsigned)((P + 255) / 256), 256, 0, s->stream>>>(P, s->w, s->g, s->am, s->av, s->wb, (float)lr,
                                                               (float)beta1, (float)beta2, (float)eps, (float)c1,
                                                               (float)c2, s->sumsq, (float)clip);
+  s->img_dirty = true;
   UPH_CUDA(cudaGetLastError());
   return UPH_OK;
 }
@@ -1155,7 +1260,7 @@ uph_status prepare_sim(uph_surrogate *s, uph_sim *sim, bool *fits)
 uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *ok)
 {
   SimView sv = sim_view(sim);
-  TRYS(forward_net(s, sv.P.n));
+  TRYS(forward_any(s, sv.P.n));
   OutScale sc;
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];

@@ -51,6 +51,8 @@ struct TcGemmArgs {
   const __nv_bfloat16 *mask; // [M x ldm] or null: zero the result where mask <= 0
   int ldm;
   int accumulate;            // add the result to c_f32's contents
+  const __nv_bfloat16 *residual;  // [M x ldr] or null: added after the bias
+  int ldr;
   float *c_f32;              // [M x ldc] or null
   __nv_bfloat16 *c_bf16;     // [M x ldc16] or null
   int ldc, ldc16;
@@ -251,6 +253,11 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
           if (g.bias)
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] += g.bias[col + j];
+          if (g.residual) {
+            const __nv_bfloat16 *rs = g.residual + (size_t)row * g.ldr + col;
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] += __bfloat162float(rs[j]);
+          }
           if (g.accumulate) {
             const float *old = g.c_f32 + (size_t)row * g.ldc + col;
 #pragma unroll
@@ -305,12 +312,12 @@ uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s)
   if (!c.A || !c.B || !c.err || c.M <= 0 || c.N <= 0 || c.K <= 0) return fail(UPH_BAD_ARG, "tc_gemm: bad arguments");
   if (c.K % kTcBK || c.N % kTcN) return fail(UPH_BAD_ARG, "tc_gemm: K must be a multiple of 64, N of 128");
   const int ldc16 = c.ldc16 > 0 ? c.ldc16 : c.ldc;
-  if (c.lda % 8 || c.ldb % 8 || c.ldc % 8 || ldc16 % 8 || (c.mask && c.ldm % 8))
+  if (c.lda % 8 || c.ldb % 8 || c.ldc % 8 || ldc16 % 8 || (c.mask && c.ldm % 8) || (c.residual && c.ldr % 8))
     return fail(UPH_BAD_ARG, "tc_gemm: leading dimensions must be multiples of 8");
   if ((c.a_trans && c.M % 8) || (c.b_trans && c.N % 8))
     return fail(UPH_BAD_ARG, "tc_gemm: a transposed operand needs a multiple of 8 rows");
   int splits = c.splits < 1 ? 1 : c.splits;
-  if (splits > 1 && (!c.partials || !c.c_f32 || c.bias || c.relu || c.c_bf16 || c.mask || c.ldc != c.N))
+  if (splits > 1 && (!c.partials || !c.c_f32 || c.bias || c.relu || c.c_bf16 || c.mask || c.residual || c.ldc != c.N))
     return fail(UPH_BAD_ARG, "tc_gemm: split-K writes a dense FP32 result only, without bias, ReLU or mask");
   if (splits == 1 && !c.c_f32 && !c.c_bf16) return fail(UPH_BAD_ARG, "tc_gemm: no output");
   if (splits == 1 && c.accumulate && !c.c_f32) return fail(UPH_BAD_ARG, "tc_gemm: accumulate needs c_f32");
@@ -339,6 +346,8 @@ uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s)
   g.mask = (const __nv_bfloat16 *)c.mask;
   g.ldm = c.ldm;
   g.accumulate = splits > 1 ? 0 : c.accumulate;
+  g.residual = (const __nv_bfloat16 *)c.residual;
+  g.ldr = c.ldr;
   g.c_f32 = splits > 1 ? nullptr : c.c_f32;
   g.c_bf16 = (__nv_bfloat16 *)c.c_bf16;
   g.ldc = c.ldc;

@@ -148,8 +148,9 @@ void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t 
 
 // BF16 tcgen05 GEMM, C[M x N] = A . B^T with FP32 accumulation.  An operand
 // is K-major ([rows x K], ld >= K) unless its *_trans flag says it is stored
-// [K x rows] (ld >= rows).  Epilogue, in order: + bias[N], + old c_f32
-// (accumulate), ReLU, zero where mask <= 0; then FP32 and/or BF16 stores.
+// [K x rows] (ld >= rows).  Epilogue, in order: + bias[N], + a BF16
+// residual, + old c_f32 (accumulate), ReLU, zero where mask <= 0; then FP32
+// and/or BF16 stores.
 // splits > 1 splits K over CTAs into `partials` (splits * M * N floats) and
 // sums them in split order into a dense c_f32 (ldc == N).
 struct GemmCall {
@@ -164,6 +165,8 @@ struct GemmCall {
   const void *mask = nullptr;
   int ldm = 0;
   int accumulate = 0;
+  const void *residual = nullptr;  // BF16 [M x ldr]
+  int ldr = 0;
   float *c_f32 = nullptr;
   void *c_bf16 = nullptr;
   int ldc = 0;

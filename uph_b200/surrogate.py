@@ -189,6 +189,10 @@ class Surrogate:
         _lib.check(self.lib.uph_sur_get_params(self.handle, a.ctypes.data, a.size), "uph_sur_get_params")
         return a
 
+    def set_fused(self, on: bool) -> None:
+        """Fused node-chain kernels (True, default) or one GEMM per layer."""
+        _lib.check(self.lib.uph_sur_set_fused(self.handle, int(bool(on))), "uph_sur_set_fused")
+
     def reset_optimizer(self) -> None:
         _lib.check(self.lib.uph_sur_reset_optimizer(self.handle), "uph_sur_reset_optimizer")
 
