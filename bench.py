@@ -274,6 +274,8 @@ def gpu_arm(args, rank, world, local_rank):
         variants["batched_tanks"] = batched_arm(args, stream.cuda_stream)
     if not args.no_dambreak:
         variants.update(dambreak_arm(args, stream))
+    if not args.no_surrogate:
+        variants["flume_surrogate"] = surrogate_arm(args, stream)
 
     return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
                 pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
@@ -327,6 +329,94 @@ def dambreak_arm(args, stream):
         s.close()
         out[label] = entry
     return out
+
+
+SURROGATE_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "uph_b200", "weights", "flume_mpnn.npz")
+
+
+def surrogate_arm(args, stream):
+    """The wave-flume configuration with the learned surrogate: flume
+    10.0 x 1.0 m, depth 0.5 m, dx = 0.005 m (200k fluid particles), piston
+    A = 0.04 m, T = 1.3 s, 3-column piston and hydrostatic walls, WCSPH.
+    After a warm-up of `--sur-warm` s from rest (plain FP32 pair), the same
+    state is advanced `--sur-steps` SPH steps
+    - plain: the plain FP64 path (one uph_sim_step per macro step's length);
+    - surrogate: uph_sur_advance with the trained network (fused BF16
+      tcgen05 kernels), the FP32-pair plain solver as the judge every 10th
+      macro step, fallback on a failed check.
+    Both are timed with CUDA events on the simulations' stream.  Errors
+    compare the surrogate's final state with the plain one: RMS and largest
+    relative density error, largest free-surface height difference per
+    5 cm bin as a fraction of the depth."""
+    import torch
+    from uph_b200 import deck as D
+    from uph_b200 import surrogate as SG
+    from uph_b200._capi import PREC_FP32_PAIR, PROFILE_WCSPH
+    from uph_b200.sim import Simulation
+    if not os.path.exists(SURROGATE_WEIGHTS):
+        return {"unavailable": "no trained weights at uph_b200/weights/flume_mpnn.npz"}
+    cfg, params = SG.Surrogate.load_file(SURROGATE_WEIGHTS)
+    L, depth = 10.0, 0.5
+    deck = D.wave_flume(L, depth, 0.005, amplitude=0.04, period=1.3, piston_layers=3, hydrostatic_walls=True)
+    K = cfg.macro_steps
+    nmacro = max(1, args.sur_steps // K)
+    steps = nmacro * K
+    warm = int(round(args.sur_warm / cfg.dt))
+    w = Simulation.from_deck(deck, PROFILE_WCSPH, PREC_FP32_PAIR)
+    w.set_stream(stream.cuda_stream)
+    w.step(warm)
+    st0 = w.download()
+    w.close()
+    nf = deck.n_fluid
+    judge = SG.Judge(depth=depth, surface_x0=0.0, surface_x1=L, surface_bins=int(L / 0.05))
+
+    def new_sim(prec):
+        sim = Simulation(deck.uph_params(PROFILE_WCSPH, prec))
+        sim.set_stream(stream.cuda_stream)
+        sim.upload(st0, warm)
+        sim.set_wall_motion(*deck.wall_table)
+        return sim
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+
+    plain = new_sim(0)
+    plain.step(K)  # first-call allocations, untimed
+    plain.upload(st0, warm)
+    t_plain, _ = timed(lambda: [plain.step(K) for _ in range(nmacro)])
+    ref = plain.download()
+    plain.close()
+    sur = SG.Surrogate(cfg, deck.n_all + 128, params)
+    sur.set_stream(stream.cuda_stream)
+    s = new_sim(PREC_FP32_PAIR)
+    t_sur, rep = timed(lambda: sur.advance(s, nmacro, judge))
+    out = s.download()
+    s.close()
+    err = SG.state_errors(out, ref, nf, depth, 0.0, L, judge.surface_bins)
+    # the network alone (no judge) over the same span, for its own drift
+    s = new_sim(PREC_FP32_PAIR)
+    t_net, _ = timed(lambda: sur.advance(s, nmacro, SG.Judge(depth=depth, surface_x0=0.0, surface_x1=L,
+                                                                surface_bins=judge.surface_bins,
+                                                                judge_every=1 << 30)))
+    net_err = SG.state_errors(s.download(), ref, nf, depth, 0.0, L, judge.surface_bins)
+    s.close()
+    sur.close()
+    # tensor work of one network evaluation: multiply-adds per node of the
+    # encoder (E1, E2, W_pq), each round (W2, N1, N2 and W_pq or Dec1, Dec2)
+    macs = 128 * 128 * 2 + 256 * 128 + cfg.rounds * (128 * 128 + 128 * 256 + 128 * 128 + 256 * 128)
+    flops_eval = 2.0 * macs * deck.n_all
+    r = rep.to_dict()
+    return {"value": nf * steps / t_sur, "plain_fp64_value": nf * steps / t_plain, "speedup_vs_plain": t_plain / t_sur,
+            "n_fluid": nf, "steps": steps, "macro_steps": K, "judge_every": judge.judge_every,
+            "errors_vs_plain": err, "network_only": {"value": nf * steps / t_net, "errors_vs_plain": net_err},
+            "report": r, "network_tflops_per_eval": flops_eval / 1e12,
+            "warm_s": args.sur_warm, "weights": os.path.relpath(SURROGATE_WEIGHTS)}
 
 
 def batched_arm(args, stream_ptr):
@@ -431,6 +521,9 @@ def main():
     ap.add_argument("--graph-replays", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-dambreak", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--sur-steps", type=int, default=4000, help="wave-flume surrogate configuration: SPH steps")
+    ap.add_argument("--sur-warm", type=float, default=1.0, help="wave-flume warm-up from rest (s)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "uph":
         args.warmup = 3

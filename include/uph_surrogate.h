@@ -128,7 +128,9 @@ typedef struct {
                                node had more than UPH_SUR_MAX_DEGREE partners
                                (each also starts a fallback) */
   int64_t rejected_steps;   /* predictions the sanity guard rejected (a value
-                               not finite, or a density beyond rho0 (1 +- 0.05));
+                               not finite, a density beyond rho0 (1 +- 0.05), a
+                               particle moved further than the graph radius or
+                               out of the simulation's domain);
                                the plain solver took the macro step and the
                                fallback after it */
   double last_rho_err, last_surface_err;

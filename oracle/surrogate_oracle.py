@@ -6,7 +6,8 @@ numpy float64 exactly what the GPU kernels compute:
 
 * the neighbour graph: every node's partners within the radius R
   (DBL_EPSILON < r^2 < R^2, r^2 = dx*dx + dy*dy in double -- the pair
-  predicate of the SPH search), sorted by node index;
+  predicate of the SPH search), sorted by node index (the GPU keeps its
+  cell-list order, which changes only the order of FP32 sums);
 * node features, edge features e_ij = ((x_j - x_i)/R, (y_j - y_i)/R, r/R);
 * the network (latent width 128, `rounds` message-passing rounds):
       h0   = Enc2 relu(Enc1 f + b) + b

@@ -8,10 +8,11 @@
 
 namespace uph {
 
-// One layer of a chain: its weight matrix as a pre-swizzled shared-memory
-// image (K/64 atoms of N rows x 128 bytes, 16-byte chunk c of row r at
-// r * 128 + ((c ^ (r % 8)) * 16)) and its FP32 bias (or null).
-struct ChainLayer {
+// One 128 x 128 weight piece of a chain as a pre-swizzled shared-memory
+// image (2 atoms of 128 rows x 128 bytes, 16-byte chunk c of row r at
+// r * 128 + ((c ^ (r % 8)) * 16)) and, on a layer's last piece, the layer's
+// FP32 bias (256 values after the two [P | Q] pieces), else null.
+struct ChainPiece {
   const uint8_t *img;
   const float *bias;
 };
@@ -23,21 +24,24 @@ enum ChainMode : int {
 };
 
 struct ChainArgs {
-  CUtensorMap tm_a;   // the first operand's rows: F (encoder) or S [n x 128] BF16
-  CUtensorMap tm_h;   // h [n x 128] BF16 (rounds)
+  CUtensorMap tm_a;     // the first operand's rows: F (encoder) or S [n x 128] BF16
+  CUtensorMap tm_h;     // h [n x 128] BF16 (rounds)
+  CUtensorMap tm_hout;  // h' [n x 128] BF16 (store_h)
+  CUtensorMap tm_pq;    // [P | Q]' [n x 256] BF16 (encoder, rounds but the last)
   int mode;
   int n, ntiles;
-  ChainLayer layer[5];
-  __nv_bfloat16 *h_out;  // [n x 128]
-  __nv_bfloat16 *pq_out; // [n x 256]
-  float *out;            // [n x 128]; the last round writes columns 0..15
+  int store_h;
+  ChainPiece piece[6];  // encoder: E1 E2 W_P W_Q; rounds: W2 N1a N1b N2 (W_P W_Q | Dec1 Dec2)
+  float *out;           // [n x 128]; the last round writes columns 0..15
   unsigned *err;
 };
 
-// 2-D BF16 tensor map over a row-major [rows x 128] matrix with row stride
-// `row_bytes`, boxes of 128 rows x 64 columns, 128-byte swizzle.
-uph_status make_row_tensor_map(CUtensorMap *map, const void *base, int rows, int row_bytes);
-// writes the shared-memory image of W [N x K] (row-major BF16) to img
+// 2-D BF16 tensor map over a row-major [rows x cols] matrix with row stride
+// `row_bytes`, boxes of 128 rows x 64 columns, 128-byte swizzle (loads and
+// stores of one shared-memory atom).
+uph_status make_row_tensor_map(CUtensorMap *map, const void *base, int rows, int cols, int row_bytes);
+// writes the shared-memory image of W [N x K] (row-major BF16) to img: K/64
+// atoms of N rows x 128 bytes
 void launch_swizzle_image(const __nv_bfloat16 *W, int N, int K, uint8_t *img, cudaStream_t s);
 uph_status launch_node_chain(const ChainArgs &a, cudaStream_t s);
 

@@ -3,7 +3,7 @@
 //
 // Data layout in HBM, nodes row-major (one row per node, padded to 128
 // columns where a tensor-core K granule needs it):
-//   graph   nbr[n][32] int32 partners (ascending), ef[n][32] float4 (dx, dy, r)/R
+//   graph   nbr[n][32] int32 partners (cell-list order), ef[n][32] float4 (dx, dy, r)/R
 //   F[n][128] BF16 features, a1[n][128] BF16
 //   per round: cat[n][256] BF16 = [h | m] (h, the residual stream, is BF16:
 //              each residual add is FP32, then rounded), PQ[n][256] BF16, S[n][128] BF16,
@@ -17,7 +17,7 @@
 // [4l, 4l + 4); partner indices and edge features are loaded by lane k for
 // partner k and broadcast by shuffles; Q_j rows are 256-byte coalesced
 // gathers (the slot order is spatially sorted, so they mostly hit L2).
-// Sums over partners run in ascending partner order and all reductions
+// Sums over partners run in the graph's (deterministic) partner order and all reductions
 // (bias and W_e gradients, loss) use fixed grids and fixed orders, so a
 // forward/backward pass is bitwise reproducible.
 #include <cuda_bf16.h>
@@ -123,8 +123,52 @@ __device__ __forceinline__ float edge_z(float p, float q, const float4 &w, float
   return __fmaf_rn(w.z, e2, __fmaf_rn(w.y, e1, __fmaf_rn(w.x, e0, __fadd_rn(p, q))));
 }
 
+// packed FP32 pairs (sm_100 f32x2 instructions): each half rounds exactly
+// like the scalar FP32 operation, so packed and scalar code agree bitwise
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pack2(float lo, float hi)
+{
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+
+__device__ __forceinline__ void unpack2(f32x2 v, float &lo, float &hi)
+{
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c)
+{
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b)
+{
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// two BF16 values (one 32-bit word) as an FP32 pair
+__device__ __forceinline__ f32x2 bf2_to_f2(uint32_t w)
+{
+  return pack2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+
+__device__ __forceinline__ f32x2 relu2(f32x2 v)
+{
+  float a, b;
+  unpack2(v, a, b);
+  return pack2(fmaxf(a, 0.0f), fmaxf(b, 0.0f));
+}
+
 // ---- graph --------------------------------------------------------------------
-// partners of every node within R (DBL_EPSILON < r^2 < R^2), ascending, and
+// partners of every node within R (DBL_EPSILON < r^2 < R^2) in cell-list
+// order (cells row by row, ids ascending inside a cell: deterministic), and
 // their edge features (dx, dy, r) / R in FP32
 __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const double *__restrict__ y, int n,
                             const int *__restrict__ cell_of, const int *__restrict__ start,
@@ -137,7 +181,6 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
   const double r2cut = R * R;
   const int c = cell_of[i];
   const int cx = c % G.ncx, cy = c / G.ncx;
-  int cand[kMaxDeg];
   int cnt = 0;
   for (int oy = -1; oy <= 1; oy++) {
     const int yy = cy + oy;
@@ -149,7 +192,10 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
       const double dx = x[j] - xi, dy = y[j] - yi;
       const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
       if (r2 > DBL_EPSILON && r2 < r2cut) {
-        if (cnt < kMaxDeg) cand[cnt] = j;
+        if (cnt < kMaxDeg) {
+          nbr[(size_t)i * kMaxDeg + cnt] = j;
+          ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R), 0.0f);
+        }
         cnt++;
       }
     }
@@ -157,22 +203,6 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
   if (cnt > kMaxDeg) {
     atomicOr(err, ERR_NEIGHBOR_OVERFLOW);
     cnt = kMaxDeg;
-  }
-  for (int a = 1; a < cnt; a++) {
-    const int v = cand[a];
-    int b = a - 1;
-    while (b >= 0 && cand[b] > v) {
-      cand[b + 1] = cand[b];
-      b--;
-    }
-    cand[b + 1] = v;
-  }
-  for (int k = 0; k < cnt; k++) {
-    const int j = cand[k];
-    const double dx = x[j] - xi, dy = y[j] - yi;
-    const double r = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-    nbr[(size_t)i * kMaxDeg + k] = j;
-    ef[(size_t)i * kMaxDeg + k] = make_float4((float)(dx / R), (float)(dy / R), (float)(r / R), 0.0f);
   }
   deg[i] = cnt;
 }
@@ -203,7 +233,9 @@ __global__ void k_sur_features(int n, const double *__restrict__ u, const double
 }
 
 // ---- edge layer -----------------------------------------------------------------
-// S_i = sum_j relu(P_i + Q_j + W_e e_ij), PQ rows = [P | Q]
+// S_i = sum_j relu(P_i + Q_j + W_e e_ij), PQ rows = [P | Q].  Channel pairs
+// in packed FP32 (the operation order of edge_z), partners summed in graph
+// order, four partners' Q rows fetched per pass.
 __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16 *__restrict__ PQ,
                                                                  const float *__restrict__ we,
                                                                  const int *__restrict__ nbr,
@@ -216,6 +248,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
   const int c0 = lane * 4;
   float4 w[4];
   for (int c = 0; c < 4; c++) w[c] = *reinterpret_cast<const float4 *>(we + (c0 + c) * 4);
+  const f32x2 w0a = pack2(w[0].x, w[1].x), w1a = pack2(w[0].y, w[1].y), w2a = pack2(w[0].z, w[1].z);
+  const f32x2 w0b = pack2(w[2].x, w[3].x), w1b = pack2(w[2].y, w[3].y), w2b = pack2(w[2].z, w[3].z);
   for (int i = gw; i < n; i += nw) {
     const int d = deg[i];
     int myj = 0;
@@ -224,18 +258,41 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
       myj = nbr[(size_t)i * kMaxDeg + lane];
       mye = ef[(size_t)i * kMaxDeg + lane];
     }
-    float p[4], acc[4] = {0.f, 0.f, 0.f, 0.f};
-    load_bf16x4(PQ + (size_t)i * 2 * kLat + c0, p);
-    for (int k = 0; k < d; k++) {
-      const int j = __shfl_sync(0xffffffffu, myj, k);
-      const float e0 = __shfl_sync(0xffffffffu, mye.x, k);
-      const float e1 = __shfl_sync(0xffffffffu, mye.y, k);
-      const float e2 = __shfl_sync(0xffffffffu, mye.z, k);
-      float q[4];
-      load_bf16x4(PQ + (size_t)j * 2 * kLat + kLat + c0, q);
+    const uint2 praw = *reinterpret_cast<const uint2 *>(PQ + (size_t)i * 2 * kLat + c0);
+    const f32x2 pa = bf2_to_f2(praw.x), pb = bf2_to_f2(praw.y);
+    f32x2 acca = pack2(0.0f, 0.0f), accb = acca;
+    int k = 0;
+    for (; k + 4 <= d; k += 4) {
+      uint2 q[4];
+      float e[4][3];
 #pragma unroll
-      for (int c = 0; c < 4; c++) acc[c] = __fadd_rn(acc[c], fmaxf(edge_z(p[c], q[c], w[c], e0, e1, e2), 0.0f));
+      for (int u = 0; u < 4; u++) {
+        const int j = __shfl_sync(0xffffffffu, myj, k + u);
+        e[u][0] = __shfl_sync(0xffffffffu, mye.x, k + u);
+        e[u][1] = __shfl_sync(0xffffffffu, mye.y, k + u);
+        e[u][2] = __shfl_sync(0xffffffffu, mye.z, k + u);
+        q[u] = *reinterpret_cast<const uint2 *>(PQ + (size_t)j * 2 * kLat + kLat + c0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const f32x2 e0 = pack2(e[u][0], e[u][0]), e1 = pack2(e[u][1], e[u][1]), e2 = pack2(e[u][2], e[u][2]);
+        acca = add2(acca, relu2(fma2(w2a, e2, fma2(w1a, e1, fma2(w0a, e0, add2(pa, bf2_to_f2(q[u].x)))))));
+        accb = add2(accb, relu2(fma2(w2b, e2, fma2(w1b, e1, fma2(w0b, e0, add2(pb, bf2_to_f2(q[u].y)))))));
+      }
     }
+    for (; k < d; k++) {
+      const int j = __shfl_sync(0xffffffffu, myj, k);
+      const float x0 = __shfl_sync(0xffffffffu, mye.x, k);
+      const float x1 = __shfl_sync(0xffffffffu, mye.y, k);
+      const float x2 = __shfl_sync(0xffffffffu, mye.z, k);
+      const uint2 q = *reinterpret_cast<const uint2 *>(PQ + (size_t)j * 2 * kLat + kLat + c0);
+      const f32x2 e0 = pack2(x0, x0), e1 = pack2(x1, x1), e2 = pack2(x2, x2);
+      acca = add2(acca, relu2(fma2(w2a, e2, fma2(w1a, e1, fma2(w0a, e0, add2(pa, bf2_to_f2(q.x)))))));
+      accb = add2(accb, relu2(fma2(w2b, e2, fma2(w1b, e1, fma2(w0b, e0, add2(pb, bf2_to_f2(q.y)))))));
+    }
+    float acc[4];
+    unpack2(acca, acc[0], acc[1]);
+    unpack2(accb, acc[2], acc[3]);
     store_bf16x4(S + (size_t)i * kLat + c0, acc);
   }
 }
@@ -440,8 +497,9 @@ __device__ __forceinline__ double tait_p(const DevParams &P, double rho)
 }
 
 struct OutScale {
-  double T;      // macro_steps * dt
+  double T;         // macro_steps * dt
   double s[kNOut];
+  double max_move;  // the sanity guard's largest displacement (the graph radius)
 };
 
 // Threshold of the sanity guard: a prediction whose density leaves
@@ -450,8 +508,9 @@ struct OutScale {
 constexpr double kMaxRhoDev = 0.05;
 
 // network prediction of the fluid slots into pred[orig][5] =
-// (x, y, u, v, rho); flags *bad when a value is non-finite or the density
-// leaves the guard band
+// (x, y, u, v, rho); flags *bad when a value is non-finite, the density
+// leaves the guard band, or a particle would move more than the graph
+// radius or leave the simulation's domain
 __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
                               double *__restrict__ pred, unsigned *bad)
 {
@@ -464,7 +523,10 @@ __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict
   const double un = u + sc.s[2] * o[2];
   const double vn = v + sc.s[3] * o[3];
   const double rho = S.rho[a] + sc.s[4] * o[4];
-  if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !(fabs(rho / P.rho0 - 1.0) <= kMaxRhoDev))
+  const bool inside = x >= P.lo_x && x <= P.hi_x && y >= P.lo_y && y <= P.hi_y;
+  const bool small_move = fabs(x - S.x[a]) <= sc.max_move && fabs(y - S.y[a]) <= sc.max_move;
+  if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !(fabs(rho / P.rho0 - 1.0) <= kMaxRhoDev) ||
+      !inside || !small_move)
     atomicOr(bad, 1u);
   double *q = pred + (size_t)S.orig[a] * kNOut;
   q[0] = x;
@@ -583,7 +645,7 @@ struct uph_surrogate {
   bool img_dirty = true;
   bool fused = true;
   bf16 *hb[2] = {};
-  CUtensorMap tm_F, tm_S, tm_H[2];
+  CUtensorMap tm_F, tm_S, tm_H[2], tm_PQ;
   // judge
   double *pred = nullptr, *jpart = nullptr;
   unsigned *bins = nullptr;
@@ -822,7 +884,9 @@ void build_images(uph_surrogate *s)
   img(o.enc1_w, kLat, kFeat);
   img(o.enc2_w, kLat, kLat);
   for (int r = 0; r < s->cfg.rounds; r++) {
-    img(o.r[r].pq_w, 2 * kLat, kLat);
+    // W_pq as two 128 x 128 pieces: the P rows, then the Q rows
+    img(o.r[r].pq_w, kLat, kLat);
+    img(o.r[r].pq_w + kLat * kLat, kLat, kLat);
     img(o.r[r].w2, kLat, kLat);
     img(o.r[r].n1_w, kLat, 2 * kLat);
     img(o.r[r].n2_w, kLat, kLat);
@@ -840,11 +904,12 @@ uph_status forward_fused(uph_surrogate *s, int n)
   const ParamOff &o = s->off;
   const float *W = s->w;
   if (s->img_dirty) build_images(s);
-  auto layer = [&](size_t w_off, const float *bias) {
-    ChainLayer l;
-    l.img = s->wimg + w_off * sizeof(bf16);
-    l.bias = bias;
-    return l;
+  constexpr size_t kHalf = (size_t)kLat * kLat * sizeof(bf16);  // one 128 x 128 piece image
+  auto piece = [&](size_t w_off, size_t byte_off, const float *bias) {
+    ChainPiece c;
+    c.img = s->wimg + w_off * sizeof(bf16) + byte_off;
+    c.bias = bias;
+    return c;
   };
   ChainArgs a;
   memset(&a, 0, sizeof a);
@@ -853,11 +918,13 @@ uph_status forward_fused(uph_surrogate *s, int n)
   a.err = s->d_err;
   a.mode = CHAIN_ENCODER;
   a.tm_a = s->tm_F;
-  a.layer[0] = layer(o.enc1_w, W + o.enc1_b);
-  a.layer[1] = layer(o.enc2_w, W + o.enc2_b);
-  a.layer[2] = layer(o.r[0].pq_w, W + o.r[0].pq_b);
-  a.h_out = s->hb[0];
-  a.pq_out = s->PQ[0];
+  a.piece[0] = piece(o.enc1_w, 0, W + o.enc1_b);
+  a.piece[1] = piece(o.enc2_w, 0, W + o.enc2_b);
+  a.piece[2] = piece(o.r[0].pq_w, 0, nullptr);
+  a.piece[3] = piece(o.r[0].pq_w, kHalf, W + o.r[0].pq_b);
+  a.tm_hout = s->tm_H[0];
+  a.tm_pq = s->tm_PQ;
+  a.store_h = 1;
   TRYS(launch_node_chain(a, s->stream));
   const int rounds = s->cfg.rounds;
   for (int r = 0; r < rounds; r++) {
@@ -868,17 +935,20 @@ uph_status forward_fused(uph_surrogate *s, int n)
     a.mode = last ? CHAIN_LAST : CHAIN_ROUND;
     a.tm_a = s->tm_S;
     a.tm_h = s->tm_H[r & 1];
-    a.layer[0] = layer(ro.w2, nullptr);
-    a.layer[1] = layer(ro.n1_w, W + ro.n1_b);
-    a.layer[2] = layer(ro.n2_w, W + ro.n2_b);
+    a.piece[0] = piece(ro.w2, 0, nullptr);
+    a.piece[1] = piece(ro.n1_w, 0, nullptr);
+    a.piece[2] = piece(ro.n1_w, kHalf, W + ro.n1_b);
+    a.piece[3] = piece(ro.n2_w, 0, W + ro.n2_b);
     if (last) {
-      a.layer[3] = layer(o.dec1_w, W + o.dec1_b);
-      a.layer[4] = layer(o.dec2_w, W + o.dec2_b);
-      a.h_out = nullptr;
+      a.piece[4] = piece(o.dec1_w, 0, W + o.dec1_b);
+      a.piece[5] = piece(o.dec2_w, 0, W + o.dec2_b);
+      a.store_h = 0;
       a.out = s->out;
     } else {
-      a.layer[3] = layer(o.r[r + 1].pq_w, W + o.r[r + 1].pq_b);
-      a.h_out = s->hb[(r + 1) & 1];
+      a.piece[4] = piece(o.r[r + 1].pq_w, 0, nullptr);
+      a.piece[5] = piece(o.r[r + 1].pq_w, kHalf, W + o.r[r + 1].pq_b);
+      a.tm_hout = s->tm_H[(r + 1) & 1];
+      a.store_h = 1;
     }
     TRYS(launch_node_chain(a, s->stream));
   }
@@ -1082,9 +1152,10 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
     return e == cudaErrorMemoryAllocation ? fail(UPH_OUT_OF_MEMORY, "uph_sur_create: out of device memory")
                                           : cuda_fail(e, "cudaMalloc");
   }
-  uph_status tr = make_row_tensor_map(&s->tm_F, s->F, s->cap, kFeat * 2);
-  if (tr == UPH_OK) tr = make_row_tensor_map(&s->tm_S, s->S[0], s->cap, kLat * 2);
-  for (int k = 0; k < 2 && tr == UPH_OK; k++) tr = make_row_tensor_map(&s->tm_H[k], s->hb[k], s->cap, kLat * 2);
+  uph_status tr = make_row_tensor_map(&s->tm_F, s->F, s->cap, kFeat, kFeat * 2);
+  if (tr == UPH_OK) tr = make_row_tensor_map(&s->tm_S, s->S[0], s->cap, kLat, kLat * 2);
+  if (tr == UPH_OK) tr = make_row_tensor_map(&s->tm_PQ, s->PQ[0], s->cap, 2 * kLat, 2 * kLat * 2);
+  for (int k = 0; k < 2 && tr == UPH_OK; k++) tr = make_row_tensor_map(&s->tm_H[k], s->hb[k], s->cap, kLat, kLat * 2);
   if (tr != UPH_OK) {
     free_all(s);
     delete s;
@@ -1264,6 +1335,7 @@ uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *ok)
   OutScale sc;
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
+  sc.max_move = s->cfg.radius;
   UPH_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(unsigned), s->stream));
   if (sv.P.nf > 0)
     k_sur_predict<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, s->pred, s->d_bad);
