@@ -129,8 +129,9 @@ typedef struct {
                                (each also starts a fallback) */
   int64_t rejected_steps;   /* predictions the sanity guard rejected (a value
                                not finite, a density beyond rho0 (1 +- 0.05), a
-                               particle moved further than the graph radius or
-                               out of the simulation's domain);
+                               particle moved further than the graph radius,
+                               out of the simulation's domain or closer than
+                               0.2 R to a wall particle);
                                the plain solver took the macro step and the
                                fallback after it */
   double last_rho_err, last_surface_err;

@@ -1,0 +1,118 @@
+"""What the trained surrogate gains over the method without it.
+
+A 4 m wave flume (the workload's cross-section and piston, 80k fluid
+particles), warmed up from rest by the plain solver, is advanced 1,200 SPH
+steps from the same state by
+  (a) the plain FP64 solver (the reference trajectory);
+  (b) the trained network with its plain-SPH judge every 10th macro step;
+  (c) a zero network (every particle keeps its velocity and density and
+      drifts by T u): the same coupling without anything learned;
+  (d) the plain solver with the network's macro step as its time step
+      (40 dt): what the method itself does with a step that long.
+(b) must stay within the workload's bounds (RMS density error <= 1 %,
+free-surface error <= 2 % of the depth) while running at most a fifth of
+the SPH steps and finishing sooner than (a); (c) must have at least twice
+(b)'s free-surface error, and (d) must fail (an error status, or errors
+beyond the bounds)."""
+import os
+
+import numpy as np
+import pytest
+
+from uph_b200 import deck as D
+from uph_b200 import surrogate as SG
+from uph_b200._capi import PREC_FP32_PAIR, PREC_FP64, PROFILE_WCSPH
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "uph_b200", "weights",
+                       "flume_mpnn.npz")
+LENGTH, DEPTH = 4.0, 0.5
+
+
+@pytest.fixture(scope="module")
+def setup():
+    from uph_b200.sim import Simulation
+    if not os.path.exists(WEIGHTS):
+        pytest.skip("no trained weights")
+    cfg, params = SG.Surrogate.load_file(WEIGHTS)
+    deck = D.wave_flume(LENGTH, DEPTH, 0.005, amplitude=0.05, period=1.25, piston_layers=3, hydrostatic_walls=True)
+    warm = int(round(0.5 / cfg.dt))
+    w = Simulation.from_deck(deck, PROFILE_WCSPH, PREC_FP32_PAIR)
+    w.step(warm)
+    st0 = w.download()
+    w.close()
+    return cfg, params, deck, warm, st0
+
+
+def _sim(deck, st0, warm, prec, dt_scale=1.0):
+    from uph_b200.sim import Simulation
+    p = deck.uph_params(PROFILE_WCSPH, prec)
+    p["time_step"] *= dt_scale
+    s = Simulation(p)
+    s.upload(st0, warm)
+    s.set_wall_motion(*deck.wall_table)
+    return s
+
+
+def _timed(fn):
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def test_trained_surrogate_gain(setup):
+    cfg, params, deck, warm, st0 = setup
+    K = cfg.macro_steps
+    nmacro = 1200 // K
+    nf = deck.n_fluid
+    judge = SG.Judge(depth=DEPTH, surface_x0=0.0, surface_x1=LENGTH, surface_bins=int(LENGTH / 0.05))
+    err = lambda a, b: SG.state_errors(a, b, nf, DEPTH, 0.0, LENGTH, judge.surface_bins)
+
+    plain = _sim(deck, st0, warm, PREC_FP64)
+    plain.step(K)  # first-call allocations
+    plain.upload(st0, warm)
+    t_plain, _ = _timed(lambda: [plain.step(K) for _ in range(nmacro)])
+    ref = plain.download()
+    plain.close()
+
+    sur = SG.Surrogate(cfg, deck.n_all, params)
+    s = _sim(deck, st0, warm, PREC_FP32_PAIR)
+    sur.advance(s, 1, judge)  # first-call allocations, then start over
+    s.close()
+    s = _sim(deck, st0, warm, PREC_FP32_PAIR)
+    t_sur, rep = _timed(lambda: sur.advance(s, nmacro, judge))
+    e_sur = err(s.download(), ref)
+    s.close()
+
+    zero = SG.Surrogate(cfg, deck.n_all, np.zeros_like(params))
+    s = _sim(deck, st0, warm, PREC_FP32_PAIR)
+    zero.advance(s, nmacro, SG.Judge(depth=DEPTH, surface_x0=0.0, surface_x1=LENGTH,
+                                     surface_bins=judge.surface_bins, judge_every=1 << 30))
+    e_zero = err(s.download(), ref)
+    s.close()
+
+    coarse_failed = False
+    s = _sim(deck, st0, warm, PREC_FP64, dt_scale=K)
+    try:
+        for _ in range(nmacro):  # one call per step: the first failure stops it
+            s.step(1)
+        e_coarse = err(s.download(), ref)
+        coarse_failed = not (e_coarse["rho_rms"] <= 0.01 and e_coarse["surface"] <= 0.02)
+    except Exception:
+        coarse_failed = True
+    s.close()
+
+    print(f"plain FP64 {t_plain:.3f} s, surrogate {t_sur:.3f} s ({t_plain / t_sur:.2f}x); report {rep.to_dict()}")
+    print(f"surrogate errors {e_sur}; zero network {e_zero}")
+    assert e_sur["rho_rms"] <= 0.01 and e_sur["surface"] <= 0.02, e_sur
+    assert rep.plain_steps <= nmacro * K // 5, rep.to_dict()
+    assert rep.network_steps >= nmacro * 4 // 5, rep.to_dict()
+    assert t_sur < t_plain
+    assert e_zero["surface"] > 2 * e_sur["surface"], (e_zero, e_sur)
+    assert coarse_failed

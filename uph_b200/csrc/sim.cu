@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <array>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -94,6 +95,7 @@ struct uph_sim {
   // the fluid state was replaced from outside (the learned surrogate): the
   // next step starts the leapfrog afresh with the first-step half kick
   bool restart = false;
+  int64_t serial = 0;  // distinct for every simulation this process creates
 };
 
 namespace {
@@ -529,6 +531,10 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &s->d_partials, (size_t)s->n_partials * 4));
   TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   s->own_stream = true;
+  {
+    static std::atomic<int64_t> created{0};
+    s->serial = ++created;
+  }
   TRY(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream));
 #undef TRY
   *out = s;
@@ -1332,6 +1338,7 @@ SimView sim_view(uph_sim *s)
   v.err = s->d_err;
   v.itime = s->itime;
   v.walls_move = walls_move(s);
+  v.serial = s->serial;
   return v;
 }
 

@@ -17,6 +17,7 @@ struct SimView {
   unsigned *err;
   int itime;      // steps completed
   bool walls_move;
+  int64_t serial;  // distinct for every simulation the process creates
 };
 
 SimView sim_view(uph_sim *s);

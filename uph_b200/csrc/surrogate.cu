@@ -233,67 +233,91 @@ __global__ void k_sur_features(int n, const double *__restrict__ u, const double
 }
 
 // ---- edge layer -----------------------------------------------------------------
-// S_i = sum_j relu(P_i + Q_j + W_e e_ij), PQ rows = [P | Q].  Channel pairs
-// in packed FP32 (the operation order of edge_z), partners summed in graph
-// order, four partners' Q rows fetched per pass.
+// S_i = sum_j relu(P_i + Q_j + W_e e_ij), PQ rows = [P | Q].  A half-warp
+// per node, lane l of the half owning channels [8l, 8l + 8) as four packed
+// FP32 pairs (the operation order of edge_z).  Each warp stages its two
+// nodes' edge records (features + partner) in shared memory, so a partner
+// costs one shared broadcast read and one 16-byte gather of its Q row;
+// partners are summed in graph order.
 __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16 *__restrict__ PQ,
                                                                  const float *__restrict__ we,
                                                                  const int *__restrict__ nbr,
                                                                  const float4 *__restrict__ ef,
                                                                  const int *__restrict__ deg, bf16 *__restrict__ S)
 {
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  const int c0 = lane * 4;
-  float4 w[4];
-  for (int c = 0; c < 4; c++) w[c] = *reinterpret_cast<const float4 *>(we + (c0 + c) * 4);
-  const f32x2 w0a = pack2(w[0].x, w[1].x), w1a = pack2(w[0].y, w[1].y), w2a = pack2(w[0].z, w[1].z);
-  const f32x2 w0b = pack2(w[2].x, w[3].x), w1b = pack2(w[2].y, w[3].y), w2b = pack2(w[2].z, w[3].z);
-  for (int i = gw; i < n; i += nw) {
-    const int d = deg[i];
-    int myj = 0;
-    float4 mye = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < d) {
-      myj = nbr[(size_t)i * kMaxDeg + lane];
-      mye = ef[(size_t)i * kMaxDeg + lane];
+  __shared__ float4 rec[kEdgeThreads / 32][2][kMaxDeg];
+  const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4, wib = threadIdx.x >> 5;
+  const int gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;  // global half-warp
+  const int nh = (gridDim.x * blockDim.x) >> 4;
+  const int c0 = hl * 8;
+  f32x2 w0[4], w1[4], w2[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float4 wa = *reinterpret_cast<const float4 *>(we + (c0 + 2 * q) * 4);
+    const float4 wb = *reinterpret_cast<const float4 *>(we + (c0 + 2 * q + 1) * 4);
+    w0[q] = pack2(wa.x, wb.x);
+    w1[q] = pack2(wa.y, wb.y);
+    w2[q] = pack2(wa.z, wb.z);
+  }
+  float4 *my = rec[wib][half];
+  const int passes = (n + nh - 1) / nh;  // the same for both halves of a warp
+  for (int ps = 0; ps < passes; ps++) {
+    const int i = gh + ps * nh;
+    const bool live = i < n;
+    const int d = live ? deg[i] : 0;
+    __syncwarp();  // the last pass's records are read
+    for (int k = hl; k < d; k += 16) {
+      const float4 e = ef[(size_t)i * kMaxDeg + k];
+      my[k] = make_float4(e.x, e.y, e.z, __int_as_float(nbr[(size_t)i * kMaxDeg + k]));
     }
-    const uint2 praw = *reinterpret_cast<const uint2 *>(PQ + (size_t)i * 2 * kLat + c0);
-    const f32x2 pa = bf2_to_f2(praw.x), pb = bf2_to_f2(praw.y);
-    f32x2 acca = pack2(0.0f, 0.0f), accb = acca;
+    __syncwarp();
+    f32x2 p[4], acc[4];
+    {
+      uint4 praw = make_uint4(0u, 0u, 0u, 0u);
+      if (live) praw = *reinterpret_cast<const uint4 *>(PQ + (size_t)i * 2 * kLat + c0);
+      p[0] = bf2_to_f2(praw.x);
+      p[1] = bf2_to_f2(praw.y);
+      p[2] = bf2_to_f2(praw.z);
+      p[3] = bf2_to_f2(praw.w);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[q] = pack2(0.0f, 0.0f);
     int k = 0;
     for (; k + 4 <= d; k += 4) {
-      uint2 q[4];
-      float e[4][3];
+      float4 e[4];
+      uint4 qv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) e[u] = my[k + u];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        qv[u] = *reinterpret_cast<const uint4 *>(PQ + (size_t)__float_as_int(e[u].w) * 2 * kLat + kLat + c0);
 #pragma unroll
       for (int u = 0; u < 4; u++) {
-        const int j = __shfl_sync(0xffffffffu, myj, k + u);
-        e[u][0] = __shfl_sync(0xffffffffu, mye.x, k + u);
-        e[u][1] = __shfl_sync(0xffffffffu, mye.y, k + u);
-        e[u][2] = __shfl_sync(0xffffffffu, mye.z, k + u);
-        q[u] = *reinterpret_cast<const uint2 *>(PQ + (size_t)j * 2 * kLat + kLat + c0);
-      }
+        const f32x2 e0 = pack2(e[u].x, e[u].x), e1 = pack2(e[u].y, e[u].y), e2 = pack2(e[u].z, e[u].z);
+        const uint32_t qw[4] = {qv[u].x, qv[u].y, qv[u].z, qv[u].w};
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const f32x2 e0 = pack2(e[u][0], e[u][0]), e1 = pack2(e[u][1], e[u][1]), e2 = pack2(e[u][2], e[u][2]);
-        acca = add2(acca, relu2(fma2(w2a, e2, fma2(w1a, e1, fma2(w0a, e0, add2(pa, bf2_to_f2(q[u].x)))))));
-        accb = add2(accb, relu2(fma2(w2b, e2, fma2(w1b, e1, fma2(w0b, e0, add2(pb, bf2_to_f2(q[u].y)))))));
+        for (int q = 0; q < 4; q++)
+          acc[q] = add2(acc[q], relu2(fma2(w2[q], e2, fma2(w1[q], e1, fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q])))))));
       }
     }
     for (; k < d; k++) {
-      const int j = __shfl_sync(0xffffffffu, myj, k);
-      const float x0 = __shfl_sync(0xffffffffu, mye.x, k);
-      const float x1 = __shfl_sync(0xffffffffu, mye.y, k);
-      const float x2 = __shfl_sync(0xffffffffu, mye.z, k);
-      const uint2 q = *reinterpret_cast<const uint2 *>(PQ + (size_t)j * 2 * kLat + kLat + c0);
-      const f32x2 e0 = pack2(x0, x0), e1 = pack2(x1, x1), e2 = pack2(x2, x2);
-      acca = add2(acca, relu2(fma2(w2a, e2, fma2(w1a, e1, fma2(w0a, e0, add2(pa, bf2_to_f2(q.x)))))));
-      accb = add2(accb, relu2(fma2(w2b, e2, fma2(w1b, e1, fma2(w0b, e0, add2(pb, bf2_to_f2(q.y)))))));
+      const float4 e = my[k];
+      const uint4 qv = *reinterpret_cast<const uint4 *>(PQ + (size_t)__float_as_int(e.w) * 2 * kLat + kLat + c0);
+      const f32x2 e0 = pack2(e.x, e.x), e1 = pack2(e.y, e.y), e2 = pack2(e.z, e.z);
+      const uint32_t qw[4] = {qv.x, qv.y, qv.z, qv.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        acc[q] = add2(acc[q], relu2(fma2(w2[q], e2, fma2(w1[q], e1, fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q])))))));
     }
-    float acc[4];
-    unpack2(acca, acc[0], acc[1]);
-    unpack2(accb, acc[2], acc[3]);
-    store_bf16x4(S + (size_t)i * kLat + c0, acc);
+    if (live) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 4; q++) unpack2(acc[q], v[2 * q], v[2 * q + 1]);
+      __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+      *reinterpret_cast<uint4 *>(S + (size_t)i * kLat + c0) = *reinterpret_cast<uint4 *>(&h[0]);
+    }
   }
 }
 
@@ -500,6 +524,7 @@ struct OutScale {
   double T;         // macro_steps * dt
   double s[kNOut];
   double max_move;  // the sanity guard's largest displacement (the graph radius)
+  double min_gap;   // the sanity guard's smallest fluid-wall distance (0.2 R)
 };
 
 // Threshold of the sanity guard: a prediction whose density leaves
@@ -509,10 +534,12 @@ constexpr double kMaxRhoDev = 0.05;
 
 // network prediction of the fluid slots into pred[orig][5] =
 // (x, y, u, v, rho); flags *bad when a value is non-finite, the density
-// leaves the guard band, or a particle would move more than the graph
-// radius or leave the simulation's domain
+// leaves the guard band, a particle would move more than the graph radius,
+// leave the simulation's domain or come closer than min_gap to a wall
+// particle (the graph of the current state gives the walls near it)
 __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
-                              double *__restrict__ pred, unsigned *bad)
+                              const int *__restrict__ nbr, const int *__restrict__ deg, double *__restrict__ pred,
+                              unsigned *bad)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.nf) return;
@@ -525,8 +552,20 @@ __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict
   const double rho = S.rho[a] + sc.s[4] * o[4];
   const bool inside = x >= P.lo_x && x <= P.hi_x && y >= P.lo_y && y <= P.hi_y;
   const bool small_move = fabs(x - S.x[a]) <= sc.max_move && fabs(y - S.y[a]) <= sc.max_move;
+  // wall clearance: no fluid particle may end closer than min_gap to a wall
+  // partner (advanced by its own velocity), unless it already was closer
+  bool clear = true;
+  const double g2 = sc.min_gap * sc.min_gap;
+  for (int k = 0; k < deg[a]; k++) {
+    const int j = nbr[(size_t)a * kMaxDeg + k];
+    if (S.itype[j] == 1) continue;
+    const double wx = S.x[j] + sc.T * S.u[j], wy = S.y[j] + sc.T * S.v[j];
+    const double dn = (x - wx) * (x - wx) + (y - wy) * (y - wy);
+    const double d0 = (S.x[a] - S.x[j]) * (S.x[a] - S.x[j]) + (S.y[a] - S.y[j]) * (S.y[a] - S.y[j]);
+    if (dn < g2 && dn < d0) clear = false;
+  }
   if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !(fabs(rho / P.rho0 - 1.0) <= kMaxRhoDev) ||
-      !inside || !small_move)
+      !inside || !small_move || !clear)
     atomicOr(bad, 1u);
   double *q = pred + (size_t)S.orig[a] * kNOut;
   q[0] = x;
@@ -655,7 +694,7 @@ struct uph_surrogate {
   // judged coupling: macro steps since the last check, plain macro steps left
   int since_judge = 0;
   int fallback_left = 0;
-  const uph_sim *last_sim = nullptr;  // the schedule restarts for another simulation
+  int64_t last_sim = 0;  // serial of the simulation the schedule belongs to
 };
 
 namespace {
@@ -1295,9 +1334,9 @@ extern "C" uph_status uph_sur_adam(uph_surrogate *s, double lr, double beta1, do
 
 namespace {
 
-// graph and features of the simulation's current state; *fits is false
-// (and the flag cleared) when a node has more partners than the graph holds
-uph_status prepare_sim(uph_surrogate *s, uph_sim *sim, bool *fits)
+// graph and features of the simulation's current state (no synchronisation:
+// a node with too many partners is found with the prediction's guard)
+uph_status prepare_sim(uph_surrogate *s, uph_sim *sim)
 {
   SimView sv = sim_view(sim);
   if (s->cap < sv.P.n) return fail(UPH_BAD_ARG, "uph_sur_advance: simulation larger than the node capacity");
@@ -1314,21 +1353,14 @@ uph_status prepare_sim(uph_surrogate *s, uph_sim *sim, bool *fits)
   nv.lo_y = sv.P.lo_y;
   nv.hi_x = sv.P.hi_x;
   nv.hi_y = sv.P.hi_y;
-  TRYS(prepare(s, nv));
-  unsigned err = 0;
-  UPH_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaStreamSynchronize(s->stream));
-  *fits = !(err & ERR_NEIGHBOR_OVERFLOW);
-  if (!*fits) {
-    err &= ~ERR_NEIGHBOR_OVERFLOW;
-    UPH_CUDA(cudaMemcpyAsync(s->d_err, &err, sizeof err, cudaMemcpyHostToDevice, s->stream));
-  }
-  return err ? check_err(s) : UPH_OK;
+  return prepare(s, nv);
 }
 
-// the prepared graph through the network into s->pred; *ok is false when
-// the sanity guard rejects the prediction
-uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *ok)
+// the prepared graph through the network into s->pred, then one
+// synchronisation for both checks: *fits is false when a node had more
+// partners than the graph holds (the flag is cleared; the prediction is not
+// to be used), *ok false when the sanity guard rejects the prediction
+uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *fits, bool *ok)
 {
   SimView sv = sim_view(sim);
   TRYS(forward_any(s, sv.P.n));
@@ -1336,12 +1368,22 @@ uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *ok)
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
   sc.max_move = s->cfg.radius;
+  sc.min_gap = 0.2 * s->cfg.radius;
   UPH_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(unsigned), s->stream));
   if (sv.P.nf > 0)
-    k_sur_predict<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, s->pred, s->d_bad);
-  unsigned bad = 0;
+    k_sur_predict<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, s->nbr, s->deg, s->pred,
+                                                                 s->d_bad);
+  unsigned bad = 0, err = 0;
   UPH_CUDA(cudaMemcpyAsync(&bad, s->d_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream));
-  TRYS(check_err(s));
+  UPH_CUDA(cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  UPH_CUDA(cudaGetLastError());
+  *fits = !(err & ERR_NEIGHBOR_OVERFLOW);
+  if (!*fits) {
+    err &= ~ERR_NEIGHBOR_OVERFLOW;
+    UPH_CUDA(cudaMemcpyAsync(s->d_err, &err, sizeof err, cudaMemcpyHostToDevice, s->stream));
+  }
+  if (err) return check_err(s);
   *ok = bad == 0;
   return UPH_OK;
 }
@@ -1380,8 +1422,8 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
   if (fabs(sv.P.dt - s->cfg.dt) > 1e-12 * s->cfg.dt)
     return fail(UPH_BAD_ARG, "uph_sur_advance: the simulation's dt differs from the network's");
   const int K = s->cfg.macro_steps;
-  if (sim != s->last_sim) {
-    s->last_sim = sim;
+  if (sv.serial != s->last_sim) {
+    s->last_sim = sv.serial;
     s->since_judge = 0;
     s->fallback_left = 0;
   }
@@ -1402,8 +1444,9 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
       continue;
     }
     s->since_judge++;
-    bool fits = true;
-    TRYS(prepare_sim(s, sim, &fits));
+    bool fits = true, ok = true;
+    TRYS(prepare_sim(s, sim));
+    TRYS(network_predict(s, sim, &fits, &ok));
     if (!fits) {
       // a state the network's graph cannot hold: the plain solver takes
       // this macro step and the fallback after it
@@ -1414,8 +1457,6 @@ extern "C" uph_status uph_sur_advance(uph_surrogate *s, uph_sim *sim, int32_t ma
       report->plain_steps += K;
       continue;
     }
-    bool ok = true;
-    TRYS(network_predict(s, sim, &ok));
     if (!ok) {
       // an implausible prediction (non-finite, or density beyond the guard
       // band) never reaches the state: the plain solver takes over

@@ -332,6 +332,50 @@ def generate_frames(batch: FlumeBatch, cfg: NetConfig, warm_steps: int, windows:
     return frames
 
 
+def collect_rollout_frames(batch: FlumeBatch, sur: "Surrogate", warm_steps: int, windows: int, window_gap_steps: int,
+                           horizons: Sequence[int], precision: int = PREC_FP32_PAIR,
+                           device: str = "cuda") -> List[Frame]:
+    """Frames from the network's own states: from plain states of the flume
+    batch, the network advances `h` macro steps (for each h in horizons),
+    then the plain solver takes one macro step from that network-made state
+    (its leapfrog restarting, as after any network step); the pair is a
+    training frame.  Teaches the network to correct the drift of its own
+    rollouts (e.g. towards the walls)."""
+    import torch
+    from .sim import Simulation
+    cfg = sur.cfg
+    K = cfg.macro_steps
+    nf = batch.deck.n_fluid
+    p = batch.deck.uph_params(PROFILE_WCSPH, precision)
+    length = batch.box[2]
+    off = Judge(depth=1.0, surface_x0=batch.box[0], surface_x1=length, surface_bins=16, judge_every=1 << 30,
+                fallback_macro=0)
+    sim = Simulation(p)
+    sim.upload(batch.state, 0)
+    sim.set_wall_motion(*batch.wall_table)
+    sim.step(warm_steps)
+    frames = []
+    for w in range(windows):
+        if w:
+            sim.step(window_gap_steps)
+        st = sim.download()
+        itime = int(sim.stats()["itime"])
+        for h in horizons:
+            s2 = Simulation(p)
+            s2.upload(st, itime)
+            s2.set_wall_motion(*batch.wall_table)
+            sur.advance(s2, h, off)
+            s_net = s2.download()
+            s2.step(K)
+            s_plain = s2.download()
+            s2.close()
+            frames.append(Frame(Nodes.from_state(s_net, nf, batch.box, device),
+                                torch.as_tensor(raw_increments(cfg, s_net, s_plain, nf), dtype=torch.float64,
+                                                device=device)))
+    sim.close()
+    return frames
+
+
 def fit_output_scales(frames: List[Frame]) -> Tuple[float, ...]:
     """Root-mean-square of each raw increment over all frames."""
     import torch
@@ -419,10 +463,15 @@ def draw_pistons(seed: int, count: int) -> List[Tuple[float, float]]:
 def train_flume(out_path: Optional[str] = None, seed: int = 0, n_flumes: int = 6, length: float = 4.0,
                 depth: float = 0.5, dx: float = 0.005, macro_steps: int = 40, warm_time: float = 1.0,
                 windows: int = 16, window_gap_time: float = 0.1, pairs_per_window: int = 10, iters: int = 3000,
-                lr: float = 5e-4, noise_vel: float = 0.0, noise_rho: float = 0.0, log=print) -> dict:
+                lr: float = 5e-4, noise_vel: float = 0.0, noise_rho: float = 0.0, dagger_rounds: int = 0,
+                dagger_iters: int = 1500, dagger_horizons: Sequence[int] = (4, 12, 24), dagger_windows: int = 6,
+                dagger_repeat: int = 3, log=print) -> dict:
     """Generates flume trajectories with the plain FP32-pair WCSPH solver,
-    trains a 3-round network on them (the last window held out) and saves
-    it.  Returns the training record (with the trained Surrogate)."""
+    trains a 3-round network on them (the last window held out), then for
+    `dagger_rounds` rounds adds frames that start from the network's own
+    rollouts (collect_rollout_frames, each repeated `dagger_repeat` times in
+    the sampling pool) and trains on, and saves it.  Returns the training
+    record (with the trained Surrogate)."""
     import time
 
     import torch
@@ -458,6 +507,14 @@ def train_flume(out_path: Optional[str] = None, seed: int = 0, n_flumes: int = 6
     t1 = time.time()
     hist = train(sur, train_frames, iters, lr=lr, seed=seed, noise_vel=noise_vel, noise_rho=noise_rho,
                  log_every=max(1, iters // 20))
+    for rnd in range(dagger_rounds):
+        t2 = time.time()
+        extra = collect_rollout_frames(batch, sur, int(round(warm_time / dt)), dagger_windows,
+                                       int(round(2 * window_gap_time / dt)), dagger_horizons)
+        train_frames = train_frames + extra * dagger_repeat
+        log(f"rollout round {rnd}: {len(extra)} frames in {time.time() - t2:.1f} s; held-out {held_loss():.4f}")
+        hist += train(sur, train_frames, dagger_iters, lr=lr * 0.3, seed=seed + 1 + rnd, noise_vel=noise_vel,
+                      noise_rho=noise_rho, log_every=max(1, dagger_iters // 5))
     torch.cuda.synchronize()
     t_train = time.time() - t1
     l1 = held_loss()
@@ -572,8 +629,9 @@ if __name__ == "__main__":
     ap.add_argument("--lr", type=float, default=5e-4)
     ap.add_argument("--noise-vel", type=float, default=0.0)
     ap.add_argument("--noise-rho", type=float, default=0.0)
+    ap.add_argument("--dagger-rounds", type=int, default=2)
     a = ap.parse_args()
     os.makedirs(os.path.dirname(a.out) or ".", exist_ok=True)
     train_flume(a.out, a.seed, a.flumes, a.length, macro_steps=a.macro_steps, warm_time=a.warm_time,
                 windows=a.windows, pairs_per_window=a.pairs, iters=a.iters, lr=a.lr, noise_vel=a.noise_vel,
-                noise_rho=a.noise_rho)
+                noise_rho=a.noise_rho, dagger_rounds=a.dagger_rounds)
