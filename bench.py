@@ -336,7 +336,7 @@ SURROGATE_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "up
 
 def surrogate_arm(args, stream):
     """The wave-flume configuration with the learned surrogate: flume
-    10.0 x 1.0 m, depth 0.5 m, dx = 0.005 m (200k fluid particles), piston
+    10.0 x 1.0 m (`--sur-length`), depth 0.5 m, dx = 0.005 m (200k fluid particles), piston
     A = 0.04 m, T = 1.3 s, 3-column piston and hydrostatic walls, WCSPH.
     After a warm-up of `--sur-warm` s from rest (plain FP32 pair), the same
     state is advanced `--sur-steps` SPH steps
@@ -356,7 +356,7 @@ def surrogate_arm(args, stream):
     if not os.path.exists(SURROGATE_WEIGHTS):
         return {"unavailable": "no trained weights at uph_b200/weights/flume_mpnn.npz"}
     cfg, params = SG.Surrogate.load_file(SURROGATE_WEIGHTS)
-    L, depth = 10.0, 0.5
+    L, depth = args.sur_length, 0.5
     deck = D.wave_flume(L, depth, 0.005, amplitude=0.04, period=1.3, piston_layers=3, hydrostatic_walls=True)
     K = cfg.macro_steps
     nmacro = max(1, args.sur_steps // K)
@@ -522,8 +522,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-dambreak", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
-    ap.add_argument("--sur-steps", type=int, default=4000, help="wave-flume surrogate configuration: SPH steps")
+    ap.add_argument("--sur-steps", type=int, default=2000, help="wave-flume surrogate configuration: SPH steps")
     ap.add_argument("--sur-warm", type=float, default=1.0, help="wave-flume warm-up from rest (s)")
+    ap.add_argument("--sur-length", type=float, default=10.0, help="wave-flume length (m); 10 m is the workload")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "uph":
         args.warmup = 3

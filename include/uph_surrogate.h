@@ -14,7 +14,8 @@
  * on the tcgen05 tensor cores, FP32 accumulation):
  *   h    = Enc2 relu(Enc1 f + b) + b                 f: node features
  *   per round:  [P | Q] = W_pq h + b
- *               s_i = sum_j relu(P_i + Q_j + W_e e_ij)    e_ij = (dx, dy, r) / R
+ *               s_i = sum_j relu(P_i + Q_j + W_e e_ij)
+ *                 e_ij = ((dx, dy, r) / R, (rho_j - rho_i) / (rho0 s_e))  (FP32)
  *               m_i = W_2 s_i
  *               h  <- h + N2 relu(N1 [h ; m] + b) + b
  *   out  = Dec2 relu(Dec1 h + b) + b                 5 normalised increments
@@ -68,6 +69,7 @@ typedef struct {
   double rho0;           /* reference density */
   double vel_scale;      /* U */
   double rho_scale;      /* s_rho */
+  double edge_rho_scale; /* s_e: unit of the edge density difference, relative to rho0 */
   double out_scale[UPH_SUR_OUTPUTS]; /* s0..s4 */
 } uph_sur_config;
 
@@ -84,7 +86,8 @@ uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_capacity, uph_
 uph_status uph_sur_destroy(uph_surrogate *s);
 uph_status uph_sur_set_stream(uph_surrogate *s, void *stream);
 /* number of FP32 parameters for `rounds` rounds (storage layout: the
- * blocks enc1.w enc1.b enc2.w enc2.b, per round pq.w pq.b we[128x4] w2 n1.w
+ * blocks enc1.w enc1.b enc2.w enc2.b, per round pq.w pq.b we[128 x 4 edge
+ * features] w2 n1.w
  * n1.b n2.w n2.b, then dec1.w dec1.b dec2.w dec2.b; matrices [out x in]) */
 int64_t uph_sur_param_count(int32_t rounds);
 uph_status uph_sur_set_params(uph_surrogate *s, const float *host, int64_t count);
@@ -129,9 +132,8 @@ typedef struct {
                                (each also starts a fallback) */
   int64_t rejected_steps;   /* predictions the sanity guard rejected (a value
                                not finite, a density beyond rho0 (1 +- 0.05), a
-                               particle moved further than the graph radius,
-                               out of the simulation's domain or closer than
-                               0.2 R to a wall particle);
+                               particle moved further than the graph radius or
+                               out of the simulation's domain);
                                the plain solver took the macro step and the
                                fallback after it */
   double last_rho_err, last_surface_err;
@@ -139,9 +141,11 @@ typedef struct {
 } uph_sur_report;
 
 /* Advances a WCSPH simulation by `macro_steps` macro steps (each
- * cfg.macro_steps SPH steps).  Every network prediction first passes a
- * sanity guard; a network step then replaces the fluid state and restarts
- * the simulation's leapfrog.  A judged step also runs the plain solver over
+ * cfg.macro_steps SPH steps).  A predicted fluid position closer than
+ * 0.25 R to a wall particle (advanced by its velocity) is moved back out to
+ * 0.25 R and its velocity into the wall removed; every prediction then
+ * passes a sanity guard; a network step replaces the fluid state and
+ * restarts the simulation's leapfrog.  A judged step also runs the plain solver over
  * the same macro step from the same state and compares the prediction with
  * its result (RMS relative density error, largest free-surface height
  * difference): a passing prediction is kept, a failing one leaves the plain

@@ -8,7 +8,8 @@ numpy float64 exactly what the GPU kernels compute:
   (DBL_EPSILON < r^2 < R^2, r^2 = dx*dx + dy*dy in double -- the pair
   predicate of the SPH search), sorted by node index (the GPU keeps its
   cell-list order, which changes only the order of FP32 sums);
-* node features, edge features e_ij = ((x_j - x_i)/R, (y_j - y_i)/R, r/R);
+* node features, edge features e_ij = ((x_j - x_i)/R, (y_j - y_i)/R, r/R,
+  (rho_j - rho_i)/rho_unit) in FP32;
 * the network (latent width 128, `rounds` message-passing rounds):
       h0   = Enc2 relu(Enc1 f + b) + b
       per round:
@@ -86,7 +87,7 @@ def bf16(x) -> np.ndarray:
 class Graph:
     """CSR neighbour lists (receiver-major, partners ascending) + edge features."""
 
-    def __init__(self, x: np.ndarray, y: np.ndarray, radius: float):
+    def __init__(self, x: np.ndarray, y: np.ndarray, radius: float, rho=None, rho_unit: float = 0.1):
         n = x.shape[0]
         r2cut = radius * radius
         indptr = [0]
@@ -118,7 +119,8 @@ class Graph:
         dx = x[self.send] - x[self.recv]
         dy = y[self.send] - y[self.recv]
         r = np.sqrt(dx * dx + dy * dy)
-        self.e = np.stack([dx / radius, dy / radius, r / radius], axis=1).astype(np.float32).astype(np.float64)
+        dr = np.zeros_like(dx) if rho is None else (rho[self.send] - rho[self.recv]) / rho_unit
+        self.e = np.stack([dx / radius, dy / radius, r / radius, dr], axis=1).astype(np.float32).astype(np.float64)
 
     def degree(self) -> np.ndarray:
         return np.diff(self.indptr)
@@ -159,7 +161,7 @@ def forward(flat: np.ndarray, F: np.ndarray, g: Graph, rounds: int = 3, emulate:
         hb = rb(h)
         PQ = rb(hb @ Wm[f"r{r}.pq.w"].T + W[f"r{r}.pq.b"])
         P, Q = PQ[:, :LATENT], PQ[:, LATENT:]
-        we = W[f"r{r}.we"][:, :3]
+        we = W[f"r{r}.we"]
         z = P[g.recv] + Q[g.send] + g.e @ we.T
         S = rb(_segsum(np.maximum(z, 0.0), g.recv, g.n))
         m = rb(S @ Wm[f"r{r}.w2"].T)
@@ -212,9 +214,7 @@ def backward(c: dict, dout: np.ndarray) -> np.ndarray:
         dze = dS[g.recv] * (R["z"] > 0)
         dP = _segsum(dze, g.recv, g.n)
         dQ = _segsum(dze, g.send, g.n)
-        gwe = np.zeros((LATENT, 4))
-        gwe[:, :3] = dze.T @ g.e
-        G[f"r{r}.we"] = gwe
+        G[f"r{r}.we"] = dze.T @ g.e
         dPQ = rb(np.concatenate([dP, dQ], axis=1))
         G[f"r{r}.pq.w"] = dPQ.T @ R["hb"]
         G[f"r{r}.pq.b"] = dPQ.sum(0)

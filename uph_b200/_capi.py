@@ -152,7 +152,7 @@ def state_struct(arrays: dict, keepalive: list) -> UphState:
 class SurConfig(C.Structure):
     _fields_ = [("rounds", C.c_int32), ("macro_steps", C.c_int32), ("radius", C.c_double), ("dt", C.c_double),
                 ("rho0", C.c_double), ("vel_scale", C.c_double), ("rho_scale", C.c_double),
-                ("out_scale", C.c_double * 5)]
+                ("edge_rho_scale", C.c_double), ("out_scale", C.c_double * 5)]
 
 
 class SurNodes(C.Structure):

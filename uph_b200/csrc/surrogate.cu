@@ -3,7 +3,8 @@
 //
 // Data layout in HBM, nodes row-major (one row per node, padded to 128
 // columns where a tensor-core K granule needs it):
-//   graph   nbr[n][32] int32 partners (cell-list order), ef[n][32] float4 (dx, dy, r)/R
+//   graph   nbr[n][32] int32 partners (cell-list order), ef[n][32] float4
+//           ((dx, dy, r)/R, (rho_j - rho_i)/(rho0 s_e))
 //   F[n][128] BF16 features, a1[n][128] BF16
 //   per round: cat[n][256] BF16 = [h | m] (h, the residual stream, is BF16:
 //              each residual add is FP32, then rounded), PQ[n][256] BF16, S[n][128] BF16,
@@ -118,9 +119,9 @@ __device__ __forceinline__ void store_bf16x4(bf16 *p, const float v[4])
 
 // the edge pre-activation, one fixed operation order shared by the forward
 // and backward kernels so both see bit-identical values
-__device__ __forceinline__ float edge_z(float p, float q, const float4 &w, float e0, float e1, float e2)
+__device__ __forceinline__ float edge_z(float p, float q, const float4 &w, float e0, float e1, float e2, float e3)
 {
-  return __fmaf_rn(w.z, e2, __fmaf_rn(w.y, e1, __fmaf_rn(w.x, e0, __fadd_rn(p, q))));
+  return __fmaf_rn(w.w, e3, __fmaf_rn(w.z, e2, __fmaf_rn(w.y, e1, __fmaf_rn(w.x, e0, __fadd_rn(p, q)))));
 }
 
 // packed FP32 pairs (sm_100 f32x2 instructions): each half rounds exactly
@@ -169,15 +170,16 @@ __device__ __forceinline__ f32x2 relu2(f32x2 v)
 // ---- graph --------------------------------------------------------------------
 // partners of every node within R (DBL_EPSILON < r^2 < R^2) in cell-list
 // order (cells row by row, ids ascending inside a cell: deterministic), and
-// their edge features (dx, dy, r) / R in FP32
-__global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const double *__restrict__ y, int n,
-                            const int *__restrict__ cell_of, const int *__restrict__ start,
-                            const int *__restrict__ list, double R, int *__restrict__ nbr,
-                            float4 *__restrict__ ef, int *__restrict__ deg, unsigned *err)
+// their edge features in FP32: (dx, dy, r) / R and the density difference
+// (rho_j - rho_i) / rho_unit
+__global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ rho, double rho_unit, int n, const int *__restrict__ cell_of,
+                            const int *__restrict__ start, const int *__restrict__ list, double R,
+                            int *__restrict__ nbr, float4 *__restrict__ ef, int *__restrict__ deg, unsigned *err)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double xi = x[i], yi = y[i];
+  const double xi = x[i], yi = y[i], ri = rho[i];
   const double r2cut = R * R;
   const int c = cell_of[i];
   const int cx = c % G.ncx, cy = c / G.ncx;
@@ -194,7 +196,8 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
       if (r2 > DBL_EPSILON && r2 < r2cut) {
         if (cnt < kMaxDeg) {
           nbr[(size_t)i * kMaxDeg + cnt] = j;
-          ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R), 0.0f);
+          ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R),
+                                                      (float)((rho[j] - ri) / rho_unit));
         }
         cnt++;
       }
@@ -246,11 +249,12 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
                                                                  const int *__restrict__ deg, bf16 *__restrict__ S)
 {
   __shared__ float4 rec[kEdgeThreads / 32][2][kMaxDeg];
+  __shared__ int recj[kEdgeThreads / 32][2][kMaxDeg];
   const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4, wib = threadIdx.x >> 5;
   const int gh = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;  // global half-warp
   const int nh = (gridDim.x * blockDim.x) >> 4;
   const int c0 = hl * 8;
-  f32x2 w0[4], w1[4], w2[4];
+  f32x2 w0[4], w1[4], w2[4], w3[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const float4 wa = *reinterpret_cast<const float4 *>(we + (c0 + 2 * q) * 4);
@@ -258,8 +262,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
     w0[q] = pack2(wa.x, wb.x);
     w1[q] = pack2(wa.y, wb.y);
     w2[q] = pack2(wa.z, wb.z);
+    w3[q] = pack2(wa.w, wb.w);
   }
   float4 *my = rec[wib][half];
+  int *myj = recj[wib][half];
   const int passes = (n + nh - 1) / nh;  // the same for both halves of a warp
   for (int ps = 0; ps < passes; ps++) {
     const int i = gh + ps * nh;
@@ -267,8 +273,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
     const int d = live ? deg[i] : 0;
     __syncwarp();  // the last pass's records are read
     for (int k = hl; k < d; k += 16) {
-      const float4 e = ef[(size_t)i * kMaxDeg + k];
-      my[k] = make_float4(e.x, e.y, e.z, __int_as_float(nbr[(size_t)i * kMaxDeg + k]));
+      my[k] = ef[(size_t)i * kMaxDeg + k];
+      myj[k] = nbr[(size_t)i * kMaxDeg + k];
     }
     __syncwarp();
     f32x2 p[4], acc[4];
@@ -290,24 +296,27 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_fwd(int n, const bf16
       for (int u = 0; u < 4; u++) e[u] = my[k + u];
 #pragma unroll
       for (int u = 0; u < 4; u++)
-        qv[u] = *reinterpret_cast<const uint4 *>(PQ + (size_t)__float_as_int(e[u].w) * 2 * kLat + kLat + c0);
+        qv[u] = *reinterpret_cast<const uint4 *>(PQ + (size_t)myj[k + u] * 2 * kLat + kLat + c0);
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const f32x2 e0 = pack2(e[u].x, e[u].x), e1 = pack2(e[u].y, e[u].y), e2 = pack2(e[u].z, e[u].z);
+        const f32x2 e3 = pack2(e[u].w, e[u].w);
         const uint32_t qw[4] = {qv[u].x, qv[u].y, qv[u].z, qv[u].w};
 #pragma unroll
         for (int q = 0; q < 4; q++)
-          acc[q] = add2(acc[q], relu2(fma2(w2[q], e2, fma2(w1[q], e1, fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q])))))));
+          acc[q] = add2(acc[q], relu2(fma2(w3[q], e3, fma2(w2[q], e2, fma2(w1[q], e1,
+                                                                              fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q]))))))));
       }
     }
     for (; k < d; k++) {
       const float4 e = my[k];
-      const uint4 qv = *reinterpret_cast<const uint4 *>(PQ + (size_t)__float_as_int(e.w) * 2 * kLat + kLat + c0);
-      const f32x2 e0 = pack2(e.x, e.x), e1 = pack2(e.y, e.y), e2 = pack2(e.z, e.z);
+      const uint4 qv = *reinterpret_cast<const uint4 *>(PQ + (size_t)myj[k] * 2 * kLat + kLat + c0);
+      const f32x2 e0 = pack2(e.x, e.x), e1 = pack2(e.y, e.y), e2 = pack2(e.z, e.z), e3 = pack2(e.w, e.w);
       const uint32_t qw[4] = {qv.x, qv.y, qv.z, qv.w};
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        acc[q] = add2(acc[q], relu2(fma2(w2[q], e2, fma2(w1[q], e1, fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q])))))));
+        acc[q] = add2(acc[q], relu2(fma2(w3[q], e3, fma2(w2[q], e2, fma2(w1[q], e1,
+                                                                            fma2(w0[q], e0, add2(p[q], bf2_to_f2(qw[q]))))))));
     }
     if (live) {
       float v[8];
@@ -338,8 +347,8 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
   const int c0 = lane * 4;
   float4 w[4];
   for (int c = 0; c < 4; c++) w[c] = *reinterpret_cast<const float4 *>(we + (c0 + c) * 4);
-  float g[4][3];
-  for (int c = 0; c < 4; c++) g[c][0] = g[c][1] = g[c][2] = 0.0f;
+  float g[4][4];
+  for (int c = 0; c < 4; c++) g[c][0] = g[c][1] = g[c][2] = g[c][3] = 0.0f;
   for (int a = gw; a < n; a += nw) {
     const int d = deg[a];
     int myj = 0;
@@ -359,6 +368,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
       const float e0 = __shfl_sync(0xffffffffu, mye.x, k);
       const float e1 = __shfl_sync(0xffffffffu, mye.y, k);
       const float e2 = __shfl_sync(0xffffffffu, mye.z, k);
+      const float e3 = __shfl_sync(0xffffffffu, mye.w, k);
       float pb[4], qb[4];
       load_bf16x4(PQ + (size_t)b * 2 * kLat + c0, pb);
       load_bf16x4(PQ + (size_t)b * 2 * kLat + kLat + c0, qb);
@@ -366,13 +376,15 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
       const float dsb[4] = {dsb4.x, dsb4.y, dsb4.z, dsb4.w};
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        if (edge_z(pa[c], qb[c], w[c], e0, e1, e2) > 0.0f) {
+        if (edge_z(pa[c], qb[c], w[c], e0, e1, e2, e3) > 0.0f) {
           dp[c] += dsa[c];
           g[c][0] = __fmaf_rn(dsa[c], e0, g[c][0]);
           g[c][1] = __fmaf_rn(dsa[c], e1, g[c][1]);
           g[c][2] = __fmaf_rn(dsa[c], e2, g[c][2]);
+          g[c][3] = __fmaf_rn(dsa[c], e3, g[c][3]);
         }
-        if (edge_z(pb[c], qa[c], w[c], -e0, -e1, e2) > 0.0f) dq[c] += dsb[c];
+        // the reverse edge: dx, dy and the density difference change sign
+        if (edge_z(pb[c], qa[c], w[c], -e0, -e1, e2, -e3) > 0.0f) dq[c] += dsb[c];
       }
     }
     store_bf16x4(dPQ + (size_t)a * 2 * kLat + c0, dp);
@@ -381,7 +393,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
   // the block's 8 warps summed in warp order: one partial row per block
   __shared__ float4 red[kEdgeThreads / 32][kLat];
   const int wib = threadIdx.x >> 5;
-  for (int c = 0; c < 4; c++) red[wib][c0 + c] = make_float4(g[c][0], g[c][1], g[c][2], 0.0f);
+  for (int c = 0; c < 4; c++) red[wib][c0 + c] = make_float4(g[c][0], g[c][1], g[c][2], g[c][3]);
   __syncthreads();
   if (threadIdx.x < kLat) {
     float4 t = red[0][threadIdx.x];
@@ -390,6 +402,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_sur_edge_bwd(int n, const bf16
       t.x += o.x;
       t.y += o.y;
       t.z += o.z;
+      t.w += o.w;
     }
     reinterpret_cast<float4 *>(we_part)[(size_t)blockIdx.x * kLat + threadIdx.x] = t;
   }
@@ -524,7 +537,7 @@ struct OutScale {
   double T;         // macro_steps * dt
   double s[kNOut];
   double max_move;  // the sanity guard's largest displacement (the graph radius)
-  double min_gap;   // the sanity guard's smallest fluid-wall distance (0.2 R)
+  double min_gap;   // smallest fluid-wall distance a prediction may reach (0.25 R)
 };
 
 // Threshold of the sanity guard: a prediction whose density leaves
@@ -533,10 +546,10 @@ struct OutScale {
 constexpr double kMaxRhoDev = 0.05;
 
 // network prediction of the fluid slots into pred[orig][5] =
-// (x, y, u, v, rho); flags *bad when a value is non-finite, the density
-// leaves the guard band, a particle would move more than the graph radius,
-// leave the simulation's domain or come closer than min_gap to a wall
-// particle (the graph of the current state gives the walls near it)
+// (x, y, u, v, rho), with the non-penetration projection against the wall
+// particles of the current graph; flags *bad when a value is non-finite,
+// the density leaves the guard band, or a particle would move more than the
+// graph radius or leave the simulation's domain
 __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict__ out, OutScale sc,
                               const int *__restrict__ nbr, const int *__restrict__ deg, double *__restrict__ pred,
                               unsigned *bad)
@@ -545,27 +558,38 @@ __global__ void k_sur_predict(DevParams P, SlotArrays S, const float *__restrict
   if (a >= P.nf) return;
   const float *o = out + (size_t)a * kOutPad;
   const double u = S.u[a], v = S.v[a];
-  const double x = S.x[a] + sc.T * u + sc.s[0] * o[0];
-  const double y = S.y[a] + sc.T * v + sc.s[1] * o[1];
-  const double un = u + sc.s[2] * o[2];
-  const double vn = v + sc.s[3] * o[3];
+  double x = S.x[a] + sc.T * u + sc.s[0] * o[0];
+  double y = S.y[a] + sc.T * v + sc.s[1] * o[1];
+  double un = u + sc.s[2] * o[2];
+  double vn = v + sc.s[3] * o[3];
   const double rho = S.rho[a] + sc.s[4] * o[4];
-  const bool inside = x >= P.lo_x && x <= P.hi_x && y >= P.lo_y && y <= P.hi_y;
-  const bool small_move = fabs(x - S.x[a]) <= sc.max_move && fabs(y - S.y[a]) <= sc.max_move;
-  // wall clearance: no fluid particle may end closer than min_gap to a wall
-  // partner (advanced by its own velocity), unless it already was closer
-  bool clear = true;
+  // non-penetration: a predicted position closer than min_gap to a wall
+  // particle (advanced by its own velocity) is moved back out to min_gap
+  // along the line from that particle, and the velocity loses its component
+  // into the wall -- unless the particle already was that close
   const double g2 = sc.min_gap * sc.min_gap;
   for (int k = 0; k < deg[a]; k++) {
     const int j = nbr[(size_t)a * kMaxDeg + k];
     if (S.itype[j] == 1) continue;
     const double wx = S.x[j] + sc.T * S.u[j], wy = S.y[j] + sc.T * S.v[j];
-    const double dn = (x - wx) * (x - wx) + (y - wy) * (y - wy);
+    const double rx = x - wx, ry = y - wy;
+    const double dn = rx * rx + ry * ry;
     const double d0 = (S.x[a] - S.x[j]) * (S.x[a] - S.x[j]) + (S.y[a] - S.y[j]) * (S.y[a] - S.y[j]);
-    if (dn < g2 && dn < d0) clear = false;
+    if (dn < g2 && dn < d0 && dn > 0.0) {
+      const double d = sqrt(dn), nx = rx / d, ny = ry / d;
+      x = wx + nx * sc.min_gap;
+      y = wy + ny * sc.min_gap;
+      const double vin = (un - S.u[j]) * nx + (vn - S.v[j]) * ny;
+      if (vin < 0.0) {
+        un -= vin * nx;
+        vn -= vin * ny;
+      }
+    }
   }
+  const bool inside = x >= P.lo_x && x <= P.hi_x && y >= P.lo_y && y <= P.hi_y;
+  const bool small_move = fabs(x - S.x[a]) <= sc.max_move && fabs(y - S.y[a]) <= sc.max_move;
   if (!isfinite(x) || !isfinite(y) || !isfinite(un) || !isfinite(vn) || !(fabs(rho / P.rho0 - 1.0) <= kMaxRhoDev) ||
-      !inside || !small_move || !clear)
+      !inside || !small_move)
     atomicOr(bad, 1u);
   double *q = pred + (size_t)S.orig[a] * kNOut;
   q[0] = x;
@@ -779,8 +803,8 @@ uph_status prepare(uph_surrogate *s, const NodesView &nv)
   launch_exclusive_scan(g.count, g.start, (int)ncell, g.block_sums, q);
   launch_cell_scatter(g, 0, nv.n, q);
   launch_cell_sort_segments(g, q);
-  k_sur_graph<<<(nv.n + 127) / 128, 128, 0, q>>>(G, nv.x, nv.y, nv.n, g.cell_of, g.start, g.list, R, s->nbr, s->ef,
-                                                 s->deg, s->d_err);
+  k_sur_graph<<<(nv.n + 127) / 128, 128, 0, q>>>(G, nv.x, nv.y, nv.rho, s->cfg.rho0 * s->cfg.edge_rho_scale, nv.n,
+                                                 g.cell_of, g.start, g.list, R, s->nbr, s->ef, s->deg, s->d_err);
   k_sur_features<<<(nv.n + 255) / 256, 256, 0, q>>>(nv.n, nv.u, nv.v, nv.rho, nv.itype, s->cfg.vel_scale,
                                                      s->cfg.rho0, s->cfg.rho_scale, s->F, s->d_err);
   UPH_CUDA(cudaGetLastError());
@@ -1129,7 +1153,7 @@ extern "C" uph_status uph_sur_create(const uph_sur_config *cfg, int32_t node_cap
   *out = nullptr;
   if (cfg->rounds < 1 || cfg->rounds > kMaxRounds) return fail(UPH_BAD_ARG, "uph_sur_create: rounds outside 1..4");
   if (!(cfg->radius > 0.0) || !(cfg->dt > 0.0) || !(cfg->rho0 > 0.0) || !(cfg->vel_scale > 0.0) ||
-      !(cfg->rho_scale > 0.0) || cfg->macro_steps < 1)
+      !(cfg->rho_scale > 0.0) || !(cfg->edge_rho_scale > 0.0) || cfg->macro_steps < 1)
     return fail(UPH_BAD_ARG, "uph_sur_create: radius, dt, rho0, scales and macro_steps must be positive");
   if (node_capacity < 1 || node_capacity > (1 << 26)) return fail(UPH_BAD_ARG, "uph_sur_create: bad node capacity");
   int dev = 0;
@@ -1368,7 +1392,7 @@ uph_status network_predict(uph_surrogate *s, uph_sim *sim, bool *fits, bool *ok)
   sc.T = s->cfg.macro_steps * s->cfg.dt;
   for (int k = 0; k < kNOut; k++) sc.s[k] = s->cfg.out_scale[k];
   sc.max_move = s->cfg.radius;
-  sc.min_gap = 0.2 * s->cfg.radius;
+  sc.min_gap = 0.25 * s->cfg.radius;
   UPH_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(unsigned), s->stream));
   if (sv.P.nf > 0)
     k_sur_predict<<<(sv.P.nf + 255) / 256, 256, 0, s->stream>>>(sv.P, sv.S, s->out, sc, s->nbr, s->deg, s->pred,

@@ -51,22 +51,23 @@ def param_layout(rounds: int = 3) -> List[Tuple[str, Tuple[int, ...]]]:
 
 def init_params(seed: int, rounds: int = 3) -> np.ndarray:
     """Uniform(+-1/sqrt(fan_in)) weights and zero biases; the residual and
-    output layers start 10x smaller.  Entries no input or output reaches (the
-    padded feature columns, W_e's 4th column, decoder rows past the 5
-    outputs) are zero and stay zero under training (their gradient is 0)."""
+    output layers start 10x smaller, W_e's density-difference column at zero.
+    Entries no input or output reaches (the padded feature columns, decoder
+    rows past the 5 outputs) are zero and stay zero under training (their
+    gradient is 0)."""
     rng = np.random.default_rng(seed)
     parts = []
     for name, shape in param_layout(rounds):
         if name.endswith(".b"):
             parts.append(np.zeros(shape, np.float32))
             continue
-        fan_in = {"enc1.w": NFEAT_USED}.get(name, 3 if name.endswith(".we") else shape[1])
+        fan_in = {"enc1.w": NFEAT_USED}.get(name, 4 if name.endswith(".we") else shape[1])
         bound = 1.0 / math.sqrt(fan_in)
         w = rng.uniform(-bound, bound, size=shape)
         if name.endswith(".n2.w") or name == "dec2.w":
             w *= 0.1
         if name.endswith(".we"):
-            w[:, 3] = 0.0
+            w[:, 3] = 0.0  # the density-difference feature starts unused
         if name == "enc1.w":
             w[:, NFEAT_USED:] = 0.0
         if name == "dec2.w":
@@ -84,6 +85,7 @@ class NetConfig:
     rho0: float = 1000.0
     vel_scale: float = 0.1     # m/s
     rho_scale: float = 0.01    # relative density
+    edge_rho_scale: float = 1e-3  # unit of the edge density difference, relative to rho0
     out_scale: Tuple[float, ...] = (1e-4, 1e-4, 1e-3, 1e-3, 1.0)
 
     @classmethod
@@ -101,6 +103,7 @@ class NetConfig:
         c.rho0 = self.rho0
         c.vel_scale = self.vel_scale
         c.rho_scale = self.rho_scale
+        c.edge_rho_scale = self.edge_rho_scale
         for k in range(NOUT):
             c.out_scale[k] = float(self.out_scale[k])
         return c
@@ -465,7 +468,7 @@ def train_flume(out_path: Optional[str] = None, seed: int = 0, n_flumes: int = 6
                 windows: int = 16, window_gap_time: float = 0.1, pairs_per_window: int = 10, iters: int = 3000,
                 lr: float = 5e-4, noise_vel: float = 0.0, noise_rho: float = 0.0, dagger_rounds: int = 0,
                 dagger_iters: int = 1500, dagger_horizons: Sequence[int] = (4, 12, 24), dagger_windows: int = 6,
-                dagger_repeat: int = 3, log=print) -> dict:
+                dagger_repeat: int = 3, edge_rho_scale: float = 1e-3, log=print) -> dict:
     """Generates flume trajectories with the plain FP32-pair WCSPH solver,
     trains a 3-round network on them (the last window held out), then for
     `dagger_rounds` rounds adds frames that start from the network's own
@@ -479,7 +482,7 @@ def train_flume(out_path: Optional[str] = None, seed: int = 0, n_flumes: int = 6
     pistons = draw_pistons(seed, n_flumes)
     batch = flume_batch(pistons, length, depth, dx)
     p = batch.deck.uph_params(PROFILE_WCSPH, PREC_FP32_PAIR)
-    cfg = NetConfig.for_params(p, macro_steps)
+    cfg = NetConfig.for_params(p, macro_steps, edge_rho_scale=edge_rho_scale)
     dt = cfg.dt
     frames = generate_frames(batch, cfg, int(round(warm_time / dt)), windows, int(round(window_gap_time / dt)),
                              pairs_per_window)
