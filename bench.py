@@ -342,8 +342,8 @@ def surrogate_arm(args, stream):
     state is advanced `--sur-steps` SPH steps
     - plain: the plain FP64 path (one uph_sim_step per macro step's length);
     - surrogate: uph_sur_advance with the trained network (fused BF16
-      tcgen05 kernels), the FP32-pair plain solver as the judge every 10th
-      macro step, fallback on a failed check.
+      tcgen05 kernels) on an FP64 simulation, whose plain solver is the judge
+      every 10th macro step and takes over after a failed check.
     Both are timed with CUDA events on the simulations' stream.  Errors
     compare the surrogate's final state with the plain one: RMS and largest
     relative density error, largest free-surface height difference per
@@ -394,13 +394,13 @@ def surrogate_arm(args, stream):
     plain.close()
     sur = SG.Surrogate(cfg, deck.n_all + 128, params)
     sur.set_stream(stream.cuda_stream)
-    s = new_sim(PREC_FP32_PAIR)
+    s = new_sim(0)
     t_sur, rep = timed(lambda: sur.advance(s, nmacro, judge))
     out = s.download()
     s.close()
     err = SG.state_errors(out, ref, nf, depth, 0.0, L, judge.surface_bins)
     # the network alone (no judge) over the same span, for its own drift
-    s = new_sim(PREC_FP32_PAIR)
+    s = new_sim(0)
     t_net, _ = timed(lambda: sur.advance(s, nmacro, SG.Judge(depth=depth, surface_x0=0.0, surface_x1=L,
                                                                 surface_bins=judge.surface_bins,
                                                                 judge_every=1 << 30)))

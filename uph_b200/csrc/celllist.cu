@@ -1,13 +1,14 @@
 // Cell list: the GPU replacement of the reference's kd-tree search
 // (src/lib/Search.cc:5-44).  Every step the interacting particles are binned
-// into square cells no smaller than the search radius by a counting sort:
+// into square cells of radius / reach by a counting sort:
 //   1. cell key per slot + histogram (atomic add per cell),
 //   2. exclusive scan of the histogram -> first entry of every cell,
 //   3. scatter of slot ids into their cell's range,
 //   4. sort of every cell's (short) range by slot id, so the order in which
 //      the pair pass visits neighbours -- and with it every floating-point
 //      sum -- does not depend on atomic arrival order.
-// A particle's neighbours then lie in the 3 x 3 block of cells around it.
+// A particle's neighbours then lie within `reach` cells of its own (a
+// (2 reach + 1)^2 block; reach 2, cells of half the radius, by default).
 #include "uph_internal.cuh"
 
 namespace uph {

@@ -1,6 +1,7 @@
 // The fused rate pass of the REF profile: one thread per fluid particle
-// gathers every pair term of the reference's derivatives() from the 3 x 3
-// cells around it, in FP64.
+// gathers every pair term of the reference's derivatives() from the cells
+// within `reach` cells of its own (5 x 5 cells of half the radius by
+// default), in FP64.
 //
 // The reference evaluates each term as a scatter loop over pairs (i < j)
 // that adds one formula to i and another to j.  Here particle a sees every

@@ -1352,11 +1352,9 @@ uph_status sim_jump(uph_sim *s, int nsteps)
     s->launches++;
   }
   s->restart = true;
+  // the storage re-sort waits for the next plain step (the state moves
+  // about 0.1 dx per jump, so the slot order stays spatially coherent)
   s->steps_since_reorder += nsteps;
-  if (s->steps_since_reorder >= s->reorder_interval) {
-    uph_status r = reorder_fluid(s);
-    if (r != UPH_OK) return r;
-  }
   UPH_CUDA(cudaGetLastError());
   return UPH_OK;
 }

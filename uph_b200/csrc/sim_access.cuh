@@ -22,9 +22,9 @@ struct SimView {
 
 SimView sim_view(uph_sim *s);
 // The fluid state in the slots now belongs to `nsteps` steps later: advance
-// the step counters, put the moving walls at the new time, restart the
-// leapfrog at the next step (first-step half kick, as after an upload) and
-// keep the storage re-sort schedule.
+// the step counters, put the moving walls at the new time and restart the
+// leapfrog at the next step (first-step half kick, as after an upload).  The
+// storage re-sort falls due at the next plain step.
 uph_status sim_jump(uph_sim *s, int nsteps);
 // the device error word as a status (synchronises the stream; the word is sticky)
 uph_status sim_check(uph_sim *s);

@@ -189,17 +189,31 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
     if (yy < 0 || yy >= G.ncy) continue;
     const int x0 = max(cx - 1, 0), x1 = min(cx + 1, G.ncx - 1);
     const int a = start[yy * G.ncx + x0], b = start[yy * G.ncx + x1 + 1];
-    for (int k = a; k < b; k++) {
-      const int j = list[k];
-      const double dx = x[j] - xi, dy = y[j] - yi;
-      const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-      if (r2 > DBL_EPSILON && r2 < r2cut) {
-        if (cnt < kMaxDeg) {
-          nbr[(size_t)i * kMaxDeg + cnt] = j;
-          ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R),
-                                                      (float)((rho[j] - ri) / rho_unit));
+    // four candidates per pass: their position loads are independent
+    for (int k0 = a; k0 < b; k0 += 4) {
+      int jj[4];
+      double cx4[4], cy4[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) jj[u] = k0 + u < b ? list[k0 + u] : -1;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        cx4[u] = jj[u] >= 0 ? x[jj[u]] : 0.0;
+        cy4[u] = jj[u] >= 0 ? y[jj[u]] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int j = jj[u];
+        if (j < 0) continue;
+        const double dx = cx4[u] - xi, dy = cy4[u] - yi;
+        const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        if (r2 > DBL_EPSILON && r2 < r2cut) {
+          if (cnt < kMaxDeg) {
+            nbr[(size_t)i * kMaxDeg + cnt] = j;
+            ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R),
+                                                        (float)((rho[j] - ri) / rho_unit));
+          }
+          cnt++;
         }
-        cnt++;
       }
     }
   }
