@@ -49,7 +49,7 @@ typedef enum uph_status {
   UPH_NO_DEVICE = 7,         /* no CUDA device is visible */
   UPH_UNSUPPORTED = 8,       /* a reference mode this library does not implement */
   UPH_OUT_OF_MEMORY = 9,
-  UPH_IO_ERROR = 10          /* a deck file is missing or malformed */
+  UPH_IO_ERROR = 10          /* a deck file is missing or malformed, or an output file cannot be written */
 } uph_status;
 
 /* Physics profiles.
@@ -229,6 +229,53 @@ uph_status uph_sim_pairs(uph_sim *sim, int64_t cap, int32_t *i_pair, int32_t *j_
                          double *w, double *dwcdx, int64_t *niac);
 
 uph_status uph_sim_stats(uph_sim *sim, uph_stats *out);
+
+/* The reference's per-evaluation diagnostics, computed on the device at the
+ * state each derivatives() call sees (before the step's corrector), as
+ * sph.cc's output() later prints them:
+ *   kinetic/potential energy: TotalKineticEnergy (derivatives.c:2254-2264),
+ *           sums of 0.5 m |v|^2 and m g y over the fluid;
+ *   point:  NeighborsToPressurePoint (derivatives.c:2290-2338) -- Gaussian-
+ *           weighted DynamicPressure over fluid within 3h of the probe with
+ *           p > 0: w = (exp(-r^2/h^2) - e^-9) m / (2 pi h^2 (0.5 - 5 e^-9) rho),
+ *           point_pressure = sum p w / sum w, pressure_norm = sum w (1 when
+ *           nothing is in range, and point_pressure then keeps its previous
+ *           value, 0 at creation), point_neighbors = count;
+ *   two:    NeighborsToPressurePointTwo + EnsembleAveragedPointPressureTwo
+ *           (derivatives.c:2340-2393) -- mean p over fluid within 2h of the
+ *           second probe with p > 0.
+ * Sums run in a fixed order (not the reference's serial one).  itime is the
+ * step whose evaluation the values belong to (0: none yet). */
+typedef struct uph_diagnostics {
+  double kinetic_energy, potential_energy;
+  double point_pressure, pressure_norm, point_pressure_two;
+  int32_t point_neighbors, point_neighbors_two;
+  int32_t itime;
+} uph_diagnostics;
+
+/* Turns the diagnostics on (one extra kernel per step) or off.  The first
+ * probe is parameters.dat's pressureProbeX/Y (System.c:91-92); the reference
+ * never sets the second one, so its (0, 0) is what reproduces its files. */
+uph_status uph_sim_set_diagnostics(uph_sim *sim, int32_t enable, double probe_x, double probe_y, double probe_x2,
+                                   double probe_y2);
+/* The values of the last evaluation (UPH_BAD_ARG while diagnostics are off). */
+uph_status uph_sim_diagnostics(uph_sim *sim, uph_diagnostics *out);
+
+/* The reference's output() (output.c:19-140) for a downloaded state, in
+ * `directory`: writes out<itime>.dat (one line per particle: index, x, y, u,
+ * v, density, mass, hsml, DynamicPressure, damGateFlag, approxVorticity,
+ * itype, specificDissipationRate, localDensity in the reference's formats;
+ * hsml is p->h, dam_gate_flag may be NULL (written as 0), and the vorticity
+ * and dissipation rate, which feed nothing on this path, are written as 0)
+ * and appends a line to TotalKineticEnergy.dat, PointPressure.dat and
+ * PointPressureTwo.dat from `diag`; at itime == number_of_initialization_steps
+ * it appends the fluid to FluidParticleInit.dat (its tempPosition and
+ * tempPositionGate columns, deck inputs nothing on this path reads, as 0).
+ * The dissipation and control-volume files (PowerCalc.dat, ControlVol*.dat)
+ * are not written.  The appended files are the caller's to truncate at the
+ * start of a run, as sph.cc does before its time loop. */
+uph_status uph_write_output(const char *directory, int32_t itime, const uph_params *p, const uph_state *st,
+                            const int32_t *dam_gate_flag, const uph_diagnostics *diag);
 
 /* Device time per kernel family since the last reset, measured with CUDA
  * events when profiling is on.  names: comma-separated list written to

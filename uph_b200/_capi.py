@@ -114,6 +114,14 @@ class UphStats(C.Structure):
     ]
 
 
+class UphDiagnostics(C.Structure):
+    _fields_ = [
+        ("kinetic_energy", f64), ("potential_energy", f64),
+        ("point_pressure", f64), ("pressure_norm", f64), ("point_pressure_two", f64),
+        ("point_neighbors", i32), ("point_neighbors_two", i32), ("itime", i32),
+    ]
+
+
 def state_shapes(n_fluid: int, n_all: int) -> dict:
     out = {}
     for name, kind, width in STATE_FIELDS:

@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from ._capi import SurConfig, SurJudge, SurNodes, SurReport, UphParams, UphStats
+from ._capi import SurConfig, SurJudge, SurNodes, SurReport, UphDiagnostics, UphParams, UphStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libuph.so")
@@ -34,6 +34,10 @@ SIGNATURES = {
     "uph_sim_derivatives": (C.c_int, [C.c_void_p, C.c_double]),
     "uph_sim_pairs": (C.c_int, [C.c_void_p, C.c_int64] + [C.c_void_p] * 5 + [C.POINTER(C.c_int64)]),
     "uph_sim_stats": (C.c_int, [C.c_void_p, C.POINTER(UphStats)]),
+    "uph_sim_set_diagnostics": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "uph_sim_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(UphDiagnostics)]),
+    "uph_write_output": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(UphParams), C.c_void_p, C.c_void_p,
+                                   C.POINTER(UphDiagnostics)]),
     "uph_sim_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "uph_sim_kernel_times": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t,
                                        C.POINTER(C.c_int32)]),

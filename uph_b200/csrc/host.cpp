@@ -200,3 +200,81 @@ extern "C" uph_status uph_deck_read(const char *deck_dir, double eta_override, u
   if (st->Pressure) memset(st->Pressure, 0, sizeof(double) * (size_t)idx);
   return UPH_OK;
 }
+
+namespace {
+
+// opens `name` in `dir` with the reference's mode and a large buffer
+FILE *open_in(const std::string &dir, const char *name, const char *mode, std::vector<char> *buf = nullptr)
+{
+  FILE *f = fopen((dir + "/" + name).c_str(), mode);
+  if (f && buf) setvbuf(f, buf->data(), _IOFBF, buf->size());
+  return f;
+}
+
+}  // namespace
+
+// output() of output.c:19-140 for the files the hot path has values for; the
+// formats are the reference's, character for character
+extern "C" uph_status uph_write_output(const char *directory, int32_t itime, const uph_params *p, const uph_state *st,
+                                       const int32_t *dam_gate_flag, const uph_diagnostics *diag)
+{
+  if (!directory || !p || !st || !diag) return fail(UPH_BAD_ARG, "uph_write_output: NULL argument");
+  if (!st->Position || !st->Velocity || !st->density || !st->mass || !st->DynamicPressure || !st->itype ||
+      !st->localDensity || !st->localVelocity)
+    return fail(UPH_BAD_ARG, "uph_write_output: the state needs Position, Velocity, localVelocity, density, "
+                             "localDensity, DynamicPressure, mass and itype");
+  const std::string dir(directory);
+  const int nf = p->n_fluid;
+  const int n = p->n_fluid + p->n_solid + p->n_fixed + p->n_moving;
+  const double t = p->time_step * itime;
+  std::vector<char> buf(1 << 22);
+  char name[64];
+  snprintf(name, sizeof name, "out%d.dat", itime);
+  FILE *f = open_in(dir, name, "w+", &buf);
+  if (!f) return fail(UPH_IO_ERROR, "uph_write_output: cannot open " + dir + "/" + name);
+  for (int i = 0; i < n; i++) {
+    fprintf(f, "%d ", i);
+    fprintf(f, "\t%.10lf\t%.10lf", st->Position[2 * i], st->Position[2 * i + 1]);
+    fprintf(f, "\t%.10lf\t%.10lf", st->Velocity[2 * i], st->Velocity[2 * i + 1]);
+    fprintf(f, "\t%.10lf\t%.10lf\t%.10lf\t%.10lf\t%d\t%.10lf\t%d\t%.10lf\t%.10lf\n", st->density[i], st->mass[i], p->h,
+            st->DynamicPressure[i], dam_gate_flag ? dam_gate_flag[i] : 0, 0.0, st->itype[i], 0.0,
+            st->localDensity[i]);
+  }
+  bool ok = fclose(f) == 0;
+  if ((f = open_in(dir, "TotalKineticEnergy.dat", "a"))) {
+    fprintf(f, "%.10lf\t%.10lf %.10lf\n", t, diag->kinetic_energy, diag->potential_energy);
+    ok = fclose(f) == 0 && ok;
+  } else {
+    ok = false;
+  }
+  if ((f = open_in(dir, "PointPressure.dat", "a"))) {
+    fprintf(f, "%.10lf\t%.10lf\t%d\t%.10lf\t%.10lf\n", t, diag->point_pressure, diag->point_neighbors,
+            diag->pressure_norm, diag->point_pressure_two);
+    ok = fclose(f) == 0 && ok;
+  } else {
+    ok = false;
+  }
+  if ((f = open_in(dir, "PointPressureTwo.dat", "a"))) {
+    fprintf(f, "%.10lf\t%d\t%.10lf\n", t, diag->point_neighbors_two, diag->point_pressure_two);
+    ok = fclose(f) == 0 && ok;
+  } else {
+    ok = false;
+  }
+  if (itime == p->number_of_initialization_steps) {
+    if ((f = open_in(dir, "FluidParticleInit.dat", "a", &buf))) {
+      fprintf(f, "%d\n", nf);
+      for (int i = 0; i < nf; i++) {
+        fprintf(f, "%.10lf\t%.10lf\t", st->Position[2 * i], st->Position[2 * i + 1]);
+        fprintf(f, "%.10lf\t%.10lf\t", st->Velocity[2 * i], st->Velocity[2 * i + 1]);
+        fprintf(f, "%.10lf\t%.10lf\t%.10lf\t%.10lf\t%.10lf\t%d\t%.10lf\t%.10lf\n", st->density[i],
+                st->DynamicPressure[i], st->mass[i], 0.0, 0.0, st->itype[i], st->localVelocity[2 * i],
+                st->localVelocity[2 * i + 1]);
+      }
+      ok = fclose(f) == 0 && ok;
+    } else {
+      ok = false;
+    }
+  }
+  if (!ok) return fail(UPH_IO_ERROR, "uph_write_output: writing the diagnostics files in " + dir + " failed");
+  return UPH_OK;
+}

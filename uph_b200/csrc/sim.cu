@@ -47,6 +47,21 @@ struct Staging {
   double *tmp_x, *tmp_y;       // positions split for the key kernel
 };
 
+// the pressure-probe points of the per-evaluation diagnostics
+struct DiagProbes {
+  double x1, y1, x2, y2;
+};
+
+// the diagnostics of the last evaluation, as the reference's System holds them
+struct DevDiag {
+  double kinetic_energy, potential_energy;
+  double point_pressure, pressure_norm, point_pressure_two;
+  int point_neighbors, point_neighbors_two;
+  int itime;
+};
+
+constexpr int kDiagRows = 7;
+
 }  // namespace
 
 struct uph_sim {
@@ -96,6 +111,13 @@ struct uph_sim {
   // next step starts the leapfrog afresh with the first-step half kick
   bool restart = false;
   int64_t serial = 0;  // distinct for every simulation this process creates
+  // per-evaluation diagnostics (off by default)
+  bool diag_enabled = false;
+  DiagProbes diag_probes = {0, 0, 0, 0};
+  int diag_blocks = 0;
+  double *d_diag_part = nullptr;  // [kDiagRows][diag_blocks]
+  unsigned *d_diag_done = nullptr;
+  DevDiag *d_diag = nullptr;
 };
 
 namespace {
@@ -529,6 +551,16 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &s->d_wall_tab, 3 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
   s->n_partials = 1024;
   TRY(dalloc(s, &s->d_partials, (size_t)s->n_partials * 4));
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int want = (p->n_fluid + 255) / 256;
+    s->diag_blocks = want < 2 * sms ? (want > 0 ? want : 1) : 2 * sms;
+  }
+  TRY(dalloc(s, &s->d_diag_part, (size_t)s->diag_blocks * kDiagRows));
+  TRY(dalloc(s, &s->d_diag_done, 1));
+  TRY(dalloc(s, &s->d_diag, 1));
   TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   s->own_stream = true;
   {
@@ -536,6 +568,8 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
     s->serial = ++created;
   }
   TRY(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream));
+  TRY(cudaMemsetAsync(s->d_diag_done, 0, sizeof(unsigned), s->stream));
+  TRY(cudaMemsetAsync(s->d_diag, 0, sizeof(DevDiag), s->stream));
 #undef TRY
   *out = s;
   return UPH_OK;
@@ -695,6 +729,8 @@ bool walls_move(const uph_sim *s)
 // the sequence is being recorded into a CUDA graph: no host synchronisation,
 // no profiling events, and an even number of storage re-sorts so the graph
 // ends on the buffer it started on.
+void launch_diagnostics(uph_sim *s);
+
 uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
 {
   const bool moving = walls_move(s);
@@ -717,6 +753,7 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
     uph_status r = rate_pass(s, first);
     if (r != UPH_OK) return r;
     if (k == 0) s->restart = false;
+    if (s->diag_enabled) launch_diagnostics(s);
     {
       Timer tm(s, KF_CORRECT);
       launch_correct(s->P, s->S, first, k + 1 < nsteps, s->d_err, s->d_itime, s->stream);
@@ -1035,7 +1072,115 @@ __global__ void k_stats(DevParams P, SlotArrays S, double *partials, int nblocks
     for (int k = 0; k < 4; k++) partials[k * nblocks_total + blockIdx.x] = sh[k][0];
 }
 
+// Per-evaluation diagnostics (TotalKineticEnergy, derivatives.c:2254-2264;
+// NeighborsToPressurePoint / ...Two, derivatives.c:2290-2393) over the fluid
+// at the state the rate pass just read.  Each block writes its partials
+// [KE, PE, sum p w, sum w, n1, sum p, n2]; the last block to finish (counted
+// with an atomic after a fence) adds them in block order and updates the
+// persistent values, so the result is deterministic and needs no host step.
+__global__ void k_diagnostics(DevParams P, SlotArrays S, DiagProbes q, double *partials, int nblocks_total,
+                              unsigned *done, DevDiag *out, const int *d_itime)
+{
+  __shared__ double sh[kDiagRows][256];
+  __shared__ bool last;
+  const double e9 = exp(-9.0);
+  const double coeff1 = 0.5 - 5.0 * e9;
+  const double h = P.h;
+  double acc[kDiagRows] = {0, 0, 0, 0, 0, 0, 0};
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.nf; a += gridDim.x * blockDim.x) {
+    const double ma = S.m[a], u = S.u[a], v = S.v[a], xa = S.x[a], ya = S.y[a];
+    acc[0] += 0.5 * ma * (u * u + v * v);
+    acc[1] += ma * P.g * ya;
+    const double pa = S.p[a];
+    if (!(pa > 0.0)) continue;
+    double dx = xa - q.x1, dy = ya - q.y1;
+    double r = sqrt(dx * dx + dy * dy);
+    if (r <= 3.0 * h) {
+      const double w = (exp(-r * r / (h * h)) - e9) * ma / (2.0 * M_PI * h * h * coeff1 * S.rho[a]);
+      acc[2] += pa * w;
+      acc[3] += w;
+      acc[4] += 1.0;
+    }
+    dx = xa - q.x2;
+    dy = ya - q.y2;
+    r = sqrt(dx * dx + dy * dy);
+    if (r < 2.0 * h) {
+      acc[5] += pa;
+      acc[6] += 1.0;
+    }
+  }
+  for (int k = 0; k < kDiagRows; k++) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int k = 0; k < kDiagRows; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kDiagRows; k++) partials[k * nblocks_total + blockIdx.x] = sh[k][0];
+    __threadfence();
+    last = atomicAdd(done, 1u) == (unsigned)nblocks_total - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if ((int)threadIdx.x < kDiagRows) {
+    const volatile double *row = partials + threadIdx.x * nblocks_total;
+    double t = 0.0;
+    for (int b = 0; b < nblocks_total; b++) t += row[b];
+    sh[threadIdx.x][0] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int n1 = (int)sh[4][0], n2 = (int)sh[6][0];
+    out->kinetic_energy = sh[0][0];
+    out->potential_energy = sh[1][0];
+    out->point_neighbors = n1;
+    out->pressure_norm = n1 ? sh[3][0] : 1.0;
+    if (n1) out->point_pressure = sh[2][0] / sh[3][0];
+    out->point_neighbors_two = n2;
+    out->point_pressure_two = n2 ? sh[5][0] / n2 : 0.0;
+    out->itime = d_itime ? *d_itime + 1 : 0;
+    *done = 0u;
+  }
+}
+
+void launch_diagnostics(uph_sim *s)
+{
+  k_diagnostics<<<s->diag_blocks, 256, 0, s->stream>>>(s->P, s->S, s->diag_probes, s->d_diag_part, s->diag_blocks,
+                                                       s->d_diag_done, s->d_diag, s->d_itime);
+  s->launches++;
+}
+
 }  // namespace
+
+extern "C" uph_status uph_sim_set_diagnostics(uph_sim *s, int32_t enable, double x, double y, double x2, double y2)
+{
+  if (!s) return fail(UPH_BAD_ARG, "uph_sim_set_diagnostics: NULL sim");
+  drop_graph(s);  // the recorded steps carry the old setting
+  s->diag_enabled = enable != 0;
+  s->diag_probes = DiagProbes{x, y, x2, y2};
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_diagnostics(uph_sim *s, uph_diagnostics *out)
+{
+  if (!s || !out) return fail(UPH_BAD_ARG, "uph_sim_diagnostics: NULL argument");
+  memset(out, 0, sizeof *out);
+  if (!s->diag_enabled) return fail(UPH_BAD_ARG, "uph_sim_diagnostics: diagnostics are off (uph_sim_set_diagnostics)");
+  DevDiag d;
+  UPH_CUDA(cudaMemcpyAsync(&d, s->d_diag, sizeof d, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  out->kinetic_energy = d.kinetic_energy;
+  out->potential_energy = d.potential_energy;
+  out->point_pressure = d.point_pressure;
+  out->pressure_norm = d.pressure_norm;
+  out->point_pressure_two = d.point_pressure_two;
+  out->point_neighbors = d.point_neighbors;
+  out->point_neighbors_two = d.point_neighbors_two;
+  out->itime = d.itime;
+  return UPH_OK;
+}
 
 extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
 {

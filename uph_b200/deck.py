@@ -187,6 +187,14 @@ class Deck:
         return st
 
 
+    def dam_gate_flag(self) -> np.ndarray:
+        """damGateFlag as input() sets it: fluid in the 0.38 m dam column 1,
+        the rest of the fluid -1 (input.c:146-159), walls 0 (inputbp.c:311)."""
+        flag = np.zeros(self.n_all, np.int32)
+        flag[:self.n_fluid] = np.where(self.fluid[:, 0] <= 0.38, 1, -1)
+        return flag
+
+
 def read_deck(directory: str, eta_override: float = 0.0) -> Deck:
     p = read_parameters(os.path.join(directory, "parameters.dat"))
     blocks = [_read_particles(os.path.join(directory, name)) for name in PARTICLE_FILES[:4]]

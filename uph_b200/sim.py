@@ -16,12 +16,14 @@ instead of the reference's printf + exit(1).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Dict, Optional
 
 import numpy as np
 
 from . import _lib
-from ._capi import (PREC_FP64, PROFILE_REF, STATE_FIELDS, UphParams, UphStats, empty_state, state_struct)
+from ._capi import (PREC_FP64, PROFILE_REF, STATE_FIELDS, UphDiagnostics, UphParams, UphStats, empty_state,
+                    state_struct)
 from .deck import Deck
 
 
@@ -123,6 +125,31 @@ class Simulation:
         _lib.check(self.lib.uph_sim_stats(self.handle, C.byref(s)), "uph_sim_stats")
         return {name: getattr(s, name) for name, _ in UphStats._fields_}
 
+    # -- diagnostics and output ----------------------------------------------------
+    def set_diagnostics(self, enable: bool = True, probe: Optional[tuple] = None,
+                        probe_two: tuple = (0.0, 0.0)) -> None:
+        """Per-evaluation kinetic energy and pressure probes (derivatives.c:2254-2393).
+
+        `probe` defaults to parameters.dat's pressureProbeX/Y; the reference
+        never sets the second probe, so (0, 0) reproduces its files."""
+        if probe is None:
+            probe = (self.params.pressure_probe_x, self.params.pressure_probe_y)
+        _lib.check(self.lib.uph_sim_set_diagnostics(self.handle, 1 if enable else 0, float(probe[0]),
+                                                    float(probe[1]), float(probe_two[0]), float(probe_two[1])),
+                   "uph_sim_set_diagnostics")
+
+    def diagnostics(self) -> dict:
+        d = UphDiagnostics()
+        _lib.check(self.lib.uph_sim_diagnostics(self.handle, C.byref(d)), "uph_sim_diagnostics")
+        return {name: getattr(d, name) for name, _ in UphDiagnostics._fields_}
+
+    def write_output(self, directory: str, itime: Optional[int] = None, state: Optional[dict] = None,
+                     dam_gate_flag: Optional[np.ndarray] = None) -> None:
+        """output(sys, itime) of output.c:19-140 for the current (or a given
+        downloaded) state, with the diagnostics of the last evaluation."""
+        write_output(directory, self.params, self.download() if state is None else state,
+                     self.diagnostics(), self.stats()["itime"] if itime is None else itime, dam_gate_flag)
+
     # -- measurement -----------------------------------------------------------
     def set_stream(self, cuda_stream: int) -> None:
         _lib.check(self.lib.uph_sim_set_stream(self.handle, C.c_void_p(cuda_stream)), "uph_sim_set_stream")
@@ -142,6 +169,25 @@ class Simulation:
 
     def launch_count(self) -> int:
         return int(self.lib.uph_sim_launch_count(self.handle))
+
+
+def write_output(directory: str, params, state: dict, diagnostics: dict, itime: int,
+                 dam_gate_flag: Optional[np.ndarray] = None) -> None:
+    """uph_write_output: the reference's out<itime>.dat and diagnostics files.
+
+    `params` is a UphParams or a dict of its fields; `diagnostics` a dict of
+    UphDiagnostics fields (Simulation.diagnostics())."""
+    lib = _lib.lib()
+    p = params if isinstance(params, UphParams) else UphParams.from_dict(params)
+    keep = []
+    st = state_struct(state, keep)
+    d = UphDiagnostics(**{k: diagnostics[k] for k, _ in UphDiagnostics._fields_})
+    gate = None
+    if dam_gate_flag is not None:
+        gate = np.ascontiguousarray(dam_gate_flag, dtype=np.int32)
+        keep.append(gate)
+    _lib.check(lib.uph_write_output(os.fsencode(directory), int(itime), C.byref(p), C.byref(st),
+                                    None if gate is None else gate.ctypes.data, C.byref(d)), "uph_write_output")
 
 
 def search_neighbors(position: np.ndarray, n_fluid: int, particle_boundary: int, dist: float,
