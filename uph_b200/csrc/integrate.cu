@@ -17,6 +17,13 @@ __device__ __forceinline__ double tait(const DevParams &P, double rho)
   return P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
 }
 
+// the FP32-pair pass's per-particle operands, rounded once from FP64
+__device__ __forceinline__ void store_pair_operands(const SlotArrays &S, int a, double m, double p, double inv_rho,
+                                                    double rho)
+{
+  S.pk[a] = make_float4((float)m, (float)(p * inv_rho * inv_rho), (float)rho, 0.0f);
+}
+
 // sph.cc:93-125 (itime != 1) for one particle whose post-step state is
 // (rho, p, u, v): *_min <- current, local* <- current, then the half kick
 // with the predictor rates and the fluctuations of the last rate
@@ -47,8 +54,10 @@ __device__ __forceinline__ void predict_one(const DevParams &P, const SlotArrays
   S.rho[a] = rn;
   S.rhot[a] = rt;
   S.p[a] = pn;
-  S.inv_rho[a] = 1.0 / rn;
+  const double ir = 1.0 / rn;
+  S.inv_rho[a] = ir;
   S.inv_rhot[a] = 1.0 / rt;
+  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pn, ir, rn);
 }
 
 __global__ void k_predict(const DevParams P, const SlotArrays S)
@@ -127,7 +136,8 @@ void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int
   k_correct<<<(n + 255) / 256, 256, 0, s>>>(P, S, first_step, predict_next, err, d_itime);
 }
 
-// 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure.
+// 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure; for
+// FP32 pair arithmetic the packed operands.
 // Needed where no predictor ran: a fresh upload and the first step.
 __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int count)
 {
@@ -135,13 +145,16 @@ __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int 
   if (k >= count) return;
   const int a = first + k;
   const double rho = S.rho[a];
-  S.inv_rho[a] = 1.0 / rho;
+  const double ir = 1.0 / rho;
+  S.inv_rho[a] = ir;
   S.inv_rhot[a] = 1.0 / S.rhot[a];
+  double pr = S.p[a];
   if (P.profile == UPH_PROFILE_WCSPH) {
-    const double pr = tait(P, rho);
+    pr = tait(P, rho);
     S.p[a] = pr;
     S.pressure[a] = pr;
   }
+  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pr, ir, rho);
 }
 
 void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s)

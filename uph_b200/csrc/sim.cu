@@ -141,6 +141,7 @@ cudaError_t alloc_slots(uph_sim *s, SlotArrays &A, int n, int nf)
     if ((e = dalloc(s, p, (size_t)n)) != cudaSuccess) return e;
   if ((e = dalloc(s, &A.itype, (size_t)n)) != cudaSuccess) return e;
   if ((e = dalloc(s, &A.orig, (size_t)n)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &A.pk, (size_t)n)) != cudaSuccess) return e;
   double **fl[] = {&A.rho_min, &A.p_min, &A.u_min, &A.v_min, &A.sponge, &A.drho, &A.dp, &A.ax, &A.ay,
                    &A.drho_a, &A.dp_a, &A.ax_a, &A.ay_a, &A.frho, &A.fp, &A.fu, &A.fv};
   for (double **p : fl)
@@ -284,6 +285,7 @@ __global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ pe
   D.ut[s] = S.ut[o]; D.vt[s] = S.vt[o]; D.rho[s] = S.rho[o]; D.rhot[s] = S.rhot[o];
   D.p[s] = S.p[o]; D.pt[s] = S.pt[o]; D.m[s] = S.m[o]; D.inv_rho[s] = S.inv_rho[o];
   D.inv_rhot[s] = S.inv_rhot[o]; D.pressure[s] = S.pressure[o]; D.itype[s] = S.itype[o]; D.orig[s] = S.orig[o];
+  D.pk[s] = S.pk[o];
   if (s < nf) {
     D.rho_min[s] = S.rho_min[o]; D.p_min[s] = S.p_min[o]; D.u_min[s] = S.u_min[o]; D.v_min[s] = S.v_min[o];
     D.sponge[s] = S.sponge[o]; D.drho[s] = S.drho[o]; D.dp[s] = S.dp[o]; D.ax[s] = S.ax[o]; D.ay[s] = S.ay[o];

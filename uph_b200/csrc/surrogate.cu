@@ -44,7 +44,10 @@ constexpr int kNOut = UPH_SUR_OUTPUTS;
 constexpr int kMaxDeg = UPH_SUR_MAX_DEGREE;
 constexpr int kMaxRounds = UPH_SUR_MAX_ROUNDS;
 constexpr int kEdgeThreads = 256;           // 8 warps
-constexpr int kEdgeBlocks = 148 * 4;        // fixed grid: per-warp partials in a fixed order
+// fixed grid (per-warp partials in a fixed order) of one wave: the edge
+// kernels take 80 registers x 256 threads, so three blocks fit an SM's 64K
+// registers; a fourth block per SM would run as a second, mostly empty wave
+constexpr int kEdgeBlocks = 148 * 3;
 constexpr int kColBlocks = 148 * 2;         // bias-gradient partial sums
 constexpr int kSplitMax = 148;              // split-K CTAs of one weight-gradient GEMM tile
 constexpr int kLossBlocks = 148;

@@ -29,6 +29,7 @@ struct SlotArrays {
   double *m;              // mass
   double *inv_rho;        // 1 / density (refreshed before every rate evaluation)
   double *inv_rhot;       // 1 / localDensity
+  float4 *pk;             // FP32 pair operands {m, p / rho^2, rho, 0}, refreshed with inv_rho
   int32_t *itype;
   int32_t *orig;          // reference index of the particle in this slot
   // fluid-only (first nf slots)

@@ -14,7 +14,9 @@
 // the per-particle sums run in FP32 from FP64 differences of positions and
 // velocities (taken before rounding, so small separations keep their
 // precision); the pair test itself stays the exact FP64 predicate so both
-// precisions see the same pairs.
+// precisions see the same pairs.  The partner's m, p / rho^2 and rho come
+// from one packed FP32 load (SlotArrays::pk, rounded once from FP64 where
+// 1/rho is refreshed) instead of four FP64 loads.
 //
 // Execution as in the REF pass: a cheap listing phase (distance test only)
 // per thread into shared memory, then the pair arithmetic over the lists.
@@ -107,9 +109,18 @@ __global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams 
   const int as = active ? a : 0;
   const double xa = S.x[as], ya = S.y[as], ua = S.u[as], va = S.v[as];
   const double ma_d = S.m[as];
-  const Real ira = (Real)S.inv_rho[as];
-  const Real pa_over = (Real)S.p[as] * ira * ira;
-  const Real rhoa = (Real)S.rho[as];
+  // FP32 pair arithmetic reads the packed operands written with 1/rho
+  constexpr bool kPacked = sizeof(Real) == sizeof(float);
+  Real pa_over, rhoa;
+  if constexpr (kPacked) {
+    const float4 k = S.pk[as];
+    pa_over = k.y;
+    rhoa = k.z;
+  } else {
+    const Real ira = (Real)S.inv_rho[as];
+    pa_over = (Real)S.p[as] * ira * ira;
+    rhoa = (Real)S.rho[as];
+  }
   const int oa = S.orig[as], ita = S.itype[as];
   const Real h = (Real)P.h, inv_h = (Real)P.inv_h, inv_h2 = (Real)P.inv_h2;
   const Real sigma = (Real)P.cs_alpha;
@@ -135,6 +146,19 @@ __global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams 
       const double dxd = xa - S.x[b], dyd = ya - S.y[b];
       const double dud = ua - S.u[b], dvd = va - S.v[b];
       const Real dx = (Real)dxd, dy = (Real)dyd, du = (Real)dud, dv = (Real)dvd;
+      // partner operands: FP64 fields, or the packed FP32 copy (one 16-byte load)
+      Real mb, pb_over, rhob;
+      if constexpr (kPacked) {
+        const float4 k = S.pk[b];
+        mb = k.x;
+        pb_over = k.y;
+        rhob = k.z;
+      } else {
+        const Real irb = (Real)S.inv_rho[b];
+        mb = (Real)S.m[b];
+        pb_over = (Real)S.p[b] * irb * irb;
+        rhob = (Real)S.rho[b];
+      }
       const Real r2 = dx * dx + dy * dy;
       const Real r = sqrt_real<Real>(r2);
       const Real q = r * inv_h;
@@ -146,16 +170,14 @@ __global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams 
         F = -sigma * (Real)0.75 * t * t * inv_h * rcp_real<Real>(r);
       }
       const Real gx = F * dx, gy = F * dy;
-      const Real mb = (Real)S.m[b];
-      const Real irb = (Real)S.inv_rho[b];
       drho += mb * (du * gx + dv * gy);
       const Real vr = du * dx + dv * dy;
       Real pi_ab = 0;
       if (vr < (Real)0) {
         const Real mu = h * vr * rcp_real<Real>(r2 + eta2);
-        pi_ab = -ac * mu * rcp_real<Real>((Real)0.5 * (rhoa + (Real)S.rho[b]));
+        pi_ab = -ac * mu * rcp_real<Real>((Real)0.5 * (rhoa + rhob));
       }
-      const Real pij = pa_over + (Real)S.p[b] * irb * irb + pi_ab;
+      const Real pij = pa_over + pb_over + pi_ab;
       ax -= mb * pij * gx;
       ay -= mb * pij * gy;
       if (isI && ita == 1) {
