@@ -148,6 +148,37 @@ def cpu_reference_run(deck, budget_s: float, max_steps: int, warmup: int = 1):
     return deck.n_fluid * steps / total, steps, threads, kind
 
 
+# ---------------------------------------------------------------- ranks ---
+
+class Ranks:
+    """Barrier and max-over-ranks of a replicated run over torch.distributed
+    (NCCL on the GPUs; any backend works, the tests use gloo on the CPU).
+    Every rank makes the same calls in the same order."""
+
+    def __init__(self, world: int, device):
+        self.world = world
+        self.device = device
+
+    def barrier(self) -> None:
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, slowest_seconds: float, world: int) -> float:
+    """Weak scaling of replicas: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / slowest_seconds
+
+
 # ---------------------------------------------------------------- GPU arm ---
 
 def gpu_arm(args, rank, world, local_rank):
@@ -162,16 +193,8 @@ def gpu_arm(args, rank, world, local_rank):
     deck = workload_deck()
     nf, n_all = deck.n_fluid, deck.n_all
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, dev)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     def timed_steps(sim, k, sampler=None):
         barrier()
@@ -204,7 +227,7 @@ def gpu_arm(args, rank, world, local_rank):
     stats = sim.stats()
     sim.profile(False)
     ms_max = max_over_ranks(ms)
-    value = world * nf * args.steps / (ms_max / 1e3)
+    value = whole_job_rate(nf * args.steps, ms_max / 1e3, world)
 
     pass_ms, pass_n = ktimes.get("rate_pass", (0.0, 0))
     pass_avg_s = pass_ms / max(pass_n, 1) / 1e3
@@ -252,7 +275,7 @@ def gpu_arm(args, rank, world, local_rank):
         itime += 1
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * nf * k_e2e / e2e_s
+    e2e_value = whole_job_rate(nf * k_e2e, e2e_s, world)
     sim.close()
 
     # --- variants: the WCSPH profile of the same configuration
@@ -268,7 +291,7 @@ def gpu_arm(args, rank, world, local_rank):
         v.close()
         vms = max_over_ranks(vms)
         p_ms, p_n = kt.get("rate_pass", (0.0, 0))
-        variants[label] = {"value": world * nf * k_var / (vms / 1e3), "steps": k_var,
+        variants[label] = {"value": whole_job_rate(nf * k_var, vms / 1e3, world), "steps": k_var,
                            "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1)}
     if not args.no_batched:
         variants["batched_tanks"] = batched_arm(args, stream.cuda_stream)
