@@ -54,6 +54,14 @@ uph_status uph_tc_gemm_bf16(const void *A, int32_t lda, const void *B, int32_t l
                             int32_t K, const float *bias, int32_t relu, float *c_f32, void *c_bf16, int32_t ldc,
                             int32_t splits, float *partials, int32_t accumulate, unsigned *err, void *stream);
 
+/* Failure-detection self test of the tensor-core kernels' bounded waits: one
+ * 128 x 128 x 64 tile (A, B device BF16 [128 x 64], c_f32 device [128 x 128])
+ * whose CTA first waits on an mbarrier that nothing arrives at.  The wait
+ * gives up after about a second, the kernel sets ERR_TIMEOUT in the device
+ * word *err, frees its TMEM and returns.  Returns UPH_TIMEOUT when that
+ * happened; the CUDA context stays usable. */
+uph_status uph_tc_wait_selftest(const void *A, const void *B, float *c_f32, unsigned *err, void *stream);
+
 typedef struct uph_surrogate uph_surrogate;
 
 #define UPH_SUR_LATENT 128

@@ -70,3 +70,30 @@ def test_tc_gemm_split_k_reduction():
     c2, _ = tc_gemm(torch, A, B, splits=24)
     assert torch.equal(c1, c2)
     assert (c1 - ref).abs().max().item() <= 1e-3 * ref.abs().max().item() + 1e-3
+
+
+def test_bounded_wait_gives_up_and_leaves_the_context_usable():
+    """Failure detection on the GPU without a fault: the self test's CTA waits
+    on an mbarrier that nothing arrives at.  The wait gives up after about a
+    second, the kernel reports ERR_TIMEOUT (UPH_TIMEOUT), frees its TMEM and
+    returns; a normal GEMM right after it is still correct."""
+    import time
+    torch = pytest.importorskip("torch")
+    from uph_b200 import _lib as L
+    lib = L.lib()
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(128, 64, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(128, 64, device="cuda", generator=g).to(torch.bfloat16)
+    c = torch.zeros(128, 128, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.time()
+    st = lib.uph_tc_wait_selftest(A.data_ptr(), B.data_ptr(), c.data_ptr(), err.data_ptr(),
+                                  torch.cuda.current_stream().cuda_stream)
+    elapsed = time.time() - t0
+    assert st == 5, (st, lib.uph_last_error())  # UPH_TIMEOUT
+    assert int(err.item()) & 8  # ERR_TIMEOUT
+    assert 0.5 <= elapsed <= 30.0, elapsed
+    out, _ = tc_gemm(torch, A, B)
+    ref = A.float() @ B.float().T
+    assert (out - ref).abs().max().item() <= 1e-3 * ref.abs().max().item() + 1e-3

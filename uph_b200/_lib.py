@@ -52,6 +52,7 @@ SIGNATURES = {
     "uph_tc_gemm_bf16": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_int32, C.c_void_p, C.c_void_p]),
+    "uph_tc_wait_selftest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "uph_sur_create": (C.c_int, [C.POINTER(SurConfig), C.c_int32, C.POINTER(C.c_void_p)]),
     "uph_sur_destroy": (C.c_int, [C.c_void_p]),
     "uph_sur_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -108,8 +108,11 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t addr)
   return d.desc_;
 }
 
+// true once the barrier's phase `parity` completed; false after kWaitNs on
+// the global timer or kWaitLimit polls, whichever comes first
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 {
+  const unsigned long long t0 = global_ns();
   for (long long i = 0; i < kWaitLimit; i++) {
     uint32_t done;
     asm volatile(
@@ -120,6 +123,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63) == 63 && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
 }

@@ -36,7 +36,7 @@ constexpr int kTcUmmaK = 16;    // K of one tcgen05.mma of kind::f16
 constexpr int kTcStages = 2;
 constexpr int kTcTileBytes = kTcM * kTcBK * 2;  // 16 KiB, same for the B slice (kTcN rows)
 constexpr int kTcSmemBytes = kTcStages * 2 * kTcTileBytes + 1024 + 64;
-constexpr long long kWaitLimit = 1LL << 26;     // ~1 s of polling
+constexpr long long kWaitLimit = 1LL << 26;     // poll cap; the time bound is kWaitNs
 
 struct TcGemmArgs {
   const __nv_bfloat16 *A;
@@ -58,6 +58,7 @@ struct TcGemmArgs {
   int ldc, ldc16;
   float *partials;           // split-K: [splits][M][N] FP32
   unsigned *err;
+  int stall;                 // self-test of the bounded waits (GemmCall::stall)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -81,8 +82,11 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr)
   return d.desc_;
 }
 
+// true once the barrier's phase `parity` completed; false after kWaitNs on
+// the global timer or kWaitLimit polls, whichever comes first
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 {
+  const unsigned long long t0 = global_ns();
   for (long long i = 0; i < kWaitLimit; i++) {
     uint32_t done;
     asm volatile(
@@ -93,6 +97,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63) == 63 && global_ns() - t0 > kWaitNs) return false;
   }
   return false;
 }
@@ -145,6 +150,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
 {
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t mbar[kTcStages];
+  __shared__ uint64_t stall_bar;  // the self-test's barrier: initialised, never arrived at
   __shared__ uint32_t tmem_base_slot;
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int m0 = blockIdx.x * kTcM, n0 = blockIdx.y * kTcN;
@@ -158,9 +164,11 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
                  "r"(kTcN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
   }
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     for (int s = 0; s < kTcStages; s++)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&stall_bar)));
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -168,7 +176,10 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
 
   const uint32_t idesc = static_cast<uint32_t>(cute::UMMA::make_instr_desc<cute::bfloat16_t, cute::bfloat16_t, float, kTcM, kTcN,
                                                                             cute::UMMA::Major::K, cute::UMMA::Major::K>());
-  bool ok = true;
+  // the self-test waits for a phase that never completes: the bounded wait
+  // gives up, no copy or MMA has been issued, and the CTA goes straight to
+  // freeing its TMEM
+  bool ok = g.stall ? mbar_wait(smem_u32(&stall_bar), 0u) : true;
   uint32_t phase[kTcStages] = {0u, 0u};
   for (int s = 0; s < nslices && ok; s++) {
     const int st = s % kTcStages;
@@ -354,6 +365,7 @@ uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s)
   g.ldc16 = ldc16;
   g.partials = splits > 1 ? c.partials : nullptr;
   g.err = c.err;
+  g.stall = c.stall;
   dim3 grid((c.M + kTcM - 1) / kTcM, c.N / kTcN, splits);
   k_tc_gemm<<<grid, 128, kTcSmemBytes, s>>>(g);
   if (splits > 1) {
@@ -394,4 +406,33 @@ extern "C" uph_status uph_tc_gemm_bf16(const void *A, int32_t lda, const void *B
   c.accumulate = accumulate;
   c.err = err;
   return launch_tc_gemm(c, (cudaStream_t)stream);
+}
+
+// Failure-detection self test: one tile whose CTA waits on a barrier nothing
+// arrives at.  The bounded wait gives up, the kernel sets ERR_TIMEOUT, frees
+// its TMEM and returns; the context stays usable.
+extern "C" uph_status uph_tc_wait_selftest(const void *A, const void *B, float *c_f32, unsigned *err, void *stream)
+{
+  if (!A || !B || !c_f32 || !err) return fail(UPH_BAD_ARG, "uph_tc_wait_selftest: NULL argument");
+  cudaStream_t q = (cudaStream_t)stream;
+  GemmCall c;
+  c.A = A;
+  c.lda = kTcBK;
+  c.B = B;
+  c.ldb = kTcBK;
+  c.M = kTcM;
+  c.N = kTcN;
+  c.K = kTcBK;
+  c.c_f32 = c_f32;
+  c.ldc = kTcN;
+  c.err = err;
+  c.stall = 1;
+  UPH_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), q));
+  uph_status r = launch_tc_gemm(c, q);
+  if (r != UPH_OK) return r;
+  unsigned e = 0;
+  UPH_CUDA(cudaMemcpyAsync(&e, err, sizeof e, cudaMemcpyDeviceToHost, q));
+  UPH_CUDA(cudaStreamSynchronize(q));
+  if (e & ERR_TIMEOUT) return fail(UPH_TIMEOUT, "uph_tc_wait_selftest: the wait gave up as intended");
+  return UPH_OK;
 }

@@ -18,6 +18,17 @@ enum : unsigned {
   ERR_TIMEOUT = 8u,
 };
 
+// Bounded device-side waits give up after this long on the GPU's global
+// timer (and after an iteration cap), set ERR_TIMEOUT and clean up.
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Particle data in storage ("slot") order.  Fluid particles occupy slots
 // [0, nf), the other interacting particles [nf, n).  Storage order is
 // spatially sorted (cell order) so that a warp's particles share neighbours.
@@ -175,6 +186,7 @@ struct GemmCall {
   int splits = 1;
   float *partials = nullptr;
   unsigned *err = nullptr;
+  int stall = 0;  // self-test: each CTA first waits on a barrier nothing arrives at
 };
 uph_status launch_tc_gemm(const GemmCall &c, cudaStream_t s);
 
