@@ -99,6 +99,71 @@ def test_search_neighbors_matches_oracle(sim_mod):
     assert np.array_equal(i, wi) and np.array_equal(j, wj) and np.array_equal(r2, wr2)
 
 
+def _brute_pairs(pos, nf, pb, dist):
+    """SearchNeighbors' filter by brute force: s < nf, s < j < pb,
+    DBL_EPSILON < d^2 < dist, d^2 rounded without contraction."""
+    eps = np.finfo(np.float64).eps
+    out = []
+    for s in range(nf):
+        d = pos[s + 1:pb] - pos[s]
+        d2 = d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]
+        for k in np.nonzero((d2 > eps) & (d2 < dist))[0]:
+            out.append((s, s + 1 + int(k), float(d2[k])))
+    return sorted(out)
+
+
+def _edge_case(case):
+    rng = np.random.default_rng(11)
+    if case == "no_fluid":
+        return rng.uniform(0, 1, (10, 2)), 0, 0.1 ** 2
+    if case == "one_particle":
+        return np.array([[0.3, 0.7]]), 1, 0.1 ** 2
+    if case == "all_coincident":
+        return np.full((50, 2), 0.25), 50, 0.1 ** 2
+    if case == "boundary_distance":
+        # d^2 == dist exactly (0.5^2) is outside; 0.49999 is inside
+        return np.array([[0.0, 0.0], [0.5, 0.0], [1.0, 0.0], [1.49999, 0.0], [3.0, 3.0]]), 4, 0.25
+    if case == "sparse_far_apart":
+        # two clusters 10^6 m apart: the cell grid widens its cells instead of
+        # allocating ~10^16 cells
+        a = rng.uniform(0, 0.3, (150, 2))
+        b = rng.uniform(0, 0.3, (150, 2)) + np.array([1.0e6, 3.0e5])
+        return np.concatenate([a, b]), 200, 0.05 ** 2
+    if case == "negative_coordinates":
+        return rng.uniform(-5.0, -3.0, (2000, 2)), 1500, 0.08 ** 2
+    raise ValueError(case)
+
+
+@pytest.mark.parametrize("case", ["no_fluid", "one_particle", "all_coincident", "boundary_distance",
+                                  "sparse_far_apart", "negative_coordinates"])
+def test_search_neighbors_edge_cases(sim_mod, case):
+    pos, nf, dist = _edge_case(case)
+    pb = pos.shape[0] - 1 if pos.shape[0] > 1 else 1
+    i, j, r2 = sim_mod.search_neighbors(pos, nf, pb, dist, number_of_neighbors=0)
+    got = sorted(zip(i.tolist(), j.tolist(), r2.tolist()))
+    assert got == _brute_pairs(pos, nf, pb, dist)
+    if case == "boundary_distance":
+        assert got == [(2, 3, (1.49999 - 1.0) ** 2)]
+
+
+@pytest.mark.parametrize("bad", [0, 3])
+def test_search_neighbors_rejects_non_finite_positions(sim_mod, bad):
+    pos = np.random.default_rng(2).uniform(0, 1, (20, 2))
+    pos[bad, 1] = np.nan if bad == 0 else np.inf
+    with pytest.raises(Exception) as e:
+        sim_mod.search_neighbors(pos, 10, 19, 0.1 ** 2, number_of_neighbors=0)
+    assert "UPH_NAN" in str(e.value)
+
+
+def test_search_neighbors_overcrowded_cell_is_reported(sim_mod):
+    """5000 points inside one search cell: more than the 4096 ids a cell may
+    hold, reported as a neighbour overflow before any kernel walks them."""
+    pos = np.random.default_rng(5).uniform(0.0, 0.01, (5000, 2))
+    with pytest.raises(Exception) as e:
+        sim_mod.search_neighbors(pos, 5000, 4999, 1.0, number_of_neighbors=0)
+    assert "UPH_NEIGHBOR_OVERFLOW" in str(e.value)
+
+
 def test_search_neighbors_knn_cap_that_binds_is_reported(sim_mod):
     pos = np.array([[0.001 * k, 0.0] for k in range(60)])
     with pytest.raises(Exception) as e:

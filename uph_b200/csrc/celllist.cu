@@ -162,11 +162,19 @@ void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s
   k_cell_scatter<<<(count + 255) / 256, 256, 0, s>>>(G.cell_of, G.start, G.fill, G.list, first, count);
 }
 
-__global__ void k_cell_sort_segments(const int *__restrict__ start, int *__restrict__ list, int ncell)
+// Each cell's ids ascending (insertion sort by one thread).  A cell holding
+// more than kMaxCellOccupancy ids is not sorted: it flags a neighbour
+// overflow instead, which bounds this kernel's work on pathological inputs
+// (a radius of the whole domain, particles piled into a border cell).
+__global__ void k_cell_sort_segments(const int *__restrict__ start, int *__restrict__ list, int ncell, unsigned *err)
 {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   const int a = start[c], b = start[c + 1];
+  if (b - a > kMaxCellOccupancy) {
+    if (err) atomicOr(err, ERR_NEIGHBOR_OVERFLOW);
+    return;
+  }
   for (int i = a + 1; i < b; i++) {
     const int v = list[i];
     int j = i - 1;
@@ -178,9 +186,9 @@ __global__ void k_cell_sort_segments(const int *__restrict__ start, int *__restr
   }
 }
 
-void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s)
+void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s)
 {
-  k_cell_sort_segments<<<(G.ncell + 255) / 256, 256, 0, s>>>(G.start, G.list, G.ncell);
+  k_cell_sort_segments<<<(G.ncell + 255) / 256, 256, 0, s>>>(G.start, G.list, G.ncell, err);
 }
 
 }  // namespace uph

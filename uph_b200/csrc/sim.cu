@@ -313,7 +313,7 @@ uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, i
   launch_exclusive_scan(G.count, G.start, G.ncell, G.block_sums, st);
   // scatter ids; list is indexed from 0 because start[] only counted this range
   launch_cell_scatter(G, first, count, st);
-  launch_cell_sort_segments(G, st);
+  launch_cell_sort_segments(G, s->d_err, st);
   s->launches += 6;
   return UPH_OK;
 }
@@ -400,6 +400,9 @@ uph_status validate(const uph_params *p)
   if (p->knn_cap != 0) return fail(UPH_UNSUPPORTED, "the k-NN cap is not implemented; use knn_cap = 0");
   if (!(p->domain_hi[0] > p->domain_lo[0]) || !(p->domain_hi[1] > p->domain_lo[1]))
     return fail(UPH_BAD_ARG, "empty cell-grid domain");
+  for (int d = 0; d < 2; d++)
+    if (!isfinite(p->domain_lo[d]) || !isfinite(p->domain_hi[d]))
+      return fail(UPH_BAD_ARG, "non-finite cell-grid domain");
   return UPH_OK;
 }
 
@@ -426,21 +429,32 @@ cudaError_t alloc_grid(uph_sim *s)
   return cudaSuccess;
 }
 
-// Cell width radius / reach; cells per axis rounded up to whole tiles.
+// Cell width radius / reach; cells per axis rounded up to whole tiles.  A
+// sparse domain (few particles spread far apart, as SearchNeighbors may be
+// given) gets wider cells so the grid stays within kMaxGridCells: the
+// stencil of `reach` cells then reaches further than the radius, which only
+// adds candidates -- the pair test is the exact distance predicate.
+constexpr double kMaxGridCells = double(1 << 26);
+
 void set_grid_geometry(DevParams &P, int reach, int tile)
 {
   P.reach = reach;
   P.tile = tile;
-  const double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
+  double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
+  double tiles_x, tiles_y;
+  for (int grow = 0; grow < 200; grow++) {  // finite domains (validate) end in a few rounds
+    const double nx = ceil((P.hi_x - P.lo_x) / cell);
+    const double ny = ceil((P.hi_y - P.lo_y) / cell);
+    tiles_x = ceil(fmax(nx, 1.0) / tile);
+    tiles_y = ceil(fmax(ny, 1.0) / tile);
+    if (tiles_x * tiles_y * tile * tile <= kMaxGridCells) break;
+    cell *= 1.5;
+  }
   P.cell = cell;
   P.inv_cell = 1.0 / cell;
-  const double nx = ceil((P.hi_x - P.lo_x) / cell);
-  const double ny = ceil((P.hi_y - P.lo_y) / cell);
-  const double tiles_x = ceil(fmax(nx, 1.0) / tile), tiles_y = ceil(fmax(ny, 1.0) / tile);
-  // clamp before converting; callers reject grids this large
-  P.ntx = (int)fmin(tiles_x, 1 << 20);
+  P.ntx = (int)tiles_x;
   P.ncx = P.ntx * tile;
-  P.ncy = (int)fmin(tiles_y, 1 << 20) * tile;
+  P.ncy = (int)tiles_y * tile;
 }
 
 DevParams make_dev_params(const uph_params *p)
@@ -1416,10 +1430,10 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
   *niac = 0;
   if (n_fluid == 0 || !(dist > 0.0)) return UPH_OK;
   double lo[2] = {position[0], position[1]}, hi[2] = {position[0], position[1]};
-  for (int k = 1; k < n_all; k++)
+  for (int k = 0; k < n_all; k++)
     for (int d = 0; d < 2; d++) {
       const double v = position[2 * k + d];
-      if (!(v == v)) return fail(UPH_NAN, "uph_search_neighbors: non-finite position");
+      if (!isfinite(v)) return fail(UPH_NAN, "uph_search_neighbors: non-finite position");
       lo[d] = fmin(lo[d], v);
       hi[d] = fmax(hi[d], v);
     }
@@ -1452,6 +1466,9 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
   }
   k_load_positions<<<(n_all + 255) / 256, 256, 0, q>>>(s->S, dpos, n_all);
   r = build_cell_list(s);
+  // an overcrowded cell (or a position outside the grid) stops here, before
+  // any kernel walks the candidates
+  if (r == UPH_OK) r = check_error_word(s);
   if (r == UPH_OK && knn > 0) {
     int mx = 0;
     cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), q);

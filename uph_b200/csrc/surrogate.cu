@@ -819,7 +819,7 @@ uph_status prepare(uph_surrogate *s, const NodesView &nv)
   launch_cell_keys(G, nv.x, nv.y, 0, nv.n, g, s->d_err, false, q);
   launch_exclusive_scan(g.count, g.start, (int)ncell, g.block_sums, q);
   launch_cell_scatter(g, 0, nv.n, q);
-  launch_cell_sort_segments(g, q);
+  launch_cell_sort_segments(g, s->d_err, q);
   k_sur_graph<<<(nv.n + 127) / 128, 128, 0, q>>>(G, nv.x, nv.y, nv.rho, s->cfg.rho0 * s->cfg.edge_rho_scale, nv.n,
                                                  g.cell_of, g.start, g.list, R, s->nbr, s->ef, s->deg, s->d_err);
   k_sur_features<<<(nv.n + 255) / 256, 256, 0, q>>>(nv.n, nv.u, nv.v, nv.rho, nv.itype, s->cfg.vel_scale,

@@ -136,7 +136,9 @@ void launch_cell_keys(const DevParams &P, const double *x, const double *y, int 
 void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s);
 int scan_block_sums_needed(int n);  // size of launch_exclusive_scan's block_sums
 void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s);
-void launch_cell_sort_segments(const CellGrid &G, cudaStream_t s);
+// a cell with more ids than this is left unsorted and flags ERR_NEIGHBOR_OVERFLOW
+constexpr int kMaxCellOccupancy = 4096;
+void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s);
 
 // REF / WCSPH rate pass over the fluid slots
 struct PassStats {
