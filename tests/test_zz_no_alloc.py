@@ -78,3 +78,34 @@ def test_noalloc_search_rejects_sizes_beyond_its_limit():
                                           C.byref(hi2), 0, None, None, None, C.byref(niac), None)
     assert st == 1
     assert b"cells" in lib.uph_last_error()
+
+
+def test_noalloc_search_reports_an_overcrowded_cell():
+    """5000 points in one search cell (more than the 4096 ids a cell may hold):
+    a neighbour overflow, with no pair walk, and the next call works again."""
+    torch = pytest.importorskip("torch")
+    from uph_b200 import _lib
+
+    lib = _lib.lib()
+    pos = np.random.default_rng(5).uniform(0.0, 0.01, (5000, 2))
+    d_pos = torch.from_numpy(pos).cuda()
+    lo = (C.c_double * 2)(-0.1, -0.1)
+    hi = (C.c_double * 2)(0.2, 0.2)
+    niac = C.c_int64(-1)
+    st = lib.uph_search_neighbors_noalloc(C.c_void_p(d_pos.data_ptr()), 5000, 5000, 4999, 1.0, C.byref(lo),
+                                          C.byref(hi), 0, None, None, None, C.byref(niac), None)
+    assert st == 3, lib.uph_last_error()  # UPH_NEIGHBOR_OVERFLOW
+    assert niac.value == 0
+    # a sane call right after it
+    pos2 = np.random.default_rng(6).uniform(0.0, 0.2, (500, 2))
+    d_pos2 = torch.from_numpy(pos2).cuda()
+    cap = 100000
+    d_i = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    d_j = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    d_r2 = torch.zeros(cap, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    st = lib.uph_search_neighbors_noalloc(C.c_void_p(d_pos2.data_ptr()), 500, 500, 499, 0.02 ** 2, C.byref(lo),
+                                          C.byref(hi), cap, C.c_void_p(d_i.data_ptr()), C.c_void_p(d_j.data_ptr()),
+                                          C.c_void_p(d_r2.data_ptr()), C.byref(niac), None)
+    assert st == 0, lib.uph_last_error()
+    assert 0 < niac.value < cap

@@ -78,11 +78,17 @@ __global__ void k_na_scatter(NoAllocGrid g, const int *__restrict__ cell_of, con
   list[start[c] + atomicAdd(&fill[c], 1)] = s;
 }
 
-__global__ void k_na_sort_cells(const int *__restrict__ start, int *__restrict__ list, int ncell)
+// a cell with more than kMaxCellOccupancy ids is not sorted: it flags a
+// neighbour overflow, and the pair kernels then do nothing
+__global__ void k_na_sort_cells(const int *__restrict__ start, int *__restrict__ list, int ncell, unsigned *err)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   const int a = start[c], b = start[c + 1];
+  if (b - a > kMaxCellOccupancy) {
+    atomicOr(err, ERR_NEIGHBOR_OVERFLOW);
+    return;
+  }
   for (int i = a + 1; i < b; i++) {
     const int v = list[i];
     int j = i - 1;
@@ -102,10 +108,15 @@ __device__ __forceinline__ double na_r2(double dx, double dy) { return __dadd_rn
 template <bool kWrite>
 __global__ void k_na_pairs(NoAllocGrid g, const double *__restrict__ pos, const int *__restrict__ cell_of,
                            const int *__restrict__ start, const int *__restrict__ list, int *__restrict__ cnt,
-                           const int *__restrict__ off, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2)
+                           const int *__restrict__ off, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
+                           const unsigned *err)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.n_fluid) return;
+  if (*err & ERR_NEIGHBOR_OVERFLOW) {  // an overcrowded cell: no walk
+    if (!kWrite) cnt[s] = 0;
+    return;
+  }
   const double xs = pos[2 * s], ys = pos[2 * s + 1];
   const int c = cell_of[s], cx = c % g.ncx, cy = c / g.ncx;
   int n = 0;
@@ -215,13 +226,13 @@ extern "C" uph_status uph_search_neighbors_noalloc(const double *position, int32
   k_na_keys<<<(n_all + tb - 1) / tb, tb, 0, q>>>(g, position, cell_of, count, err);
   launch_exclusive_scan(count, start, ncell, sums, q);
   k_na_scatter<<<(n_all + tb - 1) / tb, tb, 0, q>>>(g, cell_of, start, fill, list);
-  k_na_sort_cells<<<(ncell + tb - 1) / tb, tb, 0, q>>>(start, list, ncell);
+  k_na_sort_cells<<<(ncell + tb - 1) / tb, tb, 0, q>>>(start, list, ncell, err);
   k_na_pairs<false><<<(n_fluid + tb - 1) / tb, tb, 0, q>>>(g, position, cell_of, start, list, pcnt, nullptr, 0,
-                                                           nullptr, nullptr, nullptr);
+                                                           nullptr, nullptr, nullptr, err);
   launch_exclusive_scan(pcnt, poff, n_fluid, sums, q);
   if (cap > 0)
     k_na_pairs<true><<<(n_fluid + tb - 1) / tb, tb, 0, q>>>(g, position, cell_of, start, list, pcnt, poff, cap,
-                                                            i_pair, j_pair, rij2);
+                                                            i_pair, j_pair, rij2, err);
   UPH_CUDA(cudaGetLastError());
   int total = 0;
   unsigned errw = 0;
@@ -231,6 +242,11 @@ extern "C" uph_status uph_search_neighbors_noalloc(const double *position, int32
   *niac = total;
   if (errw & ERR_OUT_OF_DOMAIN)
     return fail(UPH_OUT_OF_DOMAIN, "uph_search_neighbors_noalloc: a particle lies outside [lo, hi]");
+  if (errw & ERR_NEIGHBOR_OVERFLOW) {
+    *niac = 0;
+    return fail(UPH_NEIGHBOR_OVERFLOW, "uph_search_neighbors_noalloc: a search cell holds more than " +
+                                           std::to_string(kMaxCellOccupancy) + " particles");
+  }
   if (total > cap)
     return fail(UPH_NEIGHBOR_OVERFLOW, "uph_search_neighbors_noalloc: " + std::to_string(total) +
                                            " pairs do not fit the capacity " + std::to_string(cap));
