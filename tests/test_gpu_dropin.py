@@ -3,7 +3,8 @@ files (input.c, inputbp.c, output.c, ...) relinked against libuph_sph.so in
 place of derivatives.c + Search.cc, compared with the unmodified reference.
 
 Both builds live in oracle/_ref/ (made by `make -C oracle ref dropin` from
-the reference's sources); the GPU box receives them prebuilt."""
+the reference's sources); a machine without those sources runs the prebuilt
+files."""
 import os
 import subprocess
 import tempfile
