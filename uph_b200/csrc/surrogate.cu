@@ -184,6 +184,9 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
   if (i >= n) return;
   const double xi = x[i], yi = y[i], ri = rho[i];
   const double r2cut = R * R;
+  // features by multiplication with reciprocals (no FP64 division or square
+  // root per edge); they are rounded to FP32 anyway
+  const double inv_R = 1.0 / R, inv_R2 = 1.0 / r2cut, inv_rho_unit = 1.0 / rho_unit;
   const int c = cell_of[i];
   const int cx = c % G.ncx, cy = c / G.ncx;
   int cnt = 0;
@@ -212,8 +215,9 @@ __global__ void k_sur_graph(DevParams G, const double *__restrict__ x, const dou
         if (r2 > DBL_EPSILON && r2 < r2cut) {
           if (cnt < kMaxDeg) {
             nbr[(size_t)i * kMaxDeg + cnt] = j;
-            ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx / R), (float)(dy / R), (float)(sqrt(r2) / R),
-                                                        (float)((rho[j] - ri) / rho_unit));
+            ef[(size_t)i * kMaxDeg + cnt] = make_float4((float)(dx * inv_R), (float)(dy * inv_R),
+                                                        sqrtf((float)(r2 * inv_R2)),
+                                                        (float)((rho[j] - ri) * inv_rho_unit));
           }
           cnt++;
         }
