@@ -303,10 +303,15 @@ uph_status uph_search_neighbors(const double *position, int32_t n_fluid, int32_t
  * start-up.  No counterpart in the reference.
  * position, i_pair, j_pair and rij2 are DEVICE buffers owned by the caller;
  * the grid box [lo, hi] must contain every position.  Scratch lives in one
- * statically sized __device__ array of the library (about 10 MiB, held by
+ * statically sized __device__ array of the library (about 11 MiB, held by
  * every GPU that loads the library until exit); no call allocates.
  * Limits: n_all <= 262,144 particles and at most 524,288 search cells of width
- * sqrt(dist) over [lo, hi]; larger inputs return UPH_BAD_ARG.
+ * sqrt(dist) over [lo, hi]; larger inputs return UPH_BAD_ARG.  A cell holding
+ * more than 4,096 particles returns UPH_NEIGHBOR_OVERFLOW with *niac = 0.
+ * Unlike uph_search_neighbors (and the reference's 40-NN search) there is no
+ * knn cap: every in-radius pair is returned.  Pair offsets and *niac are
+ * 64-bit; *niac is the full count even when it exceeds cap (then
+ * UPH_NEIGHBOR_OVERFLOW, and only the first cap pairs are written).
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture.  Calls share the array, so calls that
  * overlap on the GPU race.  The call synchronises `stream` (a cudaStream_t,
@@ -315,6 +320,14 @@ uph_status uph_search_neighbors_noalloc(const double *position, int32_t n_fluid,
                                         int32_t particle_boundary, double dist, const double lo[2],
                                         const double hi[2], int64_t cap, int32_t *i_pair, int32_t *j_pair,
                                         double *rij2, int64_t *niac, void *stream);
+
+/* ---- self-tests ------------------------------------------------------------ */
+
+/* y[k] = the reciprocal the rate passes use in place of 1.0 / x[k] (a
+ * Newton-Raphson refinement of the hardware's approximate FP64 reciprocal),
+ * for n DEVICE values on `stream`; for testing its error against IEEE
+ * division.  No counterpart in the reference (which divides). */
+uph_status uph_rcp_selftest(const double *x, double *y, int64_t n, void *stream);
 
 /* ---- errors ---------------------------------------------------------------- */
 

@@ -20,7 +20,22 @@ from uph_b200._capi import (STATE_FIELDS, UphParams, empty_state, state_struct)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_TREE = "/root/reference"
+
+
+def _reference_tree() -> str:
+    """The reference's source tree: $UPH_REFERENCE, else the default of
+    oracle/Makefile (its REF line is the one place the default is kept)."""
+    env = os.environ.get("UPH_REFERENCE")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF ?="):
+                return line.rsplit(",", 1)[-1].strip().rstrip(")")
+    return ""
+
+
+REFERENCE_TREE = _reference_tree()
 
 
 def build(reference: bool = True) -> None:

@@ -11,6 +11,7 @@ import tempfile
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from uph_b200 import _lib
 from uph_b200 import deck as D
 from uph_b200._capi import UphParams, empty_state, state_struct
@@ -121,7 +122,7 @@ def test_deck_text_roundtrip():
         assert np.array_equal(getattr(back, blk), getattr(deck, blk)), blk
 
 
-@pytest.mark.skipif(shutil.which("gcc") is None or not os.path.isdir("/root/reference/src/lib"),
+@pytest.mark.skipif(shutil.which("gcc") is None or not os.path.isdir(os.path.join(O.REFERENCE_TREE, "src", "lib")),
                     reason="needs gcc and the reference headers")
 def test_system_layout_matches_reference():
     """include/uph_system.h declares the reference's struct with the same layout."""
@@ -142,7 +143,7 @@ def test_system_layout_matches_reference():
     with tempfile.TemporaryDirectory() as tmp:
         c = os.path.join(tmp, "l.c")
         open(c, "w").write(src)
-        for hdr, inc in [('"System.h"', "/root/reference/src/lib"), ('"uph_system.h"', os.path.join(ROOT, "include"))]:
+        for hdr, inc in [('"System.h"', os.path.join(O.REFERENCE_TREE, "src", "lib")), ('"uph_system.h"', os.path.join(ROOT, "include"))]:
             exe = os.path.join(tmp, "l")
             subprocess.run(["gcc", "-std=gnu99", f"-DHDR={hdr}", "-I", inc, c, "-o", exe], check=True)
             outs.append(subprocess.run([exe], capture_output=True, text=True, check=True).stdout)

@@ -1,6 +1,7 @@
 """The hydrostatic-tank configuration (2.0 x 1.0 m water, dx = 0.002 m,
 500,000 fluid particles, 3 wall layers, 2,000 steps) against its analytic
-answer: pressure p = rho0 g (H - y) and exactly conserved mass.
+answer: pressure p = rho0 g (H - y), with the water kept in the tank and its
+volume conserved.
 
 The pressure profile is judged as the mean pressure of depth bins two
 spacings thick, away from the side walls, against rho0 g (H - y_bin):
@@ -15,6 +16,18 @@ from uph_b200 import deck as D
 pytestmark = pytest.mark.gpu
 
 RHO0, G = 1000.0, 9.81
+
+
+def _conservation(state, init, nf, width):
+    """(fluid particles outside the tank interior, relative drift of the
+    water volume sum m / rho).  Particle masses never change, so mass is
+    conserved exactly iff no fluid particle is lost: the count is what
+    shows it.  The volume sum shows the mean density holding."""
+    x, y = state["Position"][:nf, 0], state["Position"][:nf, 1]
+    outside = int(np.count_nonzero(~((x > 0.0) & (x < width) & (y > 0.0) & np.isfinite(x) & np.isfinite(y))))
+    v0 = float(np.sum(init["mass"][:nf] / init["density"][:nf]))
+    v1 = float(np.sum(state["mass"][:nf] / state["density"][:nf]))
+    return outside, abs(v1 - v0) / v0
 
 
 def _binned_error(state, nf, depth, width, dx):
@@ -49,9 +62,10 @@ def test_hydrostatic_tank_matches_rho_g_h(precision):
     nf = deck.n_fluid
     err = _binned_error(st, nf, depth, width, dx)
     assert err <= 0.03, f"pressure profile off by {100 * err:.2f} % of rho0 g H"
-    # mass: the particle masses are untouched, so the total is exact
-    assert np.array_equal(st["mass"], init["mass"])
-    assert np.all(np.isfinite(st["Position"][:nf]))
+    outside, dvol = _conservation(st, init, nf, width)
+    print(f"precision {precision}: profile error {100 * err:.3f} % of rho0 g H, volume drift {dvol:.2e}")
+    assert outside == 0, f"{outside} fluid particles left the tank"
+    assert dvol < 1e-3, f"water volume drifted by {dvol:.2e}"
     assert stats["max_abs_density_error"] < 0.01
     # the water stays put: no particle moved more than a spacing
     drift = np.abs(st["Position"][:nf] - init["Position"][:nf]).max()
@@ -61,7 +75,8 @@ def test_hydrostatic_tank_matches_rho_g_h(precision):
 def test_hydrostatic_tank_ref_profile_is_stable():
     """The reference's own formulation on the same tank (its diffusion and
     fluctuation terms make the profile converge more slowly): bounded
-    velocities, the profile within 10 % of rho0 g H, exact mass."""
+    velocities, the profile within 10 % of rho0 g H, no fluid lost and the
+    water volume held."""
     from uph_b200.sim import Simulation
 
     width, depth, dx = 2.0, 1.0, 0.002
@@ -70,6 +85,11 @@ def test_hydrostatic_tank_ref_profile_is_stable():
         s.step(2000)
         st = s.download()
     nf = deck.n_fluid
+    err = _binned_error(st, nf, depth, width, dx)
+    outside, dvol = _conservation(st, deck.initial_state(), nf, width)
+    print(f"REF: profile error {100 * err:.3f} % of rho0 g H, volume drift {dvol:.2e}, "
+          f"max |v| {np.abs(st['Velocity'][:nf]).max():.3e}")
     assert np.abs(st["Velocity"][:nf]).max() < 0.5
-    assert _binned_error(st, nf, depth, width, dx) <= 0.10
-    assert np.array_equal(st["mass"], deck.initial_state()["mass"])
+    assert err <= 0.10
+    assert outside == 0, f"{outside} fluid particles left the tank"
+    assert dvol < 1e-3, f"water volume drifted by {dvol:.2e}"

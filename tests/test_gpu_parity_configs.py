@@ -1,0 +1,76 @@
+"""Parity at the workloads' own sizes: the GPU drop-in path (REF physics,
+FP64, through the C ABI) against the reference's solver compiled from its
+sources (oracle/_ref), on
+
+* the 5,000-particle dam break: tank 4.0 x 3.0 m, water column 1.0 x 2.0 m
+  at dx = 0.02 m, 2 wall layers, h = 1.3 dx, hydrostatic initial density;
+* the 500,000-particle hydrostatic tank: 2.0 x 1.0 m at dx = 0.002 m,
+  3 wall layers, h = 1.3 dx (the bench workload).
+
+Bars, as for the golden cases: the reference's 40-NN search never truncates
+(at most 39 in-radius neighbours, so the pair set does not depend on
+libnabo's tie order); the step-1 pair list (i, j) and rij2 are bit-identical;
+all 17 fluid fields are within 1e-10 of the reference, relative to each
+field's largest magnitude, after steps 1 and 3."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from _util import FLUID_FIELDS, REL_TOL_FP64, compare_fields
+from oracle import oracle as O
+from uph_b200 import deck as D
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {
+    "dambreak_5k": lambda: D.dam_break(tank=(4.0, 3.0), column=(1.0, 2.0), dx=0.02, layers=2, hydrostatic=True),
+    "hydrostatic_500k": lambda: D.hydrostatic_tank(width=2.0, depth=1.0, dx=0.002, layers=3),
+}
+
+
+def _need_reference():
+    if not os.path.exists(os.path.join(O.REF_DIR, "libuph_ref.so")):
+        pytest.skip("oracle/_ref/libuph_ref.so not built (make -C oracle ref)")
+
+
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_workload_matches_compiled_reference(name):
+    _need_reference()
+    from uph_b200.sim import Simulation
+
+    deck = CONFIGS[name]()
+    if name == "dambreak_5k":
+        assert deck.n_fluid == 5000
+    else:
+        assert deck.n_fluid == 500000
+    with tempfile.TemporaryDirectory() as tmp:
+        deck.write(tmp)
+        run = O.RefRun(tmp, eta_override=deck.eta_override, fluid_capacity_pct=16)
+        try:
+            run.step(1)
+            assert run.truncated_queries() == 0 and run.max_inradius() <= 39, \
+                f"the reference's 40-NN cap binds (max in-radius {run.max_inradius()})"
+            ref1 = {f: run.get(f) for f in FLUID_FIELDS}
+            ri, rj = run.pairs()
+            rr2 = run.get("rij2")
+            run.step(2)
+            ref3 = {f: run.get(f) for f in FLUID_FIELDS}
+        finally:
+            run.close()
+    with Simulation.from_deck(deck) as s:
+        s.step(1)
+        e1 = compare_fields(s.download(), ref1, deck.n_fluid, REL_TOL_FP64)
+        s.step(2)
+        e3 = compare_fields(s.download(), ref3, deck.n_fluid, REL_TOL_FP64)
+    # the pairs of step 1's derivatives() call: the initial state
+    with Simulation.from_deck(deck) as s:
+        s.derivatives(deck.params["time_step"])
+        i, j, r2, _, _ = s.pairs()
+    assert i.size == ri.size, f"{i.size} pairs against the reference's {ri.size}"
+    assert np.array_equal(i, ri), "i_pair differs"
+    assert np.array_equal(j, rj), "j_pair differs"
+    assert np.array_equal(r2, rr2), "rij2 not bit-identical"
+    print(f"{name}: {ri.size} pairs bit-identical; max field error step 1 {max(e1.values()):.2e}, "
+          f"step 3 {max(e3.values()):.2e}")

@@ -109,3 +109,39 @@ def test_noalloc_search_reports_an_overcrowded_cell():
                                           C.c_void_p(d_r2.data_ptr()), C.byref(niac), None)
     assert st == 0, lib.uph_last_error()
     assert 0 < niac.value < cap
+
+
+def test_noalloc_search_dense_queries_and_short_capacity():
+    """A dense cluster: every query has about a thousand partners, so each
+    query's pairs come from the merge of nine long cell lists.  The pairs
+    equal the allocating search's; with a capacity below the total the call
+    reports the full 64-bit count, writes exactly the first `cap` pairs and
+    returns UPH_NEIGHBOR_OVERFLOW."""
+    torch = pytest.importorskip("torch")
+    from uph_b200 import _lib
+    from uph_b200.sim import search_neighbors
+
+    lib = _lib.lib()
+    n = 3000
+    pos = np.random.default_rng(21).uniform(0.0, 0.06, (n, 2))
+    dist = 0.03 ** 2
+    want_i, want_j, want_r2 = search_neighbors(pos, n, n - 1, dist, number_of_neighbors=0)
+    assert want_i.size > 500 * n
+    lo = (C.c_double * 2)(-0.01, -0.01)
+    hi = (C.c_double * 2)(0.07, 0.07)
+    d_pos = torch.from_numpy(pos).cuda()
+    for cap in (want_i.size, want_i.size // 3):
+        d_i = torch.full((cap,), -1, dtype=torch.int32, device="cuda")
+        d_j = torch.full((cap,), -1, dtype=torch.int32, device="cuda")
+        d_r2 = torch.zeros(cap, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        niac = C.c_int64(-1)
+        st = lib.uph_search_neighbors_noalloc(C.c_void_p(d_pos.data_ptr()), n, n, n - 1, dist, C.byref(lo),
+                                              C.byref(hi), cap, C.c_void_p(d_i.data_ptr()),
+                                              C.c_void_p(d_j.data_ptr()), C.c_void_p(d_r2.data_ptr()),
+                                              C.byref(niac), None)
+        assert niac.value == want_i.size
+        assert st == (0 if cap == want_i.size else 3), lib.uph_last_error()
+        assert np.array_equal(d_i.cpu().numpy(), want_i[:cap])
+        assert np.array_equal(d_j.cpu().numpy(), want_j[:cap])
+        assert np.array_equal(d_r2.cpu().numpy(), want_r2[:cap])

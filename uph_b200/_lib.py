@@ -48,6 +48,7 @@ SIGNATURES = {
                                                C.POINTER(C.c_double * 2), C.POINTER(C.c_double * 2), C.c_int64,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
                                                C.c_void_p]),
+    "uph_rcp_selftest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     # include/uph_surrogate.h
     "uph_tc_gemm_bf16": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,

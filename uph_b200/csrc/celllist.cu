@@ -56,77 +56,83 @@ constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_PER_THREAD = 4;
 constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_PER_THREAD;
 
-__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_tot, int &total)
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T *warp_tot, T &total)
 {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int incl = v;
+  T incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    T t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
   if (lane == 31) warp_tot[wid] = incl;
   __syncthreads();
   if (wid == 0) {
-    int wv = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
-    int wi = wv;
+    T wv = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : T(0);
+    T wi = wv;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, wi, o);
+      T t = __shfl_up_sync(0xffffffffu, wi, o);
       if (lane >= o) wi += t;
     }
     warp_tot[lane] = wi - wv;  // exclusive prefix of warp totals
     if (lane == 31) warp_tot[32] = wi;
   }
   __syncthreads();
-  const int out = incl - v + warp_tot[wid];
+  const T out = incl - v + warp_tot[wid];
   total = warp_tot[32];
   __syncthreads();
   return out;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunk_sums(const int *__restrict__ in, int n,
-                                                                  int *__restrict__ sums)
+// In: counts of type C; out, the chunk sums and the running totals: type T
+// (int for cell histograms, long long for pair counts that may pass 2^31).
+template <typename C, typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunk_sums(const C *__restrict__ in, int n,
+                                                                  T *__restrict__ sums)
 {
-  __shared__ int wt[33];
+  __shared__ T wt[33];
   const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER_THREAD;
-  int v = 0;
+  T v = 0;
 #pragma unroll
   for (int k = 0; k < SCAN_PER_THREAD; k++)
-    if (base + k < n) v += in[base + k];
-  int total;
-  block_exclusive_scan(v, wt, total);
+    if (base + k < n) v += (T)in[base + k];
+  T total;
+  block_exclusive_scan<T>(v, wt, total);
   if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int *sums, int nsums)
+template <typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(T *sums, int nsums)
 {
-  __shared__ int wt[33];
-  int carry = 0;
+  __shared__ T wt[33];
+  T carry = 0;
   for (int base = 0; base < nsums; base += SCAN_THREADS) {
     const int i = base + threadIdx.x;
-    const int v = (i < nsums) ? sums[i] : 0;
-    int total;
-    const int ex = block_exclusive_scan(v, wt, total);
+    const T v = (i < nsums) ? sums[i] : T(0);
+    T total;
+    const T ex = block_exclusive_scan<T>(v, wt, total);
     if (i < nsums) sums[i] = ex + carry;
     carry += total;
   }
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunks(const int *__restrict__ in, int *__restrict__ out,
-                                                              int n, const int *__restrict__ sums)
+template <typename C, typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_chunks(const C *__restrict__ in, T *__restrict__ out,
+                                                              int n, const T *__restrict__ sums)
 {
-  __shared__ int wt[33];
+  __shared__ T wt[33];
   const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER_THREAD;
-  int v[SCAN_PER_THREAD];
-  int tsum = 0;
+  T v[SCAN_PER_THREAD];
+  T tsum = 0;
 #pragma unroll
   for (int k = 0; k < SCAN_PER_THREAD; k++) {
-    v[k] = (base + k < n) ? in[base + k] : 0;
+    v[k] = (base + k < n) ? (T)in[base + k] : T(0);
     tsum += v[k];
   }
-  int total;
-  int run = block_exclusive_scan(tsum, wt, total) + sums[blockIdx.x];
+  T total;
+  T run = block_exclusive_scan<T>(tsum, wt, total) + sums[blockIdx.x];
 #pragma unroll
   for (int k = 0; k < SCAN_PER_THREAD; k++) {
     if (base + k < n) out[base + k] = run;
@@ -141,9 +147,17 @@ int scan_block_sums_needed(int n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
 void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s)
 {
   const int nb = scan_block_sums_needed(n);
-  k_scan_chunk_sums<<<nb, SCAN_THREADS, 0, s>>>(in, n, block_sums);
-  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(block_sums, nb);
-  k_scan_chunks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, block_sums);
+  k_scan_chunk_sums<int, int><<<nb, SCAN_THREADS, 0, s>>>(in, n, block_sums);
+  k_scan_sums<int><<<1, SCAN_THREADS, 0, s>>>(block_sums, nb);
+  k_scan_chunks<int, int><<<nb, SCAN_THREADS, 0, s>>>(in, out, n, block_sums);
+}
+
+void launch_exclusive_scan64(const int *in, long long *out, int n, long long *block_sums, cudaStream_t s)
+{
+  const int nb = scan_block_sums_needed(n);
+  k_scan_chunk_sums<int, long long><<<nb, SCAN_THREADS, 0, s>>>(in, n, block_sums);
+  k_scan_sums<long long><<<1, SCAN_THREADS, 0, s>>>(block_sums, nb);
+  k_scan_chunks<int, long long><<<nb, SCAN_THREADS, 0, s>>>(in, out, n, block_sums);
 }
 
 __global__ void k_cell_scatter(const int *__restrict__ cell_of, const int *__restrict__ start, int *fill,

@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_node_chain(const __grid_constan
   __shared__ uint64_t bars[5];
   __shared__ uint32_t tmem_slot;
   __shared__ int s_abort;
+  __shared__ int s_mma_pending;  // set by the final drain: an MMA never completed
   __shared__ float s_bias[256];  // the current layer's bias
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t sb = su32(sm);
@@ -260,6 +261,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_node_chain(const __grid_constan
     for (int b = 0; b < 5; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bars[b])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
+    s_mma_pending = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -282,10 +284,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_node_chain(const __grid_constan
     s_abort = 1;
     atomicOr(a.err, ERR_TIMEOUT);
   };
-  auto wait0 = [&](uint32_t bar, uint32_t &ph, bool &pend) {  // thread 0
+  // thread 0; a wait that gave up leaves the phase pending, so the final
+  // drain waits for that same phase again
+  auto wait0 = [&](uint32_t bar, uint32_t &ph, bool &pend) {
     const bool ok = mbar_wait(bar, ph);
-    ph ^= 1u;
-    pend = false;
+    if (ok) {
+      ph ^= 1u;
+      pend = false;
+    }
     return ok;
   };
   // thread 0: piece g (piece g % NP of iteration g / NP) into the weight slot
@@ -351,10 +357,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_node_chain(const __grid_constan
       __syncthreads();
       if (s_abort) break;
       bool ok = mbar_wait(bar_m, ph_m);
-      ph_m ^= 1u;
-      if (tid == 0) pend_m = false;
-      if (!ok) fail_wait();
-      ok = __all_sync(0xffffffffu, ok);  // the warp-wide TMEM loads below need the whole warp
+      if (ok) {
+        ph_m ^= 1u;
+        if (tid == 0) pend_m = false;
+      } else {
+        fail_wait();
+      }
+      // Each thread polls on its own clock, so a wait can give up in some
+      // threads only.  The warp-wide TMEM loads below need the whole warp;
+      // s_abort, read after the next block barrier, stops every warp.
+      ok = __all_sync(0xffffffffu, ok);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (ok) {
         // the MMA has read its operands: refill what it freed
@@ -448,17 +460,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_node_chain(const __grid_constan
     }
   }
   // normal end or a failed wait: let every copy, store or MMA in flight land
+  // (bounded again).  An MMA that still has not completed may write the
+  // accumulator: its TMEM is then left allocated rather than freed under it.
   if (tid == 0) {
+    bool mma_done = true;
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     if (pend_x) mbar_wait(bar_x, ph_x);
     if (pend_h) mbar_wait(bar_h, ph_h);
     if (pend_w) mbar_wait(bar_w, ph_w);
-    if (pend_mi) mbar_wait(bar_mi, ph_mi);
-    if (pend_m) mbar_wait(bar_m, ph_m);
+    if (pend_mi && !mbar_wait(bar_mi, ph_mi)) mma_done = false;
+    if (pend_m && !mbar_wait(bar_m, ph_m)) mma_done = false;
+    if (!mma_done) {
+      fail_wait();
+      s_mma_pending = 1;
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+  if (warp == 0 && !s_mma_pending)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
 }
 
 __global__ void k_swizzle_image(const __nv_bfloat16 *__restrict__ W, int N, int K, uint8_t *__restrict__ img)

@@ -290,4 +290,20 @@ void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G,
   k_ref_pass<<<(P.nf + kPassThreads - 1) / kPassThreads, kPassThreads, 0, s>>>(P, S, G, st);
 }
 
+__global__ void k_rcp_selftest(const double *__restrict__ x, double *__restrict__ y, int64_t n)
+{
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    y[k] = rcp_nr(x[k]);
+}
+
 }  // namespace uph
+
+extern "C" uph_status uph_rcp_selftest(const double *x, double *y, int64_t n, void *stream)
+{
+  if (n < 0 || (n > 0 && (!x || !y))) return uph::fail(UPH_BAD_ARG, "uph_rcp_selftest: bad arguments");
+  if (n == 0) return UPH_OK;
+  const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  uph::k_rcp_selftest<<<blocks, 256, 0, (cudaStream_t)stream>>>(x, y, n);
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}

@@ -9,10 +9,16 @@
 //
 // Limits: at most kNoAllocMaxParticles particles and kNoAllocMaxCells cells
 // of the search grid (cells are as wide as the search radius, over the
-// caller's [lo, hi] box).  Every GPU that loads the library holds the array
-// (about 10 MiB) until the process exits.  All calls share the array, so
-// calls that overlap on the GPU (different streams or host threads) race.
+// caller's [lo, hi] box), and at most kMaxCellOccupancy particles in one
+// cell.  Every GPU that loads the library holds the array (about 12 MiB)
+// until the process exits.  All calls share the array, so calls that overlap
+// on the GPU (different streams or host threads) race.
+//
+// Unlike uph_search_neighbors (and the reference's 40-nearest-neighbour
+// search), this search is not capped: it returns every in-radius pair.
+// Pair offsets and the total are 64-bit, like `cap` and `*niac`.
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <string.h>
 
@@ -28,16 +34,18 @@ constexpr int kNoAllocMaxCells = 1 << 19;      // 524,288
 constexpr int kNoAllocScanSums = (kNoAllocMaxCells + 4095) / 4096 + 1;
 constexpr int kNoAllocMaxDevices = 64;
 
-// scratch layout, in ints
-constexpr size_t kOffCount = 0;
-constexpr size_t kOffStart = kOffCount + kNoAllocMaxCells;          // ncell + 1
-constexpr size_t kOffFill = kOffStart + kNoAllocMaxCells + 1;
-constexpr size_t kOffList = kOffFill + kNoAllocMaxCells;
-constexpr size_t kOffCellOf = kOffList + kNoAllocMaxParticles;
-constexpr size_t kOffPairCnt = kOffCellOf + kNoAllocMaxParticles;   // n_fluid + 1
-constexpr size_t kOffPairOff = kOffPairCnt + kNoAllocMaxParticles + 1;  // n_fluid + 1
-constexpr size_t kOffScan = kOffPairOff + kNoAllocMaxParticles + 1;
-constexpr size_t kOffWords = kOffScan + kNoAllocScanSums;            // error word, pad
+// scratch layout, in ints; 64-bit regions start on an even int offset
+constexpr size_t even(size_t k) { return (k + 1) & ~size_t(1); }
+constexpr size_t kOffCount = 0;                                       // int [ncell]
+constexpr size_t kOffStart = kOffCount + kNoAllocMaxCells;            // int [ncell + 1]
+constexpr size_t kOffFill = kOffStart + kNoAllocMaxCells + 1;         // int [ncell]
+constexpr size_t kOffList = kOffFill + kNoAllocMaxCells;              // int [n]
+constexpr size_t kOffCellOf = kOffList + kNoAllocMaxParticles;        // int [n]
+constexpr size_t kOffPairCnt = kOffCellOf + kNoAllocMaxParticles;     // int [n_fluid]
+constexpr size_t kOffPairOff = even(kOffPairCnt + kNoAllocMaxParticles);          // int64 [n_fluid + 1]
+constexpr size_t kOffScan = kOffPairOff + 2 * (kNoAllocMaxParticles + 1);         // int [scan sums]
+constexpr size_t kOffScan64 = even(kOffScan + kNoAllocScanSums);                  // int64 [scan sums]
+constexpr size_t kOffWords = kOffScan64 + 2 * kNoAllocScanSums;                   // error word, pad
 constexpr size_t kScratchInts = kOffWords + 64;
 
 static __device__ __align__(256) int g_noalloc_scratch[kScratchInts];
@@ -102,14 +110,45 @@ __global__ void k_na_sort_cells(const int *__restrict__ start, int *__restrict__
 
 __device__ __forceinline__ double na_r2(double dx, double dy) { return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)); }
 
-// pass 0: count each query's pairs; pass 1: write them (ascending j, because
-// cells are visited in row order and each cell's list is sorted -- the rows
-// of the 3 x 3 block are merged below to keep the output sorted by j)
+// The 3 x 3 cells around a query, each cell's ids ascending.
+struct NaBlock {
+  int k[9], e[9];
+};
+
+__device__ __forceinline__ void na_block(const NoAllocGrid &g, const int *__restrict__ start,
+                                         const int *__restrict__ list, int c, int s, NaBlock &B)
+{
+  const int cx = c % g.ncx, cy = c / g.ncx;
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    const int xx = cx + q % 3 - 1, yy = cy + q / 3 - 1;
+    if (xx < 0 || yy < 0 || xx >= g.ncx || yy >= g.ncy) {
+      B.k[q] = B.e[q] = 0;
+      continue;
+    }
+    // first id > s by bisection: ids <= s never form a pair with query s
+    int lo = start[yy * g.ncx + xx], hi = start[yy * g.ncx + xx + 1];
+    B.e[q] = hi;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (list[mid] <= s)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    B.k[q] = lo;
+  }
+}
+
+// pass 0: count each query's pairs; pass 1: write them in ascending j by a
+// 9-way merge of the (sorted) cell lists -- O(candidates) per query, with
+// no reordering of what is already written.  Counts per query are int
+// (at most 9 kMaxCellOccupancy candidates); offsets are 64-bit.
 template <bool kWrite>
 __global__ void k_na_pairs(NoAllocGrid g, const double *__restrict__ pos, const int *__restrict__ cell_of,
                            const int *__restrict__ start, const int *__restrict__ list, int *__restrict__ cnt,
-                           const int *__restrict__ off, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
-                           const unsigned *err)
+                           const long long *__restrict__ off, int64_t cap, int32_t *i_pair, int32_t *j_pair,
+                           double *rij2, const unsigned *err)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.n_fluid) return;
@@ -118,58 +157,104 @@ __global__ void k_na_pairs(NoAllocGrid g, const double *__restrict__ pos, const 
     return;
   }
   const double xs = pos[2 * s], ys = pos[2 * s + 1];
-  const int c = cell_of[s], cx = c % g.ncx, cy = c / g.ncx;
-  int n = 0;
-  const int base = kWrite ? off[s] : 0;
-  for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.ncy - 1); yy++) {
-    const int k0 = start[yy * g.ncx + max(cx - 1, 0)], k1 = start[yy * g.ncx + min(cx + 1, g.ncx - 1) + 1];
-    for (int k = k0; k < k1; k++) {
-      const int j = list[k];
-      if (j <= s || j >= g.pb) continue;
-      const double r2 = na_r2(xs - pos[2 * j], ys - pos[2 * j + 1]);
-      if (!(r2 < g.r2cut && r2 > DBL_EPSILON)) continue;
-      if (kWrite) {
-        // insertion into the query's segment keeps it sorted by j
-        const int64_t o = (int64_t)base + n;
-        if (o < cap) {
-          int64_t p = o;
-          while (p > base && j_pair[p - 1] > j) {
-            j_pair[p] = j_pair[p - 1];
-            rij2[p] = rij2[p - 1];
-            p--;
-          }
-          i_pair[o] = s;
-          j_pair[p] = j;
-          rij2[p] = r2;
-        }
+  NaBlock B;
+  na_block(g, start, list, cell_of[s], s, B);
+  if (!kWrite) {
+    int n = 0;
+#pragma unroll
+    for (int q = 0; q < 9; q++)
+      for (int k = B.k[q]; k < B.e[q]; k++) {
+        const int j = list[k];
+        if (j >= g.pb) break;  // ids ascend: the rest of the cell is excluded too
+        const double r2 = na_r2(xs - pos[2 * j], ys - pos[2 * j + 1]);
+        n += (r2 < g.r2cut && r2 > DBL_EPSILON);
       }
-      n++;
-    }
+    cnt[s] = n;
+    return;
   }
-  if (!kWrite) cnt[s] = n;
+  const long long base = off[s];
+  long long o = base;
+  int head[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) head[q] = B.k[q] < B.e[q] ? list[B.k[q]] : INT_MAX;
+  for (;;) {
+    int j = INT_MAX, qm = 0;
+#pragma unroll
+    for (int q = 0; q < 9; q++)
+      if (head[q] < j) {
+        j = head[q];
+        qm = q;
+      }
+    if (j >= g.pb) break;  // every remaining head is excluded (or exhausted)
+#pragma unroll
+    for (int q = 0; q < 9; q++)
+      if (q == qm) {
+        B.k[q]++;
+        head[q] = B.k[q] < B.e[q] ? list[B.k[q]] : INT_MAX;
+      }
+    const double r2 = na_r2(xs - pos[2 * j], ys - pos[2 * j + 1]);
+    if (!(r2 < g.r2cut && r2 > DBL_EPSILON)) continue;
+    if (o >= 0 && o < cap) {
+      i_pair[o] = s;
+      j_pair[o] = j;
+      rij2[o] = r2;
+    }
+    o++;
+  }
 }
 
 std::mutex g_setup_mutex;
-int *g_scratch_ptr[kNoAllocMaxDevices] = {nullptr};
+struct ScratchAddress {
+  void *ctx;
+  int *ptr;
+};
+ScratchAddress g_scratch[kNoAllocMaxDevices] = {};
+
+// the calling thread's current driver context (nullptr when it cannot be
+// read): a device reset replaces the context and re-registers the module,
+// which moves g_noalloc_scratch
+void *current_context()
+{
+  typedef int (*CtxGetCurrent)(void **);
+  static CtxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrent)f;
+  });
+  void *ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 // Device address of g_noalloc_scratch for the current device.  Host code
 // cannot use the symbol's name as a pointer (on the host it names a
 // stand-in, not device memory), so the address is looked up once per device
-// with that device current and reused afterwards.
+// (and again if that device's context was replaced), with that device
+// current, and reused afterwards.
 uph_status scratch_address(int **out)
 {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(UPH_BAD_ARG, "device ordinal out of range");
+  // cudaFree(0) makes the runtime's context current without allocating
+  e = cudaFree(nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFree(nullptr)");
+  void *ctx = current_context();
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
+  ScratchAddress &a = g_scratch[dev];
+  if (!a.ptr || a.ctx != ctx) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    g_scratch_ptr[dev] = (int *)p;
+    a.ptr = (int *)p;
+    a.ctx = ctx;
   }
-  *out = g_scratch_ptr[dev];
+  *out = a.ptr;
   return UPH_OK;
 }
 
@@ -216,7 +301,9 @@ extern "C" uph_status uph_search_neighbors_noalloc(const double *position, int32
   cudaStream_t q = (cudaStream_t)stream;
   int *count = scratch + kOffCount, *start = scratch + kOffStart, *fill = scratch + kOffFill;
   int *list = scratch + kOffList, *cell_of = scratch + kOffCellOf, *pcnt = scratch + kOffPairCnt;
-  int *poff = scratch + kOffPairOff, *sums = scratch + kOffScan;
+  long long *poff = reinterpret_cast<long long *>(scratch + kOffPairOff);
+  int *sums = scratch + kOffScan;
+  long long *sums64 = reinterpret_cast<long long *>(scratch + kOffScan64);
   unsigned *err = (unsigned *)(scratch + kOffWords);
   // the array keeps the previous call's contents: clear what must start at zero
   UPH_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * ncell, q));
@@ -229,14 +316,14 @@ extern "C" uph_status uph_search_neighbors_noalloc(const double *position, int32
   k_na_sort_cells<<<(ncell + tb - 1) / tb, tb, 0, q>>>(start, list, ncell, err);
   k_na_pairs<false><<<(n_fluid + tb - 1) / tb, tb, 0, q>>>(g, position, cell_of, start, list, pcnt, nullptr, 0,
                                                            nullptr, nullptr, nullptr, err);
-  launch_exclusive_scan(pcnt, poff, n_fluid, sums, q);
+  launch_exclusive_scan64(pcnt, poff, n_fluid, sums64, q);
   if (cap > 0)
     k_na_pairs<true><<<(n_fluid + tb - 1) / tb, tb, 0, q>>>(g, position, cell_of, start, list, pcnt, poff, cap,
                                                             i_pair, j_pair, rij2, err);
   UPH_CUDA(cudaGetLastError());
-  int total = 0;
+  long long total = 0;
   unsigned errw = 0;
-  UPH_CUDA(cudaMemcpyAsync(&total, poff + n_fluid, sizeof(int), cudaMemcpyDeviceToHost, q));
+  UPH_CUDA(cudaMemcpyAsync(&total, poff + n_fluid, sizeof(long long), cudaMemcpyDeviceToHost, q));
   UPH_CUDA(cudaMemcpyAsync(&errw, err, sizeof(unsigned), cudaMemcpyDeviceToHost, q));
   UPH_CUDA(cudaStreamSynchronize(q));
   *niac = total;

@@ -179,16 +179,22 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
   // the self-test waits for a phase that never completes: the bounded wait
   // gives up, no copy or MMA has been issued, and the CTA goes straight to
   // freeing its TMEM
+  // Every thread polls on its own clock, so a wait that gives up near the
+  // limit can give up in some threads only: each outcome is made uniform
+  // over the block before anyone acts on it.
   bool ok = g.stall ? mbar_wait(smem_u32(&stall_bar), 0u) : true;
-  uint32_t phase[kTcStages] = {0u, 0u};
+  ok = __syncthreads_and(ok) != 0;
+  int issued = 0;  // slices whose MMAs were issued (and committed to their stage's barrier)
   for (int s = 0; s < nslices && ok; s++) {
     const int st = s % kTcStages;
     uint8_t *ta = smem + st * 2 * kTcTileBytes;
     uint8_t *tb = ta + kTcTileBytes;
-    // the stage's previous MMAs must be done before its tiles are overwritten
+    // the stage's previous MMAs must be done before its tiles are overwritten:
+    // commit number s / kTcStages - 1 of this stage completes phase parity
+    // (s / kTcStages - 1) & 1
     if (s >= kTcStages) {
-      ok = mbar_wait(smem_u32(&mbar[st]), phase[st]);
-      phase[st] ^= 1u;
+      ok = mbar_wait(smem_u32(&mbar[st]), (uint32_t)((s / kTcStages - 1) & 1));
+      ok = __syncthreads_and(ok) != 0;
       if (!ok) break;
     }
     const int k0 = kbeg + s * kTcBK;
@@ -224,17 +230,21 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
                        smem_u32(&mbar[st]))
                    : "memory");
     }
+    issued = s + 1;
   }
-  // wait for the MMAs still in flight: every stage that was used has exactly
-  // one commit the loop has not waited for (its last one)
-  for (int st = 0; st < kTcStages && ok; st++) {
-    if (nslices > st) {
-      if (!mbar_wait(smem_u32(&mbar[st]), phase[st])) ok = false;
-      phase[st] ^= 1u;
-    }
+  // Drain: wait for the last commit of every stage that was used, on the
+  // normal path and after a failed wait alike, so that no MMA still writes
+  // the accumulator when TMEM is freed.  A stage with c commits has its last
+  // one complete phase parity (c - 1) & 1; waiting on a phase that already
+  // completed returns at once.
+  bool drained = true;
+  for (int st = 0; st < kTcStages; st++) {
+    const int c = (issued - st + kTcStages - 1) / kTcStages;
+    if (c > 0 && !mbar_wait(smem_u32(&mbar[st]), (uint32_t)((c - 1) & 1))) drained = false;
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  __syncthreads();
+  drained = __syncthreads_and(drained) != 0;
+  ok = ok && drained;
 
   if (!ok) {
     if (threadIdx.x == 0) atomicOr(g.err, ERR_TIMEOUT);
@@ -303,7 +313,11 @@ __global__ void __launch_bounds__(128) k_tc_gemm(TcGemmArgs g)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN));
+  // an MMA that never completed may still write the accumulator: its TMEM
+  // is then left allocated rather than freed under it (the error word
+  // already says the tensor core stopped answering)
+  if (warp == 0 && drained)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcN));
 }
 
 // out[m][n] (+)= sum over splits of partials[s][m][n], in split order

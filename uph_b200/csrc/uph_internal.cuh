@@ -135,6 +135,8 @@ void launch_cell_keys(const DevParams &P, const double *x, const double *y, int 
                       CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s);
 void launch_exclusive_scan(const int *in, int *out, int n, int *block_sums, cudaStream_t s);
 int scan_block_sums_needed(int n);  // size of launch_exclusive_scan's block_sums
+// the same scan with 64-bit offsets and totals (pair counts); out has n + 1 entries
+void launch_exclusive_scan64(const int *in, long long *out, int n, long long *block_sums, cudaStream_t s);
 void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s);
 // a cell with more ids than this is left unsorted and flags ERR_NEIGHBOR_OVERFLOW
 constexpr int kMaxCellOccupancy = 4096;
