@@ -142,10 +142,13 @@ def cpu_reference_run(deck, budget_s: float, max_steps: int, warmup: int = 1):
         t1 = time.perf_counter()
         step(n)
         total = first + (time.perf_counter() - t1)
+        inputbp_share = None
         if kind == "reference":
+            # the per-step re-read of the boundary decks inside derivatives()
+            inputbp_share = run.time_inputbp(3) / (total / (n + 1))
             run.close()
     steps = n + 1
-    return deck.n_fluid * steps / total, steps, threads, kind
+    return deck.n_fluid * steps / total, steps, threads, kind, inputbp_share
 
 
 # ---------------------------------------------------------------- ranks ---
@@ -276,11 +279,35 @@ def gpu_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = whole_job_rate(nf * k_e2e, e2e_s, world)
+    niac = int(stats["niac"])
     sim.close()
 
-    # --- variants: the WCSPH profile of the same configuration
+    # --- e2e through the reference-facing call: derivatives(System*, t) of
+    # libuph_sph.so once per step, the leapfrog on the host (libuph_driver.so
+    # restates src/bin/sph.cc:90-168), host System arrays in and out every step
+    e2e_dropin = {}
+    if not args.no_dropin_e2e:
+        from uph_b200.dropin import DropInRun
+        k_dr = max(1, min(args.steps, args.e2e_steps))
+        for level in (2, 0):
+            run = DropInRun(deck.uph_params(), deck.initial_state(), pair_export=level)
+            run.step(1)  # first call: device state, page-locking of the System's arrays
+            barrier()
+            t0 = time.perf_counter()
+            run.step(k_dr)
+            dt_s = max_over_ranks(time.perf_counter() - t0)
+            run.close()
+            bi, bo = DropInRun.bytes_per_step(nf, n_all, niac, level)
+            e2e_dropin[f"pair_export_{level}"] = {
+                "value": whole_job_rate(nf * k_dr, dt_s, world), "unit": UNIT, "steps": k_dr,
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
+
+    # --- variants: the WCSPH profile of the same configuration, FP64 and
+    # FP32 pair arithmetic, from the same state for the same steps; the FP32
+    # path's per-field error against the FP64 one is reported with it
     variants = {}
     k_var = max(1, min(args.steps, args.variant_steps))
+    finals = {}
     for label, prof, prec in [("wcsph_fp64", PROFILE_WCSPH, 0), ("wcsph_fp32_pair", PROFILE_WCSPH, PREC_FP32_PAIR)]:
         v = Simulation.from_deck(deck, profile=prof, precision=prec)
         v.set_stream(stream.cuda_stream)
@@ -288,11 +315,14 @@ def gpu_arm(args, rank, world, local_rank):
         v.profile(True)
         vms, _, _ = timed_steps(v, k_var)
         kt = v.kernel_times()
+        finals[label] = v.download()
         v.close()
         vms = max_over_ranks(vms)
         p_ms, p_n = kt.get("rate_pass", (0.0, 0))
         variants[label] = {"value": whole_job_rate(nf * k_var, vms / 1e3, world), "steps": k_var,
-                           "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1)}
+                           "ms_per_step": vms / k_var, "rate_pass_ms": p_ms / max(p_n, 1),
+                           "state_after_steps": args.warmup + k_var}
+    variants["wcsph_fp32_pair"]["error_vs_fp64"] = field_errors(finals["wcsph_fp32_pair"], finals["wcsph_fp64"], nf)
     if not args.no_batched:
         variants["batched_tanks"] = batched_arm(args, stream.cuda_stream)
     if not args.no_dambreak:
@@ -303,7 +333,26 @@ def gpu_arm(args, rank, world, local_rank):
     return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
                 pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
                 traffic=traffic, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
-                deck=deck)
+                deck=deck, e2e_dropin=e2e_dropin)
+
+
+ERROR_FIELDS = ["density", "DynamicPressure", "Velocity", "dvdt", "Position"]
+
+
+def field_errors(got, want, nf):
+    """Per-field error of one state against another over the fluid:
+    max |got - want| / max |want| (norm-wise), and for Position the largest
+    displacement difference in metres."""
+    out = {}
+    for f in ERROR_FIELDS:
+        g = np.asarray(got[f])[:nf]
+        w = np.asarray(want[f])[:nf]
+        if f == "Position":
+            out["Position_max_abs_m"] = float(np.abs(g - w).max())
+        else:
+            scale = float(np.abs(w).max())
+            out[f] = float(np.abs(g - w).max() / scale) if scale > 0 else float(np.abs(g - w).max())
+    return out
 
 
 def dambreak_arm(args, stream):
@@ -319,12 +368,15 @@ def dambreak_arm(args, stream):
     from uph_b200.sim import Simulation
 
     out = {}
+    big = D.dam_break(tank=(8.0, 4.0), column=(2.0, 4.0), dx=0.002, layers=2, hydrostatic=True, local_depth=4.0)
     cases = [("dambreak_5k_fp64_graph", D.dam_break(tank=(4.0, 3.0), column=(1.0, 2.0), dx=0.02, layers=2,
                                                     hydrostatic=True), 0, 1000, True),
              # c0 = 10 sqrt(g H) with H = 4 m, the column height (the 5k case's
-             # 10 sqrt(2 g) belongs to its own 2 m column)
-             ("dambreak_2M_fp32_pair", D.dam_break(tank=(8.0, 4.0), column=(2.0, 4.0), dx=0.002, layers=2,
-                                                   hydrostatic=True, local_depth=4.0), 1, 500, False)]
+             # 10 sqrt(2 g) belongs to its own 2 m column); FP32 pair
+             # arithmetic (the configuration) and FP64 (what FP32 buys)
+             ("dambreak_2M_fp32_pair", big, 1, 500, False),
+             ("dambreak_2M_fp64", big, 0, 500, False)]
+    finals = {}
     for label, deck, prec, steps, graph in cases:
         s = Simulation.from_deck(deck, profile=1, precision=prec)
         s.set_stream(stream.cuda_stream)
@@ -348,9 +400,17 @@ def dambreak_arm(args, stream):
             ms, n = s.kernel_times().get("rate_pass", (0.0, 0))
             entry["rate_pass_ms"] = ms / max(n, 1)
         st = s.stats()
-        entry["max_abs_density_error"] = st["max_abs_density_error"]
+        # largest |rho - rho0| / rho0 over the fluid: the weak compressibility
+        # the configuration allows (about 1 %), not an error against a reference
+        entry["max_density_deviation_from_rho0"] = st["max_abs_density_error"]
+        if deck is big:
+            finals[label] = s.download()
         s.close()
         out[label] = entry
+    out["dambreak_2M_fp32_pair"]["error_vs_fp64"] = field_errors(finals["dambreak_2M_fp32_pair"],
+                                                                 finals["dambreak_2M_fp64"], big.n_fluid)
+    out["dambreak_2M_fp32_pair"]["speedup_vs_fp64"] = (out["dambreak_2M_fp32_pair"]["value"] /
+                                                       out["dambreak_2M_fp64"]["value"])
     return out
 
 
@@ -549,6 +609,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-dambreak", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-dropin-e2e", action="store_true")
     ap.add_argument("--sur-steps", type=int, default=2000, help="wave-flume surrogate configuration: SPH steps")
     ap.add_argument("--sur-warm", type=float, default=1.0, help="wave-flume warm-up from rest (s)")
     ap.add_argument("--sur-length", type=float, default=10.0, help="wave-flume length (m); 10 m is the workload")
@@ -567,14 +628,15 @@ def main():
         if rank != 0:
             return
         deck = workload_deck()
-        value, steps, threads, kind = cpu_reference_run(deck, budget_s=60.0, max_steps=max(2, args.steps),
-                                                        warmup=min(args.warmup, 1))
+        value, steps, threads, kind, share = cpu_reference_run(deck, budget_s=60.0, max_steps=max(2, args.steps),
+                                                               warmup=min(args.warmup, 1))
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": deck.n_fluid / value * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host OpenMP"},
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                                 "sample": f"{steps} leapfrog steps of the full 500k-particle tank (bounded to ~60 s)"},
+                                 "sample": f"{steps} leapfrog steps of the full 500k-particle tank (bounded to ~60 s)",
+                                 "inputbp_share_of_step": share},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -593,8 +655,8 @@ def main():
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        v, steps, threads, kind = cpu_reference_run(r["deck"], budget_s=args.cpu_budget, max_steps=1000)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+        v, steps, threads, kind, share = cpu_reference_run(r["deck"], budget_s=args.cpu_budget, max_steps=1000)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "inputbp_share_of_step": share,
                "sample": f"{steps} leapfrog steps of the same 500k-particle tank on the host "
                          f"(reference solver compiled from its sources; search stand-in for libnabo)"}
     kt = {k: {"ms_total": round(v[0], 4), "launches": v[1]} for k, v in r["ktimes"].items() if v[1]}
@@ -614,6 +676,10 @@ def main():
                 "d2h_bytes_per_step": r["d2h"], "steps": r["k_e2e"],
                 "how": "per step: uph_sim_upload of the full state from pinned host memory, uph_sim_step(1), "
                        "uph_sim_download of the full state"},
+        "e2e_dropin": dict(r["e2e_dropin"], how="per step: the host leapfrog of src/bin/sph.cc:90-168 "
+                           "(libuph_driver.so) around derivatives(System*, t) of libuph_sph.so, the reference's own "
+                           "entry point: the fields it reads copied in and its rates, fluctuations, Tait pressure and "
+                           "(pair_export_2) the full pair list copied out"),
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
         "kernel_ms": kt,

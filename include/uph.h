@@ -105,8 +105,12 @@ typedef struct uph_params {
 
   /* Neighbour search.  knn_cap = 0 keeps every pair inside the radius.  The
    * reference keeps only each fluid query's 40 nearest points
-   * (derivatives.c:1085); both agree whenever no query has more than 39
-   * in-radius neighbours, which uph_sim_stats reports. */
+   * (derivatives.c:1085, Search.cc:27-33): knn_cap = 40 does the same --
+   * query i keeps its knn_cap nearest in-radius points, ties ordered by
+   * reference index, and a pair (i, j) exists iff j is kept by i.  Both
+   * settings agree whenever no query has more than knn_cap in-radius
+   * neighbours (uph_sim_stats reports the largest count).  REF profile
+   * only; at most 64. */
   int32_t knn_cap;
 
   /* Cell-grid domain: every interacting particle must stay inside
@@ -290,9 +294,9 @@ int64_t uph_sim_launch_count(const uph_sim *sim);
 
 /* SearchNeighbors semantics (Search.cc:5-44): pairs (s, j) with s <
  * n_fluid, j > s, rij2 < dist, j < particle_boundary, DBL_EPSILON < rij2
- * (no self matches), ordered by s then j.  knn (the reference passes 40)
- * caps each query's neighbour list; queries where the cap removes in-radius
- * points return UPH_UNSUPPORTED.  Host arrays in, host arrays out. */
+ * (no self matches), ordered by s then j.  knn (the reference passes 40;
+ * at most 64, 0 = no cap) keeps each query's knn nearest in-radius points,
+ * ties by index, as uph_params.knn_cap.  Host arrays in, host arrays out. */
 uph_status uph_search_neighbors(const double *position, int32_t n_fluid, int32_t n_all,
                                 int32_t particle_boundary, int32_t knn, double dist, int64_t cap,
                                 int32_t *i_pair, int32_t *j_pair, double *rij2, int64_t *niac);

@@ -155,6 +155,16 @@ void derivatives(System *sys, double t);
 int SearchNeighbors(const double **Position, int *i_pair, int *j_pair, double *rij2, const int NumberOfFluidParticles,
                     const int NumberOfParticles, int ParticleBoundary, const int NumberOfNeighbors, const double dist);
 
+/* What derivatives() copies back of the pair list it computes (no
+ * counterpart in the reference, whose derivatives() always fills it):
+ *   2 (default) i_pair, j_pair, rij2, w, dwcdx and NumberOfInteractingParticles;
+ *   1           i_pair, j_pair, rij2 and the count;
+ *   0           the count only.
+ * The reference's own callers (sph.cc, output.c, inputbp.c, inoutflow.c)
+ * read only the count; a caller that reads none of the arrays saves their
+ * device-to-host copy (40 bytes per pair) with level 0. */
+void uph_dropin_set_pair_export(int level);
+
 #ifdef __cplusplus
 }
 #endif

@@ -170,6 +170,8 @@ def ref_lib() -> C.CDLL:
         lib.ref_set.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_void_p]
         lib.ref_get_itype.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         lib.ref_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ref_time_inputbp.restype = C.c_double
+        lib.ref_time_inputbp.argtypes = [C.c_void_p, C.c_int]
         lib.uph_standin_reset_stats.argtypes = []
         lib.uph_standin_truncated_queries.restype = C.c_long
         lib.uph_standin_max_inradius.restype = C.c_int
@@ -251,6 +253,11 @@ class RefRun:
         j = np.zeros(n, np.int32)
         self.lib.ref_pairs(self.h, i.ctypes.data, j.ctypes.data)
         return i, j
+
+    def time_inputbp(self, ncalls: int = 3) -> float:
+        """Seconds per call of the reference's inputbp() (the boundary decks'
+        per-step re-read and the wall-motion law) at the next step's time."""
+        return float(self.lib.ref_time_inputbp(self.h, ncalls)) / max(ncalls, 1)
 
     def truncated_queries(self) -> int:
         return int(self.lib.uph_standin_truncated_queries())

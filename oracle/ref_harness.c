@@ -38,11 +38,13 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include <unistd.h>
 
 #include "System.h"
 #include "derivatives.h"
 #include "input.h"
+#include "inputbp.h"
 
 /* defined by shim/search_standin.c; absent when the hot path is the GPU drop-in */
 extern void uph_standin_set_capacity(long cap) __attribute__((weak));
@@ -177,6 +179,23 @@ int ref_derivatives(ref_run *run, double t)
   derivatives(run->sys, t);
   if (chdir(cwd)) return -1;
   return 0;
+}
+
+/* Seconds of `ncalls` calls of the reference's inputbp() at the next step's
+ * time -- the per-step re-read of the boundary decks (inputbp.c:28-191) plus
+ * the wall-motion law that derivatives() runs first (derivatives.c:3168).
+ * Calling it again at the same time changes nothing the next step sees. */
+double ref_time_inputbp(ref_run *run, int ncalls)
+{
+  char cwd[8192];
+  if (!getcwd(cwd, sizeof cwd) || chdir(run->deck)) return -1.0;
+  const double t = (run->itime + 1) * run->sys->timeStep;
+  struct timespec a, b;
+  clock_gettime(CLOCK_MONOTONIC, &a);
+  for (int k = 0; k < ncalls; k++) inputbp(run->sys, t);
+  clock_gettime(CLOCK_MONOTONIC, &b);
+  if (chdir(cwd)) return -1.0;
+  return (double)(b.tv_sec - a.tv_sec) + 1e-9 * (double)(b.tv_nsec - a.tv_nsec);
 }
 
 /* The time loop of src/bin/sph.cc:90-168 for `nsteps` more steps. */

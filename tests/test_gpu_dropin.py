@@ -1,6 +1,7 @@
 """The drop-in: the reference's own driver (src/bin/sph.cc) and libSPH host
 files (input.c, inputbp.c, output.c, ...) relinked against libuph_sph.so in
-place of derivatives.c + Search.cc, compared with the unmodified reference.
+place of derivatives.c + Search.cc, compared with the unmodified reference;
+and the package's own host caller of derivatives() (libuph_driver.so).
 
 Both builds live in oracle/_ref/ (made by `make -C oracle ref dropin` from
 the reference's sources); a machine without those sources runs the prebuilt
@@ -117,3 +118,21 @@ def test_unmodified_sph_driver_with_dropin_library(case, deck):
         assert a.shape == b.shape
         # 10 printed decimals: allow one unit in the last place
         assert np.max(np.abs(a - b)) <= 1.5e-10 * max(1.0, np.max(np.abs(a)))
+
+
+@pytest.mark.parametrize("case,pair_export", [("dambreak_h13", 2), ("flume_piston_sponge", 0), ("ragged_solid", 1)])
+def test_driver_library_with_dropin(case, pair_export):
+    """libuph_driver.so (the package's own host caller: sph.cc's leapfrog on
+    the host around the drop-in derivatives()) against the reference's
+    goldens after steps 1 and 3, with every pair-export level; the exported
+    pair arrays equal the reference's where they are exported."""
+    from uph_b200.dropin import DropInRun
+
+    g = load_golden(case)
+    deck = deck_from_golden(g)
+    st = deck.initial_state()
+    with DropInRun(deck.uph_params(), st, pair_export=pair_export) as run:
+        run.step(1)
+        compare_fields(run.state(), {f: g[f"s1_{f}"] for f in FLUID_FIELDS}, deck.n_fluid, REL_TOL_FP64)
+        run.step(2)
+        compare_fields(run.state(), {f: g[f"s3_{f}"] for f in FLUID_FIELDS}, deck.n_fluid, REL_TOL_FP64)

@@ -164,11 +164,44 @@ def test_search_neighbors_overcrowded_cell_is_reported(sim_mod):
     assert "UPH_NEIGHBOR_OVERFLOW" in str(e.value)
 
 
-def test_search_neighbors_knn_cap_that_binds_is_reported(sim_mod):
-    pos = np.array([[0.001 * k, 0.0] for k in range(60)])
-    with pytest.raises(Exception) as e:
-        sim_mod.search_neighbors(pos, 60, 59, 1.0, number_of_neighbors=40)
-    assert "UPH_UNSUPPORTED" in str(e.value)
+def _brute_knn_pairs(pos, nf, pb, dist, knn):
+    """SearchNeighbors with the k-nearest cap (Search.cc:27-33 as the
+    reference's search stand-in restates libnabo's exact k-NN): each query s
+    keeps its knn nearest points with DBL_EPSILON < d^2 < dist, ties by index;
+    then pairs (s, j) with j > s, j < pb, in ascending j."""
+    eps = np.finfo(np.float64).eps
+    out = []
+    for s in range(nf):
+        d = pos - pos[s]
+        d2 = d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]
+        cand = np.nonzero((d2 > eps) & (d2 < dist))[0]
+        cand = cand[cand != s]
+        keep = sorted(cand.tolist(), key=lambda j: (d2[j], j))[:knn]
+        out += [(s, j, float(d2[j])) for j in sorted(keep) if s < j < pb]
+    return out
+
+
+@pytest.mark.parametrize("case", ["line", "lattice_ties", "cloud"])
+def test_search_neighbors_knn_cap_keeps_the_nearest(sim_mod, case):
+    """The 40-nearest cap where it binds: a line of 60 points all in radius,
+    a lattice whose 40th neighbour falls inside a ring of equal distances
+    (ties broken by index), and a random cloud."""
+    rng = np.random.default_rng(13)
+    if case == "line":
+        pos, dist = np.array([[0.001 * k, 0.0] for k in range(60)]), 1.0
+    elif case == "lattice_ties":
+        ix, iy = np.meshgrid(np.arange(30), np.arange(30))
+        pos, dist = np.stack([ix.ravel() * 0.01, iy.ravel() * 0.01], 1), (0.054) ** 2
+    else:
+        pos, dist = rng.uniform(0, 0.3, (1500, 2)), 0.03 ** 2
+    n = pos.shape[0]
+    nf, pb = (n, n - 1) if case != "cloud" else (1000, n - 3)
+    i, j, r2 = sim_mod.search_neighbors(pos, nf, pb, dist, number_of_neighbors=40)
+    got = list(zip(i.tolist(), j.tolist(), r2.tolist()))
+    want = _brute_knn_pairs(pos, nf, pb, dist, 40)
+    assert got == want
+    # the cap binds here: fewer pairs than with no cap
+    assert len(want) < sim_mod.search_neighbors(pos, nf, pb, dist, number_of_neighbors=0)[0].size
 
 
 def test_particle_leaving_domain_is_reported(sim_mod):

@@ -74,3 +74,52 @@ def test_workload_matches_compiled_reference(name):
     assert np.array_equal(r2, rr2), "rij2 not bit-identical"
     print(f"{name}: {ri.size} pairs bit-identical; max field error step 1 {max(e1.values()):.2e}, "
           f"step 3 {max(e3.values()):.2e}")
+
+
+def _nn91_deck():
+    """A dam break with the reference decks' own smoothing length,
+    nearNeighbor = 91 (eta = sqrt(91 / 4 pi) = 2.69): about 90 points lie in
+    each fluid query's radius, so the reference's 40-nearest cap binds
+    everywhere, including across rings of equal distances on the lattice."""
+    d = D.dam_break(tank=(1.0, 1.0), column=(0.4, 0.6), dx=0.02, layers=2, eta=0.0, hydrostatic=True,
+                    thermal_diffusivity0=0.015)
+    d.params["near_neighbor"] = 91
+    return d
+
+
+def test_capped_search_matches_compiled_reference():
+    """The k-nearest cap (knn_cap = 40, derivatives.c:1085, Search.cc:27-33)
+    against the compiled reference, whose search stand-in keeps each query's
+    40 nearest in-radius points with ties by index.  libnabo's own tie order
+    is not known (it is not vendored), so this pins the capped path to the
+    stand-in's order, not to libnabo's."""
+    _need_reference()
+    from uph_b200.sim import Simulation
+
+    deck = _nn91_deck()
+    with tempfile.TemporaryDirectory() as tmp:
+        deck.write(tmp)
+        run = O.RefRun(tmp, eta_override=deck.eta_override)
+        try:
+            run.step(1)
+            assert run.truncated_queries() > deck.n_fluid // 2, "the cap should bind for most queries"
+            ref1 = {f: run.get(f) for f in FLUID_FIELDS}
+            ri, rj = run.pairs()
+            rr2 = run.get("rij2")
+            run.step(2)
+            ref3 = {f: run.get(f) for f in FLUID_FIELDS}
+        finally:
+            run.close()
+    with Simulation.from_deck(deck, knn_cap=40) as s:
+        s.step(1)
+        e1 = compare_fields(s.download(), ref1, deck.n_fluid, REL_TOL_FP64)
+        s.step(2)
+        e3 = compare_fields(s.download(), ref3, deck.n_fluid, REL_TOL_FP64)
+        assert s.stats()["max_neighbors"] > 40
+    with Simulation.from_deck(deck, knn_cap=40) as s:
+        s.derivatives(deck.params["time_step"])
+        i, j, r2, _, _ = s.pairs()
+    assert np.array_equal(i, ri) and np.array_equal(j, rj), "capped pair list differs"
+    assert np.array_equal(r2, rr2)
+    print(f"nn91: {ri.size} capped pairs bit-identical; max field error step 1 {max(e1.values()):.2e}, "
+          f"step 3 {max(e3.values()):.2e}")

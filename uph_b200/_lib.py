@@ -13,6 +13,7 @@ from ._capi import SurConfig, SurJudge, SurNodes, SurReport, UphDiagnostics, Uph
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libuph.so")
 LIB_SPH_PATH = os.path.join(HERE, "libuph_sph.so")
+LIB_DRIVER_PATH = os.path.join(HERE, "libuph_driver.so")
 
 _lib = None
 

@@ -2,9 +2,10 @@
 
     python -m uph_b200.build          # libuph.so and libuph_sph.so next to this file
 
-libuph.so      the C ABI of include/uph.h (kernels + host code)
-libuph_sph.so  derivatives() / SearchNeighbors() with the reference's own
-               signatures (include/uph_system.h), linked against libuph.so
+libuph.so         the C ABI of include/uph.h (kernels + host code)
+libuph_sph.so     derivatives() / SearchNeighbors() with the reference's own
+                  signatures (include/uph_system.h), linked against libuph.so
+libuph_driver.so  a host caller of derivatives() (include/uph_driver.h)
 
 Objects are rebuilt only when a source or header is newer than the object.
 """
@@ -43,6 +44,11 @@ DROPIN_SOURCES = [("dropin.cpp", [])]
 
 LIB = os.path.join(HERE, "libuph.so")
 LIB_SPH = os.path.join(HERE, "libuph_sph.so")
+# a host caller of the drop-in (include/uph_driver.h): plain C++, OpenMP, no
+# fused multiply-add so its leapfrog rounds as the reference's
+DRIVER_SRC = os.path.join(CSRC, "driver.cpp")
+LIB_DRIVER = os.path.join(HERE, "libuph_driver.so")
+CXX = "g++"  # the system compiler (its OpenMP runtime is the one the oracle builds use)
 
 
 def _headers():
@@ -101,6 +107,9 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     if _newer(LIB_SPH, dobjs + [LIB]):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB_SPH] + dobjs +
              ["-L" + HERE, "-luph", "-Xlinker", "-rpath,$ORIGIN", "-lcudart"], verbose)
+    if _newer(LIB_DRIVER, [DRIVER_SRC, LIB_SPH] + _headers()):
+        _run([CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-shared", "-I" + INCLUDE,
+              "-o", LIB_DRIVER, DRIVER_SRC, "-L" + HERE, "-luph_sph", "-luph", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

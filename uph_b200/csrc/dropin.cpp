@@ -8,6 +8,8 @@
 
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "uph.h"
 #include "uph_system.h"
 
@@ -22,9 +24,50 @@ namespace {
 struct DropIn {
   uph_sim *sim = nullptr;
   uph_params p;
+  // the System whose arrays past its particles were zeroed, and the host
+  // ranges registered (pinned) for direct copies
+  const System *zeroed = nullptr;
+  int zeroed_n = 0, zeroed_max = 0;
+  const System *pinned = nullptr;
+  std::vector<void *> pinned_ranges;
+  int pair_export = 2;  // uph_dropin_set_pair_export
 };
 
 DropIn g;
+
+void unpin_all()
+{
+  for (void *p : g.pinned_ranges) cudaHostUnregister(p);
+  g.pinned_ranges.clear();
+  g.pinned = nullptr;
+}
+
+// Page-locks the System arrays derivatives() copies to and from the device,
+// once per System: copies from page-locked memory go straight to the device
+// instead of through the driver's staging buffers.  A range that cannot be
+// registered (e.g. already registered by the caller) is copied as is.
+void pin_system(const System *sys)
+{
+  if (g.pinned == sys) return;
+  unpin_all();
+  g.pinned = sys;
+  const size_t M = (size_t)sys->MaxNumberOfParticles;
+  auto reg = [](void *p, size_t bytes) {
+    if (!p || bytes == 0) return;
+    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess)
+      g.pinned_ranges.push_back(p);
+    else
+      cudaGetLastError();  // clear the sticky error of a refused registration
+  };
+  for (double *v : {sys->Position[0], sys->Velocity[0], sys->localVelocity[0], sys->dvdt[0], sys->dvdt_approx[0],
+                    sys->velocityFluctuation[0], sys->dwcdx[0]})
+    reg(v, sizeof(double) * 2 * M);
+  for (double *v : {sys->density, sys->localDensity, sys->DynamicPressure, sys->localPressure, sys->mass,
+                    sys->spongeFactor, sys->ddensitydt, sys->dpdt, sys->ddensitydt_approx, sys->dpdt_approx,
+                    sys->densityFluctuation, sys->pressureFluctuation, sys->Pressure, sys->rij2, sys->w})
+    reg(v, sizeof(double) * M);
+  for (int *v : {sys->itype, sys->i_pair, sys->j_pair}) reg(v, sizeof(int) * M);
+}
 
 [[noreturn]] void die(const char *where, uph_status s)
 {
@@ -88,7 +131,7 @@ void params_from_system(const System *sys, uph_params *p)
   p->sponge_position0 = sys->spongePosition0;
   p->wave_absorption = sys->waveAbsorption;
   p->av_alpha = sys->alpha;
-  p->knn_cap = 0;
+  p->knn_cap = 40;  // SearchNeighbors' k (derivatives.c:1085)
 }
 
 // The library uses one smoothing length, one viscosity and one diffusivity;
@@ -146,13 +189,22 @@ void ensure_sim(const System *sys, int n)
 extern "C" void derivatives(System *sys, double t)
 {
   const int nf = sys->NumberOfFluidParticles;
-  // derivatives.c:3147-3157 (the stress arrays feed stressType 2 only)
-  memset(sys->ddensitydt, 0, sizeof(double) * sys->MaxNumberOfParticles);
-  memset(sys->dpdt, 0, sizeof(double) * sys->MaxNumberOfParticles);
-  memset(sys->dvdt[0], 0, sizeof(double) * sys->MaxNumberOfParticles * 2);
-  memset(sys->ddensitydt_approx, 0, sizeof(double) * sys->MaxNumberOfParticles);
-  memset(sys->dpdt_approx, 0, sizeof(double) * sys->MaxNumberOfParticles);
-  memset(sys->dvdt_approx[0], 0, sizeof(double) * sys->MaxNumberOfParticles * 2);
+  const int nall = nf + sys->NumberOfSolidParticles + sys->NumberOfBoundaryParticles;
+  // derivatives.c:3147-3157 zeroes the rate arrays (MaxNumberOfParticles
+  // long; the stress arrays feed stressType 2 only).  The fluid entries are
+  // overwritten below; the other particles' are zeroed every call; entries
+  // past the particles, which nothing writes, once per System.
+  const size_t M = (size_t)sys->MaxNumberOfParticles;
+  const bool first = g.zeroed != sys || g.zeroed_n != nall || g.zeroed_max != sys->MaxNumberOfParticles;
+  const size_t z0 = (size_t)nf, z1 = first ? M : (size_t)nall;
+  if (z1 > z0) {
+    for (double *v : {sys->ddensitydt, sys->dpdt, sys->ddensitydt_approx, sys->dpdt_approx})
+      memset(v + z0, 0, sizeof(double) * (z1 - z0));
+    for (double *v : {sys->dvdt[0], sys->dvdt_approx[0]}) memset(v + 2 * z0, 0, sizeof(double) * 2 * (z1 - z0));
+  }
+  g.zeroed = sys;
+  g.zeroed_n = nall;
+  g.zeroed_max = sys->MaxNumberOfParticles;
   if (t > 0) inoutflow(sys);  // derivatives.c:3162-3164
   inputbp(sys, t);            // derivatives.c:3168: re-reads the boundary decks, moves walls
   // derivatives.c:3171-3182 only feeds inoutflow's inflow branch, whose
@@ -165,6 +217,7 @@ extern "C" void derivatives(System *sys, double t)
   const int n = nf + ns + nb;
   check_uniform(sys, n);
   ensure_sim(sys, n);
+  pin_system(sys);
 
   uph_state in;
   memset(&in, 0, sizeof in);
@@ -205,9 +258,17 @@ extern "C" void derivatives(System *sys, double t)
   }
   // pair list (CalculateKernel's outputs, derivatives.c:1076-1105)
   int64_t niac = 0;
-  s = uph_sim_pairs(g.sim, sys->MaxNumberOfParticles, sys->i_pair, sys->j_pair, sys->rij2, sys->w, sys->dwcdx[0],
-                    &niac);
-  if (s != UPH_OK) die("derivatives", s);
+  if (g.pair_export == 0) {
+    uph_stats st;
+    s = uph_sim_stats(g.sim, &st);
+    if (s != UPH_OK) die("derivatives", s);
+    niac = st.niac;
+  } else {
+    const bool all = g.pair_export >= 2;
+    s = uph_sim_pairs(g.sim, sys->MaxNumberOfParticles, sys->i_pair, sys->j_pair, sys->rij2, all ? sys->w : nullptr,
+                      all ? sys->dwcdx[0] : nullptr, &niac);
+    if (s != UPH_OK) die("derivatives", s);
+  }
   sys->NumberOfInteractingParticles = (int)niac;
   // TotalKineticEnergy, derivatives.c:2254-2264
   double ke = 0.0, pe = 0.0;
@@ -233,4 +294,9 @@ extern "C" int SearchNeighbors(const double **Position, int *i_pair, int *j_pair
                            NumberOfNeighbors, dist, niac, i_pair, j_pair, rij2, &niac);
   if (s != UPH_OK) die("SearchNeighbors", s);
   return (int)niac;
+}
+
+extern "C" void uph_dropin_set_pair_export(int level)
+{
+  g.pair_export = level < 0 ? 0 : level > 2 ? 2 : level;
 }

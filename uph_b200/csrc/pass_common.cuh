@@ -130,4 +130,35 @@ __device__ __forceinline__ int list_partners(const DevParams &P, const SlotArray
   return cnt;
 }
 
+// LeonnardJonesBoundaryForces (mode 1, derivatives.c:1184-1211) and
+// MonaghanBoundaryForce (default mode, :1919-1953): every fluid particle
+// against every boundary particle, no pair-list filter.
+__device__ __forceinline__ void brute_wall_force(const DevParams &P, double r2, double dxa, double dya, double mb,
+                                                 double &fx, double &fy)
+{
+  if (P.boundary_force == 1) {
+    const double r0 = P.dx;
+    if (r2 < r0 * r0) {
+      double rr = r0 / sqrt(r2);
+      rr *= rr;
+      rr *= rr;
+      const double pb = P.lj_coeff * rr * (rr * rr - 1.) / r2;
+      fx += pb * dxa;
+      fy += pb * dya;
+    }
+  } else {
+    const double r = sqrt(r2);
+    const double q = r / P.h;
+    double phi = 0.0;
+    if (q >= 0.0 && q < 2.0) {
+      const double t = 2.0 - q;
+      phi = 0.125 * (1.0 + 1.5 * q) * t * t * t;
+    }
+    const double gama = P.mach_c * P.mach_c / (P.rho0 * P.dx * P.dy);
+    const double c = gama * phi * mb / r2;
+    fx += c * dxa;
+    fy += c * dya;
+  }
+}
+
 }  // namespace uph

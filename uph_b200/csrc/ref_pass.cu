@@ -46,13 +46,17 @@
 // derivatives.c:1082-1084), DBL_EPSILON < r^2 < (h h) 4 where r^2 is
 // dx*dx + dy*dy rounded exactly like the reference (no fused multiply-add).
 //
-// Execution: one thread per fluid slot.  Each thread first walks its 5 x 5
-// block of half-radius cells with only the exact distance test and lists the
-// in-radius partners in shared memory (kNbChunk at a time); then the warp runs the heavy FP64 pair
-// arithmetic over those lists.  The lists have nearly equal lengths, so the
-// lanes of a warp stay converged in the expensive loop instead of idling while
-// their neighbours reject out-of-radius candidates.
-#include "pass_common.cuh"
+// Execution: one CTA per storage tile of T x T cells (tile_pass.cuh).  The
+// CTA stages the records of its tile and of the `reach` cells around it in
+// shared memory, once; each thread then owns one fluid particle of the tile.
+// Per particle, a cheap listing phase walks its (2 reach + 1)^2 stencil in
+// shared memory with only the exact distance test and lists the in-radius
+// partners; then the warp runs the FP64 pair arithmetic over those lists,
+// which have nearly equal lengths, so the lanes of a warp stay converged in
+// the expensive loop.
+#include <limits.h>
+
+#include "tile_pass.cuh"
 
 namespace uph {
 
@@ -106,174 +110,324 @@ __device__ __forceinline__ void wall_pair_force(const DevParams &P, int itb, dou
   }
 }
 
-// LeonnardJonesBoundaryForces (mode 1, derivatives.c:1184-1211) and
-// MonaghanBoundaryForce (default mode, :1919-1953): every fluid particle
-// against every boundary particle, no pair-list filter.
-__device__ __forceinline__ void brute_wall_force(const DevParams &P, double r2, double dxa, double dya, double mb,
-                                                 double &fx, double &fy)
+// ---- partner records -----------------------------------------------------------
+// One particle's fields as the pair loop reads them: the SoA state plus the
+// per-particle factors every pair would otherwise recompute (Tait's
+// rho0 c0^2 + gamma p, 1/rho^2, rhot/rho, m/rho).  144 bytes, read as nine
+// 16-byte shared-memory loads.
+struct __align__(16) RefRec {
+  double x, y, u, v, ut, vt, rho, rhot, p, pt, m, ir, irt, P, ir2, C, V;
+  int orig, itype;
+};
+static_assert(sizeof(RefRec) == 144, "RefRec is nine 16-byte chunks");
+
+__device__ __forceinline__ RefRec load_ref_rec(const DevParams &P, const SlotArrays &S, int s)
 {
-  if (P.boundary_force == 1) {
-    const double r0 = P.dx;
-    if (r2 < r0 * r0) {
-      double rr = r0 / sqrt(r2);
-      rr *= rr;
-      rr *= rr;
-      const double pb = P.lj_coeff * rr * (rr * rr - 1.) / r2;
-      fx += pb * dxa;
-      fy += pb * dya;
+  RefRec r;
+  r.x = S.x[s];
+  r.y = S.y[s];
+  r.u = S.u[s];
+  r.v = S.v[s];
+  r.ut = S.ut[s];
+  r.vt = S.vt[s];
+  r.rho = S.rho[s];
+  r.rhot = S.rhot[s];
+  r.p = S.p[s];
+  r.pt = S.pt[s];
+  r.m = S.m[s];
+  r.ir = S.inv_rho[s];
+  r.irt = S.inv_rhot[s];
+  r.P = fma(P.gamma, r.p, P.rho0c2);
+  r.ir2 = r.ir * r.ir;
+  r.C = r.rhot * r.ir;
+  r.V = r.m * r.ir;
+  r.orig = S.orig[s];
+  r.itype = S.itype[s];
+  return r;
+}
+
+// The particle a thread owns, with its per-particle constants.
+struct RefOwn {
+  RefRec r;
+  double IPa;  // P_a / rho_a
+  double G4a;  // 4 gamma kappa P_a
+  double KPa;  // kappa P_a
+  double A1a;  // p_a / rho_a^2
+};
+
+__device__ __forceinline__ RefOwn make_own(const DevParams &P, const RefRec &r)
+{
+  RefOwn o;
+  o.r = r;
+  o.IPa = r.ir * r.P;
+  o.G4a = 4.0 * (P.gamma * P.kappa) * r.P;
+  o.KPa = P.kappa * r.P;
+  o.A1a = r.p * r.ir2;
+  return o;
+}
+
+// The per-a sums of one pair (a, b), a = the own particle.  With
+// g = F (x_a - x_b) and the header's formulas, rearranged so that the pair
+// shares one reciprocal and per-particle factors come from the records:
+//   1 / (r^2 + 0.01 h^2), 1 / (P_a + P_b) and 1 / (1/rho_a + 1/rho_b)
+//   all from rr = 1 / ((r^2 + 0.01 h^2)(P_a + P_b)(1/rho_a + 1/rho_b));
+//   (x_a - x_b) . g = F r^2;
+//   S . g = -F r^2 (v_a - v_b) for the deviatoric S of the viscous terms
+//   (its terms in dx dy dv cancel exactly), so both viscous forces are
+//   multiples of (v_a - v_b).
+__device__ __forceinline__ void ref_pair(const DevParams &P, const RefOwn &a, const RefRec &b, bool isI, RefAcc &A)
+{
+  const double dxa = a.r.x - b.x, dya = a.r.y - b.y;
+  const double r2 = exact_r2(dxa, dya);
+  // poly-7 convolution W and deconvolution gradient factor, functions of q^2
+  const double q2 = r2 * P.inv_h2;
+  const double t = fma(-0.25, q2, 1.0);
+  const double t2 = t * t, t4 = t2 * t2;
+  const double t7 = t4 * t2 * t, t8 = t4 * t4;
+  const double pp = fma(fma(fma(fma(fma(fma(305.0, q2, -628.0), q2, 1184.0), q2, -1984.0), q2, 2816.0), q2, -3072.0), q2, 2048.0);
+  const double pp7 = fma(fma(fma(fma(fma(fma(305.0, q2, -1106.0), q2, 1912.0), q2, -2912.0), q2, 3712.0), q2, -3584.0), q2, 2048.0);
+  const double W = P.w_alpha * t8 * pp;
+  const double F = P.dw_alpha_h2 * t7 * pp7;
+  const double Fr2 = F * r2;
+
+  const double De = r2 + P.eta2;
+  const double SP = a.r.P + b.P;
+  const double Sr = a.r.ir + b.ir;
+  const double SPSr = SP * Sr;
+  const double rr = rcp_nr(De * SPSr);
+  const double inv_r2e = rr * SPSr;
+  const double invSP = rr * (De * Sr);
+  const double nu = Fr2 * inv_r2e;
+
+  const double dux = a.r.u - b.u, duy = a.r.v - b.v;
+  const double eux = a.r.u - b.ut, euy = a.r.v - b.vt;
+  const double Vd = fma(dux, dxa, duy * dya);
+  const double Ed = fma(eux, dxa, euy * dya);
+  const double pdx = isI ? eux : a.r.ut - b.u;
+  const double pdy = isI ? euy : a.r.vt - b.v;
+  const double Pd = fma(pdx, dxa, pdy * dya);
+  const double ms = isI ? b.m : a.r.m;
+  const double mbF = b.m * F;
+
+  // predictor density (PredictingDensityEquation)
+  A.drho_a = fma(ms * F, Pd, A.drho_a);
+  // predictor pressure (PredictingDynamicPressureEquation)
+  const double dpp = a.r.p - b.p, dr = a.r.rho - b.rho;
+  const double brk = fma(-(a.KPa * dr), Sr, a.G4a * dpp * invSP);
+  A.dp_a = fma(mbF * a.IPa, Vd, A.dp_a);
+  A.dp_a = fma(ms * b.ir * nu, brk, A.dp_a);
+  // fluctuations
+  const double VW = b.V * W;
+  A.frho = fma(-VW, dr, A.frho);
+  A.fp = fma(-VW, dpp, A.fp);
+  const double cfv = isI ? fma(a.r.m, b.irt, -(b.m * a.r.irt)) * W : 0.0;
+  A.fu = fma(dux, cfv, A.fu);
+  A.fv = fma(duy, cfv, A.fv);
+  // continuity (DensityEquation)
+  const double VrF = b.V * b.rhot * F;
+  A.drho = fma(VrF, Ed, A.drho);
+  // rate-form Tait with diffusion (DynamicPressureEquation)
+  const double dpt = a.r.p - b.pt, drt = a.r.rho - b.rhot;
+  const double brk2 = fma(-(a.KPa * drt), Sr, a.G4a * dpt * invSP);
+  A.dp = fma(VrF * a.IPa, Ed, A.dp);
+  A.dp = fma(b.V * nu, brk2, A.dp);
+  // pressure gradients (PredictingPressureGradientForce, PressureGradientForce)
+  const double A1b = b.p * b.ir2;
+  const double c1 = mbF * (a.A1a + A1b);
+  const double c2 = mbF * fma(a.A1a, b.C, A1b * a.r.C);
+  A.ax_a = fma(-c1, dxa, A.ax_a);
+  A.ay_a = fma(-c1, dya, A.ay_a);
+  A.ax = fma(-c2, dxa, A.ax);
+  A.ay = fma(-c2, dya, A.ay);
+  // deviatoric viscous stress (ViscousForcesSingleStep and its predictor):
+  // m_b mu_ab / (r^2 + 0.01 h^2) times F r^2 = m_b 2 mu rr (P_a + P_b) F r^2
+  if (P.stress_type == 1) {
+    const double vis = b.m * P.two_mu0 * rr * SP * Fr2;
+    const double D = fma(b.C, a.r.ir2, -(a.r.C * b.ir2));
+    const double sv = (isI ? vis : -vis) * D;
+    const double vp = vis * (a.r.ir2 + b.ir2);
+    A.ax = fma(-sv, dux, A.ax);
+    A.ay = fma(-sv, duy, A.ay);
+    A.ax_a = fma(-vp, dux, A.ax_a);
+    A.ay_a = fma(-vp, duy, A.ay_a);
+  }
+  // wall forces: only pairs whose i is this fluid particle
+  if (isI && a.r.itype == 1 && b.itype >= 2) wall_pair_force(P, b.itype, r2, dxa, dya, dux, duy, a.r.m, A);
+}
+
+// gravity, sponge, Tait pressure, stores
+__device__ __forceinline__ void ref_epilogue(const DevParams &P, const SlotArrays &S, int a, const RefOwn &o,
+                                             RefAcc &A, double bx, double by)
+{
+  A.ax += bx;
+  A.ay += by;
+  if (P.gravity_flag == 1) {
+    A.ay -= P.g;
+    A.ay_a -= P.g;
+  }
+  if (P.moving_boundary == 1 && P.wave_absorption == 1) A.ax -= S.sponge[a] * o.r.u;
+  S.drho[a] = A.drho;
+  S.dp[a] = A.dp;
+  S.ax[a] = A.ax;
+  S.ay[a] = A.ay;
+  S.drho_a[a] = A.drho_a;
+  S.dp_a[a] = A.dp_a;
+  S.ax_a[a] = A.ax_a;
+  S.ay_a[a] = A.ay_a;
+  S.frho[a] = A.frho;
+  S.fp[a] = A.fp;
+  S.fu[a] = A.fu;
+  S.fv[a] = A.fv;
+  S.pressure[a] = P.B * (pow(o.r.rho / P.rho0, P.gamma) - 1.0);
+}
+
+// ---- the two partner sources ---------------------------------------------------------
+// Staged: records in shared memory, list entries are record indices.
+struct StagedSrc {
+  const RefRec *rec;
+  const double *cut_d2;  // the knn cap's cut per record (kKnn only)
+  const int *cut_j;
+  __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
+  __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
+  __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
+  __device__ __forceinline__ RefRec get(int k) const { return rec[k]; }
+  __device__ __forceinline__ void cut(int k, double &d2, int &j) const
+  {
+    d2 = cut_d2[k];
+    j = cut_j[k];
+  }
+};
+// Global: the SoA arrays, list entries are slots.
+struct GlobalSrc {
+  DevParams P;
+  SlotArrays S;
+  __device__ __forceinline__ double2 xy(int s) const { return make_double2(S.x[s], S.y[s]); }
+  __device__ __forceinline__ int orig(int s) const { return S.orig[s]; }
+  __device__ __forceinline__ double mass(int s) const { return S.m[s]; }
+  __device__ __forceinline__ RefRec get(int s) const { return load_ref_rec(P, S, s); }
+  __device__ __forceinline__ void cut(int s, double &d2, int &j) const
+  {
+    d2 = P.kcut_d2[s];
+    j = P.kcut_j[s];
+  }
+};
+// Phase 1 and 2 for one own particle until its stencil is exhausted.
+template <bool kBrute, bool kKnn, typename Src, typename Cursor, typename Entry>
+__device__ __forceinline__ void ref_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
+                                             const RefOwn &o, Entry *s_nb, RefAcc &A, double &bx, double &by,
+                                             unsigned &my_pairs, int &my_nb, double cd, int cj)
+{
+  constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
+  const int col = threadIdx.x;
+  bool more = active;
+  while (__any_sync(0xffffffffu, more)) {
+    const int cnt = tile_list<kBrute, kTileChunk, kKnn>(P, src, cur, more, self, o.r.orig, o.r.x, o.r.y, s_nb, col,
+                                                        my_pairs, my_nb, bx, by, cd, cj);
+    __syncwarp();
+    for (int e = 0; e < cnt; e++) {
+      const Entry ent = s_nb[e * kTileThreads + col];
+      const RefRec b = src.get((int)(ent & (Entry)~kRole));
+      ref_pair(P, o, b, (ent & kRole) != 0, A);
     }
-  } else {
-    const double r = sqrt(r2);
-    const double q = r / P.h;
-    double phi = 0.0;
-    if (q >= 0.0 && q < 2.0) {
-      const double t = 2.0 - q;
-      phi = 0.125 * (1.0 + 1.5 * q) * t * t * t;
-    }
-    const double gama = P.mach_c * P.mach_c / (P.rho0 * P.dx * P.dy);
-    const double c = gama * phi * mb / r2;
-    fx += c * dxa;
-    fy += c * dya;
+    __syncwarp();
   }
 }
 
-__global__ void __launch_bounds__(kPassThreads, 4) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+// Dynamic shared memory of the tiled pass and its record capacity; with the
+// knn cap every record also carries its query's cut (12 bytes).
+template <bool kKnn>
+__host__ __device__ constexpr int ref_rec_cap() { return kKnn ? 560 : 640; }
+constexpr size_t kRefListBytes = sizeof(unsigned short) * kTileChunk * kTileThreads;
+template <bool kKnn>
+constexpr size_t ref_smem()
+{
+  return sizeof(TileBlock) + kRefListBytes + (sizeof(RefRec) + (kKnn ? 12 : 0)) * ref_rec_cap<kKnn>();
+}
+static_assert(sizeof(RefRec) * 560 >= sizeof(unsigned) * kTileChunk * kTileThreads,
+              "the fallback's 32-bit lists live in the record area");
+
+// One CTA per storage tile (see tile_pass.cuh).  Phase 1 lists in-radius
+// partners per thread (the exact distance test only); phase 2 runs the FP64
+// pair arithmetic over the lists, so the lanes of a warp stay converged in
+// the expensive loop.
+// kBrute: the wall modes that act on every boundary particle within the
+// radius (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on
+// listed pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
+template <bool kBrute, bool kKnn>
+__global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
                                                            PassStats st)
 {
-  __shared__ unsigned s_nb[kNbChunk][kPassThreads];
-  const int tid = threadIdx.x;
-  const int a = blockIdx.x * blockDim.x + tid;
-  const bool active = a < P.nf;
+  constexpr int kCap = ref_rec_cap<kKnn>();
+  extern __shared__ __align__(16) unsigned char smem[];
+  TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
+  unsigned short *s_nb16 = reinterpret_cast<unsigned short *>(smem + sizeof(TileBlock));
+  RefRec *rec = reinterpret_cast<RefRec *>(smem + sizeof(TileBlock) + kRefListBytes);
+  double *s_cd = reinterpret_cast<double *>(rec + kCap);
+  int *s_cj = reinterpret_cast<int *>(s_cd + kCap);
+  tile_setup(P, G, blockIdx.x, B);
+  const int ncore = B.ncore;
+  if (ncore == 0) return;
+  const bool staged = B.nrec <= kCap;
   unsigned my_pairs = 0;
   int my_nb = 0;
-  const int as = active ? a : 0;
-  const double xa = S.x[as], ya = S.y[as];
-  const double ua = S.u[as], va = S.v[as], uta = S.ut[as], vta = S.vt[as];
-  const double rhoa = S.rho[as], rhota = S.rhot[as], pa = S.p[as], ma = S.m[as];
-  const double ira = S.inv_rho[as], irta = S.inv_rhot[as];
-  const int oa = S.orig[as], ita = S.itype[as];
-  const double Pa = P.rho0c2 + P.gamma * pa;
-  const double ira2 = ira * ira;
-  const double gk = P.gamma * P.kappa;
-  const bool brute_walls = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
-  RefAcc A = {};
-  double bx = 0.0, by = 0.0;  // mode-1 / default wall force (dvdt only)
-
-  NeighbourCursor cur;
-  cur.init(P, G, G.cell_of[as]);
-  bool more = active;
-  while (__any_sync(0xffffffffu, more)) {
-    // phase 1: list up to kNbChunk partners (distance test and pair filter only)
-    const int cnt = list_partners(P, S, G, cur, more, a, oa, xa, ya, s_nb, tid, my_pairs, my_nb,
-                                  [&](int b, int ob, double r2, double dxa, double dya) {
-                                    if (brute_walls && ob >= P.b0 && ob < P.b1)
-                                      brute_wall_force(P, r2, dxa, dya, S.m[b], bx, by);
-                                  });
-    __syncwarp();
-    // phase 2: the pair terms
-    for (int e = 0; e < cnt; e++) {
-      const unsigned ent = s_nb[e][tid];
-      const int b = (int)(ent & ~kRoleI);
-      const bool isI = (ent & kRoleI) != 0;
-      const double dxa = xa - S.x[b], dya = ya - S.y[b];
-      const double r2 = exact_r2(dxa, dya);
-      const double ub = S.u[b], vb = S.v[b], utb = S.ut[b], vtb = S.vt[b];
-      const double rhob = S.rho[b], rhotb = S.rhot[b], pb = S.p[b], ptb = S.pt[b], mb = S.m[b];
-      const double irb = S.inv_rho[b], irtb = S.inv_rhot[b];
-
-      // poly-7 convolution W and deconvolution gradient factor: functions of q^2 only
-      const double q2 = r2 * P.inv_h2;
-      const double t = fma(-0.25, q2, 1.0);
-      const double t2 = t * t, t4 = t2 * t2;
-      const double t7 = t4 * t2 * t, t8 = t4 * t4;
-      const double pp = fma(fma(fma(fma(fma(fma(305.0, q2, -628.0), q2, 1184.0), q2, -1984.0), q2, 2816.0), q2, -3072.0), q2, 2048.0);
-      const double pp7 = fma(fma(fma(fma(fma(fma(305.0, q2, -1106.0), q2, 1912.0), q2, -2912.0), q2, 3712.0), q2, -3584.0), q2, 2048.0);
-      const double W = P.w_alpha * t8 * pp;
-      const double F = P.dw_alpha * P.inv_h2 * t7 * pp7;
-      const double gx = F * dxa, gy = F * dya;
-
-      const double Pb = fma(P.gamma, pb, P.rho0c2);
-      const double Vb = mb * irb;
-      const double ms = isI ? mb : ma;
-      const double rhosum = ira + irb;
-      const double inv_r2e = rcp_nr(r2 + P.eta2);
-      const double nu = (dxa * gx + dya * gy) * inv_r2e;
-      const double ep = 4.0 * Pa * rcp_nr(Pa + Pb);
-
-      // predictor density
-      const double pdx = isI ? (ua - utb) : (uta - ub);
-      const double pdy = isI ? (va - vtb) : (vta - vb);
-      A.drho_a += ms * (pdx * gx + pdy * gy);
-      // predictor pressure
-      const double dux = ua - ub, duy = va - vb;
-      const double vdw = dux * gx + duy * gy;
-      const double msb = ms * irb;
-      A.dp_a += (mb * ira) * Pa * vdw + gk * msb * (pa - pb) * nu * ep - P.kappa * Pa * msb * (rhoa - rhob) * rhosum * nu;
-      // predictor pressure gradient
-      const double pij_p = pa * ira2 + pb * irb * irb;
-      A.ax_a -= mb * pij_p * gx;
-      A.ay_a -= mb * pij_p * gy;
-      // fluctuations
-      A.frho -= Vb * (rhoa - rhob) * W;
-      A.fp -= Vb * (pa - pb) * W;
-      const double cfv = isI ? (ma * irtb - mb * irta) * W : 0.0;
-      A.fu += dux * cfv;
-      A.fv += duy * cfv;
-      // continuity
-      const double vdwt = (ua - utb) * gx + (va - vtb) * gy;
-      const double Vr = Vb * rhotb;
-      A.drho += Vr * vdwt;
-      // rate-form Tait with diffusion
-      A.dp += Vr * ira * Pa * vdwt + gk * Vb * (pa - ptb) * nu * ep - P.kappa * Pa * Vb * (rhoa - rhotb) * rhosum * nu;
-      // pressure gradient
-      const double pij = pa * rhotb * ira2 * irb + pb * rhota * irb * irb * ira;
-      A.ax -= mb * pij * gx;
-      A.ay -= mb * pij * gy;
-      // deviatoric viscous stress
-      if (P.stress_type == 1) {
-        const double meff = 2.0 * P.mu0 * rcp_nr(rhosum);
-        const double s00 = (-dxa) * dux - (-dya) * duy;
-        const double s01 = (-dxa) * duy + (-dya) * dux;
-        const double sgx = s00 * gx + s01 * gy;
-        const double sgy = s01 * gx - s00 * gy;
-        const double base = mb * meff * inv_r2e;
-        const double D = rhotb * ira2 * irb - rhota * irb * irb * ira;
-        const double sD = (isI ? base : -base) * D;
-        A.ax += sD * sgx;
-        A.ay += sD * sgy;
-        const double Dp = base * (ira2 + irb * irb);
-        A.ax_a += Dp * sgx;
-        A.ay_a += Dp * sgy;
-      }
-      // wall forces: only pairs whose i is this fluid particle
-      if (isI && ita == 1) {
-        const int itb = S.itype[b];
-        if (itb >= 2) wall_pair_force(P, itb, r2, dxa, dya, dux, duy, ma, A);
+  if (staged) {
+    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
+      const int slot = G.list[tile_record_pos(B, k)];
+      rec[k] = load_ref_rec(P, S, slot);
+      if constexpr (kKnn) {
+        // only fluid queries have a cut; other records are never a pair's i
+        // seen from a fluid particle that is its j
+        s_cd[k] = slot < P.nf ? P.kcut_d2[slot] : 0.0;
+        s_cj[k] = slot < P.nf ? P.kcut_j[slot] : 0;
       }
     }
-    __syncwarp();
-  }
-  if (active) {
-    A.ax += bx;
-    A.ay += by;
-    if (P.gravity_flag == 1) {
-      A.ay -= P.g;
-      A.ay_a -= P.g;
+    __syncthreads();
+    const StagedSrc src{rec, s_cd, s_cj};
+    for (int base = 0; base < ncore; base += kTileThreads) {
+      const int k = base + threadIdx.x;
+      int kr = 0, pos = 0, a = 0;
+      if (k < ncore) {
+        tile_core(B, k, kr, pos);
+        a = G.list[pos];
+      }
+      const bool active = k < ncore && a < P.nf;
+      const RefOwn o = make_own(P, rec[active ? kr : 0]);
+      StagedCursor cur;
+      const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
+      cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
+      double cd = 0.0;
+      int cj = 0;
+      if (kKnn && active) src.cut(kr, cd, cj);
+      RefAcc A = {};
+      double bx = 0.0, by = 0.0;
+      ref_particle<kBrute, kKnn>(P, src, cur, active, kr, o, s_nb16, A, bx, by, my_pairs, my_nb, cd, cj);
+      if (active) ref_epilogue(P, S, a, o, A, bx, by);
     }
-    if (P.moving_boundary == 1 && P.wave_absorption == 1) A.ax -= S.sponge[a] * ua;
-    S.drho[a] = A.drho;
-    S.dp[a] = A.dp;
-    S.ax[a] = A.ax;
-    S.ay[a] = A.ay;
-    S.drho_a[a] = A.drho_a;
-    S.dp_a[a] = A.dp_a;
-    S.ax_a[a] = A.ax_a;
-    S.ay_a[a] = A.ay_a;
-    S.frho[a] = A.frho;
-    S.fp[a] = A.fp;
-    S.fu[a] = A.fu;
-    S.fv[a] = A.fv;
-    S.pressure[a] = P.B * (pow(rhoa / P.rho0, P.gamma) - 1.0);
+  } else {
+    // a crowded tile: the same walk over the cell list in global memory
+    unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
+    const GlobalSrc src{P, S};
+    for (int base = 0; base < ncore; base += kTileThreads) {
+      const int k = base + threadIdx.x;
+      int kr = 0, pos = 0, a = 0;
+      if (k < ncore) {
+        tile_core(B, k, kr, pos);
+        a = G.list[pos];
+      }
+      const bool active = k < ncore && a < P.nf;
+      const int as = active ? a : 0;
+      const RefOwn o = make_own(P, load_ref_rec(P, S, as));
+      GlobalCursor cur;
+      cur.list = G.list;
+      cur.c.init(P, G, G.cell_of[as]);
+      double cd = 0.0;
+      int cj = 0;
+      if (kKnn && active) src.cut(as, cd, cj);
+      RefAcc A = {};
+      double bx = 0.0, by = 0.0;
+      ref_particle<kBrute, kKnn>(P, src, cur, active, as, o, s_nb32, A, bx, by, my_pairs, my_nb, cd, cj);
+      if (active) ref_epilogue(P, S, a, o, A, bx, by);
+    }
   }
   // pass statistics: one atomic per warp
   const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
@@ -284,10 +438,77 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_ref_pass(const DevParams P,
   }
 }
 
+template <bool kBrute, bool kKnn>
+void launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+{
+  static bool attr_set[64] = {};  // once per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    cudaFuncSetAttribute(k_ref_pass<kBrute, kKnn>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ref_smem<kKnn>());
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  const int ntiles = P.ntx * (P.ncy / P.tile);
+  k_ref_pass<kBrute, kKnn><<<ntiles, kTileThreads, ref_smem<kKnn>(), s>>>(P, S, G, st);
+}
+
 void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
   if (P.nf <= 0) return;
-  k_ref_pass<<<(P.nf + kPassThreads - 1) / kPassThreads, kPassThreads, 0, s>>>(P, S, G, st);
+  const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
+  if (P.knn > 0)
+    brute ? launch_ref<true, true>(P, S, G, st, s) : launch_ref<false, true>(P, S, G, st, s);
+  else
+    brute ? launch_ref<true, false>(P, S, G, st, s) : launch_ref<false, false>(P, S, G, st, s);
+}
+
+// The knn cap's cut of every fluid query: walk the stencil (the global cell
+// list, in its order), keep the knn smallest keys (r^2, reference index) of
+// the in-radius points (DBL_EPSILON < r^2 < (h h) 4, the own point and
+// coincident points excluded, as in SearchNeighbors) in a sorted array, and
+// record the largest kept key if more than knn points were in radius.
+__global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotArrays S, const CellGrid G)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const int K = P.knn;
+  double kd[kKnnMax];
+  int kj[kKnnMax];
+  int m = 0, count = 0;
+  const double xa = S.x[a], ya = S.y[a];
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[a]);
+  int pos;
+  while (cur.next(pos)) {
+    const int b = G.list[pos];
+    if (b == a) continue;
+    const double r2 = exact_r2(xa - S.x[b], ya - S.y[b]);
+    if (!(r2 < P.r2cut) || r2 <= DBL_EPSILON) continue;
+    const int ob = S.orig[b];
+    count++;
+    if (m == K && knn_key_le(kd[K - 1], kj[K - 1], r2, ob)) continue;  // not among the K smallest
+    int i = m < K ? m++ : K - 1;  // the slot the new key may take
+    while (i > 0 && !knn_key_le(kd[i - 1], kj[i - 1], r2, ob)) {
+      kd[i] = kd[i - 1];
+      kj[i] = kj[i - 1];
+      i--;
+    }
+    kd[i] = r2;
+    kj[i] = ob;
+  }
+  if (count > K) {
+    P.kcut_d2[a] = kd[K - 1];
+    P.kcut_j[a] = kj[K - 1];
+  } else {
+    P.kcut_d2[a] = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+    P.kcut_j[a] = INT_MAX;
+  }
+}
+
+void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s)
+{
+  if (P.nf <= 0 || P.knn <= 0) return;
+  k_knn_cut<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G);
 }
 
 __global__ void k_rcp_selftest(const double *__restrict__ x, double *__restrict__ y, int64_t n)

@@ -11,6 +11,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <array>
 #include <atomic>
 #include <map>
@@ -18,7 +19,7 @@
 #include <string>
 #include <vector>
 
-#include "pass_common.cuh"
+#include "tile_pass.cuh"
 #include "sim_access.cuh"
 
 using namespace uph;
@@ -303,25 +304,19 @@ __global__ void k_iota(int *p, int first, int count)
 // counting sort of ids [first, first+count) by cell, result: G.list[0, count)
 // = ids in key order, ties by id.  storage_order selects the tile-major
 // storage key instead of the row-major cell-list id.
-uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order)
+uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order,
+                      const PassStats *stats = nullptr)
 {
-  CellGrid &G = s->G;
-  cudaStream_t st = s->stream;
-  UPH_CUDA(cudaMemsetAsync(G.count, 0, sizeof(int) * G.ncell, st));
-  UPH_CUDA(cudaMemsetAsync(G.fill, 0, sizeof(int) * G.ncell, st));
-  launch_cell_keys(s->P, x, y, first, count, G, s->d_err, storage_order, st);
-  launch_exclusive_scan(G.count, G.start, G.ncell, G.block_sums, st);
-  // scatter ids; list is indexed from 0 because start[] only counted this range
-  launch_cell_scatter(G, first, count, st);
-  launch_cell_sort_segments(G, s->d_err, st);
-  s->launches += 6;
-  return UPH_OK;
+  uph_status r = launch_cell_build(s->P, x, y, first, count, s->G, s->d_err, storage_order, stats, s->stream);
+  s->launches += 1;
+  return r;
 }
 
-uph_status build_cell_list(uph_sim *s)
+// the cell list of all interacting particles; zeroes the pass statistics
+uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr)
 {
   Timer t(s, KF_CELLS);
-  return sort_range(s, s->S.x, s->S.y, 0, s->P.n, false);
+  return sort_range(s, s->S.x, s->S.y, 0, s->P.n, false, stats);
 }
 
 uph_status reorder_fluid(uph_sim *s)
@@ -350,7 +345,14 @@ uph_status check_error_word(uph_sim *s)
   if (err & ERR_NAN) return fail(UPH_NAN, "a non-finite value appeared in the particle state");
   if (err & ERR_OUT_OF_DOMAIN) return fail(UPH_OUT_OF_DOMAIN, "a particle left the cell-grid domain");
   if (err & ERR_NEIGHBOR_OVERFLOW) return fail(UPH_NEIGHBOR_OVERFLOW, "neighbour capacity exceeded");
-  if (err & ERR_TIMEOUT) return fail(UPH_TIMEOUT, "a device-side wait timed out");
+  if (err & ERR_TIMEOUT) {
+    // a cell-list build that gave up at a grid barrier leaves its histogram
+    // and barrier words part-way: clear them for the next build
+    cudaMemsetAsync(s->G.count, 0, sizeof(int) * s->G.ncell, s->stream);
+    cudaMemsetAsync(s->G.bar, 0, 2 * sizeof(unsigned), s->stream);
+    cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream);
+    return fail(UPH_TIMEOUT, "a device-side wait timed out");
+  }
   return UPH_OK;
 }
 
@@ -358,17 +360,19 @@ uph_status check_error_word(uph_sim *s)
 // predictor that ran since the last state change has done it already
 uph_status rate_pass(uph_sim *s, bool refresh)
 {
-  UPH_CUDA(cudaMemsetAsync(s->d_niac, 0, sizeof(unsigned long long), s->stream));
-  UPH_CUDA(cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), s->stream));
   if (refresh) {
     Timer t(s, KF_REFRESH);
     launch_refresh_inverse(s->P, s->S, 0, s->P.nf, s->stream);
     s->launches++;
   }
-  uph_status r = build_cell_list(s);
-  if (r != UPH_OK) return r;
-  Timer t(s, KF_PASS);
   PassStats st{s->d_niac, s->d_max_nb};
+  uph_status r = build_cell_list(s, &st);
+  if (r != UPH_OK) return r;
+  if (s->P.knn > 0) {
+    launch_knn_cut(s->P, s->S, s->G, s->stream);
+    s->launches++;
+  }
+  Timer t(s, KF_PASS);
   if (s->P.profile == UPH_PROFILE_REF)
     launch_ref_pass(s->P, s->S, s->G, st, s->stream);
   else
@@ -397,7 +401,11 @@ uph_status validate(const uph_params *p)
   if (vt == 1 || vt == 3 || vt == 4 || vt == 5 || vt == 7 || vt == 8)
     return fail(UPH_UNSUPPORTED, "virtual mirror particles (virtualType 1,3,4,5,7,8) are not implemented");
   if (p->stress_type == 2) return fail(UPH_UNSUPPORTED, "stressType 2 (two-step viscous stress) is not implemented");
-  if (p->knn_cap != 0) return fail(UPH_UNSUPPORTED, "the k-NN cap is not implemented; use knn_cap = 0");
+  if (p->knn_cap < 0) return fail(UPH_BAD_ARG, "negative knn_cap");
+  if (p->knn_cap > kKnnMax)
+    return fail(UPH_UNSUPPORTED, "knn_cap above " + std::to_string(kKnnMax) + " is not implemented");
+  if (p->knn_cap > 0 && p->profile != UPH_PROFILE_REF)
+    return fail(UPH_UNSUPPORTED, "the k-NN cap is implemented for the REF profile only");
   if (!(p->domain_hi[0] > p->domain_lo[0]) || !(p->domain_hi[1] > p->domain_lo[1]))
     return fail(UPH_BAD_ARG, "empty cell-grid domain");
   for (int d = 0; d < 2; d++)
@@ -425,6 +433,8 @@ cudaError_t alloc_grid(uph_sim *s)
   if ((e = cudaMalloc((void **)&G.start, sizeof(int) * (ncell + 1))) != cudaSuccess) return e;
   if ((e = cudaMalloc((void **)&G.fill, sizeof(int) * ncell)) != cudaSuccess) return e;
   if ((e = cudaMalloc((void **)&G.block_sums, sizeof(int) * (G.nblock_sums + 1))) != cudaSuccess) return e;
+  // the one-launch build keeps count all zero between builds
+  if ((e = cudaMemset(G.count, 0, sizeof(int) * ncell)) != cudaSuccess) return e;
   s->grid_capacity = ncell;
   return cudaSuccess;
 }
@@ -477,6 +487,7 @@ DevParams make_dev_params(const uph_params *p)
   P.eta2 = 0.01 * h * h;
   P.w_alpha = 2145.0 / (1347584.0 * M_PI * h * h);      // derivatives.c:769
   P.dw_alpha = -1.0 * (2145.0 / (192512.0 * M_PI * h * h));  // derivatives.c:788, 817
+  P.dw_alpha_h2 = P.dw_alpha * P.inv_h2;
   P.cs_alpha = 10.0 / (7. * M_PI * h * h);              // derivatives.c:46
   P.rho0 = p->density0;
   P.gamma = p->adiabatic_constant;
@@ -486,6 +497,7 @@ DevParams make_dev_params(const uph_params *p)
   P.g = p->gravity;
   P.gravity_flag = p->gravity_flag;
   P.mu0 = p->viscosity0;
+  P.two_mu0 = 2.0 * p->viscosity0;
   P.kappa = p->thermal_diffusivity0;
   P.eps = p->epsilon;
   P.stress_type = p->stress_type;
@@ -508,8 +520,17 @@ DevParams make_dev_params(const uph_params *p)
   P.hi_x = p->domain_hi[0];
   P.hi_y = p->domain_hi[1];
   // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
-  // against 36 h^2 for a 3 x 3 block of radius-wide cells
-  set_grid_geometry(P, kCellReach, kCellTile);
+  // against 36 h^2 for a 3 x 3 block of radius-wide cells.  A cell then holds
+  // about (h / dx)^2 particles of a lattice; the default tile (12 cells at
+  // h = 1.3 dx) shrinks for wider kernels so a tile's block stays within the
+  // tiled passes' shared-memory records.
+  int tile = kCellTile;
+  const double hdx = p->dx > 0 ? h / p->dx : 1.0;
+  if (hdx > 1.6) tile = std::max(2, (int)floor(kCellTile * 1.3 / hdx) - 1);
+  set_grid_geometry(P, kCellReach, tile);
+  P.knn = p->knn_cap;
+  P.kcut_d2 = nullptr;
+  P.kcut_j = nullptr;
   return P;
 }
 
@@ -548,6 +569,14 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   CellGrid &G = s->G;
   TRY(dalloc(s, &G.list, (size_t)n));
   TRY(dalloc(s, &G.cell_of, (size_t)n));
+  if (s->P.knn > 0) {
+    TRY(dalloc(s, &s->P.kcut_d2, (size_t)nf));
+    TRY(dalloc(s, &s->P.kcut_j, (size_t)nf));
+  }
+  TRY(dalloc(s, &G.rank, (size_t)n));
+  TRY(dalloc(s, &G.totals, (size_t)kCellBuildMaxBlocks + 1));
+  TRY(dalloc(s, &G.bar, 2));
+  TRY(cudaMemset(G.bar, 0, 2 * sizeof(unsigned)));
   TRY(alloc_grid(s));
   Staging &T = s->T;
   double **tall[] = {&T.rho, &T.lrho, &T.p, &T.lp, &T.mass, &T.pressure, &T.tmp_x, &T.tmp_y};
@@ -918,6 +947,8 @@ __global__ void k_pair_count(DevParams P, SlotArrays S, CellGrid G, int *__restr
   if (a >= P.nf) return;
   const double xa = S.x[a], ya = S.y[a];
   const int oa = S.orig[a];
+  const double cd = P.knn > 0 ? P.kcut_d2[a] : 0.0;
+  const int cj = P.knn > 0 ? P.kcut_j[a] : 0;
   NeighbourCursor cur;
   cur.init(P, G, G.cell_of[a]);
   int cnt = 0, k;
@@ -926,7 +957,7 @@ __global__ void k_pair_count(DevParams P, SlotArrays S, CellGrid G, int *__restr
     const int ob = S.orig[b];
     if (ob <= oa || ob >= P.pb) continue;
     const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
-    if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
+    if (r2 < P.r2cut && r2 > DBL_EPSILON && (P.knn <= 0 || knn_key_le(r2, ob, cd, cj))) cnt++;
   }
   cnt_by_orig[oa] = cnt;
 }
@@ -939,6 +970,8 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
   const double xa = S.x[a], ya = S.y[a];
   const int oa = S.orig[a];
   const int base = off[oa];
+  const double cd = P.knn > 0 ? P.kcut_d2[a] : 0.0;
+  const int cj = P.knn > 0 ? P.kcut_j[a] : 0;
   int cnt = 0, k;
   NeighbourCursor cur;
   cur.init(P, G, G.cell_of[a]);
@@ -949,6 +982,7 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
     const double dx = xa - S.x[b], dy = ya - S.y[b];
     const double r2 = pr2(dx, dy);
     if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
+    if (P.knn > 0 && !knn_key_le(r2, ob, cd, cj)) continue;
     const double r = sqrt(r2), q = r * P.inv_h;
     double W, F;
     if (P.profile == UPH_PROFILE_REF) {
@@ -1007,6 +1041,10 @@ extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, in
   // the cell list of the last evaluation is still valid unless a reorder moved slots since
   uph_status r = build_cell_list(s);
   if (r != UPH_OK) return r;
+  if (s->P.knn > 0) {
+    launch_knn_cut(s->P, s->S, s->G, q);
+    s->launches++;
+  }
   int *cnt = nullptr, *off = nullptr, *bsum = nullptr;
   const int nb = scan_block_sums_needed(nf > 0 ? nf : 1);
   UPH_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * (nf + 1), q));
@@ -1230,7 +1268,9 @@ extern "C" uph_status uph_sim_set_tuning(uph_sim *s, int32_t reach, int32_t tile
 {
   if (!s) return fail(UPH_BAD_ARG, "NULL sim");
   if (reach < 1 || reach > 3) return fail(UPH_BAD_ARG, "cell reach must be 1, 2 or 3");
-  if (tile < 1 || tile > 32 || (tile & (tile - 1))) return fail(UPH_BAD_ARG, "tile must be a power of two <= 32");
+  // the tiled pass stages a tile plus `reach` cells on each side: at most 32 cells per axis
+  if (tile < 1 || tile + 2 * reach > kTileRowsMax)
+    return fail(UPH_BAD_ARG, "tile must be positive and tile + 2 reach at most 32");
   if (reorder_interval < 1 || reorder_interval > 4096) return fail(UPH_BAD_ARG, "reorder interval out of range");
   DevParams P2 = s->P;
   set_grid_geometry(P2, reach, tile);
@@ -1286,7 +1326,7 @@ uph_status time_steps(uph_sim *s, int steps, double *ms)
 }  // namespace
 
 // Coordinate search over (cell reach, storage tile, re-sort interval): the
-// reach first with tile 8 and interval 16, then the tile at the best reach,
+// reach first with tile 12 and interval 16, then the tile at the best reach,
 // then the interval.  Each trial times `trial_steps` steps of this very
 // simulation, so tuning advances it by about 9 (trial_steps + 2) steps.
 // Results are cached per size class (profile, precision, log2 of the fluid
@@ -1318,7 +1358,7 @@ extern "C" uph_status uph_sim_autotune(uph_sim *s, int32_t trial_steps, int32_t 
     };
     best_ms = 1e300;
     for (int axis = 0; axis < 3; axis++) {
-      static const int options[3][3] = {{1, 2, 3}, {4, 8, 16}, {8, 16, 32}};
+      static const int options[3][3] = {{1, 2, 3}, {8, 12, 16}, {8, 16, 32}};
       std::array<int, 3> axis_best = best;
       for (int v : options[axis]) {
         std::array<int, 3> c = best;
@@ -1399,25 +1439,6 @@ __global__ void k_load_positions(SlotArrays S, const double *__restrict__ pos, i
   S.orig[k] = k;
 }
 
-// largest in-radius candidate count (any index, no self matches) of a query
-__global__ void k_inradius_max(DevParams P, SlotArrays S, CellGrid G, int *mx)
-{
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  int cnt = 0;
-  if (a < P.nf) {
-    const double xa = S.x[a], ya = S.y[a];
-    NeighbourCursor cur;
-    cur.init(P, G, G.cell_of[a]);
-    int k;
-    while (cur.next(k)) {
-      const int b = G.list[k];
-      const double r2 = pr2(xa - S.x[b], ya - S.y[b]);
-      if (r2 < P.r2cut && r2 > DBL_EPSILON) cnt++;
-    }
-  }
-  const int w = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
-  if ((threadIdx.x & 31) == 0 && w) atomicMax(mx, w);
-}
 
 }  // namespace
 
@@ -1446,6 +1467,8 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
   p.dx = 1.0;
   p.h = 0.5 * sqrt(dist);
   p.density0 = 1.0;
+  if (knn > kKnnMax) return fail(UPH_UNSUPPORTED, "knn above " + std::to_string(kKnnMax) + " is not implemented");
+  p.knn_cap = knn > 0 ? knn : 0;
   const double pad = sqrt(dist);
   p.domain_lo[0] = lo[0] - pad;
   p.domain_lo[1] = lo[1] - pad;
@@ -1469,16 +1492,6 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
   // an overcrowded cell (or a position outside the grid) stops here, before
   // any kernel walks the candidates
   if (r == UPH_OK) r = check_error_word(s);
-  if (r == UPH_OK && knn > 0) {
-    int mx = 0;
-    cudaMemsetAsync(s->d_max_nb, 0, sizeof(int), q);
-    k_inradius_max<<<(n_fluid + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, s->d_max_nb);
-    cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, q);
-    cudaStreamSynchronize(q);
-    if (mx > knn - 1)
-      r = fail(UPH_UNSUPPORTED, "a query has " + std::to_string(mx) + " in-radius neighbours; the reference's " +
-                                    std::to_string(knn) + "-NN cap would bind and its tie order is not reproduced");
-  }
   if (r == UPH_OK) r = check_error_word(s);
   if (r == UPH_OK) {
     s->have_rates = true;

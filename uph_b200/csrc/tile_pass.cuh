@@ -1,0 +1,231 @@
+// Tiled execution of a rate pass: one CTA per storage tile of T x T cells.
+//
+// The CTA stages every particle of its tile and of the `reach` cells around
+// it (the "block") into shared memory as one record each, then lets each
+// thread own one fluid particle of the tile's core cells and walk its
+// neighbour stencil inside the block.  A record is read from global memory
+// once per CTA instead of once per neighbour (about 20 times), and the pair
+// loop reads partners with a few 16-byte shared-memory loads.
+//
+// Order: the block's records are the cell list's row ranges, row by row, so
+// a stencil row is one contiguous range of records, and partners are visited
+// in exactly the cell list's order (rows bottom to top, cells left to right,
+// each cell's slots ascending) -- the order of the global walk.  A CTA whose
+// block holds more records than fit (a crowded tile) walks the cell list in
+// global memory instead, with the same arithmetic and the same order, so
+// either way every particle's sums are the same.
+#pragma once
+
+#include "pass_common.cuh"
+
+namespace uph {
+
+constexpr int kTileThreads = 256;  // threads of a tiled pass CTA
+constexpr int kTileChunk = 24;     // partners listed per thread before they are processed
+constexpr int kTileRowsMax = 32;   // rows and columns of a block (tile + 2 reach)
+constexpr int kTileTabMax = (kTileRowsMax + 1) * kTileRowsMax;
+constexpr unsigned short kRoleI16 = 0x8000u;  // list-entry flag: this particle is the pair's i
+
+// one CTA's tile and block, in shared memory
+struct TileBlock {
+  int bx0, by0, W, H;          // block: first cell (x, y) and size in cells
+  int ncore;                   // particles (of any kind) in the core cells
+  int nrec;                    // particles in the block
+  int gs[kTileRowsMax];        // cell-list position of each block row's first particle
+  int roff[kTileRowsMax + 1];  // record index of each block row's first particle
+  int cs0[kTileRowsMax];       // cell-list position of each core row's first particle
+  int coff[kTileRowsMax + 1];  // index among the core's particles of each row's first
+  int tab[kTileTabMax];        // record index of block cell (r, c): tab[r (W + 1) + c]
+};
+
+// Fills B for tile `tile_id` (all threads; ends with a barrier).
+__device__ __forceinline__ void tile_setup(const DevParams &P, const CellGrid &G, int tile_id, TileBlock &B)
+{
+  const int T = P.tile, R = P.reach;
+  const int tx = tile_id % P.ntx, ty = tile_id / P.ntx;
+  const int cx0 = tx * T, cy0 = ty * T;
+  const int bx0 = max(cx0 - R, 0), bx1 = min(cx0 + T - 1 + R, P.ncx - 1);
+  const int by0 = max(cy0 - R, 0), by1 = min(cy0 + T - 1 + R, P.ncy - 1);
+  const int W = bx1 - bx0 + 1, H = by1 - by0 + 1;
+  if (threadIdx.x < 32) {
+    const int r = threadIdx.x;
+    int len = 0, clen = 0, gsr = 0, cs0r = 0;
+    if (r < H) {
+      const int row = (by0 + r) * P.ncx;
+      gsr = G.start[row + bx0];
+      len = G.start[row + bx1 + 1] - gsr;
+      const int cr = by0 + r - cy0;
+      if (cr >= 0 && cr < T) {
+        cs0r = G.start[row + cx0];
+        clen = G.start[row + cx0 + T] - cs0r;
+      }
+    }
+    int il = len, ic = clen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int a = __shfl_up_sync(0xffffffffu, il, o);
+      const int c = __shfl_up_sync(0xffffffffu, ic, o);
+      if (r >= o) {
+        il += a;
+        ic += c;
+      }
+    }
+    B.gs[r] = gsr;
+    B.roff[r] = il - len;
+    B.cs0[r] = cs0r;
+    B.coff[r] = ic - clen;
+    if (r == 31) {
+      B.roff[32] = il;
+      B.coff[32] = ic;
+      B.nrec = il;
+      B.ncore = ic;
+      B.bx0 = bx0;
+      B.by0 = by0;
+      B.W = W;
+      B.H = H;
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < (W + 1) * H; e += blockDim.x) {
+    const int r = e / (W + 1), c = e % (W + 1);
+    B.tab[e] = B.roff[r] + (G.start[(by0 + r) * P.ncx + bx0 + c] - B.gs[r]);
+  }
+  __syncthreads();
+}
+
+// the largest r with off[r] <= k, for k in [0, off[32])
+__device__ __forceinline__ int tile_row_of(const int *off, int k)
+{
+  int r = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    if (off[r + step] <= k) r += step;
+  return r;
+}
+
+// record index and cell-list position of the k-th particle of the core
+__device__ __forceinline__ void tile_core(const TileBlock &B, int k, int &rec, int &pos)
+{
+  const int r = tile_row_of(B.coff, k);
+  pos = B.cs0[r] + (k - B.coff[r]);
+  const int br = r;  // core rows are block rows with the same index
+  rec = B.roff[br] + (pos - B.gs[br]);
+}
+
+// cell-list position of record k of the block
+__device__ __forceinline__ int tile_record_pos(const TileBlock &B, int k)
+{
+  const int r = tile_row_of(B.roff, k);
+  return B.gs[r] + (k - B.roff[r]);
+}
+
+// Walks a particle's stencil inside the block: (2 reach + 1) rows of
+// (2 reach + 1) cells, each row one range of record indices.
+struct BlockCursor {
+  int row, row1, c0, c1, k, kend, stride;
+  const int *tab;
+
+  __device__ __forceinline__ void init(const TileBlock &B, int reach, int cx, int cy)
+  {
+    const int lc = cx - B.bx0, lr = cy - B.by0;
+    c0 = max(lc - reach, 0);
+    c1 = min(lc + reach, B.W - 1);
+    row = max(lr - reach, 0);
+    row1 = min(lr + reach, B.H - 1);
+    stride = B.W + 1;
+    tab = B.tab;
+    k = tab[row * stride + c0];
+    kend = tab[row * stride + c1 + 1];
+  }
+  __device__ __forceinline__ bool advance()
+  {
+    while (k >= kend) {
+      if (++row > row1) return false;
+      k = tab[row * stride + c0];
+      kend = tab[row * stride + c1 + 1];
+    }
+    return true;
+  }
+  template <int kBatch>
+  __device__ __forceinline__ int next_batch(int &pos)
+  {
+    if (!advance()) return 0;
+    pos = k;
+    const int n = min(kBatch, kend - k);
+    k += n;
+    return n;
+  }
+};
+
+// The cell list's walk as a source of slots (the global fallback).
+struct GlobalCursor {
+  NeighbourCursor c;
+  const int *list;
+  template <int kBatch>
+  __device__ __forceinline__ int next_batch(int &pos) { return c.next_batch<kBatch>(pos); }
+  __device__ __forceinline__ int at(int pos) const { return list[pos]; }
+};
+struct StagedCursor {
+  BlockCursor c;
+  template <int kBatch>
+  __device__ __forceinline__ int next_batch(int &pos) { return c.next_batch<kBatch>(pos); }
+  __device__ __forceinline__ int at(int pos) const { return pos; }
+};
+
+// Phase 1 of a rate pass: lists up to kChunk in-radius partners of the own
+// particle (index `self` in the source) into column `col` of s_nb (row
+// stride kTileThreads), four candidates at a time, each entry the partner's
+// index with the role flag set when the own particle is the pair's i.  A
+// partner is in-radius and in the reference's pair list exactly as in
+// list_partners (pass_common.cuh).  The brute-force wall modes see every
+// in-radius boundary candidate.  The source gives xy(k), orig(k), mass(k).
+// kKnn: the reference's k-nearest cap (DevParams::knn): a pair is kept iff
+// the partner is among query i's kept points -- the own particle's cut
+// (cd, cj) when it is i, the partner's (src.cut(b)) when the partner is i.
+template <bool kBrute, int kChunk, bool kKnn = false, typename Src, typename Cursor, typename Entry>
+__device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cursor &cur, bool &more, int self,
+                                        int oa, double xa, double ya, Entry *s_nb, int col, unsigned &my_pairs,
+                                        int &my_nb, double &bx, double &by, double cd = 0.0, int cj = 0)
+{
+  constexpr int kB = 4;
+  constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
+  int cnt = 0;
+  while (more && cnt <= kChunk - kB) {
+    int pos;
+    const int n = cur.template next_batch<kB>(pos);
+    if (n == 0) {
+      more = false;
+      break;
+    }
+    int b[kB];
+    double2 q[kB];
+#pragma unroll
+    for (int u = 0; u < kB; u++) b[u] = (u < n) ? cur.at(pos + u) : self;
+#pragma unroll
+    for (int u = 0; u < kB; u++) q[u] = src.xy(b[u]);
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      if (b[u] == self) continue;
+      const double dxa = xa - q[u].x, dya = ya - q[u].y;
+      const double r2 = exact_r2(dxa, dya);
+      if (!(r2 < P.r2cut)) continue;
+      const int ob = src.orig(b[u]);
+      if (kBrute && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, src.mass(b[u]), bx, by);
+      if (r2 <= DBL_EPSILON) continue;
+      my_nb++;
+      if (max(oa, ob) >= P.pb) continue;
+      const bool isI = ob > oa;
+      if constexpr (kKnn) {
+        double pd;
+        int pj;
+        if (!isI) src.cut(b[u], pd, pj);
+        if (!(isI ? knn_key_le(r2, ob, cd, cj) : knn_key_le(r2, oa, pd, pj))) continue;
+      }
+      my_pairs += isI;
+      s_nb[cnt++ * kTileThreads + col] = (Entry)b[u] | (isI ? kRole : (Entry)0);
+    }
+  }
+  return cnt;
+}
+
+}  // namespace uph

@@ -64,10 +64,12 @@ struct DevParams {
   double eta2;      // 0.01 h^2
   double w_alpha;   // poly-7 convolution normalisation (derivatives.c:769)
   double dw_alpha;  // -alpha_0 of the poly-7 deconvolution (derivatives.c:788)
+  double dw_alpha_h2;  // dw_alpha / h^2
   double cs_alpha;  // cubic spline sigma = 10 / (7 pi h^2) (derivatives.c:46)
   double rho0, gamma, c0, B, rho0c2, g;
   int gravity_flag;
   double mu0, kappa, eps;
+  double two_mu0;  // 2 mu0
   int stress_type;
   int boundary_force;
   double k_spring, c_damp, dx, dy;
@@ -83,16 +85,33 @@ struct DevParams {
   int tile;      // storage-order tile edge in cells
   int ntx;       // tiles per row
   int reach;     // cells are >= radius / reach wide; partners lie within `reach` cells
+  // k-nearest cap of the reference's search (derivatives.c:1085 passes 40):
+  // 0 = every in-radius pair; else each fluid query s keeps its knn nearest
+  // in-radius points, ordered by (r^2, reference index), and a pair (i, j)
+  // exists iff j is among query i's kept points.  kcut_* [nf], by slot: the
+  // largest kept key of the query, (+inf, INT_MAX) when nothing is cut.
+  int knn;
+  double *kcut_d2;
+  int *kcut_j;
 };
+
+constexpr int kKnnMax = 64;  // largest knn cap the kernels keep per query
+
+// (r2, j) <= (cd, cj) in the cap's order
+__host__ __device__ __forceinline__ bool knn_key_le(double r2, int j, double cd, int cj)
+{
+  return r2 < cd || (r2 == cd && j <= cj);
+}
 
 // The cell list numbers cells row-major (cy * ncx + cx), so the cells of one
 // stencil row are one contiguous range of the list.  Particle *storage* is
 // sorted by a tile-major key instead: kCellTile x kCellTile cells form a
-// tile, tiles row-major, cells inside a tile row-major.  A block's 128
-// consecutive slots then cover a compact 2-D patch whose neighbours stay in
-// the SM's L1, rather than a long strip of one cell row.
-// The tile edge is a tuning parameter (DevParams::tile, default 8).
-constexpr int kCellTile = 8;
+// tile, tiles row-major, cells inside a tile row-major.  The REF rate pass
+// runs one CTA per tile (tile_pass.cuh), so a tile's fluid particles are
+// nearly contiguous slots.  The tile edge is a tuning parameter
+// (DevParams::tile, default 12: 144 half-radius cells hold about 240
+// particles of a lattice at h = 1.3 dx, one per thread of a 256-thread CTA).
+constexpr int kCellTile = 12;
 
 __host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx, int tile)
 {
@@ -117,6 +136,12 @@ struct CellGrid {
   int *cell_of;  // [n]
   int *block_sums;
   int nblock_sums;
+  // one-launch build (launch_cell_build): rank of each slot in its cell,
+  // per-block totals and the grid barrier's two words; count is all zero
+  // between builds
+  int *rank;       // [n]
+  int *totals;     // [kCellBuildMaxBlocks + 1]
+  unsigned *bar;   // [2]
 };
 
 std::string &last_error();
@@ -141,6 +166,15 @@ void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s
 // a cell with more ids than this is left unsorted and flags ERR_NEIGHBOR_OVERFLOW
 constexpr int kMaxCellOccupancy = 4096;
 void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s);
+// The whole build (keys and histogram, scan, scatter, per-cell sort) as one
+// cooperative launch with three bounded grid barriers; also zeroes the rate
+// pass's statistics when `stats` is given.  count must be all zero on entry
+// and is again on return.
+constexpr int kCellBuildThreads = 512;
+constexpr int kCellBuildMaxBlocks = 1024;
+struct PassStats;
+uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
+                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s);
 
 // REF / WCSPH rate pass over the fluid slots
 struct PassStats {
@@ -148,6 +182,8 @@ struct PassStats {
   int *max_nb;               // largest in-radius neighbour count of a fluid particle
 };
 void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+// the knn cap's cut of every fluid query (P.kcut_*), from the cell list
+void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
 void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
 
 // leapfrog

@@ -20,7 +20,7 @@
 //
 // Execution as in the REF pass: a cheap listing phase (distance test only)
 // per thread into shared memory, then the pair arithmetic over the lists.
-#include "pass_common.cuh"
+#include "tile_pass.cuh"
 
 namespace uph {
 
@@ -69,140 +69,201 @@ __device__ __forceinline__ void wcsph_wall_pair(const DevParams &P, int itb, dou
   }
 }
 
-// modes 1 / default: every boundary particle, no pair filter (FP64, as the REF pass)
-__device__ __forceinline__ void wcsph_wall_brute(const DevParams &P, double r2d, double dxd, double dyd, double mb,
-                                                 double &wx, double &wy)
+// One staged particle.  Positions, velocities and the mass stay FP64 (the
+// exact pair test, the FP64 differences and the FP64 wall forces need them);
+// m, p / rho^2 and rho as the pair arithmetic reads them, in Real (for FP32,
+// rounded once from FP64 -- the values of SlotArrays::pk).
+template <typename Real>
+struct __align__(16) WcRec {
+  double x, y, u, v, m;
+  Real mr, A1, rho;
+  int orig, itype;
+};
+
+template <typename Real>
+__device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s)
 {
-  if (P.boundary_force == 1) {
-    const double r0 = P.dx;
-    if (r2d < r0 * r0) {
-      double rr = r0 / sqrt(r2d);
-      rr *= rr;
-      rr *= rr;
-      const double pb = P.lj_coeff * rr * (rr * rr - 1.) / r2d;
-      wx += pb * dxd;
-      wy += pb * dyd;
-    }
+  WcRec<Real> r;
+  r.x = S.x[s];
+  r.y = S.y[s];
+  r.u = S.u[s];
+  r.v = S.v[s];
+  r.m = S.m[s];
+  const double ir = S.inv_rho[s];
+  r.mr = (Real)r.m;
+  r.A1 = (Real)(S.p[s] * ir * ir);
+  r.rho = (Real)S.rho[s];
+  r.orig = S.orig[s];
+  r.itype = S.itype[s];
+  return r;
+}
+
+template <typename Real>
+struct WcStagedSrc {
+  const WcRec<Real> *rec;
+  __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
+  __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
+  __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
+  __device__ __forceinline__ WcRec<Real> get(int k) const { return rec[k]; }
+};
+template <typename Real>
+struct WcGlobalSrc {
+  SlotArrays S;
+  __device__ __forceinline__ double2 xy(int s) const { return make_double2(S.x[s], S.y[s]); }
+  __device__ __forceinline__ int orig(int s) const { return S.orig[s]; }
+  __device__ __forceinline__ double mass(int s) const { return S.m[s]; }
+  __device__ __forceinline__ WcRec<Real> get(int s) const { return load_wc_rec<Real>(S, s); }
+};
+
+struct WcAcc {
+  double wx, wy;  // wall forces, FP64 like the reference
+};
+
+// the sums of one pair (a, b), a = the own particle
+template <typename Real>
+__device__ __forceinline__ void wc_pair(const DevParams &P, const WcRec<Real> &a, const WcRec<Real> &b, bool isI,
+                                        Real &drho, Real &ax, Real &ay, WcAcc &W)
+{
+  const Real h = (Real)P.h, inv_h = (Real)P.inv_h, inv_h2 = (Real)P.inv_h2;
+  const Real sigma = (Real)P.cs_alpha;
+  const Real eta2 = (Real)P.eta2, ac = (Real)P.av_alpha_c0;
+  const double dxd = a.x - b.x, dyd = a.y - b.y;
+  const double dud = a.u - b.u, dvd = a.v - b.v;
+  const Real dx = (Real)dxd, dy = (Real)dyd, du = (Real)dud, dv = (Real)dvd;
+  const Real mb = b.mr;
+  const Real r2 = dx * dx + dy * dy;
+  const Real r = sqrt_real<Real>(r2);
+  const Real q = r * inv_h;
+  Real F;
+  if (q < (Real)1) {
+    F = sigma * ((Real)-3 + (Real)2.25 * q) * inv_h2;
   } else {
-    const double rr = sqrt(r2d), q = rr / P.h;
-    double phi = 0.0;
-    if (q < 2.0) {
-      const double t = 2.0 - q;
-      phi = 0.125 * (1.0 + 1.5 * q) * t * t * t;
+    const Real t = (Real)2 - q;
+    F = -sigma * (Real)0.75 * t * t * inv_h * rcp_real<Real>(r);
+  }
+  const Real gx = F * dx, gy = F * dy;
+  drho += mb * (du * gx + dv * gy);
+  const Real vr = du * dx + dv * dy;
+  Real pi_ab = 0;
+  if (vr < (Real)0) {
+    const Real mu = h * vr * rcp_real<Real>(r2 + eta2);
+    pi_ab = -ac * mu * rcp_real<Real>((Real)0.5 * (a.rho + b.rho));
+  }
+  const Real pij = a.A1 + b.A1 + pi_ab;
+  ax -= mb * pij * gx;
+  ay -= mb * pij * gy;
+  if (isI && a.itype == 1 && b.itype >= 2) wcsph_wall_pair(P, b.itype, exact_r2(dxd, dyd), dxd, dyd, dud, dvd, a.m, W.wx, W.wy);
+}
+
+template <bool kBrute, typename Real, typename Src, typename Cursor, typename Entry>
+__device__ __forceinline__ void wc_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
+                                            const WcRec<Real> &o, Entry *s_nb, Real &drho, Real &ax, Real &ay,
+                                            WcAcc &W, unsigned &my_pairs, int &my_nb)
+{
+  constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
+  const int col = threadIdx.x;
+  bool more = active;
+  while (__any_sync(0xffffffffu, more)) {
+    const int cnt = tile_list<kBrute, kTileChunk>(P, src, cur, more, self, o.orig, o.x, o.y, s_nb, col, my_pairs,
+                                                  my_nb, W.wx, W.wy);
+    __syncwarp();
+    for (int e = 0; e < cnt; e++) {
+      const Entry ent = s_nb[e * kTileThreads + col];
+      const WcRec<Real> b = src.get((int)(ent & (Entry)~kRole));
+      wc_pair<Real>(P, o, b, (ent & kRole) != 0, drho, ax, ay, W);
     }
-    const double c = P.mach_c * P.mach_c / (P.rho0 * P.dx * P.dy) * phi * mb / r2d;
-    wx += c * dxd;
-    wy += c * dyd;
+    __syncwarp();
   }
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+__device__ __forceinline__ void wc_epilogue(const DevParams &P, const SlotArrays &S, int a, const WcRec<Real> &o,
+                                            Real drho, Real ax, Real ay, const WcAcc &W)
+{
+  double axd = (double)ax + W.wx, ayd = (double)ay + W.wy;
+  if (P.gravity_flag == 1) ayd -= P.g;
+  if (P.moving_boundary == 1 && P.wave_absorption == 1) axd -= S.sponge[a] * o.u;
+  S.drho[a] = (double)drho;
+  S.dp[a] = 0.0;
+  S.ax[a] = axd;
+  S.ay[a] = ayd;
+  S.drho_a[a] = (double)drho;
+  S.dp_a[a] = 0.0;
+  S.ax_a[a] = axd;
+  S.ay_a[a] = ayd;
+  S.frho[a] = 0.0;
+  S.fp[a] = 0.0;
+  S.fu[a] = 0.0;
+  S.fv[a] = 0.0;
+}
+
+constexpr int kWcRecCap = 640;
+constexpr size_t kWcListBytes = sizeof(unsigned short) * kTileChunk * kTileThreads;
+template <typename Real>
+constexpr size_t wc_smem()
+{
+  return sizeof(TileBlock) + kWcListBytes + sizeof(WcRec<Real>) * kWcRecCap;
+}
+static_assert(sizeof(WcRec<float>) * kWcRecCap >= sizeof(unsigned) * kTileChunk * kTileThreads,
+              "the fallback's 32-bit lists live in the record area");
+
+// One CTA per storage tile, as the REF pass (tile_pass.cuh).
+template <bool kBrute, typename Real>
+__global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
                                                              PassStats st)
 {
-  __shared__ unsigned s_nb[kNbChunk][kPassThreads];
-  const int tid = threadIdx.x;
-  const int a = blockIdx.x * blockDim.x + tid;
-  const bool active = a < P.nf;
+  extern __shared__ __align__(16) unsigned char smem[];
+  TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
+  unsigned short *s_nb16 = reinterpret_cast<unsigned short *>(smem + sizeof(TileBlock));
+  WcRec<Real> *rec = reinterpret_cast<WcRec<Real> *>(smem + sizeof(TileBlock) + kWcListBytes);
+  tile_setup(P, G, blockIdx.x, B);
+  const int ncore = B.ncore;
+  if (ncore == 0) return;
+  const bool staged = B.nrec <= kWcRecCap;
   unsigned my_pairs = 0;
   int my_nb = 0;
-  const int as = active ? a : 0;
-  const double xa = S.x[as], ya = S.y[as], ua = S.u[as], va = S.v[as];
-  const double ma_d = S.m[as];
-  // FP32 pair arithmetic reads the packed operands written with 1/rho
-  constexpr bool kPacked = sizeof(Real) == sizeof(float);
-  Real pa_over, rhoa;
-  if constexpr (kPacked) {
-    const float4 k = S.pk[as];
-    pa_over = k.y;
-    rhoa = k.z;
-  } else {
-    const Real ira = (Real)S.inv_rho[as];
-    pa_over = (Real)S.p[as] * ira * ira;
-    rhoa = (Real)S.rho[as];
-  }
-  const int oa = S.orig[as], ita = S.itype[as];
-  const Real h = (Real)P.h, inv_h = (Real)P.inv_h, inv_h2 = (Real)P.inv_h2;
-  const Real sigma = (Real)P.cs_alpha;
-  const Real eta2 = (Real)P.eta2, ac = (Real)P.av_alpha_c0;
-  const bool brute_walls = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
-  Real drho = 0, ax = 0, ay = 0;
-  double wx = 0.0, wy = 0.0;  // wall forces, FP64 like the reference
-
-  NeighbourCursor cur;
-  cur.init(P, G, G.cell_of[as]);
-  bool more = active;
-  while (__any_sync(0xffffffffu, more)) {
-    const int cnt = list_partners(P, S, G, cur, more, a, oa, xa, ya, s_nb, tid, my_pairs, my_nb,
-                                  [&](int b, int ob, double r2d, double dxd, double dyd) {
-                                    if (brute_walls && ob >= P.b0 && ob < P.b1)
-                                      wcsph_wall_brute(P, r2d, dxd, dyd, S.m[b], wx, wy);
-                                  });
-    __syncwarp();
-    for (int e = 0; e < cnt; e++) {
-      const unsigned ent = s_nb[e][tid];
-      const int b = (int)(ent & ~kRoleI);
-      const bool isI = (ent & kRoleI) != 0;
-      const double dxd = xa - S.x[b], dyd = ya - S.y[b];
-      const double dud = ua - S.u[b], dvd = va - S.v[b];
-      const Real dx = (Real)dxd, dy = (Real)dyd, du = (Real)dud, dv = (Real)dvd;
-      // partner operands: FP64 fields, or the packed FP32 copy (one 16-byte load)
-      Real mb, pb_over, rhob;
-      if constexpr (kPacked) {
-        const float4 k = S.pk[b];
-        mb = k.x;
-        pb_over = k.y;
-        rhob = k.z;
-      } else {
-        const Real irb = (Real)S.inv_rho[b];
-        mb = (Real)S.m[b];
-        pb_over = (Real)S.p[b] * irb * irb;
-        rhob = (Real)S.rho[b];
+  if (staged) {
+    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) rec[k] = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)]);
+    __syncthreads();
+    const WcStagedSrc<Real> src{rec};
+    for (int base = 0; base < ncore; base += kTileThreads) {
+      const int k = base + threadIdx.x;
+      int kr = 0, pos = 0, a = 0;
+      if (k < ncore) {
+        tile_core(B, k, kr, pos);
+        a = G.list[pos];
       }
-      const Real r2 = dx * dx + dy * dy;
-      const Real r = sqrt_real<Real>(r2);
-      const Real q = r * inv_h;
-      Real F;
-      if (q < (Real)1) {
-        F = sigma * ((Real)-3 + (Real)2.25 * q) * inv_h2;
-      } else {
-        const Real t = (Real)2 - q;
-        F = -sigma * (Real)0.75 * t * t * inv_h * rcp_real<Real>(r);
-      }
-      const Real gx = F * dx, gy = F * dy;
-      drho += mb * (du * gx + dv * gy);
-      const Real vr = du * dx + dv * dy;
-      Real pi_ab = 0;
-      if (vr < (Real)0) {
-        const Real mu = h * vr * rcp_real<Real>(r2 + eta2);
-        pi_ab = -ac * mu * rcp_real<Real>((Real)0.5 * (rhoa + rhob));
-      }
-      const Real pij = pa_over + pb_over + pi_ab;
-      ax -= mb * pij * gx;
-      ay -= mb * pij * gy;
-      if (isI && ita == 1) {
-        const int itb = S.itype[b];
-        if (itb >= 2) wcsph_wall_pair(P, itb, exact_r2(dxd, dyd), dxd, dyd, dud, dvd, ma_d, wx, wy);
-      }
+      const bool active = k < ncore && a < P.nf;
+      const WcRec<Real> o = rec[active ? kr : 0];
+      StagedCursor cur;
+      const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
+      cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
+      Real drho = 0, ax = 0, ay = 0;
+      WcAcc W = {0.0, 0.0};
+      wc_particle<kBrute, Real>(P, src, cur, active, kr, o, s_nb16, drho, ax, ay, W, my_pairs, my_nb);
+      if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
     }
-    __syncwarp();
-  }
-  if (active) {
-    double axd = (double)ax + wx, ayd = (double)ay + wy;
-    if (P.gravity_flag == 1) ayd -= P.g;
-    if (P.moving_boundary == 1 && P.wave_absorption == 1) axd -= S.sponge[a] * ua;
-    S.drho[a] = (double)drho;
-    S.dp[a] = 0.0;
-    S.ax[a] = axd;
-    S.ay[a] = ayd;
-    S.drho_a[a] = (double)drho;
-    S.dp_a[a] = 0.0;
-    S.ax_a[a] = axd;
-    S.ay_a[a] = ayd;
-    S.frho[a] = 0.0;
-    S.fp[a] = 0.0;
-    S.fu[a] = 0.0;
-    S.fv[a] = 0.0;
+  } else {
+    unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
+    const WcGlobalSrc<Real> src{S};
+    for (int base = 0; base < ncore; base += kTileThreads) {
+      const int k = base + threadIdx.x;
+      int kr = 0, pos = 0, a = 0;
+      if (k < ncore) {
+        tile_core(B, k, kr, pos);
+        a = G.list[pos];
+      }
+      const bool active = k < ncore && a < P.nf;
+      const int as = active ? a : 0;
+      const WcRec<Real> o = load_wc_rec<Real>(S, as);
+      GlobalCursor cur;
+      cur.list = G.list;
+      cur.c.init(P, G, G.cell_of[as]);
+      Real drho = 0, ax = 0, ay = 0;
+      WcAcc W = {0.0, 0.0};
+      wc_particle<kBrute, Real>(P, src, cur, active, as, o, s_nb32, drho, ax, ay, W, my_pairs, my_nb);
+      if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
+    }
   }
   const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
   const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
@@ -212,14 +273,29 @@ __global__ void __launch_bounds__(kPassThreads, 5) k_wcsph_pass(const DevParams 
   }
 }
 
+template <bool kBrute, typename Real>
+void launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+{
+  static bool attr_set[64] = {};  // once per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    cudaFuncSetAttribute(k_wcsph_pass<kBrute, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wc_smem<Real>());
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  const int ntiles = P.ntx * (P.ncy / P.tile);
+  k_wcsph_pass<kBrute, Real><<<ntiles, kTileThreads, wc_smem<Real>(), s>>>(P, S, G, st);
+}
+
 void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
   if (P.nf <= 0) return;
-  const int blocks = (P.nf + kPassThreads - 1) / kPassThreads;
-  if (P.precision == UPH_PREC_FP32_PAIR)
-    k_wcsph_pass<float><<<blocks, kPassThreads, 0, s>>>(P, S, G, st);
+  const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
+  const bool f32 = P.precision == UPH_PREC_FP32_PAIR;
+  if (f32)
+    brute ? launch_wc<true, float>(P, S, G, st, s) : launch_wc<false, float>(P, S, G, st, s);
   else
-    k_wcsph_pass<double><<<blocks, kPassThreads, 0, s>>>(P, S, G, st);
+    brute ? launch_wc<true, double>(P, S, G, st, s) : launch_wc<false, double>(P, S, G, st, s);
 }
 
 }  // namespace uph

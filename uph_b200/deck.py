@@ -142,12 +142,13 @@ class Deck:
         _write_particles(os.path.join(directory, "FrozenParticle.dat"), np.zeros((0, 12)))
 
     def uph_params(self, profile: int = PROFILE_REF, precision: int = PREC_FP64,
-                   av_alpha: Optional[float] = None) -> dict:
-        """A dict for UphParams.from_dict: file fields, derived fields, counts."""
+                   av_alpha: Optional[float] = None, knn_cap: int = 0) -> dict:
+        """A dict for UphParams.from_dict: file fields, derived fields, counts.
+        knn_cap = 40 is the reference's own 40-nearest cap (derivatives.c:1085)."""
         p = derive_params(self.params, self.eta_override)
         p.update(profile=profile, precision=precision, n_fluid=self.n_fluid,
                  n_solid=int(self.solid.shape[0]), n_fixed=int(self.fixed.shape[0]),
-                 n_moving=int(self.moving.shape[0]), knn_cap=0,
+                 n_moving=int(self.moving.shape[0]), knn_cap=knn_cap,
                  av_alpha=self.params["alpha"] if av_alpha is None else av_alpha)
         lo, hi = self.domain()
         p["domain_lo"] = list(lo)

@@ -39,8 +39,8 @@ class Simulation:
 
     @classmethod
     def from_deck(cls, deck: Deck, profile: int = PROFILE_REF, precision: int = PREC_FP64,
-                  av_alpha: Optional[float] = None) -> "Simulation":
-        sim = cls(deck.uph_params(profile, precision, av_alpha))
+                  av_alpha: Optional[float] = None, knn_cap: int = 0) -> "Simulation":
+        sim = cls(deck.uph_params(profile, precision, av_alpha, knn_cap))
         sim.upload(deck.initial_state(), 0)
         if deck.wall_table is not None:
             sim.set_wall_motion(*deck.wall_table)
