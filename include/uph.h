@@ -220,6 +220,14 @@ uph_status uph_sim_autotune(uph_sim *sim, int32_t trial_steps, int32_t choice[3]
 uph_status uph_sim_set_wall_motion(uph_sim *sim, const double *x0, const double *half_stroke,
                                    const double *omega);
 
+/* Base coordinates of the lid (movingBoundary 3: x = base + lidVelocity t)
+ * or the gate (movingBoundary 2: y = base + lidVelocity min(t, t_stop)),
+ * one per moving boundary particle in reference order: the reference's
+ * tempPosition / tempPositionGate deck columns (inputbp.c:209-243).  An
+ * upload sets them from the uploaded positions (at itime 0: the positions
+ * themselves); this call replaces them. */
+uph_status uph_sim_set_wall_base(uph_sim *sim, const double *base);
+
 /* One rate evaluation at time t on the uploaded state, no integration: what
  * the reference's derivatives() computes for the hot path. */
 uph_status uph_sim_derivatives(uph_sim *sim, double t);

@@ -165,6 +165,13 @@ int SearchNeighbors(const double **Position, int *i_pair, int *j_pair, double *r
  * device-to-host copy (40 bytes per pair) with level 0. */
 void uph_dropin_set_pair_export(int level);
 
+/* The two libSPH functions derivatives() calls back, inputbp(sys, t) and
+ * inoutflow(sys) (derivatives.c:3162-3168).  By default they are the ones
+ * linked with the caller (its own libSPH); a caller without a libSPH, or one
+ * that loads several callers into one process, names its own here (NULL
+ * restores the default).  No counterpart in the reference. */
+void uph_dropin_set_callbacks(void (*inputbp_fn)(System *sys, double t), void (*inoutflow_fn)(System *sys));
+
 #ifdef __cplusplus
 }
 #endif

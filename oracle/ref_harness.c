@@ -45,9 +45,18 @@
 #include "derivatives.h"
 #include "input.h"
 #include "inputbp.h"
+#include "inoutflow.h"
 
 /* defined by shim/search_standin.c; absent when the hot path is the GPU drop-in */
 extern void uph_standin_set_capacity(long cap) __attribute__((weak));
+/* the drop-in build (libuph_dropin.so) hands derivatives() the reference's
+ * own inputbp / inoutflow before every call, so another caller of the
+ * drop-in loaded into the same process cannot take their place */
+extern void uph_dropin_set_callbacks(void (*)(System *, double), void (*)(System *)) __attribute__((weak));
+static void use_reference_callbacks(void)
+{
+  if (uph_dropin_set_callbacks) uph_dropin_set_callbacks(inputbp, inoutflow);
+}
 
 typedef struct {
   System *sys;
@@ -176,6 +185,7 @@ int ref_derivatives(ref_run *run, double t)
 {
   char cwd[8192];
   if (!getcwd(cwd, sizeof cwd) || chdir(run->deck)) return -1;
+  use_reference_callbacks();
   derivatives(run->sys, t);
   if (chdir(cwd)) return -1;
   return 0;
@@ -234,6 +244,7 @@ int ref_step(ref_run *run, int nsteps)
     if (itime == 1)
       memcpy(sys->Velocity_xsph[0], sys->Velocity[0], sizeof(double) * sys->dim * sys->MaxNumberOfParticles);
 
+    use_reference_callbacks();
     derivatives(sys, t);
 
     if (itime == 1) {

@@ -32,6 +32,7 @@ SIGNATURES = {
     "uph_sim_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "uph_sim_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32 * 3), C.POINTER(C.c_double)]),
     "uph_sim_set_wall_motion": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "uph_sim_set_wall_base": (C.c_int, [C.c_void_p, C.c_void_p]),
     "uph_sim_derivatives": (C.c_int, [C.c_void_p, C.c_double]),
     "uph_sim_pairs": (C.c_int, [C.c_void_p, C.c_int64] + [C.c_void_p] * 5 + [C.POINTER(C.c_int64)]),
     "uph_sim_stats": (C.c_int, [C.c_void_p, C.POINTER(UphStats)]),

@@ -12,6 +12,7 @@ Objects are rebuilt only when a source or header is newer than the object.
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
 
@@ -108,8 +109,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         _run([NVCC] + ARCH + ["-shared", "-o", LIB_SPH] + dobjs +
              ["-L" + HERE, "-luph", "-Xlinker", "-rpath,$ORIGIN", "-lcudart"], verbose)
     if _newer(LIB_DRIVER, [DRIVER_SRC, LIB_SPH] + _headers()):
+        cuda = os.path.dirname(os.path.dirname(shutil.which(NVCC) or "/usr/local/cuda/bin/nvcc"))
         _run([CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-shared", "-I" + INCLUDE,
-              "-o", LIB_DRIVER, DRIVER_SRC, "-L" + HERE, "-luph_sph", "-luph", "-Wl,-rpath,$ORIGIN"], verbose)
+              "-I" + os.path.join(cuda, "include"), "-o", LIB_DRIVER, DRIVER_SRC, "-L" + HERE, "-luph_sph", "-luph",
+              "-L" + os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 

@@ -218,6 +218,8 @@ struct CellBuildArgs {
   unsigned long long *niac;  // rate-pass statistics to zero (or null)
   int *max_nb;
   int storage_order;
+  unsigned *rebuild;  // non-null: skip unless set; clear it and record the binned positions
+  double *xbin, *ybin;
 };
 
 // Grid-wide barrier over co-resident blocks: arrive on bar[0]; the last
@@ -296,16 +298,25 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
   int *cnt = A.G.count, *start = A.G.start, *fill = A.G.fill, *list = A.G.list;
   int *cell_of = A.G.cell_of, *rank = A.G.rank;
 
-  // 1. keys and histogram
-  for (int k = b * kCellBuildThreads + t; k < A.count; k += stride) {
-    const int s = A.first + k;
-    const int c = cell_of_position(A.P, A.x[s], A.y[s], A.err, A.storage_order != 0);
-    cell_of[s] = c;
-    rank[s] = atomicAdd(&cnt[c], 1);
-  }
   if (b == 0 && t == 0 && A.niac) {
     *A.niac = 0ull;
     *A.max_nb = 0;
+  }
+  // the list from the last build is still complete: nothing to do (every
+  // block reads the flag before any block can clear it, in phase 4)
+  if (A.rebuild && *(volatile unsigned *)A.rebuild == 0u) return;
+
+  // 1. keys and histogram
+  for (int k = b * kCellBuildThreads + t; k < A.count; k += stride) {
+    const int s = A.first + k;
+    const double px = A.x[s], py = A.y[s];
+    const int c = cell_of_position(A.P, px, py, A.err, A.storage_order != 0);
+    cell_of[s] = c;
+    rank[s] = atomicAdd(&cnt[c], 1);
+    if (A.rebuild) {
+      A.xbin[s] = px;
+      A.ybin[s] = py;
+    }
   }
   if (!cell_grid_barrier(A.G.bar, A.err)) return;
 
@@ -362,6 +373,7 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
   if (!cell_grid_barrier(A.G.bar, A.err)) return;
 
   // 4. per-cell sort by slot
+  if (A.rebuild && b == 0 && t == 0) *A.rebuild = 0u;
   for (int c = b * kCellBuildThreads + t; c < ncell; c += stride) {
     const int a0 = start[c], a1 = start[c + 1];
     if (a1 - a0 > kMaxCellOccupancy) {
@@ -381,7 +393,8 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
 }
 
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s)
+                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s,
+                             bool check_rebuild)
 {
   // co-resident blocks: the cooperative launch refuses a grid that does not fit
   static int max_blocks[64] = {};
@@ -410,6 +423,9 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   A.niac = stats ? stats->niac : nullptr;
   A.max_nb = stats ? stats->max_nb : nullptr;
   A.storage_order = storage_order ? 1 : 0;
+  A.rebuild = check_rebuild ? P.rebuild : nullptr;
+  A.xbin = P.xbin;
+  A.ybin = P.ybin;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(kCellBuildThreads);

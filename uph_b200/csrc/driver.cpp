@@ -17,6 +17,8 @@
 #include <new>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "uph_driver.h"
 
 namespace {
@@ -26,16 +28,26 @@ namespace {
 struct Owned {
   System sys;
   int itime = 0;
-  std::vector<void *> blocks;
+  std::vector<void *> blocks;  // posix_memalign
+  std::vector<void *> pinned;  // cudaMallocHost
 };
 
+// The System's arrays are page-locked host memory (cudaMallocHost), so the
+// drop-in's copies to and from the device go straight over the bus; plain
+// host memory if page-locking is refused.
 template <typename T>
 T *alloc_array(Owned *o, size_t count)
 {
+  const size_t bytes = sizeof(T) * (count ? count : 1);
   void *p = nullptr;
-  if (posix_memalign(&p, 64, sizeof(T) * (count ? count : 1)) != 0) throw std::bad_alloc();
-  memset(p, 0, sizeof(T) * (count ? count : 1));
-  o->blocks.push_back(p);
+  if (cudaMallocHost(&p, bytes) == cudaSuccess) {
+    o->pinned.push_back(p);
+  } else {
+    cudaGetLastError();
+    if (posix_memalign(&p, 64, bytes) != 0) throw std::bad_alloc();
+    o->blocks.push_back(p);
+  }
+  memset(p, 0, bytes);
   return (T *)p;
 }
 
@@ -53,15 +65,18 @@ Owned *owned(System *s) { return reinterpret_cast<Owned *>(s); }
 }  // namespace
 
 // ---- the two libSPH functions derivatives() calls back ------------------------
+// (handed to the drop-in with uph_dropin_set_callbacks before every call, so
+// another caller loaded into the same process cannot take their place)
+namespace {
 
-extern "C" void inoutflow(System *) {}
+void driver_inoutflow(System *) {}
 
 // The state effects of inputbp (src/lib/inputbp.c:192-299) for the walls of
 // the resident path: boundary and solid particles carry the rest density and
 // zero local pressure, and the piston (movingBoundary 1) sits at
 // x = S/2 (1 - cos w t) with velocity S/2 w sin w t.  The reference also
 // re-reads the boundary decks from disk here; the driver keeps them in memory.
-extern "C" void inputbp(System *sys, double t)
+void driver_inputbp(System *sys, double t)
 {
   const int nf = sys->NumberOfFluidParticles;
   const int nw = sys->NumberOfBoundaryParticles + sys->NumberOfSolidParticles;
@@ -80,6 +95,8 @@ extern "C" void inputbp(System *sys, double t)
     }
   }
 }
+
+}  // namespace
 
 // ---- the driver ------------------------------------------------------------------
 
@@ -231,6 +248,7 @@ extern "C" uph_status uph_driver_step(System *sys, int32_t nsteps)
     } else {
       memcpy(sys->Velocity_xsph[0], sys->Velocity[0], sizeof(double) * 2 * n);
     }
+    uph_dropin_set_callbacks(driver_inputbp, driver_inoutflow);
     derivatives(sys, t);
     if (itime == 1) {
       // sph.cc:131-146
@@ -310,5 +328,6 @@ extern "C" void uph_driver_destroy(System *sys)
   if (!sys) return;
   Owned *o = owned(sys);
   for (void *b : o->blocks) free(b);
+  for (void *b : o->pinned) cudaFreeHost(b);
   delete o;
 }

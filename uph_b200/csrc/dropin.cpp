@@ -8,15 +8,15 @@
 
 #include <vector>
 
-#include <cuda_runtime.h>
-
 #include "uph.h"
 #include "uph_system.h"
 
 extern "C" {
-// the caller's own libSPH provides these (inputbp.c:12, inoutflow.c:14)
-void inputbp(System *sys, double t);
-void inoutflow(System *sys);
+// the caller's own libSPH provides these (inputbp.c:12, inoutflow.c:14);
+// weak, so a caller without a libSPH can load the library and register its
+// own through uph_dropin_set_callbacks instead
+void inputbp(System *sys, double t) __attribute__((weak));
+void inoutflow(System *sys) __attribute__((weak));
 }
 
 namespace {
@@ -24,50 +24,16 @@ namespace {
 struct DropIn {
   uph_sim *sim = nullptr;
   uph_params p;
-  // the System whose arrays past its particles were zeroed, and the host
-  // ranges registered (pinned) for direct copies
+  // the System whose arrays past its particles were zeroed
   const System *zeroed = nullptr;
   int zeroed_n = 0, zeroed_max = 0;
-  const System *pinned = nullptr;
-  std::vector<void *> pinned_ranges;
   int pair_export = 2;  // uph_dropin_set_pair_export
+  // uph_dropin_set_callbacks; null: the libSPH functions linked with the caller
+  void (*inputbp)(System *, double) = nullptr;
+  void (*inoutflow)(System *) = nullptr;
 };
 
 DropIn g;
-
-void unpin_all()
-{
-  for (void *p : g.pinned_ranges) cudaHostUnregister(p);
-  g.pinned_ranges.clear();
-  g.pinned = nullptr;
-}
-
-// Page-locks the System arrays derivatives() copies to and from the device,
-// once per System: copies from page-locked memory go straight to the device
-// instead of through the driver's staging buffers.  A range that cannot be
-// registered (e.g. already registered by the caller) is copied as is.
-void pin_system(const System *sys)
-{
-  if (g.pinned == sys) return;
-  unpin_all();
-  g.pinned = sys;
-  const size_t M = (size_t)sys->MaxNumberOfParticles;
-  auto reg = [](void *p, size_t bytes) {
-    if (!p || bytes == 0) return;
-    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess)
-      g.pinned_ranges.push_back(p);
-    else
-      cudaGetLastError();  // clear the sticky error of a refused registration
-  };
-  for (double *v : {sys->Position[0], sys->Velocity[0], sys->localVelocity[0], sys->dvdt[0], sys->dvdt_approx[0],
-                    sys->velocityFluctuation[0], sys->dwcdx[0]})
-    reg(v, sizeof(double) * 2 * M);
-  for (double *v : {sys->density, sys->localDensity, sys->DynamicPressure, sys->localPressure, sys->mass,
-                    sys->spongeFactor, sys->ddensitydt, sys->dpdt, sys->ddensitydt_approx, sys->dpdt_approx,
-                    sys->densityFluctuation, sys->pressureFluctuation, sys->Pressure, sys->rij2, sys->w})
-    reg(v, sizeof(double) * M);
-  for (int *v : {sys->itype, sys->i_pair, sys->j_pair}) reg(v, sizeof(int) * M);
-}
 
 [[noreturn]] void die(const char *where, uph_status s)
 {
@@ -205,8 +171,15 @@ extern "C" void derivatives(System *sys, double t)
   g.zeroed = sys;
   g.zeroed_n = nall;
   g.zeroed_max = sys->MaxNumberOfParticles;
-  if (t > 0) inoutflow(sys);  // derivatives.c:3162-3164
-  inputbp(sys, t);            // derivatives.c:3168: re-reads the boundary decks, moves walls
+  void (*cb_inoutflow)(System *) = g.inoutflow ? g.inoutflow : inoutflow;
+  void (*cb_inputbp)(System *, double) = g.inputbp ? g.inputbp : inputbp;
+  if (!cb_inoutflow || !cb_inputbp) {
+    printf("derivatives: no inputbp()/inoutflow(): link the caller's libSPH or call uph_dropin_set_callbacks\n");
+    fflush(stdout);
+    exit(1);
+  }
+  if (t > 0) cb_inoutflow(sys);  // derivatives.c:3162-3164
+  cb_inputbp(sys, t);            // derivatives.c:3168: re-reads the boundary decks, moves walls
   // derivatives.c:3171-3182 only feeds inoutflow's inflow branch, whose
   // threshold (x > 5000.1, inoutflow.c:26) no deck reaches; it is not repeated.
   sys->inflowParticles = 0;
@@ -217,7 +190,6 @@ extern "C" void derivatives(System *sys, double t)
   const int n = nf + ns + nb;
   check_uniform(sys, n);
   ensure_sim(sys, n);
-  pin_system(sys);
 
   uph_state in;
   memset(&in, 0, sizeof in);
@@ -299,4 +271,10 @@ extern "C" int SearchNeighbors(const double **Position, int *i_pair, int *j_pair
 extern "C" void uph_dropin_set_pair_export(int level)
 {
   g.pair_export = level < 0 ? 0 : level > 2 ? 2 : level;
+}
+
+extern "C" void uph_dropin_set_callbacks(void (*inputbp_fn)(System *, double), void (*inoutflow_fn)(System *))
+{
+  g.inputbp = inputbp_fn;
+  g.inoutflow = inoutflow_fn;
 }

@@ -75,6 +75,15 @@ void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s)
 // sph.cc:137-168: the corrector with the rates just evaluated, then the
 // drift x += dt v.  With predict_next the predictor of the following step
 // runs right after.  Flags non-finite results.
+// A particle now at (x, y): raise the cell list's rebuild flag if it left
+// its skin since the last build, and report it if it left the domain (the
+// build, which also checks, may not run this step).
+__device__ __forceinline__ void note_moved(const DevParams &P, int slot, double x, double y, unsigned *err)
+{
+  if (P.rebuild && (fabs(x - P.xbin[slot]) > P.skin || fabs(y - P.ybin[slot]) > P.skin)) atomicOr(P.rebuild, 1u);
+  if (!(x >= P.lo_x && y >= P.lo_y && x <= P.hi_x && y <= P.hi_y)) atomicOr(err, ERR_OUT_OF_DOMAIN);
+}
+
 __global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, int predict_next, unsigned *err,
                           int *d_itime)
 {
@@ -115,6 +124,7 @@ __global__ void k_correct(const DevParams P, const SlotArrays S, int first_step,
   S.y[a] = y;
   if (!isfinite(rho) || !isfinite(p) || !isfinite(x) || !isfinite(y) || !isfinite(u) || !isfinite(v))
     atomicOr(err, ERR_NAN);
+  note_moved(P, a, x, y, err);
   if (predict_next) {
     predict_one(P, S, a, rho, p, u, v);
   } else {
@@ -166,11 +176,16 @@ void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, 
 // their slot's reference index.
 //  - inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
 //    x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt;
+//  - inputbp.c:209-223 (movingBoundary 3, the lid): x = x0 + U t,
+//    u = ut = U, from each particle's base x0;
+//  - inputbp.c:224-243 (movingBoundary 2, the gate): y = y0 + U t and
+//    v = U while 0 < t < t_stop, else y = y0 + U t_stop and v = 0 (the
+//    reference leaves the gate's local velocity alone);
 //  - a WallTable shakes each particle about its own rest position with its
 //    own half stroke and frequency (one entry per particle, e.g. every wall
 //    of a sloshing tank moving rigidly).
 __global__ void k_wall_motion(const DevParams P, const SlotArrays S, const WallTable W, double t_host,
-                              const int *d_itime)
+                              const int *d_itime, unsigned *err)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = P.nf + k;
@@ -178,6 +193,29 @@ __global__ void k_wall_motion(const DevParams P, const SlotArrays S, const WallT
   const int o = S.orig[s];
   if (o < P.m0 || o >= P.b1) return;
   const double t = d_itime ? (*d_itime + 1) * P.dt : t_host;
+  if (!W.enabled && P.moving_boundary == 3) {
+    const double U = P.lid_velocity;
+    const double x = U * t + W.base[o - P.m0];
+    S.x[s] = x;
+    S.u[s] = U;
+    S.ut[s] = U;
+    note_moved(P, s, x, S.y[s], err);
+    return;
+  }
+  if (!W.enabled && P.moving_boundary == 2) {
+    const double U = P.lid_velocity;
+    double y;
+    if (t > 0.0 && t < P.gate_stop) {
+      y = U * t + W.base[o - P.m0];
+      S.v[s] = U;
+    } else {
+      y = U * P.gate_stop + W.base[o - P.m0];
+      S.v[s] = 0.0;
+    }
+    S.y[s] = y;
+    note_moved(P, s, S.x[s], y, err);
+    return;
+  }
   double x, u;
   if (W.enabled) {
     const int m = o - P.m0;
@@ -191,13 +229,14 @@ __global__ void k_wall_motion(const DevParams P, const SlotArrays S, const WallT
   S.x[s] = x;
   S.u[s] = u;
   S.ut[s] = u;
+  note_moved(P, s, x, S.y[s], err);
 }
 
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
-                        const int *d_itime, cudaStream_t s)
+                        const int *d_itime, unsigned *err, cudaStream_t s)
 {
   const int n = P.n - P.nf;
-  if (n > 0) k_wall_motion<<<(n + 255) / 256, 256, 0, s>>>(P, S, W, t_host, d_itime);
+  if (n > 0) k_wall_motion<<<(n + 255) / 256, 256, 0, s>>>(P, S, W, t_host, d_itime, err);
 }
 
 // EquationOfState for the non-fluid slots (derivatives.c:1674-1682); their

@@ -118,14 +118,18 @@ __device__ __forceinline__ void wall_pair_force(const DevParams &P, int itb, dou
 struct __align__(16) RefRec {
   double x, y, u, v, ut, vt, rho, rhot, p, pt, m, ir, irt, P, ir2, C, V;
   int orig, itype;
+  float xr, yr;  // position relative to the CTA's block origin, for the listing's FP32 pre-test
 };
-static_assert(sizeof(RefRec) == 144, "RefRec is nine 16-byte chunks");
+static_assert(sizeof(RefRec) == 160, "RefRec is ten 16-byte chunks");
 
-__device__ __forceinline__ RefRec load_ref_rec(const DevParams &P, const SlotArrays &S, int s)
+__device__ __forceinline__ RefRec load_ref_rec(const DevParams &P, const SlotArrays &S, int s, double ox = 0.0,
+                                               double oy = 0.0)
 {
   RefRec r;
   r.x = S.x[s];
   r.y = S.y[s];
+  r.xr = (float)(r.x - ox);
+  r.yr = (float)(r.y - oy);
   r.u = S.u[s];
   r.v = S.v[s];
   r.ut = S.ut[s];
@@ -288,6 +292,7 @@ struct StagedSrc {
   const double *cut_d2;  // the knn cap's cut per record (kKnn only)
   const int *cut_j;
   __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
+  __device__ __forceinline__ float2 xyf(int k) const { return *reinterpret_cast<const float2 *>(&rec[k].xr); }
   __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
   __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
   __device__ __forceinline__ RefRec get(int k) const { return rec[k]; }
@@ -302,6 +307,7 @@ struct GlobalSrc {
   DevParams P;
   SlotArrays S;
   __device__ __forceinline__ double2 xy(int s) const { return make_double2(S.x[s], S.y[s]); }
+  __device__ __forceinline__ float2 xyf(int) const { return make_float2(0.f, 0.f); }  // not used: no pre-test
   __device__ __forceinline__ int orig(int s) const { return S.orig[s]; }
   __device__ __forceinline__ double mass(int s) const { return S.m[s]; }
   __device__ __forceinline__ RefRec get(int s) const { return load_ref_rec(P, S, s); }
@@ -312,17 +318,17 @@ struct GlobalSrc {
   }
 };
 // Phase 1 and 2 for one own particle until its stencil is exhausted.
-template <bool kBrute, bool kKnn, typename Src, typename Cursor, typename Entry>
+template <bool kBrute, bool kKnn, bool kF32, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ void ref_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
-                                             const RefOwn &o, Entry *s_nb, RefAcc &A, double &bx, double &by,
-                                             unsigned &my_pairs, int &my_nb, double cd, int cj)
+                                             const RefOwn &o, const F32Test &ft, Entry *s_nb, RefAcc &A, double &bx,
+                                             double &by, unsigned &my_pairs, int &my_nb, double cd, int cj)
 {
   constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
   const int col = threadIdx.x;
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
-    const int cnt = tile_list<kBrute, kTileChunk, kKnn>(P, src, cur, more, self, o.r.orig, o.r.x, o.r.y, s_nb, col,
-                                                        my_pairs, my_nb, bx, by, cd, cj);
+    const int cnt = tile_list<kBrute, kTileChunk, kKnn, kF32>(P, src, cur, more, self, o.r.orig, o.r.x, o.r.y, ft,
+                                                              s_nb, col, my_pairs, my_nb, bx, by, cd, cj);
     __syncwarp();
     for (int e = 0; e < cnt; e++) {
       const Entry ent = s_nb[e * kTileThreads + col];
@@ -336,14 +342,14 @@ __device__ __forceinline__ void ref_particle(const DevParams &P, const Src &src,
 // Dynamic shared memory of the tiled pass and its record capacity; with the
 // knn cap every record also carries its query's cut (12 bytes).
 template <bool kKnn>
-__host__ __device__ constexpr int ref_rec_cap() { return kKnn ? 560 : 640; }
+__host__ __device__ constexpr int ref_rec_cap() { return kKnn ? 540 : 600; }
 constexpr size_t kRefListBytes = sizeof(unsigned short) * kTileChunk * kTileThreads;
 template <bool kKnn>
 constexpr size_t ref_smem()
 {
   return sizeof(TileBlock) + kRefListBytes + (sizeof(RefRec) + (kKnn ? 12 : 0)) * ref_rec_cap<kKnn>();
 }
-static_assert(sizeof(RefRec) * 560 >= sizeof(unsigned) * kTileChunk * kTileThreads,
+static_assert(sizeof(RefRec) * 540 >= sizeof(unsigned) * kTileChunk * kTileThreads,
               "the fallback's 32-bit lists live in the record area");
 
 // One CTA per storage tile (see tile_pass.cuh).  Phase 1 lists in-radius
@@ -368,12 +374,14 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
   const int ncore = B.ncore;
   if (ncore == 0) return;
   const bool staged = B.nrec <= kCap;
+  // the origin of the block: the listing's FP32 positions are relative to it
+  const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
   unsigned my_pairs = 0;
-  int my_nb = 0;
+  int my_nb = 0;  // largest in-radius count of this thread's particles
   if (staged) {
     for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
       const int slot = G.list[tile_record_pos(B, k)];
-      rec[k] = load_ref_rec(P, S, slot);
+      rec[k] = load_ref_rec(P, S, slot, ox, oy);
       if constexpr (kKnn) {
         // only fluid queries have a cut; other records are never a pair's i
         // seen from a fluid particle that is its j
@@ -398,9 +406,12 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
       double cd = 0.0;
       int cj = 0;
       if (kKnn && active) src.cut(kr, cd, cj);
+      const F32Test ft = make_f32_test(P, B, o.r.xr, o.r.yr);
       RefAcc A = {};
       double bx = 0.0, by = 0.0;
-      ref_particle<kBrute, kKnn>(P, src, cur, active, kr, o, s_nb16, A, bx, by, my_pairs, my_nb, cd, cj);
+      int nb = 0;
+      ref_particle<kBrute, kKnn, true>(P, src, cur, active, kr, o, ft, s_nb16, A, bx, by, my_pairs, nb, cd, cj);
+      my_nb = max(my_nb, nb);
       if (active) ref_epilogue(P, S, a, o, A, bx, by);
     }
   } else {
@@ -423,9 +434,12 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
       double cd = 0.0;
       int cj = 0;
       if (kKnn && active) src.cut(as, cd, cj);
+      const F32Test ft = {};
       RefAcc A = {};
       double bx = 0.0, by = 0.0;
-      ref_particle<kBrute, kKnn>(P, src, cur, active, as, o, s_nb32, A, bx, by, my_pairs, my_nb, cd, cj);
+      int nb = 0;
+      ref_particle<kBrute, kKnn, false>(P, src, cur, active, as, o, ft, s_nb32, A, bx, by, my_pairs, nb, cd, cj);
+      my_nb = max(my_nb, nb);
       if (active) ref_epilogue(P, S, a, o, A, bx, by);
     }
   }

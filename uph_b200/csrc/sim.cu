@@ -29,7 +29,10 @@ namespace uph {
 
 namespace {
 
-constexpr int kReorderInterval = 16;
+// Storage re-sorts keep a tile's particles in nearby slots; the tiled
+// passes find particles through the cell list, so a stale order only costs
+// coalescing.
+constexpr int kReorderInterval = 64;
 constexpr int kErrorCheckInterval = 64;
 constexpr int kCellReach = 2;
 
@@ -295,6 +298,31 @@ __global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ pe
   }
 }
 
+bool p_lid_or_gate(const DevParams &P)
+{
+  return (P.moving_boundary == 2 || P.moving_boundary == 3) && P.flag_init_simul == 1;
+}
+
+// The base coordinate of the lid (x, movingBoundary 3) or gate (y,
+// movingBoundary 2) particles, per reference index - m0, such that the wall
+// law at the upload's time t0 reproduces the uploaded position; at t0 = 0 (a
+// fresh deck) the base is the position itself, as the reference's
+// tempPosition / tempPositionGate columns are for its decks.
+__global__ void k_wall_base(DevParams P, SlotArrays S, double *base, double t0)
+{
+  const int s = P.nf + blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.n) return;
+  const int o = S.orig[s];
+  if (o < P.m0 || o >= P.b1) return;
+  const double U = P.lid_velocity;
+  double b;
+  if (P.moving_boundary == 3)
+    b = S.x[s] - U * t0;
+  else
+    b = S.y[s] - (t0 <= 0.0 ? 0.0 : U * fmin(t0, P.gate_stop));
+  base[o - P.m0] = b;
+}
+
 __global__ void k_iota(int *p, int first, int count)
 {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -316,7 +344,17 @@ uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, i
 uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr)
 {
   Timer t(s, KF_CELLS);
-  return sort_range(s, s->S.x, s->S.y, 0, s->P.n, false, stats);
+  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, stats, s->stream, true);
+  s->launches += 1;
+  return r;
+}
+
+// the next cell-list build must bin every particle afresh (positions or
+// slots changed outside the leapfrog)
+uph_status force_rebuild(uph_sim *s)
+{
+  UPH_CUDA(cudaMemsetAsync(s->P.rebuild, 1, sizeof(unsigned), s->stream));
+  return UPH_OK;
 }
 
 uph_status reorder_fluid(uph_sim *s)
@@ -333,7 +371,7 @@ uph_status reorder_fluid(uph_sim *s)
   s->S = s->S2;
   s->S2 = tmp;
   s->steps_since_reorder = 0;
-  return UPH_OK;
+  return force_rebuild(s);
 }
 
 uph_status check_error_word(uph_sim *s)
@@ -450,7 +488,7 @@ void set_grid_geometry(DevParams &P, int reach, int tile)
 {
   P.reach = reach;
   P.tile = tile;
-  double cell = sqrt(P.r2cut) / P.reach * (1.0 + 1e-9);
+  double cell = sqrt(P.r2cut) / P.reach * (1.0 + kCellSkin) * (1.0 + 1e-9);
   double tiles_x, tiles_y;
   for (int grow = 0; grow < 200; grow++) {  // finite domains (validate) end in a few rounds
     const double nx = ceil((P.hi_x - P.lo_x) / cell);
@@ -462,6 +500,9 @@ void set_grid_geometry(DevParams &P, int reach, int tile)
   }
   P.cell = cell;
   P.inv_cell = 1.0 / cell;
+  // a pair within the radius stays within `reach` cells of where both were
+  // binned while each moved at most (reach cell - radius) / 2 per axis
+  P.skin = 0.5 * (P.reach * cell * (1.0 - 1e-9) - sqrt(P.r2cut));
   P.ntx = (int)tiles_x;
   P.ncx = P.ntx * tile;
   P.ncy = (int)tiles_y * tile;
@@ -513,6 +554,9 @@ DevParams make_dev_params(const uph_params *p)
   P.wave_absorption = p->wave_absorption;
   P.stroke = p->stroke;
   P.omega = p->omega;
+  P.lid_velocity = p->lid_velocity;
+  // inputbp.c:226 (a zero speed never starts the gate: stop at t = 0)
+  P.gate_stop = p->lid_velocity != 0.0 ? 1.5 * (p->local_depth - 15.0 * p->dx) / p->lid_velocity : 0.0;
   P.av_alpha_c0 = p->av_alpha * p->speed_of_sound;
   P.dt = p->time_step;
   P.lo_x = p->domain_lo[0];
@@ -521,16 +565,19 @@ DevParams make_dev_params(const uph_params *p)
   P.hi_y = p->domain_hi[1];
   // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
   // against 36 h^2 for a 3 x 3 block of radius-wide cells.  A cell then holds
-  // about (h / dx)^2 particles of a lattice; the default tile (12 cells at
-  // h = 1.3 dx) shrinks for wider kernels so a tile's block stays within the
-  // tiled passes' shared-memory records.
+  // about ((1 + skin) h / dx)^2 particles of a lattice; the default tile (10
+  // cells at h = 1.3 dx) shrinks for wider kernels so that a tile's
+  // particles fit one round of a CTA and its block the tiled passes'
+  // shared-memory records.
   int tile = kCellTile;
   const double hdx = p->dx > 0 ? h / p->dx : 1.0;
-  if (hdx > 1.6) tile = std::max(2, (int)floor(kCellTile * 1.3 / hdx) - 1);
+  if (hdx > 1.4) tile = std::max(2, (int)floor(kCellTile * 1.3 / hdx));
   set_grid_geometry(P, kCellReach, tile);
   P.knn = p->knn_cap;
   P.kcut_d2 = nullptr;
   P.kcut_j = nullptr;
+  P.xbin = P.ybin = nullptr;
+  P.rebuild = nullptr;
   return P;
 }
 
@@ -573,6 +620,10 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
     TRY(dalloc(s, &s->P.kcut_d2, (size_t)nf));
     TRY(dalloc(s, &s->P.kcut_j, (size_t)nf));
   }
+  TRY(dalloc(s, &s->P.xbin, (size_t)n));
+  TRY(dalloc(s, &s->P.ybin, (size_t)n));
+  TRY(dalloc(s, &s->P.rebuild, 1));
+  TRY(cudaMemset(s->P.rebuild, 1, sizeof(unsigned)));
   TRY(dalloc(s, &G.rank, (size_t)n));
   TRY(dalloc(s, &G.totals, (size_t)kCellBuildMaxBlocks + 1));
   TRY(dalloc(s, &G.bar, 2));
@@ -593,7 +644,8 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &s->d_max_nb, 1));
   TRY(dalloc(s, &s->d_perm, (size_t)n));
   TRY(dalloc(s, &s->d_itime, 1));
-  TRY(dalloc(s, &s->d_wall_tab, 3 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
+  TRY(dalloc(s, &s->d_wall_tab, 4 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
+  s->W.base = s->d_wall_tab + 3 * (size_t)(p->n_moving > 0 ? p->n_moving : 1);
   s->n_partials = 1024;
   TRY(dalloc(s, &s->d_partials, (size_t)s->n_partials * 4));
   {
@@ -719,10 +771,18 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
   k_gather_upload<<<(n + 255) / 256, 256, 0, q>>>(s->S, T, s->d_perm, n, nf, s->P.rho0);
   launch_refresh_inverse(s->P, s->S, 0, n, q);
   launch_wall_pressure(s->P, s->S, q);
+  if (p_lid_or_gate(s->P) && s->hp.n_moving > 0) {
+    // the lid's / gate's base coordinates from the uploaded positions
+    const int nw = n - nf;
+    k_wall_base<<<(nw + 255) / 256, 256, 0, q>>>(s->P, s->S, const_cast<double *>(s->W.base), itime * s->P.dt);
+    s->launches++;
+  }
   s->launches += 3;
   s->itime = itime;
   UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, q));
   s->steps_since_reorder = 0;
+  r = force_rebuild(s);
+  if (r != UPH_OK) return r;
   s->have_rates = false;
   s->restart = false;
   return check_error_word(s);
@@ -767,7 +827,8 @@ namespace {
 
 bool walls_move(const uph_sim *s)
 {
-  return s->hp.n_moving > 0 && (s->W.enabled || (s->P.moving_boundary == 1 && s->P.flag_init_simul == 1));
+  const int mb = s->P.moving_boundary;
+  return s->hp.n_moving > 0 && (s->W.enabled || ((mb == 1 || mb == 2 || mb == 3) && s->P.flag_init_simul == 1));
 }
 
 // Enqueues `nsteps` leapfrog steps on the sim's stream.  With `capturing`
@@ -792,7 +853,7 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
     }
     if (moving) {
       Timer tm(s, KF_WALLS);
-      launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->stream);
+      launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->d_err, s->stream);
       s->launches++;
     }
     uph_status r = rate_pass(s, first);
@@ -919,13 +980,25 @@ extern "C" uph_status uph_sim_set_wall_motion(uph_sim *s, const double *x0, cons
   return UPH_OK;
 }
 
+extern "C" uph_status uph_sim_set_wall_base(uph_sim *s, const double *base)
+{
+  if (!s || !base) return fail(UPH_BAD_ARG, "uph_sim_set_wall_base: NULL argument");
+  const int nm = s->hp.n_moving;
+  if (nm <= 0) return fail(UPH_BAD_ARG, "uph_sim_set_wall_base: the sim has no moving boundary particles");
+  UPH_CUDA(cudaMemcpyAsync(const_cast<double *>(s->W.base), base, sizeof(double) * nm, cudaMemcpyHostToDevice,
+                           s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  drop_graph(s);
+  return UPH_OK;
+}
+
 extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
 {
   if (!s) return fail(UPH_BAD_ARG, "NULL sim");
   // the piston position is a closed form of t, so applying it again after the
   // caller's own inputbp() changes nothing
   if (walls_move(s)) {
-    launch_wall_motion(s->P, s->S, s->W, t, nullptr, s->stream);
+    launch_wall_motion(s->P, s->S, s->W, t, nullptr, s->d_err, s->stream);
     s->launches++;
   }
   uph_status r = rate_pass(s, true);
@@ -1326,7 +1399,7 @@ uph_status time_steps(uph_sim *s, int steps, double *ms)
 }  // namespace
 
 // Coordinate search over (cell reach, storage tile, re-sort interval): the
-// reach first with tile 12 and interval 16, then the tile at the best reach,
+// reach first with tile 10 and interval 64, then the tile at the best reach,
 // then the interval.  Each trial times `trial_steps` steps of this very
 // simulation, so tuning advances it by about 9 (trial_steps + 2) steps.
 // Results are cached per size class (profile, precision, log2 of the fluid
@@ -1358,7 +1431,7 @@ extern "C" uph_status uph_sim_autotune(uph_sim *s, int32_t trial_steps, int32_t 
     };
     best_ms = 1e300;
     for (int axis = 0; axis < 3; axis++) {
-      static const int options[3][3] = {{1, 2, 3}, {8, 12, 16}, {8, 16, 32}};
+      static const int options[3][3] = {{1, 2, 3}, {8, 10, 12}, {16, 64, 256}};
       std::array<int, 3> axis_best = best;
       for (int v : options[axis]) {
         std::array<int, 3> c = best;
@@ -1488,7 +1561,8 @@ extern "C" uph_status uph_search_neighbors(const double *position, int32_t n_flu
     return fail(UPH_CUDA_ERROR, "uph_search_neighbors: upload failed");
   }
   k_load_positions<<<(n_all + 255) / 256, 256, 0, q>>>(s->S, dpos, n_all);
-  r = build_cell_list(s);
+  r = force_rebuild(s);
+  if (r == UPH_OK) r = build_cell_list(s);
   // an overcrowded cell (or a position outside the grid) stops here, before
   // any kernel walks the candidates
   if (r == UPH_OK) r = check_error_word(s);
@@ -1525,10 +1599,14 @@ uph_status sim_jump(uph_sim *s, int nsteps)
   UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, s->stream));
   // the moving walls at the new time, as after a step that ended there
   if (walls_move(s)) {
-    launch_wall_motion(s->P, s->S, s->W, s->itime * s->P.dt, nullptr, s->stream);
+    launch_wall_motion(s->P, s->S, s->W, s->itime * s->P.dt, nullptr, s->d_err, s->stream);
     s->launches++;
   }
   s->restart = true;
+  {
+    uph_status r = force_rebuild(s);
+    if (r != UPH_OK) return r;
+  }
   // the storage re-sort waits for the next plain step (the state moves
   // about 0.1 dx per jump, so the slot order stays spatially coherent)
   s->steps_since_reorder += nsteps;

@@ -172,20 +172,45 @@ struct StagedCursor {
   __device__ __forceinline__ int at(int pos) const { return pos; }
 };
 
+// The single-precision pre-test of phase 1: positions relative to the CTA's
+// block origin in FP32 (exact enough to decide every candidate whose r^2 is
+// not within a relative `band` of the cut-off), the exact FP64 test only
+// for the rest.  `band` bounds the FP32 error of r^2 relative to the cut-off
+// with a wide margin: the block spans E = max(W, H) cells, so each relative
+// coordinate carries at most E cell 2^-24 of rounding and r^2 at most
+// 4 R E cell 2^-24 + R^2 2^-23; band = 32 (E cell / R) 2^-23 + 2^-20.
+struct F32Test {
+  float xa, ya;  // own position relative to the origin
+  float lo, hi;  // r2cut (1 -+ band): surely inside below lo, surely outside above hi
+  float tiny;    // below this, r^2 may be at the DBL_EPSILON coincidence test: exact
+};
+
+__device__ __forceinline__ F32Test make_f32_test(const DevParams &P, const TileBlock &B, float xa, float ya)
+{
+  const double R = sqrt(P.r2cut);
+  const double E = (double)max(B.W, B.H) * P.cell;
+  const double band = 32.0 * (E / R) * 0x1p-23 + 0x1p-20;
+  return F32Test{xa, ya, (float)(P.r2cut * (1.0 - band)), (float)(P.r2cut * (1.0 + band)),
+                 (float)(P.r2cut * 1e-3)};
+}
+
 // Phase 1 of a rate pass: lists up to kChunk in-radius partners of the own
 // particle (index `self` in the source) into column `col` of s_nb (row
 // stride kTileThreads), four candidates at a time, each entry the partner's
 // index with the role flag set when the own particle is the pair's i.  A
 // partner is in-radius and in the reference's pair list exactly as in
-// list_partners (pass_common.cuh).  The brute-force wall modes see every
-// in-radius boundary candidate.  The source gives xy(k), orig(k), mass(k).
+// list_partners (pass_common.cuh): the decision is always the exact FP64
+// predicate; with kF32 the FP32 pre-test (F32Test) settles the candidates
+// far from the cut-off and the FP64 r^2 is computed only near it.  The
+// brute-force wall modes see every in-radius boundary candidate.  The source
+// gives xy(k), xyf(k) (kF32), orig(k), mass(k).
 // kKnn: the reference's k-nearest cap (DevParams::knn): a pair is kept iff
 // the partner is among query i's kept points -- the own particle's cut
 // (cd, cj) when it is i, the partner's (src.cut(b)) when the partner is i.
-template <bool kBrute, int kChunk, bool kKnn = false, typename Src, typename Cursor, typename Entry>
+template <bool kBrute, int kChunk, bool kKnn, bool kF32, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cursor &cur, bool &more, int self,
-                                        int oa, double xa, double ya, Entry *s_nb, int col, unsigned &my_pairs,
-                                        int &my_nb, double &bx, double &by, double cd = 0.0, int cj = 0)
+                                        int oa, double xa, double ya, const F32Test &ft, Entry *s_nb, int col,
+                                        unsigned &my_pairs, int &my_nb, double &bx, double &by, double cd, int cj)
 {
   constexpr int kB = 4;
   constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
@@ -198,20 +223,39 @@ __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cur
       break;
     }
     int b[kB];
-    double2 q[kB];
 #pragma unroll
     for (int u = 0; u < kB; u++) b[u] = (u < n) ? cur.at(pos + u) : self;
+    bool sure[kB];  // FP32 says: surely inside and not coincident
+    if constexpr (kF32) {
+      float2 f[kB];
 #pragma unroll
-    for (int u = 0; u < kB; u++) q[u] = src.xy(b[u]);
+      for (int u = 0; u < kB; u++) f[u] = src.xyf(b[u]);
+#pragma unroll
+      for (int u = 0; u < kB; u++) {
+        const float dxf = ft.xa - f[u].x, dyf = ft.ya - f[u].y;
+        const float r2f = fmaf(dxf, dxf, dyf * dyf);
+        if (r2f > ft.hi) b[u] = self;  // surely outside: drop
+        sure[u] = r2f < ft.lo && r2f > ft.tiny;
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < kB; u++) sure[u] = false;
+    }
 #pragma unroll
     for (int u = 0; u < kB; u++) {
       if (b[u] == self) continue;
-      const double dxa = xa - q[u].x, dya = ya - q[u].y;
-      const double r2 = exact_r2(dxa, dya);
-      if (!(r2 < P.r2cut)) continue;
+      double r2 = 0.0, dxa = 0.0, dya = 0.0;
+      const bool exact = !sure[u] || kBrute || kKnn;
+      if (exact) {
+        const double2 q = src.xy(b[u]);
+        dxa = xa - q.x;
+        dya = ya - q.y;
+        r2 = exact_r2(dxa, dya);
+        if (!(r2 < P.r2cut)) continue;
+      }
       const int ob = src.orig(b[u]);
       if (kBrute && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, src.mass(b[u]), bx, by);
-      if (r2 <= DBL_EPSILON) continue;
+      if (exact && r2 <= DBL_EPSILON) continue;
       my_nb++;
       if (max(oa, ob) >= P.pb) continue;
       const bool isI = ob > oa;

@@ -76,6 +76,8 @@ struct DevParams {
   double lj_coeff, mach_c;  // LennardCoefficient, machNumber * SpeedOfSound
   int moving_boundary, flag_init_simul, wave_absorption;
   double stroke, omega;
+  double lid_velocity;  // lidVelocity: the lid (movingBoundary 3) and gate (2) speed
+  double gate_stop;     // the gate stops at 1.5 (LocalDepth - 15 dx) / lidVelocity (inputbp.c:226)
   double av_alpha_c0;       // WCSPH: alpha * c0
   double dt;
   // cell grid
@@ -93,7 +95,17 @@ struct DevParams {
   int knn;
   double *kcut_d2;
   int *kcut_j;
+  // Skin of the cell list: cells are (1 + kCellSkin) radius / reach wide, so
+  // the list stays complete while no particle has moved more than `skin`
+  // (per axis) from where the last build binned it (xbin, ybin by slot).
+  // The corrector and the wall motion raise *rebuild when one has; the
+  // build kernel skips its work while *rebuild is 0.
+  double skin;
+  double *xbin, *ybin;
+  unsigned *rebuild;
 };
+
+constexpr double kCellSkin = 0.1;
 
 constexpr int kKnnMax = 64;  // largest knn cap the kernels keep per query
 
@@ -109,9 +121,10 @@ __host__ __device__ __forceinline__ bool knn_key_le(double r2, int j, double cd,
 // tile, tiles row-major, cells inside a tile row-major.  The REF rate pass
 // runs one CTA per tile (tile_pass.cuh), so a tile's fluid particles are
 // nearly contiguous slots.  The tile edge is a tuning parameter
-// (DevParams::tile, default 12: 144 half-radius cells hold about 240
-// particles of a lattice at h = 1.3 dx, one per thread of a 256-thread CTA).
-constexpr int kCellTile = 12;
+// (DevParams::tile, default 10: 100 cells of (1 + skin) h hold about 205
+// particles of a lattice at h = 1.3 dx, one per thread of a 256-thread CTA,
+// with room for compression before a second round of the CTA is needed).
+constexpr int kCellTile = 10;
 
 __host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx, int tile)
 {
@@ -125,6 +138,9 @@ __host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx, int
 struct WallTable {
   const double *x0, *hs, *om;
   int enabled;
+  // the lid's and the gate's per-particle base coordinate (the reference's
+  // tempPosition / tempPositionGate), indexed by reference index - m0
+  const double *base;
 };
 
 struct CellGrid {
@@ -173,8 +189,11 @@ void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s)
 constexpr int kCellBuildThreads = 512;
 constexpr int kCellBuildMaxBlocks = 1024;
 struct PassStats;
+// check_rebuild: build only when *P.rebuild is set (and then clear it and
+// record the binned positions); otherwise always build.
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s);
+                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s,
+                             bool check_rebuild = false);
 
 // REF / WCSPH rate pass over the fluid slots
 struct PassStats {
@@ -195,7 +214,7 @@ void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, 
 // counter lives on the device so CUDA-graph replays see the right time),
 // else t = t_host
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
-                        const int *d_itime, cudaStream_t s);
+                        const int *d_itime, unsigned *err, cudaStream_t s);
 void launch_wall_pressure(const DevParams &P, const SlotArrays &S, cudaStream_t s);
 
 // BF16 tcgen05 GEMM, C[M x N] = A . B^T with FP32 accumulation.  An operand

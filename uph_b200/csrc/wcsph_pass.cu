@@ -24,20 +24,6 @@
 
 namespace uph {
 
-template <typename Real>
-__device__ __forceinline__ Real rcp_real(Real x);
-template <>
-__device__ __forceinline__ double rcp_real<double>(double x) { return rcp_nr(x); }
-template <>
-__device__ __forceinline__ float rcp_real<float>(float x) { return __frcp_rn(x); }
-
-template <typename Real>
-__device__ __forceinline__ Real sqrt_real(Real x);
-template <>
-__device__ __forceinline__ double sqrt_real<double>(double x) { return sqrt(x); }
-template <>
-__device__ __forceinline__ float sqrt_real<float>(float x) { return __fsqrt_rn(x); }
-
 // selectBoundaryForce modes that act on listed pairs (i side = this fluid particle)
 __device__ __forceinline__ void wcsph_wall_pair(const DevParams &P, int itb, double r2d, double dxd, double dyd,
                                                 double dud, double dvd, double ma, double &wx, double &wy)
@@ -69,19 +55,30 @@ __device__ __forceinline__ void wcsph_wall_pair(const DevParams &P, int itb, dou
   }
 }
 
-// One staged particle.  Positions, velocities and the mass stay FP64 (the
-// exact pair test, the FP64 differences and the FP64 wall forces need them);
-// m, p / rho^2 and rho as the pair arithmetic reads them, in Real (for FP32,
-// rounded once from FP64 -- the values of SlotArrays::pk).
+// One staged particle.  FP64 position, velocity and mass always (the exact
+// pair test and the FP64 wall forces need them); the pair arithmetic's
+// operands in Real: for FP32, the position relative to the CTA's block
+// origin and the velocity, and m, p / rho^2 and rho rounded once from FP64,
+// so the pair loop runs in FP32 without a per-pair FP64 difference.
 template <typename Real>
-struct __align__(16) WcRec {
+struct WcRec;
+template <>
+struct __align__(16) WcRec<double> {
+  double x, y, u, v, m, A1, rho;
+  int orig, itype;
+  float xr, yr;  // relative position for the listing's FP32 pre-test
+};
+template <>
+struct __align__(16) WcRec<float> {
   double x, y, u, v, m;
-  Real mr, A1, rho;
+  float xr, yr, ur, vr, mr, A1, rho;
   int orig, itype;
 };
+static_assert(sizeof(WcRec<double>) == 80 && sizeof(WcRec<float>) == 80, "record sizes");
 
+// (ox, oy): the origin FP32 positions are taken relative to
 template <typename Real>
-__device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s)
+__device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s, double ox, double oy)
 {
   WcRec<Real> r;
   r.x = S.x[s];
@@ -90,9 +87,15 @@ __device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s)
   r.v = S.v[s];
   r.m = S.m[s];
   const double ir = S.inv_rho[s];
-  r.mr = (Real)r.m;
   r.A1 = (Real)(S.p[s] * ir * ir);
   r.rho = (Real)S.rho[s];
+  r.xr = (float)(r.x - ox);
+  r.yr = (float)(r.y - oy);
+  if constexpr (sizeof(Real) == sizeof(float)) {
+    r.ur = (float)r.u;
+    r.vr = (float)r.v;
+    r.mr = (float)r.m;
+  }
   r.orig = S.orig[s];
   r.itype = S.itype[s];
   return r;
@@ -102,6 +105,7 @@ template <typename Real>
 struct WcStagedSrc {
   const WcRec<Real> *rec;
   __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
+  __device__ __forceinline__ float2 xyf(int k) const { return make_float2(rec[k].xr, rec[k].yr); }
   __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
   __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
   __device__ __forceinline__ WcRec<Real> get(int k) const { return rec[k]; }
@@ -109,10 +113,12 @@ struct WcStagedSrc {
 template <typename Real>
 struct WcGlobalSrc {
   SlotArrays S;
+  double ox, oy;
   __device__ __forceinline__ double2 xy(int s) const { return make_double2(S.x[s], S.y[s]); }
+  __device__ __forceinline__ float2 xyf(int) const { return make_float2(0.f, 0.f); }  // not used: no pre-test
   __device__ __forceinline__ int orig(int s) const { return S.orig[s]; }
   __device__ __forceinline__ double mass(int s) const { return S.m[s]; }
-  __device__ __forceinline__ WcRec<Real> get(int s) const { return load_wc_rec<Real>(S, s); }
+  __device__ __forceinline__ WcRec<Real> get(int s) const { return load_wc_rec<Real>(S, s, ox, oy); }
 };
 
 struct WcAcc {
@@ -127,45 +133,73 @@ __device__ __forceinline__ void wc_pair(const DevParams &P, const WcRec<Real> &a
   const Real h = (Real)P.h, inv_h = (Real)P.inv_h, inv_h2 = (Real)P.inv_h2;
   const Real sigma = (Real)P.cs_alpha;
   const Real eta2 = (Real)P.eta2, ac = (Real)P.av_alpha_c0;
-  const double dxd = a.x - b.x, dyd = a.y - b.y;
-  const double dud = a.u - b.u, dvd = a.v - b.v;
-  const Real dx = (Real)dxd, dy = (Real)dyd, du = (Real)dud, dv = (Real)dvd;
-  const Real mb = b.mr;
+  Real dx, dy, du, dv, mb, r, inv_r;
+  if constexpr (sizeof(Real) == sizeof(float)) {
+    // FP32 throughout: block-relative positions, approximate square root
+    // and reciprocals (MUFU), errors far below the FP32 sums'
+    dx = a.xr - b.xr;
+    dy = a.yr - b.yr;
+    du = a.ur - b.ur;
+    dv = a.vr - b.vr;
+    mb = b.mr;
+  } else {
+    dx = a.x - b.x;
+    dy = a.y - b.y;
+    du = a.u - b.u;
+    dv = a.v - b.v;
+    mb = b.m;
+  }
   const Real r2 = dx * dx + dy * dy;
-  const Real r = sqrt_real<Real>(r2);
+  if constexpr (sizeof(Real) == sizeof(float)) {
+    inv_r = r2 > 0.0f ? rsqrtf(r2) : 0.0f;
+    r = r2 * inv_r;
+  } else {
+    r = sqrt(r2);
+  }
   const Real q = r * inv_h;
   Real F;
   if (q < (Real)1) {
     F = sigma * ((Real)-3 + (Real)2.25 * q) * inv_h2;
   } else {
     const Real t = (Real)2 - q;
-    F = -sigma * (Real)0.75 * t * t * inv_h * rcp_real<Real>(r);
+    if constexpr (sizeof(Real) == sizeof(float))
+      F = -sigma * 0.75f * t * t * inv_h * inv_r;
+    else
+      F = -sigma * 0.75 * t * t * inv_h * rcp_nr(r);
   }
   const Real gx = F * dx, gy = F * dy;
   drho += mb * (du * gx + dv * gy);
   const Real vr = du * dx + dv * dy;
   Real pi_ab = 0;
   if (vr < (Real)0) {
-    const Real mu = h * vr * rcp_real<Real>(r2 + eta2);
-    pi_ab = -ac * mu * rcp_real<Real>((Real)0.5 * (a.rho + b.rho));
+    if constexpr (sizeof(Real) == sizeof(float)) {
+      const float mu = h * vr * __fdividef(1.0f, r2 + eta2);
+      pi_ab = -ac * mu * __fdividef(2.0f, a.rho + b.rho);
+    } else {
+      const double mu = h * vr * rcp_nr(r2 + eta2);
+      pi_ab = -ac * mu * rcp_nr(0.5 * (a.rho + b.rho));
+    }
   }
   const Real pij = a.A1 + b.A1 + pi_ab;
   ax -= mb * pij * gx;
   ay -= mb * pij * gy;
-  if (isI && a.itype == 1 && b.itype >= 2) wcsph_wall_pair(P, b.itype, exact_r2(dxd, dyd), dxd, dyd, dud, dvd, a.m, W.wx, W.wy);
+  if (isI && a.itype == 1 && b.itype >= 2) {
+    const double dxd = a.x - b.x, dyd = a.y - b.y;
+    wcsph_wall_pair(P, b.itype, exact_r2(dxd, dyd), dxd, dyd, a.u - b.u, a.v - b.v, a.m, W.wx, W.wy);
+  }
 }
 
-template <bool kBrute, typename Real, typename Src, typename Cursor, typename Entry>
+template <bool kBrute, bool kF32, typename Real, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ void wc_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
-                                            const WcRec<Real> &o, Entry *s_nb, Real &drho, Real &ax, Real &ay,
-                                            WcAcc &W, unsigned &my_pairs, int &my_nb)
+                                            const WcRec<Real> &o, const F32Test &ft, Entry *s_nb, Real &drho,
+                                            Real &ax, Real &ay, WcAcc &W, unsigned &my_pairs, int &my_nb)
 {
   constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
   const int col = threadIdx.x;
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
-    const int cnt = tile_list<kBrute, kTileChunk>(P, src, cur, more, self, o.orig, o.x, o.y, s_nb, col, my_pairs,
-                                                  my_nb, W.wx, W.wy);
+    const int cnt = tile_list<kBrute, kTileChunk, false, kF32>(P, src, cur, more, self, o.orig, o.x, o.y, ft, s_nb,
+                                                               col, my_pairs, my_nb, W.wx, W.wy, 0.0, 0);
     __syncwarp();
     for (int e = 0; e < cnt; e++) {
       const Entry ent = s_nb[e * kTileThreads + col];
@@ -220,10 +254,13 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams 
   const int ncore = B.ncore;
   if (ncore == 0) return;
   const bool staged = B.nrec <= kWcRecCap;
+  // the origin of the block: FP32 positions are taken relative to it
+  const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
   unsigned my_pairs = 0;
-  int my_nb = 0;
+  int my_nb = 0;  // largest in-radius count of this thread's particles
   if (staged) {
-    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) rec[k] = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)]);
+    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads)
+      rec[k] = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)], ox, oy);
     __syncthreads();
     const WcStagedSrc<Real> src{rec};
     for (int base = 0; base < ncore; base += kTileThreads) {
@@ -238,14 +275,17 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams 
       StagedCursor cur;
       const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
       cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
+      const F32Test ft = make_f32_test(P, B, o.xr, o.yr);
       Real drho = 0, ax = 0, ay = 0;
       WcAcc W = {0.0, 0.0};
-      wc_particle<kBrute, Real>(P, src, cur, active, kr, o, s_nb16, drho, ax, ay, W, my_pairs, my_nb);
+      int nb = 0;
+      wc_particle<kBrute, true, Real>(P, src, cur, active, kr, o, ft, s_nb16, drho, ax, ay, W, my_pairs, nb);
+      my_nb = max(my_nb, nb);
       if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
     }
   } else {
     unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
-    const WcGlobalSrc<Real> src{S};
+    const WcGlobalSrc<Real> src{S, ox, oy};
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0;
@@ -255,13 +295,16 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams 
       }
       const bool active = k < ncore && a < P.nf;
       const int as = active ? a : 0;
-      const WcRec<Real> o = load_wc_rec<Real>(S, as);
+      const WcRec<Real> o = load_wc_rec<Real>(S, as, ox, oy);
       GlobalCursor cur;
       cur.list = G.list;
       cur.c.init(P, G, G.cell_of[as]);
+      const F32Test ft = {};
       Real drho = 0, ax = 0, ay = 0;
       WcAcc W = {0.0, 0.0};
-      wc_particle<kBrute, Real>(P, src, cur, active, as, o, s_nb32, drho, ax, ay, W, my_pairs, my_nb);
+      int nb = 0;
+      wc_particle<kBrute, false, Real>(P, src, cur, active, as, o, ft, s_nb32, drho, ax, ay, W, my_pairs, nb);
+      my_nb = max(my_nb, nb);
       if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
     }
   }

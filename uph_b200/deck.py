@@ -369,3 +369,48 @@ def wave_flume(length=10.0, depth=0.5, dx=0.005, layers=3, eta=1.3, amplitude=0.
     deck.domain_lo = (-pad, -pad)
     deck.domain_hi = (length + pad, depth * 2.0 + pad)
     return deck
+
+
+def lid_cavity(size=0.4, dx=0.02, layers=2, eta=1.3, lid_velocity=1.0, **over) -> Deck:
+    """A lid-driven cavity: water filling a size x size box whose top is a
+    row of moving particles sliding at lid_velocity (movingBoundary 3,
+    inputbp.c:209-223: x = tempPosition + U t).  Gravity off."""
+    over = dict(over)
+    over.setdefault("gravity_flag", 0)
+    p = base_params(dx, eta=eta, moving_boundary=3, lid_velocity=lid_velocity, **over)
+    n = int(round(size / dx))
+    x, y = lattice(0.5 * dx, 0.5 * dx, n, n, dx)
+    mass = p["density0"] * dx * dx
+    fluid = _rows(x, y, p["density0"], 0.0, mass, FLUID_ITYPE)
+    fixed = tank_walls(size, size, dx, layers, p["density0"], mass)
+    nxl = n + 2 * layers
+    xs = np.concatenate([-(layers - 0.5) * dx + np.arange(nxl) * dx for _ in range(layers)])
+    ys = np.concatenate([np.full(nxl, size + (k + 0.5) * dx) for k in range(layers)])
+    moving = _rows(xs, ys, p["density0"], 0.0, mass, 3)
+    moving[:, 7] = xs  # tempPosition
+    moving[:, 8] = ys  # tempPositionGate
+    deck = Deck(p, fluid, np.zeros((0, 12)), fixed, moving, eta_override=eta)
+    pad = 4 * eta * dx + layers * dx
+    deck.domain_lo = (-pad - 0.5 * size, -pad)
+    deck.domain_hi = (size + pad + 0.5 * size, size + pad + layers * dx)
+    return deck
+
+
+def gate_dam_break(tank=(1.0, 0.6), column=(0.3, 0.4), dx=0.02, layers=2, eta=1.3, gate_velocity=1.0,
+                   **over) -> Deck:
+    """A dam break released by a gate (movingBoundary 2, inputbp.c:224-243):
+    a column of moving particles one spacing right of the water, lifted at
+    gate_velocity until 1.5 (LocalDepth - 15 dx) / gate_velocity."""
+    over = dict(over)
+    over.setdefault("local_depth", column[1])
+    d = dam_break(tank=tank, column=column, dx=dx, layers=layers, eta=eta, hydrostatic=True, moving_boundary=2,
+                  lid_velocity=gate_velocity, **over)
+    ny = int(round(column[1] / dx))
+    ys = 0.5 * dx + np.arange(ny) * dx
+    xs = np.full(ny, column[0] + 0.5 * dx)
+    moving = _rows(xs, ys, d.params["density0"], 0.0, d.params["density0"] * dx * dx, 3)
+    moving[:, 7] = xs
+    moving[:, 8] = ys
+    d.moving = moving
+    return d
+

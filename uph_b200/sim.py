@@ -44,6 +44,10 @@ class Simulation:
         sim.upload(deck.initial_state(), 0)
         if deck.wall_table is not None:
             sim.set_wall_motion(*deck.wall_table)
+        mb = deck.params.get("moving_boundary", 0)
+        if mb in (2, 3) and deck.moving.shape[0]:
+            # the decks' tempPosition (lid) / tempPositionGate (gate) columns
+            sim.set_wall_base(deck.moving[:, 0 if mb == 3 else 8])
         return sim
 
     def close(self) -> None:
@@ -100,6 +104,11 @@ class Simulation:
         self._wall = [np.ascontiguousarray(a, dtype=np.float64) for a in (x0, half_stroke, omega)]
         _lib.check(self.lib.uph_sim_set_wall_motion(self.handle, *(a.ctypes.data for a in self._wall)),
                    "uph_sim_set_wall_motion")
+
+    def set_wall_base(self, base) -> None:
+        """Base coordinates of the lid (x) or gate (y) particles, reference order."""
+        self._base = np.ascontiguousarray(base, dtype=np.float64)
+        _lib.check(self.lib.uph_sim_set_wall_base(self.handle, self._base.ctypes.data), "uph_sim_set_wall_base")
 
     def derivatives(self, t: float) -> None:
         _lib.check(self.lib.uph_sim_derivatives(self.handle, t), "uph_sim_derivatives")
