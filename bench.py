@@ -617,7 +617,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "uph":
         args.warmup = 3
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    # the reference's per-thread scratch has 64 rows (System.c:209)
+    os.environ.setdefault("OMP_NUM_THREADS", str(min(64, os.cpu_count() or 1)))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

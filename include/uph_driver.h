@@ -23,9 +23,11 @@
 extern "C" {
 #endif
 
-/* A System for p's counts, sized for max_particles (>= all particles; the
- * pair arrays hold max_particles pairs, as the reference's MaxNumberOfParticles
- * sizes them), filled from `init` (Position, Velocity, density,
+/* A System for p's counts with MaxNumberOfParticles = max_particles (>= all
+ * particles): the pair arrays and the rate arrays derivatives() zeroes hold
+ * max_particles entries, the other per-particle arrays the particles; all
+ * in page-locked host memory when the driver grants it.  Filled from `init`
+ * (Position, Velocity, density,
  * DynamicPressure, mass and itype required; localVelocity / localDensity /
  * localPressure default to the plain fields).  NULL on bad arguments or
  * when host memory runs out. */

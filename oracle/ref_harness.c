@@ -40,6 +40,7 @@
 #include <string.h>
 #include <time.h>
 #include <unistd.h>
+#include <omp.h>
 
 #include "System.h"
 #include "derivatives.h"
@@ -104,8 +105,16 @@ static int copy_file(const char *src_dir, const char *dst_dir, const char *name)
 }
 
 /* Returns NULL on a missing deck file (the reference itself would exit). */
+/* The reference's per-thread scratch has 64 rows (System.c:209,
+ * CreateMatrix(64, ...)), indexed by omp_get_thread_num() in every pair loop
+ * (derivatives.c:1741 and its siblings): a larger team writes past it. */
+enum { kRefMaxThreads = 64 };
+
+int ref_threads(void) { return omp_get_max_threads(); }
+
 ref_run *ref_open(const char *deck_dir, double eta_override, int fluid_capacity_pct)
 {
+  if (omp_get_max_threads() > kRefMaxThreads) omp_set_num_threads(kRefMaxThreads);
   char cwd[8192];
   if (!getcwd(cwd, sizeof cwd)) return NULL;
   ref_run *run = (ref_run *)calloc(1, sizeof(ref_run));
@@ -142,6 +151,13 @@ ref_run *ref_open(const char *deck_dir, double eta_override, int fluid_capacity_
   }
 
   System *sys = CreateSystem(128, 128); /* sph.cc:23 */
+  /* CreateSystem leaves inflowParticles unset, and the first derivatives()
+   * call with t > 0 runs inoutflow (derivatives.c:3162-3164), which walks
+   * i_inflow[0, inflowParticles) before the inflow scan (:3172) first sets
+   * the count: with whatever the heap held there it read arbitrary
+   * Position rows and crashed now and then.  Zero, as the scan would leave it
+   * for a deck with no inflow. */
+  sys->inflowParticles = 0;
   if (use_scratch) {
     const char *names[] = {"FluidParticle.dat", "FixedBoundaryParticle.dat", "MovingBoundaryParticle.dat",
                            "SolidParticle.dat", "FrozenParticle.dat", "parameters.dat"};

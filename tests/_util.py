@@ -56,3 +56,14 @@ def compare_fields(got: dict, want: dict, n_fluid: int, tol: float, fields=FLUID
     bad = {k: v for k, v in errs.items() if not v <= tol}
     assert not bad, f"fields above {tol:g}: {bad}"
     return errs
+
+
+def ref_env() -> dict:
+    """The environment for the reference's own executables: at most 64
+    OpenMP threads, the rows of its per-thread scratch (System.c:209); and
+    heap blocks that start zeroed (glibc's MALLOC_PERTURB_=255 fills each new
+    block with 0x00), because its first inoutflow() call reads
+    sys->inflowParticles before anything sets it (derivatives.c:3163 before
+    :3172; System.c never initialises it)."""
+    import os
+    return dict(os.environ, OMP_NUM_THREADS=str(min(64, os.cpu_count() or 1)), MALLOC_PERTURB_="255")

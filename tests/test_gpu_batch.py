@@ -102,7 +102,7 @@ def test_autotune_choice_and_cache():
     s = Simulation.from_deck(batch.deck, profile=1, precision=1)
     s.set_wall_motion(batch.wall_x0, batch.wall_hs, batch.wall_om)
     choice, ms = s.autotune(trial_steps=5)
-    assert choice[0] in (1, 2, 3) and choice[1] in (8, 10, 12) and choice[2] in (16, 64, 256)
+    assert choice[0] in (1, 2, 3) and choice[1] in (9, 11, 13) and choice[2] in (16, 64, 256)
     assert ms > 0.0
     s.step(10)
     assert np.all(np.isfinite(s.download()["Position"]))

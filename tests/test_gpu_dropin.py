@@ -13,7 +13,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from _util import FLUID_FIELDS, REL_TOL_FP64, compare_fields, deck_from_golden, load_golden, rel_err
+from _util import FLUID_FIELDS, REL_TOL_FP64, compare_fields, deck_from_golden, load_golden, ref_env, rel_err
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -109,7 +109,7 @@ def test_unmodified_sph_driver_with_dropin_library(case, deck):
     for exe in (SPH, SPH_UPH):
         with tempfile.TemporaryDirectory() as tmp:
             deck.write(tmp)
-            r = subprocess.run([exe, "3"], cwd=tmp, capture_output=True, text=True, timeout=300)
+            r = subprocess.run([exe, "3"], cwd=tmp, capture_output=True, text=True, timeout=300, env=ref_env())
             assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
             tables.append([_out_table(os.path.join(tmp, f"out{k}.dat"))[:, OUT_COLUMNS] for k in (1, 2, 3)] +
                           [_out_table(os.path.join(tmp, "TotalKineticEnergy.dat"))])

@@ -17,7 +17,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from _util import deck_from_golden, load_golden
+from _util import deck_from_golden, load_golden, ref_env
 from oracle import oracle as O
 from uph_b200._capi import PREC_FP64, PROFILE_REF
 
@@ -58,7 +58,7 @@ def test_resident_output_matches_reference_driver(case, deck):
     deck.params["pressure_probe_y"] = float(fl[:, 1].min() + 0.25 * np.ptp(fl[:, 1]))
     with tempfile.TemporaryDirectory() as ref_dir, tempfile.TemporaryDirectory() as gpu_dir:
         deck.write(ref_dir)
-        r = subprocess.run([SPH, "3"], cwd=ref_dir, capture_output=True, text=True, timeout=300)
+        r = subprocess.run([SPH, "3"], cwd=ref_dir, capture_output=True, text=True, timeout=300, env=ref_env())
         assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
         gate = deck.dam_gate_flag()
         with Simulation.from_deck(deck, PROFILE_REF, PREC_FP64) as sim:

@@ -1,0 +1,69 @@
+"""The reference's own decks (its tests/hydrostaticPressure, tests/dambreak
+and tests/waves directories, read unchanged) on the GPU path, against the
+reference's solver compiled from its sources, for 3 steps.
+
+Two of them (dambreak, waves: nearNeighbor 91, a smoothing length of 2.7
+spacings) put about 90 points in every fluid query's radius, so the
+reference's 40-nearest cap binds everywhere; the GPU path applies the same
+cap (knn_cap = 40) with ties broken by index, as the compiled reference's
+search stand-in does.  libnabo's own tie order is not known, so these pair
+sets are pinned to the stand-in, not to libnabo.
+
+The decks are read from the reference tree ($UPH_REFERENCE, else the
+oracle's default); where it is absent the test is skipped.  Bars: pairs
+bit-identical, all 17 fluid fields within 1e-10 after steps 1 and 3."""
+import os
+import shutil
+import tempfile
+
+import numpy as np
+import pytest
+
+from _util import FLUID_FIELDS, REL_TOL_FP64, compare_fields
+from oracle import oracle as O
+from uph_b200 import deck as D
+
+pytestmark = pytest.mark.gpu
+
+DECKS = ["hydrostaticPressure", "dambreak", "waves"]
+INPUTS = ["parameters.dat", "FluidParticle.dat", "SolidParticle.dat", "FixedBoundaryParticle.dat",
+          "MovingBoundaryParticle.dat", "FrozenParticle.dat"]
+
+
+@pytest.mark.parametrize("name", DECKS)
+def test_reference_deck_matches_compiled_reference(name):
+    src = os.path.join(O.REFERENCE_TREE, "tests", name)
+    if not os.path.isdir(src):
+        pytest.skip(f"reference deck {src} not present")
+    if not os.path.exists(os.path.join(O.REF_DIR, "libuph_ref.so")):
+        pytest.skip("oracle/_ref/libuph_ref.so not built (make -C oracle ref)")
+    from uph_b200.sim import Simulation
+
+    with tempfile.TemporaryDirectory() as tmp:
+        for f in INPUTS:
+            if os.path.exists(os.path.join(src, f)):
+                shutil.copy(os.path.join(src, f), tmp)
+        deck = D.read_deck(tmp)
+        run = O.RefRun(tmp)
+        try:
+            run.step(1)
+            capped = run.truncated_queries()
+            ref1 = {f: run.get(f) for f in FLUID_FIELDS}
+            ri, rj = run.pairs()
+            rr2 = run.get("rij2")
+            run.step(2)
+            ref3 = {f: run.get(f) for f in FLUID_FIELDS}
+        finally:
+            run.close()
+    with Simulation.from_deck(deck, knn_cap=40) as s:
+        s.step(1)
+        e1 = compare_fields(s.download(), ref1, deck.n_fluid, REL_TOL_FP64)
+        s.step(2)
+        e3 = compare_fields(s.download(), ref3, deck.n_fluid, REL_TOL_FP64)
+    with Simulation.from_deck(deck, knn_cap=40) as s:
+        s.derivatives(deck.params["time_step"])
+        i, j, r2, _, _ = s.pairs()
+    assert np.array_equal(i, ri) and np.array_equal(j, rj), "pair list differs"
+    assert np.array_equal(r2, rr2)
+    print(f"{name}: {deck.n_fluid} fluid, {deck.n_all} particles, {ri.size} pairs bit-identical, "
+          f"{capped} queries capped at 40; max field error step 1 {max(e1.values()):.2e}, step 3 {max(e3.values()):.2e}")

@@ -15,7 +15,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from _util import deck_from_golden, load_golden
+from _util import deck_from_golden, load_golden, ref_env
 from oracle import oracle as O
 from uph_b200._capi import empty_state
 from uph_b200.sim import write_output
@@ -65,7 +65,7 @@ def test_writer_reproduces_reference_files():
     nf, n = deck.n_fluid, deck.n_all
     with tempfile.TemporaryDirectory() as ref_dir, tempfile.TemporaryDirectory() as out_dir:
         deck.write(ref_dir)
-        r = subprocess.run([SPH, "2"], cwd=ref_dir, capture_output=True, text=True, timeout=300)
+        r = subprocess.run([SPH, "2"], cwd=ref_dir, capture_output=True, text=True, timeout=300, env=ref_env())
         assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
         ke = np.loadtxt(os.path.join(ref_dir, "TotalKineticEnergy.dat"), ndmin=2)
         pp = np.loadtxt(os.path.join(ref_dir, "PointPressure.dat"), ndmin=2)

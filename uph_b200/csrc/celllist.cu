@@ -11,7 +11,10 @@
 // (2 reach + 1)^2 block; reach 2, cells of half the radius, by default).
 #include <algorithm>
 
-#include "uph_internal.cuh"
+#include <mutex>
+#include <vector>
+
+#include "tile_pass.cuh"
 
 namespace uph {
 
@@ -57,36 +60,6 @@ void launch_cell_keys(const DevParams &P, const double *x, const double *y, int 
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_PER_THREAD = 4;
 constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_PER_THREAD;
-
-template <typename T>
-__device__ __forceinline__ T block_exclusive_scan(T v, T *warp_tot, T &total)
-{
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  T incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    T t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) warp_tot[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    T wv = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : T(0);
-    T wi = wv;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      T t = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t;
-    }
-    warp_tot[lane] = wi - wv;  // exclusive prefix of warp totals
-    if (lane == 31) warp_tot[32] = wi;
-  }
-  __syncthreads();
-  const T out = incl - v + warp_tot[wid];
-  total = warp_tot[32];
-  __syncthreads();
-  return out;
-}
 
 // In: counts of type C; out, the chunk sums and the running totals: type T
 // (int for cell histograms, long long for pair counts that may pass 2^31).
@@ -209,192 +182,18 @@ void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s)
 
 // ---- the build as one cooperative launch ---------------------------------------
 
-struct CellBuildArgs {
-  DevParams P;
-  const double *x, *y;
-  int first, count;
-  CellGrid G;
-  unsigned *err;
-  unsigned long long *niac;  // rate-pass statistics to zero (or null)
-  int *max_nb;
-  int storage_order;
-  unsigned *rebuild;  // non-null: skip unless set; clear it and record the binned positions
-  double *xbin, *ybin;
-};
-
-// Grid-wide barrier over co-resident blocks: arrive on bar[0]; the last
-// block resets it and bumps the generation bar[1]; the others wait for the
-// bump.  The wait gives up after kWaitNs on the global timer (setting
-// ERR_TIMEOUT); the result is uniform over the block.
-__device__ __forceinline__ bool cell_grid_barrier(unsigned *bar, unsigned *err)
-{
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    volatile unsigned *vgen = bar + 1;
-    const unsigned gen = *vgen;
-    __threadfence();
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
-    } else {
-      const unsigned long long t0 = global_ns();
-      long long polls = 0;
-      while (*vgen == gen) {
-        if ((++polls & 255) == 0 && global_ns() - t0 > kWaitNs) {
-          atomicOr(err, ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-      }
-    }
-    __threadfence();
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-__device__ __forceinline__ int cell_of_position(const DevParams &P, double px, double py, unsigned *err,
-                                                bool storage_order)
-{
-  const double fx = (px - P.lo_x) * P.inv_cell;
-  const double fy = (py - P.lo_y) * P.inv_cell;
-  const bool inside = px >= P.lo_x && py >= P.lo_y && px <= P.hi_x && py <= P.hi_y;
-  int cx = 0, cy = 0;
-  if (inside) {
-    cx = min((int)floor(fx), P.ncx - 1);
-    cy = min((int)floor(fy), P.ncy - 1);
-  } else {
-    atomicOr(err, ERR_OUT_OF_DOMAIN);
-    if (fx > 0.0) cx = (int)fmin(fx, (double)(P.ncx - 1));
-    if (fy > 0.0) cy = (int)fmin(fy, (double)(P.ncy - 1));
-  }
-  return storage_order ? storage_key(cx, cy, P.ntx, P.tile) : cy * P.ncx + cx;
-}
-
-// Phases (B = grid barrier):
-//   1. cell of every slot, histogram; a slot's rank in its cell is the
-//      value its atomic add returned                                    B
-//   2. each block scans its chunk of cells: local prefixes into fill[],
-//      the chunk's total into totals[]; count is zeroed as it is read     B
-//   3. every block scans totals[] in shared memory, writes the final
-//      start[] of its chunk and scatters its slots to
-//      fill[c] + offset(chunk of c) + rank                               B
-//   4. each cell's slots sorted ascending (insertion sort, short cells),
-//      so the order does not depend on atomic arrival order; a cell with
-//      more than kMaxCellOccupancy slots is left unsorted and flags a
-//      neighbour overflow.
-// The same formulas as the multi-launch build (k_cell_keys and the rest).
 __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuildArgs A)
 {
   __shared__ int s_off[kCellBuildMaxBlocks + 1];
   __shared__ int s_wt[33];
-  const int nb = gridDim.x, b = blockIdx.x, t = threadIdx.x;
-  const int stride = nb * kCellBuildThreads;
-  const int ncell = A.G.ncell;
-  int *cnt = A.G.count, *start = A.G.start, *fill = A.G.fill, *list = A.G.list;
-  int *cell_of = A.G.cell_of, *rank = A.G.rank;
-
-  if (b == 0 && t == 0 && A.niac) {
-    *A.niac = 0ull;
-    *A.max_nb = 0;
-  }
   // the list from the last build is still complete: nothing to do (every
   // block reads the flag before any block can clear it, in phase 4)
   if (A.rebuild && *(volatile unsigned *)A.rebuild == 0u) return;
-
-  // 1. keys and histogram
-  for (int k = b * kCellBuildThreads + t; k < A.count; k += stride) {
-    const int s = A.first + k;
-    const double px = A.x[s], py = A.y[s];
-    const int c = cell_of_position(A.P, px, py, A.err, A.storage_order != 0);
-    cell_of[s] = c;
-    rank[s] = atomicAdd(&cnt[c], 1);
-    if (A.rebuild) {
-      A.xbin[s] = px;
-      A.ybin[s] = py;
-    }
-  }
-  if (!cell_grid_barrier(A.G.bar, A.err)) return;
-
-  // 2. chunk scans
-  const int chunk = (ncell + nb - 1) / nb;
-  const int c0 = min(b * chunk, ncell), c1 = min(c0 + chunk, ncell);
-  int carry = 0;
-  for (int base = c0; base < c1; base += kCellBuildThreads * 4) {
-    int v[4], sum = 0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = base + t * 4 + j;
-      v[j] = 0;
-      if (c < c1) {
-        v[j] = cnt[c];
-        cnt[c] = 0;
-      }
-      sum += v[j];
-    }
-    int total;
-    int run = block_exclusive_scan<int>(sum, s_wt, total) + carry;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = base + t * 4 + j;
-      if (c < c1) fill[c] = run;
-      run += v[j];
-    }
-    carry += total;
-  }
-  if (t == 0) A.G.totals[b] = carry;
-  if (!cell_grid_barrier(A.G.bar, A.err)) return;
-
-  // 3. chunk offsets, final starts, scatter
-  {
-    int run = 0;
-    for (int base = 0; base < nb; base += kCellBuildThreads) {
-      const int i = base + t;
-      const int v = i < nb ? A.G.totals[i] : 0;
-      int total;
-      const int ex = block_exclusive_scan<int>(v, s_wt, total);
-      if (i < nb) s_off[i] = ex + run;
-      run += total;
-    }
-    if (t == 0) s_off[nb] = run;
-    __syncthreads();
-  }
-  for (int c = c0 + t; c < c1; c += kCellBuildThreads) start[c] = fill[c] + s_off[b];
-  if (b == nb - 1 && t == 0) start[ncell] = s_off[nb];
-  for (int k = b * kCellBuildThreads + t; k < A.count; k += stride) {
-    const int s = A.first + k;
-    const int c = cell_of[s];
-    list[fill[c] + s_off[c / chunk] + rank[s]] = s;
-  }
-  if (!cell_grid_barrier(A.G.bar, A.err)) return;
-
-  // 4. per-cell sort by slot
-  if (A.rebuild && b == 0 && t == 0) *A.rebuild = 0u;
-  for (int c = b * kCellBuildThreads + t; c < ncell; c += stride) {
-    const int a0 = start[c], a1 = start[c + 1];
-    if (a1 - a0 > kMaxCellOccupancy) {
-      atomicOr(A.err, ERR_NEIGHBOR_OVERFLOW);
-      continue;
-    }
-    for (int i = a0 + 1; i < a1; i++) {
-      const int v = list[i];
-      int j = i - 1;
-      while (j >= a0 && list[j] > v) {
-        list[j + 1] = list[j];
-        j--;
-      }
-      list[j + 1] = v;
-    }
-  }
+  cell_build_phases(A, s_off, s_wt);
 }
 
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s,
-                             bool check_rebuild)
+                             CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s, bool check_rebuild)
 {
   // co-resident blocks: the cooperative launch refuses a grid that does not fit
   static int max_blocks[64] = {};
@@ -420,8 +219,6 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   A.count = std::max(count, 0);
   A.G = G;
   A.err = err;
-  A.niac = stats ? stats->niac : nullptr;
-  A.max_nb = stats ? stats->max_nb : nullptr;
   A.storage_order = storage_order ? 1 : 0;
   A.rebuild = check_rebuild ? P.rebuild : nullptr;
   A.xbin = P.xbin;
@@ -438,6 +235,27 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   cfg.numAttrs = 1;
   UPH_CUDA(cudaLaunchKernelEx(&cfg, k_cell_build, A));
   return UPH_OK;
+}
+
+int persistent_blocks(const void *kernel, int dev, size_t smem_bytes)
+{
+  struct Entry {
+    const void *kernel;
+    int dev, blocks;
+  };
+  static std::mutex mutex;
+  static std::vector<Entry> cache;
+  std::lock_guard<std::mutex> lock(mutex);
+  for (const Entry &e : cache)
+    if (e.kernel == kernel && e.dev == dev) return e.blocks;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) != cudaSuccess)
+    return 0;
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileThreads, smem_bytes) != cudaSuccess) return 0;
+  const int blocks = std::min(std::min(sms * per_sm, kPassMaxBlocks), kCellBuildMaxBlocks);
+  cache.push_back({kernel, dev, blocks});
+  return blocks;
 }
 
 }  // namespace uph

@@ -111,23 +111,27 @@ extern "C" System *uph_driver_create(const uph_params *p, const uph_state *init,
   Owned *o = new Owned();
   memset(&o->sys, 0, sizeof(System));
   System *s = &o->sys;
-  const size_t M = (size_t)max_particles;
+  // The arrays derivatives() may write past the particles -- the rate
+  // arrays it zeroes and the pair list -- hold max_particles entries, as the
+  // reference sizes all of them (System.c:195-260); the others hold the n
+  // particles, which is all that derivatives() and the leapfrog read.
+  const size_t M = (size_t)max_particles, N = (size_t)n;
   try {
-    s->itype = alloc_array<int>(o, M);
-    s->Position = alloc_matrix(o, M, 2);
-    s->Velocity = alloc_matrix(o, M, 2);
-    s->Velocity_xsph = alloc_matrix(o, M, 2);
-    s->Velocity_min = alloc_matrix(o, M, 2);
-    s->localVelocity = alloc_matrix(o, M, 2);
+    s->itype = alloc_array<int>(o, N);
+    s->Position = alloc_matrix(o, N, 2);
+    s->Velocity = alloc_matrix(o, N, 2);
+    s->Velocity_xsph = alloc_matrix(o, N, 2);
+    s->Velocity_min = alloc_matrix(o, N, 2);
+    s->localVelocity = alloc_matrix(o, N, 2);
+    s->velocityFluctuation = alloc_matrix(o, N, 2);
     s->dvdt = alloc_matrix(o, M, 2);
     s->dvdt_approx = alloc_matrix(o, M, 2);
-    s->velocityFluctuation = alloc_matrix(o, M, 2);
     s->dwcdx = alloc_matrix(o, M, 2);
-    for (double **f : {&s->mass, &s->Pressure, &s->hsml, &s->density, &s->ddensitydt, &s->density_min,
-                       &s->viscosity, &s->DynamicPressure, &s->DynamicPressure_min, &s->dpdt,
-                       &s->densityFluctuation, &s->pressureFluctuation, &s->localDensity, &s->localPressure,
-                       &s->thermalDiffusivity, &s->spongeFactor, &s->ddensitydt_approx, &s->dpdt_approx, &s->rij2,
-                       &s->w})
+    for (double **f : {&s->mass, &s->Pressure, &s->hsml, &s->density, &s->density_min, &s->viscosity,
+                       &s->DynamicPressure, &s->DynamicPressure_min, &s->densityFluctuation, &s->pressureFluctuation,
+                       &s->localDensity, &s->localPressure, &s->thermalDiffusivity, &s->spongeFactor})
+      *f = alloc_array<double>(o, N);
+    for (double **f : {&s->ddensitydt, &s->dpdt, &s->ddensitydt_approx, &s->dpdt_approx, &s->rij2, &s->w})
       *f = alloc_array<double>(o, M);
     s->i_pair = alloc_array<int>(o, M);
     s->j_pair = alloc_array<int>(o, M);

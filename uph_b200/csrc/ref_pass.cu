@@ -115,21 +115,19 @@ __device__ __forceinline__ void wall_pair_force(const DevParams &P, int itb, dou
 // per-particle factors every pair would otherwise recompute (Tait's
 // rho0 c0^2 + gamma p, 1/rho^2, rhot/rho, m/rho).  144 bytes, read as nine
 // 16-byte shared-memory loads.
+// (The listing's FP32 positions, relative to the CTA's block origin, are a
+// separate shared-memory array: the pair loop never reads them.)
 struct __align__(16) RefRec {
   double x, y, u, v, ut, vt, rho, rhot, p, pt, m, ir, irt, P, ir2, C, V;
   int orig, itype;
-  float xr, yr;  // position relative to the CTA's block origin, for the listing's FP32 pre-test
 };
-static_assert(sizeof(RefRec) == 160, "RefRec is ten 16-byte chunks");
+static_assert(sizeof(RefRec) == 144, "RefRec is nine 16-byte chunks");
 
-__device__ __forceinline__ RefRec load_ref_rec(const DevParams &P, const SlotArrays &S, int s, double ox = 0.0,
-                                               double oy = 0.0)
+__device__ __forceinline__ RefRec load_ref_rec(const DevParams &P, const SlotArrays &S, int s)
 {
   RefRec r;
   r.x = S.x[s];
   r.y = S.y[s];
-  r.xr = (float)(r.x - ox);
-  r.yr = (float)(r.y - oy);
   r.u = S.u[s];
   r.v = S.v[s];
   r.ut = S.ut[s];
@@ -245,15 +243,19 @@ __device__ __forceinline__ void ref_pair(const DevParams &P, const RefOwn &a, co
   A.ay = fma(-c2, dya, A.ay);
   // deviatoric viscous stress (ViscousForcesSingleStep and its predictor):
   // m_b mu_ab / (r^2 + 0.01 h^2) times F r^2 = m_b 2 mu rr (P_a + P_b) F r^2
-  if (P.stress_type == 1) {
+  // stressType 2 keeps the single-step predictor; its corrector force is
+  // added after the pass (launch_viscous_two_step)
+  if (P.stress_type == 1 || P.stress_type == 2) {
     const double vis = b.m * P.two_mu0 * rr * SP * Fr2;
-    const double D = fma(b.C, a.r.ir2, -(a.r.C * b.ir2));
-    const double sv = (isI ? vis : -vis) * D;
     const double vp = vis * (a.r.ir2 + b.ir2);
-    A.ax = fma(-sv, dux, A.ax);
-    A.ay = fma(-sv, duy, A.ay);
     A.ax_a = fma(-vp, dux, A.ax_a);
     A.ay_a = fma(-vp, duy, A.ay_a);
+    if (P.stress_type == 1) {
+      const double D = fma(b.C, a.r.ir2, -(a.r.C * b.ir2));
+      const double sv = (isI ? vis : -vis) * D;
+      A.ax = fma(-sv, dux, A.ax);
+      A.ay = fma(-sv, duy, A.ay);
+    }
   }
   // wall forces: only pairs whose i is this fluid particle
   if (isI && a.r.itype == 1 && b.itype >= 2) wall_pair_force(P, b.itype, r2, dxa, dya, dux, duy, a.r.m, A);
@@ -289,10 +291,11 @@ __device__ __forceinline__ void ref_epilogue(const DevParams &P, const SlotArray
 // Staged: records in shared memory, list entries are record indices.
 struct StagedSrc {
   const RefRec *rec;
+  const float2 *posf;    // block-relative FP32 positions
   const double *cut_d2;  // the knn cap's cut per record (kKnn only)
   const int *cut_j;
   __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
-  __device__ __forceinline__ float2 xyf(int k) const { return *reinterpret_cast<const float2 *>(&rec[k].xr); }
+  __device__ __forceinline__ float2 xyf(int k) const { return posf[k]; }
   __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
   __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
   __device__ __forceinline__ RefRec get(int k) const { return rec[k]; }
@@ -342,14 +345,15 @@ __device__ __forceinline__ void ref_particle(const DevParams &P, const Src &src,
 // Dynamic shared memory of the tiled pass and its record capacity; with the
 // knn cap every record also carries its query's cut (12 bytes).
 template <bool kKnn>
-__host__ __device__ constexpr int ref_rec_cap() { return kKnn ? 540 : 600; }
+__host__ __device__ constexpr int ref_rec_cap() { return kKnn ? 560 : 620; }
 constexpr size_t kRefListBytes = sizeof(unsigned short) * kTileChunk * kTileThreads;
+// per record: the record, its FP32 position and (kKnn) its cut
 template <bool kKnn>
 constexpr size_t ref_smem()
 {
-  return sizeof(TileBlock) + kRefListBytes + (sizeof(RefRec) + (kKnn ? 12 : 0)) * ref_rec_cap<kKnn>();
+  return sizeof(TileBlock) + kRefListBytes + (sizeof(RefRec) + 8 + (kKnn ? 12 : 0)) * ref_rec_cap<kKnn>();
 }
-static_assert(sizeof(RefRec) * 540 >= sizeof(unsigned) * kTileChunk * kTileThreads,
+static_assert(sizeof(RefRec) * 560 >= sizeof(unsigned) * kTileChunk * kTileThreads,
               "the fallback's 32-bit lists live in the record area");
 
 // One CTA per storage tile (see tile_pass.cuh).  Phase 1 lists in-radius
@@ -359,29 +363,34 @@ static_assert(sizeof(RefRec) * 540 >= sizeof(unsigned) * kTileChunk * kTileThrea
 // kBrute: the wall modes that act on every boundary particle within the
 // radius (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on
 // listed pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
+// One tile (see tile_pass.cuh): stage the block's records, then each thread
+// owns a fluid particle of the tile's core.  Phase 1 lists in-radius
+// partners per thread (the exact distance test, after the FP32 pre-test);
+// phase 2 runs the FP64 pair arithmetic over the lists, so the lanes of a
+// warp stay converged in the expensive loop.
 template <bool kBrute, bool kKnn>
-__global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                           PassStats st)
+__device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G, int tile,
+                                         unsigned char *smem, unsigned &my_pairs, int &my_nb)
 {
   constexpr int kCap = ref_rec_cap<kKnn>();
-  extern __shared__ __align__(16) unsigned char smem[];
   TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
   unsigned short *s_nb16 = reinterpret_cast<unsigned short *>(smem + sizeof(TileBlock));
   RefRec *rec = reinterpret_cast<RefRec *>(smem + sizeof(TileBlock) + kRefListBytes);
-  double *s_cd = reinterpret_cast<double *>(rec + kCap);
+  float2 *s_posf = reinterpret_cast<float2 *>(rec + kCap);
+  double *s_cd = reinterpret_cast<double *>(s_posf + kCap);
   int *s_cj = reinterpret_cast<int *>(s_cd + kCap);
-  tile_setup(P, G, blockIdx.x, B);
+  tile_setup(P, G, tile, B);
   const int ncore = B.ncore;
   if (ncore == 0) return;
   const bool staged = B.nrec <= kCap;
   // the origin of the block: the listing's FP32 positions are relative to it
   const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
-  unsigned my_pairs = 0;
-  int my_nb = 0;  // largest in-radius count of this thread's particles
   if (staged) {
     for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
       const int slot = G.list[tile_record_pos(B, k)];
-      rec[k] = load_ref_rec(P, S, slot, ox, oy);
+      const RefRec r = load_ref_rec(P, S, slot);
+      rec[k] = r;
+      s_posf[k] = make_float2((float)(r.x - ox), (float)(r.y - oy));
       if constexpr (kKnn) {
         // only fluid queries have a cut; other records are never a pair's i
         // seen from a fluid particle that is its j
@@ -390,7 +399,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
       }
     }
     __syncthreads();
-    const StagedSrc src{rec, s_cd, s_cj};
+    const StagedSrc src{rec, s_posf, s_cd, s_cj};
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0;
@@ -406,7 +415,8 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
       double cd = 0.0;
       int cj = 0;
       if (kKnn && active) src.cut(kr, cd, cj);
-      const F32Test ft = make_f32_test(P, B, o.r.xr, o.r.yr);
+      const float2 of = s_posf[active ? kr : 0];
+      const F32Test ft = make_f32_test(P, B, of.x, of.y);
       RefAcc A = {};
       double bx = 0.0, by = 0.0;
       int nb = 0;
@@ -443,37 +453,42 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P,
       if (active) ref_epilogue(P, S, a, o, A, bx, by);
     }
   }
-  // pass statistics: one atomic per warp
-  const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
-  const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
-  if ((threadIdx.x & 31) == 0) {
-    if (wp) atomicAdd(st.niac, (unsigned long long)wp);
-    if (wn) atomicMax(st.max_nb, wn);
-  }
+}
+
+// The REF rate pass: one persistent cooperative launch (tile_pass.cuh).
+// kBrute: the wall modes that act on every boundary particle within the
+// radius (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on
+// listed pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
+template <bool kBrute, bool kKnn>
+__global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                           PassStats st, const CellBuildArgs BA, int build_cells)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned my_pairs = 0;
+  int my_nb = 0;  // largest in-radius count of this thread's particles
+  persistent_pass(P, BA, build_cells != 0, smem, st, my_pairs, my_nb,
+                  [&](int tile) { ref_tile<kBrute, kKnn>(P, S, G, tile, smem, my_pairs, my_nb); });
 }
 
 template <bool kBrute, bool kKnn>
-void launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
+                      unsigned *err, cudaStream_t s)
 {
-  static bool attr_set[64] = {};  // once per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    cudaFuncSetAttribute(k_ref_pass<kBrute, kKnn>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ref_smem<kKnn>());
-    if (dev >= 0 && dev < 64) attr_set[dev] = true;
-  }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  k_ref_pass<kBrute, kKnn><<<ntiles, kTileThreads, ref_smem<kKnn>(), s>>>(P, S, G, st);
+  return launch_persistent(k_ref_pass<kBrute, kKnn>, ref_smem<kKnn>(), ntiles, s, P, S, G, st,
+                           pass_build_args(P, S, G, err), build_cells ? 1 : 0);
 }
 
-void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
+                           unsigned *err, cudaStream_t s)
 {
-  if (P.nf <= 0) return;
+  if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
   if (P.knn > 0)
-    brute ? launch_ref<true, true>(P, S, G, st, s) : launch_ref<false, true>(P, S, G, st, s);
-  else
-    brute ? launch_ref<true, false>(P, S, G, st, s) : launch_ref<false, false>(P, S, G, st, s);
+    return brute ? launch_ref<true, true>(P, S, G, st, build_cells, err, s)
+                 : launch_ref<false, true>(P, S, G, st, build_cells, err, s);
+  return brute ? launch_ref<true, false>(P, S, G, st, build_cells, err, s)
+               : launch_ref<false, false>(P, S, G, st, build_cells, err, s);
 }
 
 // The knn cap's cut of every fluid query: walk the stencil (the global cell
@@ -523,6 +538,124 @@ void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, 
 {
   if (P.nf <= 0 || P.knn <= 0) return;
   k_knn_cut<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G);
+}
+
+// ---- stressType 2 (ClassicShearStress, derivatives.c:1686-1721, and
+// ViscousForcesTwoStep, :1724-1768) -----------------------------------------------
+// Both walk the reference's pair list: every pair sums into both of its
+// particles.  Seen from particle a with partner b, d = x_a - x_b and the
+// pair's dwcdx = F d (sign included), both roles of a pair give the same
+// terms:
+//   sigma_a    = -mu sum_b (m_b / rho_b)(rhot_b / rho_a) (dv (x) dw + dw (x) dv)
+//                with dv = v_a - vt_b, so sigma_xy = sigma_yx;
+//   dv_a/dt   += sum_b m_b (sigma_a / rho_a^2 * rhot_b / rho_b
+//                           + sigma_b / rho_b^2 * rhot_a / rho_a) . dw
+// (fluid a only; b runs over fluid and wall partners, walls carrying the
+// stress of their own fluid pairs).
+
+// the listing rule of the pass (tile_pass.cuh): in the radius, not
+// coincident, both below ParticleBoundary, the smaller index a fluid query,
+// and with the knn cap the larger index among that query's kept points
+template <bool kKnn>
+__device__ __forceinline__ bool ref_listed(const DevParams &P, int a, int oa, int b, int ob, double r2)
+{
+  if (!(r2 < P.r2cut) || r2 <= DBL_EPSILON) return false;
+  if (max(oa, ob) >= P.pb || min(oa, ob) >= P.nf) return false;
+  if constexpr (kKnn) {
+    const int q = ob > oa ? a : b;  // the query's slot: a fluid slot
+    return knn_key_le(r2, max(oa, ob), P.kcut_d2[q], P.kcut_j[q]);
+  }
+  return true;
+}
+
+// the poly-7 deconvolution gradient factor F of ref_pair: dwcdx = F d
+__device__ __forceinline__ double ref_grad_factor(const DevParams &P, double r2)
+{
+  const double q2 = r2 * P.inv_h2;
+  const double t = fma(-0.25, q2, 1.0);
+  const double t2 = t * t, t4 = t2 * t2;
+  const double pp7 = fma(fma(fma(fma(fma(fma(305.0, q2, -1106.0), q2, 1912.0), q2, -2912.0), q2, 3712.0), q2, -3584.0), q2, 2048.0);
+  return P.dw_alpha_h2 * (t4 * t2 * t) * pp7;
+}
+
+template <bool kKnn>
+__global__ void __launch_bounds__(128) k_shear_stress(const DevParams P, const SlotArrays S, const CellGrid G)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.n) return;
+  const int oa = S.orig[a];
+  double sxx = 0.0, sxy = 0.0, syy = 0.0;
+  const double ira = S.inv_rho[a];
+  if (oa < P.pb) {
+    const double xa = S.x[a], ya = S.y[a], ua = S.u[a], va = S.v[a];
+    NeighbourCursor cur;
+    cur.init(P, G, G.cell_of[a]);
+    int k;
+    while (cur.next(k)) {
+      const int b = G.list[k];
+      if (b == a) continue;
+      const double dx = xa - S.x[b], dy = ya - S.y[b];
+      const double r2 = exact_r2(dx, dy);
+      if (!ref_listed<kKnn>(P, a, oa, b, S.orig[b], r2)) continue;
+      const double F = ref_grad_factor(P, r2);
+      const double dwx = F * dx, dwy = F * dy;
+      const double dvx = ua - S.ut[b], dvy = va - S.vt[b];
+      // viscosity * reduced volume (m_b / rho_b) rhot_b / rho_a
+      const double c = P.mu0 * (S.m[b] * S.inv_rho[b]) * S.rhot[b] * ira;
+      sxx -= c * (dvx * dwx + dvx * dwx);
+      sxy -= c * (dvx * dwy + dvy * dwx);
+      syy -= c * (dvy * dwy + dvy * dwy);
+    }
+  }
+  const double ir2 = ira * ira;
+  P.str_xx[a] = sxx * ir2;
+  P.str_xy[a] = sxy * ir2;
+  P.str_yy[a] = syy * ir2;
+}
+
+template <bool kKnn>
+__global__ void __launch_bounds__(128) k_viscous_two_step(const DevParams P, const SlotArrays S, const CellGrid G)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const int oa = S.orig[a];
+  const double xa = S.x[a], ya = S.y[a];
+  const double Ca = S.rhot[a] * S.inv_rho[a];
+  const double axx = P.str_xx[a], axy = P.str_xy[a], ayy = P.str_yy[a];
+  double fx = 0.0, fy = 0.0;
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[a]);
+  int k;
+  while (cur.next(k)) {
+    const int b = G.list[k];
+    if (b == a) continue;
+    const double dx = xa - S.x[b], dy = ya - S.y[b];
+    const double r2 = exact_r2(dx, dy);
+    if (!ref_listed<kKnn>(P, a, oa, b, S.orig[b], r2)) continue;
+    const double F = ref_grad_factor(P, r2);
+    const double dwx = F * dx, dwy = F * dy;
+    const double Cb = S.rhot[b] * S.inv_rho[b];
+    const double txx = fma(axx, Cb, P.str_xx[b] * Ca);
+    const double txy = fma(axy, Cb, P.str_xy[b] * Ca);
+    const double tyy = fma(ayy, Cb, P.str_yy[b] * Ca);
+    const double mb = S.m[b];
+    fx = fma(mb, fma(txx, dwx, txy * dwy), fx);
+    fy = fma(mb, fma(txy, dwx, tyy * dwy), fy);
+  }
+  S.ax[a] += fx;
+  S.ay[a] += fy;
+}
+
+void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s)
+{
+  if (P.nf <= 0 || P.stress_type != 2) return;
+  if (P.knn > 0) {
+    k_shear_stress<true><<<(P.n + 127) / 128, 128, 0, s>>>(P, S, G);
+    k_viscous_two_step<true><<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G);
+  } else {
+    k_shear_stress<false><<<(P.n + 127) / 128, 128, 0, s>>>(P, S, G);
+    k_viscous_two_step<false><<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G);
+  }
 }
 
 __global__ void k_rcp_selftest(const double *__restrict__ x, double *__restrict__ y, int64_t n)

@@ -77,8 +77,10 @@ struct uph_sim {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   unsigned *d_err = nullptr;
+  // the rate pass's statistics, one entry per block of its last launch
   unsigned long long *d_niac = nullptr;
   int *d_max_nb = nullptr;
+  int *d_pass_nblocks = nullptr;
   int *d_perm = nullptr;  // scratch for uploads and reorders
   int itime = 0;
   int steps_since_reorder = 0;
@@ -332,19 +334,18 @@ __global__ void k_iota(int *p, int first, int count)
 // counting sort of ids [first, first+count) by cell, result: G.list[0, count)
 // = ids in key order, ties by id.  storage_order selects the tile-major
 // storage key instead of the row-major cell-list id.
-uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order,
-                      const PassStats *stats = nullptr)
+uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order)
 {
-  uph_status r = launch_cell_build(s->P, x, y, first, count, s->G, s->d_err, storage_order, stats, s->stream);
+  uph_status r = launch_cell_build(s->P, x, y, first, count, s->G, s->d_err, storage_order, s->stream);
   s->launches += 1;
   return r;
 }
 
-// the cell list of all interacting particles; zeroes the pass statistics
-uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr)
+// the cell list of all interacting particles, when the skin test asks for it
+uph_status build_cell_list(uph_sim *s)
 {
   Timer t(s, KF_CELLS);
-  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, stats, s->stream, true);
+  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, s->stream, true);
   s->launches += 1;
   return r;
 }
@@ -387,7 +388,7 @@ uph_status check_error_word(uph_sim *s)
     // a cell-list build that gave up at a grid barrier leaves its histogram
     // and barrier words part-way: clear them for the next build
     cudaMemsetAsync(s->G.count, 0, sizeof(int) * s->G.ncell, s->stream);
-    cudaMemsetAsync(s->G.bar, 0, 2 * sizeof(unsigned), s->stream);
+    cudaMemsetAsync(s->G.bar, 0, kGridWords * sizeof(unsigned), s->stream);
     cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream);
     return fail(UPH_TIMEOUT, "a device-side wait timed out");
   }
@@ -403,19 +404,26 @@ uph_status rate_pass(uph_sim *s, bool refresh)
     launch_refresh_inverse(s->P, s->S, 0, s->P.nf, s->stream);
     s->launches++;
   }
-  PassStats st{s->d_niac, s->d_max_nb};
-  uph_status r = build_cell_list(s, &st);
-  if (r != UPH_OK) return r;
-  if (s->P.knn > 0) {
+  const PassStats st{s->d_niac, s->d_max_nb, s->d_pass_nblocks};
+  // the pass rebuilds the cell list itself (when the skin test asks for it)
+  // unless the knn cut must read the list first
+  const bool fused = s->P.knn <= 0;
+  if (!fused) {
+    uph_status r = build_cell_list(s);
+    if (r != UPH_OK) return r;
     launch_knn_cut(s->P, s->S, s->G, s->stream);
     s->launches++;
   }
   Timer t(s, KF_PASS);
-  if (s->P.profile == UPH_PROFILE_REF)
-    launch_ref_pass(s->P, s->S, s->G, st, s->stream);
-  else
-    launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
+  uph_status r = s->P.profile == UPH_PROFILE_REF
+                     ? launch_ref_pass(s->P, s->S, s->G, st, fused, s->d_err, s->stream)
+                     : launch_wcsph_pass(s->P, s->S, s->G, st, fused, s->d_err, s->stream);
+  if (r != UPH_OK) return r;
   s->launches++;
+  if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF) {
+    launch_viscous_two_step(s->P, s->S, s->G, s->stream);
+    s->launches += 2;
+  }
   s->have_rates = true;
   return UPH_OK;
 }
@@ -438,7 +446,8 @@ uph_status validate(const uph_params *p)
   const int vt = p->virtual_type;
   if (vt == 1 || vt == 3 || vt == 4 || vt == 5 || vt == 7 || vt == 8)
     return fail(UPH_UNSUPPORTED, "virtual mirror particles (virtualType 1,3,4,5,7,8) are not implemented");
-  if (p->stress_type == 2) return fail(UPH_UNSUPPORTED, "stressType 2 (two-step viscous stress) is not implemented");
+  if (p->stress_type == 2 && p->profile != UPH_PROFILE_REF)
+    return fail(UPH_UNSUPPORTED, "stressType 2 belongs to the REF profile");
   if (p->knn_cap < 0) return fail(UPH_BAD_ARG, "negative knn_cap");
   if (p->knn_cap > kKnnMax)
     return fail(UPH_UNSUPPORTED, "knn_cap above " + std::to_string(kKnnMax) + " is not implemented");
@@ -565,7 +574,7 @@ DevParams make_dev_params(const uph_params *p)
   P.hi_y = p->domain_hi[1];
   // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
   // against 36 h^2 for a 3 x 3 block of radius-wide cells.  A cell then holds
-  // about ((1 + skin) h / dx)^2 particles of a lattice; the default tile (10
+  // about ((1 + skin) h / dx)^2 particles of a lattice; the default tile (11
   // cells at h = 1.3 dx) shrinks for wider kernels so that a tile's
   // particles fit one round of a CTA and its block the tiled passes'
   // shared-memory records.
@@ -576,6 +585,7 @@ DevParams make_dev_params(const uph_params *p)
   P.knn = p->knn_cap;
   P.kcut_d2 = nullptr;
   P.kcut_j = nullptr;
+  P.str_xx = P.str_xy = P.str_yy = nullptr;
   P.xbin = P.ybin = nullptr;
   P.rebuild = nullptr;
   return P;
@@ -620,14 +630,19 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
     TRY(dalloc(s, &s->P.kcut_d2, (size_t)nf));
     TRY(dalloc(s, &s->P.kcut_j, (size_t)nf));
   }
+  if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF) {
+    TRY(dalloc(s, &s->P.str_xx, (size_t)n));
+    TRY(dalloc(s, &s->P.str_xy, (size_t)n));
+    TRY(dalloc(s, &s->P.str_yy, (size_t)n));
+  }
   TRY(dalloc(s, &s->P.xbin, (size_t)n));
   TRY(dalloc(s, &s->P.ybin, (size_t)n));
   TRY(dalloc(s, &s->P.rebuild, 1));
   TRY(cudaMemset(s->P.rebuild, 1, sizeof(unsigned)));
   TRY(dalloc(s, &G.rank, (size_t)n));
   TRY(dalloc(s, &G.totals, (size_t)kCellBuildMaxBlocks + 1));
-  TRY(dalloc(s, &G.bar, 2));
-  TRY(cudaMemset(G.bar, 0, 2 * sizeof(unsigned)));
+  TRY(dalloc(s, &G.bar, kGridWords));
+  TRY(cudaMemset(G.bar, 0, kGridWords * sizeof(unsigned)));
   TRY(alloc_grid(s));
   Staging &T = s->T;
   double **tall[] = {&T.rho, &T.lrho, &T.p, &T.lp, &T.mass, &T.pressure, &T.tmp_x, &T.tmp_y};
@@ -640,8 +655,10 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   double **tfl2[] = {&T.vmin, &T.acc, &T.acc_a, &T.fvel};
   for (double **q : tfl2) TRY(dalloc(s, q, 2 * (size_t)nf));
   TRY(dalloc(s, &s->d_err, 1));
-  TRY(dalloc(s, &s->d_niac, 1));
-  TRY(dalloc(s, &s->d_max_nb, 1));
+  TRY(dalloc(s, &s->d_niac, kPassMaxBlocks));
+  TRY(dalloc(s, &s->d_max_nb, kPassMaxBlocks));
+  TRY(dalloc(s, &s->d_pass_nblocks, 1));
+  TRY(cudaMemset(s->d_pass_nblocks, 0, sizeof(int)));
   TRY(dalloc(s, &s->d_perm, (size_t)n));
   TRY(dalloc(s, &s->d_itime, 1));
   TRY(dalloc(s, &s->d_wall_tab, 4 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
@@ -1317,12 +1334,22 @@ extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
   k_stats<<<nb, 256, 0, s->stream>>>(s->P, s->S, s->d_partials, nb);
   s->launches++;
   std::vector<double> part(4 * (size_t)nb);
+  std::vector<unsigned long long> niac_b(kPassMaxBlocks);
+  std::vector<int> nb_b(kPassMaxBlocks);
+  int pass_blocks = 0;
+  UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(&pass_blocks, s->d_pass_nblocks, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(niac_b.data(), s->d_niac, sizeof(unsigned long long) * kPassMaxBlocks,
+                           cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(nb_b.data(), s->d_max_nb, sizeof(int) * kPassMaxBlocks, cudaMemcpyDeviceToHost,
+                           s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
   unsigned long long niac = 0;
   int mx = 0;
-  UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaMemcpyAsync(&niac, s->d_niac, sizeof niac, cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  for (int b = 0; b < std::min(pass_blocks, kPassMaxBlocks); b++) {
+    niac += niac_b[b];
+    mx = std::max(mx, nb_b[b]);
+  }
   for (int b = 0; b < nb; b++) {
     out->kinetic_energy += part[b];
     out->potential_energy += part[nb + b];
@@ -1399,7 +1426,7 @@ uph_status time_steps(uph_sim *s, int steps, double *ms)
 }  // namespace
 
 // Coordinate search over (cell reach, storage tile, re-sort interval): the
-// reach first with tile 10 and interval 64, then the tile at the best reach,
+// reach first with tile 11 and interval 64, then the tile at the best reach,
 // then the interval.  Each trial times `trial_steps` steps of this very
 // simulation, so tuning advances it by about 9 (trial_steps + 2) steps.
 // Results are cached per size class (profile, precision, log2 of the fluid
@@ -1431,7 +1458,7 @@ extern "C" uph_status uph_sim_autotune(uph_sim *s, int32_t trial_steps, int32_t 
     };
     best_ms = 1e300;
     for (int axis = 0; axis < 3; axis++) {
-      static const int options[3][3] = {{1, 2, 3}, {8, 10, 12}, {16, 64, 256}};
+      static const int options[3][3] = {{1, 2, 3}, {9, 11, 13}, {16, 64, 256}};
       std::array<int, 3> axis_best = best;
       for (int v : options[axis]) {
         std::array<int, 3> c = best;

@@ -95,6 +95,9 @@ struct DevParams {
   int knn;
   double *kcut_d2;
   int *kcut_j;
+  // stressType 2: each particle's shear stress over its density squared,
+  // sigma / rho^2 (xx, xy = yx, yy), indexed by slot
+  double *str_xx, *str_xy, *str_yy;
   // Skin of the cell list: cells are (1 + kCellSkin) radius / reach wide, so
   // the list stays complete while no particle has moved more than `skin`
   // (per axis) from where the last build binned it (xbin, ybin by slot).
@@ -105,7 +108,7 @@ struct DevParams {
   unsigned *rebuild;
 };
 
-constexpr double kCellSkin = 0.1;
+constexpr double kCellSkin = 0.05;
 
 constexpr int kKnnMax = 64;  // largest knn cap the kernels keep per query
 
@@ -121,10 +124,10 @@ __host__ __device__ __forceinline__ bool knn_key_le(double r2, int j, double cd,
 // tile, tiles row-major, cells inside a tile row-major.  The REF rate pass
 // runs one CTA per tile (tile_pass.cuh), so a tile's fluid particles are
 // nearly contiguous slots.  The tile edge is a tuning parameter
-// (DevParams::tile, default 10: 100 cells of (1 + skin) h hold about 205
+// (DevParams::tile, default 11: 121 cells of (1 + skin) h hold about 225
 // particles of a lattice at h = 1.3 dx, one per thread of a 256-thread CTA,
 // with room for compression before a second round of the CTA is needed).
-constexpr int kCellTile = 10;
+constexpr int kCellTile = 11;
 
 __host__ __device__ __forceinline__ int storage_key(int cx, int cy, int ntx, int tile)
 {
@@ -143,6 +146,8 @@ struct WallTable {
   const double *base;
 };
 
+constexpr int kGridWords = 4;
+
 struct CellGrid {
   int ncell;
   int *count;    // [ncell]
@@ -153,11 +158,12 @@ struct CellGrid {
   int *block_sums;
   int nblock_sums;
   // one-launch build (launch_cell_build): rank of each slot in its cell,
-  // per-block totals and the grid barrier's two words; count is all zero
-  // between builds
+  // per-block totals, the grid barrier's two words and the persistent rate
+  // pass's tile ticket and finish count; count and bar are all zero between
+  // launches
   int *rank;       // [n]
   int *totals;     // [kCellBuildMaxBlocks + 1]
-  unsigned *bar;   // [2]
+  unsigned *bar;   // [kGridWords]
 };
 
 std::string &last_error();
@@ -183,27 +189,37 @@ void launch_cell_scatter(const CellGrid &G, int first, int count, cudaStream_t s
 constexpr int kMaxCellOccupancy = 4096;
 void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s);
 // The whole build (keys and histogram, scan, scatter, per-cell sort) as one
-// cooperative launch with three bounded grid barriers; also zeroes the rate
-// pass's statistics when `stats` is given.  count must be all zero on entry
-// and is again on return.
+// cooperative launch with three bounded grid barriers.  count must be all
+// zero on entry and is again on return.
 constexpr int kCellBuildThreads = 512;
 constexpr int kCellBuildMaxBlocks = 1024;
-struct PassStats;
 // check_rebuild: build only when *P.rebuild is set (and then clear it and
 // record the binned positions); otherwise always build.
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats, cudaStream_t s,
+                             CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s,
                              bool check_rebuild = false);
 
 // REF / WCSPH rate pass over the fluid slots
+// Statistics of a rate pass, one entry per block of its (persistent) grid,
+// so that nothing needs zeroing between passes: pairs (i < j) counted from
+// the i side, and the largest in-radius neighbour count of a fluid particle.
+constexpr int kPassMaxBlocks = 1024;
 struct PassStats {
-  unsigned long long *niac;  // pairs (i < j) counted from the i side
-  int *max_nb;               // largest in-radius neighbour count of a fluid particle
+  unsigned long long *niac;  // [kPassMaxBlocks]
+  int *max_nb;               // [kPassMaxBlocks]
+  int *nblocks;              // the grid size of the last pass (one int)
 };
-void launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+// The rate passes run as one persistent cooperative launch; with
+// build_cells they first rebuild the cell list when *P.rebuild is set.
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
+                           unsigned *err, cudaStream_t s);
 // the knn cap's cut of every fluid query (P.kcut_*), from the cell list
 void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
-void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+// stressType 2, after the rate pass: the shear stress of every listed
+// particle (P.str_*), then its divergence added to the corrector's dv/dt
+void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
+uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                             bool build_cells, unsigned *err, cudaStream_t s);
 
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);

@@ -66,7 +66,6 @@ template <>
 struct __align__(16) WcRec<double> {
   double x, y, u, v, m, A1, rho;
   int orig, itype;
-  float xr, yr;  // relative position for the listing's FP32 pre-test
 };
 template <>
 struct __align__(16) WcRec<float> {
@@ -74,7 +73,7 @@ struct __align__(16) WcRec<float> {
   float xr, yr, ur, vr, mr, A1, rho;
   int orig, itype;
 };
-static_assert(sizeof(WcRec<double>) == 80 && sizeof(WcRec<float>) == 80, "record sizes");
+static_assert(sizeof(WcRec<double>) == 64 && sizeof(WcRec<float>) == 80, "record sizes");
 
 // (ox, oy): the origin FP32 positions are taken relative to
 template <typename Real>
@@ -89,9 +88,9 @@ __device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s, d
   const double ir = S.inv_rho[s];
   r.A1 = (Real)(S.p[s] * ir * ir);
   r.rho = (Real)S.rho[s];
-  r.xr = (float)(r.x - ox);
-  r.yr = (float)(r.y - oy);
   if constexpr (sizeof(Real) == sizeof(float)) {
+    r.xr = (float)(r.x - ox);
+    r.yr = (float)(r.y - oy);
     r.ur = (float)r.u;
     r.vr = (float)r.v;
     r.mr = (float)r.m;
@@ -104,8 +103,9 @@ __device__ __forceinline__ WcRec<Real> load_wc_rec(const SlotArrays &S, int s, d
 template <typename Real>
 struct WcStagedSrc {
   const WcRec<Real> *rec;
+  const float2 *posf;  // block-relative FP32 positions for the listing
   __device__ __forceinline__ double2 xy(int k) const { return *reinterpret_cast<const double2 *>(&rec[k].x); }
-  __device__ __forceinline__ float2 xyf(int k) const { return make_float2(rec[k].xr, rec[k].yr); }
+  __device__ __forceinline__ float2 xyf(int k) const { return posf[k]; }
   __device__ __forceinline__ int orig(int k) const { return rec[k].orig; }
   __device__ __forceinline__ double mass(int k) const { return rec[k].m; }
   __device__ __forceinline__ WcRec<Real> get(int k) const { return rec[k]; }
@@ -236,33 +236,34 @@ constexpr size_t kWcListBytes = sizeof(unsigned short) * kTileChunk * kTileThrea
 template <typename Real>
 constexpr size_t wc_smem()
 {
-  return sizeof(TileBlock) + kWcListBytes + sizeof(WcRec<Real>) * kWcRecCap;
+  return sizeof(TileBlock) + kWcListBytes + (sizeof(WcRec<Real>) + sizeof(float2)) * kWcRecCap;
 }
 static_assert(sizeof(WcRec<float>) * kWcRecCap >= sizeof(unsigned) * kTileChunk * kTileThreads,
               "the fallback's 32-bit lists live in the record area");
 
-// One CTA per storage tile, as the REF pass (tile_pass.cuh).
+// One tile of the WCSPH pass, as the REF pass's (tile_pass.cuh).
 template <bool kBrute, typename Real>
-__global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                             PassStats st)
+__device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G, int tile,
+                                        unsigned char *smem, unsigned &my_pairs, int &my_nb)
 {
-  extern __shared__ __align__(16) unsigned char smem[];
   TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
   unsigned short *s_nb16 = reinterpret_cast<unsigned short *>(smem + sizeof(TileBlock));
   WcRec<Real> *rec = reinterpret_cast<WcRec<Real> *>(smem + sizeof(TileBlock) + kWcListBytes);
-  tile_setup(P, G, blockIdx.x, B);
+  float2 *s_posf = reinterpret_cast<float2 *>(rec + kWcRecCap);
+  tile_setup(P, G, tile, B);
   const int ncore = B.ncore;
   if (ncore == 0) return;
   const bool staged = B.nrec <= kWcRecCap;
   // the origin of the block: FP32 positions are taken relative to it
   const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
-  unsigned my_pairs = 0;
-  int my_nb = 0;  // largest in-radius count of this thread's particles
   if (staged) {
-    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads)
-      rec[k] = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)], ox, oy);
+    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
+      const WcRec<Real> r = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)], ox, oy);
+      rec[k] = r;
+      s_posf[k] = make_float2((float)(r.x - ox), (float)(r.y - oy));
+    }
     __syncthreads();
-    const WcStagedSrc<Real> src{rec};
+    const WcStagedSrc<Real> src{rec, s_posf};
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0;
@@ -275,7 +276,8 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams 
       StagedCursor cur;
       const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
       cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
-      const F32Test ft = make_f32_test(P, B, o.xr, o.yr);
+      const float2 of = s_posf[active ? kr : 0];
+      const F32Test ft = make_f32_test(P, B, of.x, of.y);
       Real drho = 0, ax = 0, ay = 0;
       WcAcc W = {0.0, 0.0};
       int nb = 0;
@@ -308,37 +310,40 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams 
       if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
     }
   }
-  const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
-  const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
-  if ((threadIdx.x & 31) == 0) {
-    if (wp) atomicAdd(st.niac, (unsigned long long)wp);
-    if (wn) atomicMax(st.max_nb, wn);
-  }
+}
+
+// The WCSPH rate pass: one persistent cooperative launch (tile_pass.cuh).
+template <bool kBrute, typename Real>
+__global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                             PassStats st, const CellBuildArgs BA, int build_cells)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned my_pairs = 0;
+  int my_nb = 0;  // largest in-radius count of this thread's particles
+  persistent_pass(P, BA, build_cells != 0, smem, st, my_pairs, my_nb,
+                  [&](int tile) { wc_tile<kBrute, Real>(P, S, G, tile, smem, my_pairs, my_nb); });
 }
 
 template <bool kBrute, typename Real>
-void launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
+                     unsigned *err, cudaStream_t s)
 {
-  static bool attr_set[64] = {};  // once per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-    cudaFuncSetAttribute(k_wcsph_pass<kBrute, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wc_smem<Real>());
-    if (dev >= 0 && dev < 64) attr_set[dev] = true;
-  }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  k_wcsph_pass<kBrute, Real><<<ntiles, kTileThreads, wc_smem<Real>(), s>>>(P, S, G, st);
+  return launch_persistent(k_wcsph_pass<kBrute, Real>, wc_smem<Real>(), ntiles, s, P, S, G, st,
+                           pass_build_args(P, S, G, err), build_cells ? 1 : 0);
 }
 
-void launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                             bool build_cells, unsigned *err, cudaStream_t s)
 {
-  if (P.nf <= 0) return;
+  if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
   const bool f32 = P.precision == UPH_PREC_FP32_PAIR;
   if (f32)
-    brute ? launch_wc<true, float>(P, S, G, st, s) : launch_wc<false, float>(P, S, G, st, s);
-  else
-    brute ? launch_wc<true, double>(P, S, G, st, s) : launch_wc<false, double>(P, S, G, st, s);
+    return brute ? launch_wc<true, float>(P, S, G, st, build_cells, err, s)
+                 : launch_wc<false, float>(P, S, G, st, build_cells, err, s);
+  return brute ? launch_wc<true, double>(P, S, G, st, build_cells, err, s)
+               : launch_wc<false, double>(P, S, G, st, build_cells, err, s);
 }
 
 }  // namespace uph
