@@ -183,10 +183,13 @@ VECTOR_FIELDS = {"Position", "Velocity", "localVelocity", "Velocity_min", "dvdt"
                  "velocityFluctuation", "dwcdx"}
 
 
-class RefRun:
+class RefRunInProcess:
     """The reference solver (CreateSystem + input + sph.cc's loop) on a deck
-    directory.  fluid_capacity_pct > 0 shrinks the reference's 100 Nf
-    particle capacity (see oracle/ref_harness.c)."""
+    directory, in this process: what RefRun's child process runs, and the
+    base of harnesses over the same API that must share this process (the
+    drop-in build, whose derivatives() runs on this process's GPU).
+    fluid_capacity_pct > 0 shrinks the reference's 100 Nf particle capacity
+    (see oracle/ref_harness.c)."""
 
     def __init__(self, deck_dir: str, eta_override: float = 0.0, fluid_capacity_pct: int = 0):
         self.lib = ref_lib()
@@ -264,6 +267,150 @@ class RefRun:
 
     def max_inradius(self) -> int:
         return int(self.lib.uph_standin_max_inradius())
+
+
+# The compiled reference runs in a child process of its own (spawned, never
+# forked: the parent may hold a CUDA context).  There it shares no heap or
+# OpenMP runtime with CUDA, torch or the GPU library, and a crash of the
+# reference's C code ends the child, not the caller: the call raises
+# ReferenceCrash.  Its heap blocks start zeroed (glibc's MALLOC_PERTURB_=255),
+# so what the reference reads before writing is zero on every run, as on a
+# fresh heap: CreateSystem leaves fields such as inflowParticles unset
+# (System.c:195-250), which derivatives.c:3163 reads before :3172 sets it.
+
+class ReferenceCrash(RuntimeError):
+    pass
+
+
+def _ref_worker_main(conn) -> None:
+    runs = {}
+    while True:
+        try:
+            msg = conn.recv()
+        except EOFError:
+            return
+        h, method, args = msg
+        try:
+            if method == "open":
+                run = RefRunInProcess(*args)
+                runs[id(run)] = run
+                val = id(run)
+            elif method == "close":
+                run = runs.pop(h, None)
+                if run is not None:
+                    run.close()
+                val = None
+            elif method == "exit":
+                conn.send((True, None))
+                return
+            else:
+                val = getattr(runs[h], method)(*args)
+            conn.send((True, val))
+        except Exception as e:  # the reference's own errors go back to the caller
+            conn.send((False, e))
+
+
+class _RefWorker:
+    def __init__(self):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.conn, child = ctx.Pipe()
+        saved = {k: os.environ.get(k) for k in ("MALLOC_PERTURB_",)}
+        os.environ["MALLOC_PERTURB_"] = "255"
+        try:
+            self.proc = ctx.Process(target=_ref_worker_main, args=(child,), daemon=True)
+            self.proc.start()
+        finally:
+            for k, v in saved.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        child.close()
+
+    def alive(self) -> bool:
+        return self.proc.is_alive()
+
+    def call(self, h, method, *args):
+        try:
+            self.conn.send((h, method, args))
+            ok, val = self.conn.recv()
+        except (EOFError, BrokenPipeError, ConnectionResetError):
+            self.proc.join(5)
+            raise ReferenceCrash(f"the compiled reference's process ended (exit code {self.proc.exitcode}) "
+                                 f"in {method}{args}") from None
+        if not ok:
+            raise val
+        return val
+
+
+_worker = None
+
+
+def _ref_worker() -> _RefWorker:
+    global _worker
+    if _worker is None or not _worker.alive():
+        _worker = _RefWorker()
+    return _worker
+
+
+class RefRun:
+    """The reference solver (CreateSystem + input + sph.cc's loop) on a deck
+    directory, run in the reference's own child process (see above).
+    fluid_capacity_pct > 0 shrinks the reference's 100 Nf particle capacity
+    (see oracle/ref_harness.c)."""
+
+    def __init__(self, deck_dir: str, eta_override: float = 0.0, fluid_capacity_pct: int = 0):
+        self.w = _ref_worker()
+        self.h = self.w.call(None, "open", os.path.abspath(deck_dir), float(eta_override), int(fluid_capacity_pct))
+
+    def _call(self, method, *args):
+        return self.w.call(self.h, method, *args)
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            h, self.h = self.h, None
+            if self.w.alive():
+                self.w.call(h, "close")
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def counts(self) -> dict:
+        return self._call("counts")
+
+    def scalars(self) -> dict:
+        return self._call("scalars")
+
+    def step(self, nsteps: int = 1) -> None:
+        self._call("step", int(nsteps))
+
+    def derivatives(self, t: float) -> None:
+        self._call("derivatives", float(t))
+
+    def get(self, name: str, first: int = 0, n: int = None) -> np.ndarray:
+        return self._call("get", name, first, n)
+
+    def set(self, name: str, values: np.ndarray, first: int = 0) -> None:
+        self._call("set", name, np.ascontiguousarray(values, dtype=np.float64), first)
+
+    def itype(self, first: int = 0, n: int = None) -> np.ndarray:
+        return self._call("itype", first, n)
+
+    def pairs(self):
+        return self._call("pairs")
+
+    def time_inputbp(self, ncalls: int = 3) -> float:
+        return self._call("time_inputbp", ncalls)
+
+    def truncated_queries(self) -> int:
+        return self._call("truncated_queries")
+
+    def max_inradius(self) -> int:
+        return self._call("max_inradius")
 
 
 # fields compared after a step (reference name -> uph_state name is the same)

@@ -368,6 +368,7 @@ static double *scal_field(System *s, const char *name)
   if (!strcmp(name, "hsml")) return s->hsml;
   if (!strcmp(name, "rij2")) return s->rij2;
   if (!strcmp(name, "w")) return s->w;
+  if (!strcmp(name, "spongeFactor")) return s->spongeFactor;
   return NULL;
 }
 

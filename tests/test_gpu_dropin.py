@@ -29,7 +29,7 @@ def _need(*paths):
             pytest.skip(f"{p} not built (make -C oracle ref dropin)")
 
 
-class DropInRun(O.RefRun):
+class DropInRun(O.RefRunInProcess):
     """The harness API over the reference host code + libuph_sph.so."""
     _lib = None
 

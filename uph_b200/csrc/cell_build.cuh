@@ -1,5 +1,4 @@
-// The one-launch cell-list build (celllist.cu) as device code, so that a
-// persistent cooperative rate pass can run it before its tiles.
+// The phases of the one-launch cell-list build (celllist.cu).
 #pragma once
 
 #include "uph_internal.cuh"
@@ -46,6 +45,7 @@ struct CellBuildArgs {
   int storage_order;
   unsigned *rebuild;  // non-null: skip unless set; clear it and record the binned positions
   double *xbin, *ybin;
+  PassStats stats;    // non-null niac: zeroed for the rate pass that follows, built or not
 };
 
 // Grid-wide barrier over co-resident blocks: arrive on bar[0]; the last

@@ -11,10 +11,8 @@
 // (2 reach + 1)^2 block; reach 2, cells of half the radius, by default).
 #include <algorithm>
 
-#include <mutex>
-#include <vector>
 
-#include "tile_pass.cuh"
+#include "cell_build.cuh"
 
 namespace uph {
 
@@ -186,6 +184,10 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
 {
   __shared__ int s_off[kCellBuildMaxBlocks + 1];
   __shared__ int s_wt[33];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.stats.niac) {
+    *A.stats.niac = 0ull;
+    *A.stats.max_nb = 0;
+  }
   // the list from the last build is still complete: nothing to do (every
   // block reads the flag before any block can clear it, in phase 4)
   if (A.rebuild && *(volatile unsigned *)A.rebuild == 0u) return;
@@ -193,7 +195,8 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
 }
 
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s, bool check_rebuild)
+                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats,
+                             cudaStream_t s, bool check_rebuild)
 {
   // co-resident blocks: the cooperative launch refuses a grid that does not fit
   static int max_blocks[64] = {};
@@ -223,6 +226,7 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   A.rebuild = check_rebuild ? P.rebuild : nullptr;
   A.xbin = P.xbin;
   A.ybin = P.ybin;
+  A.stats = stats ? *stats : PassStats{nullptr, nullptr};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(kCellBuildThreads);
@@ -237,25 +241,5 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   return UPH_OK;
 }
 
-int persistent_blocks(const void *kernel, int dev, size_t smem_bytes)
-{
-  struct Entry {
-    const void *kernel;
-    int dev, blocks;
-  };
-  static std::mutex mutex;
-  static std::vector<Entry> cache;
-  std::lock_guard<std::mutex> lock(mutex);
-  for (const Entry &e : cache)
-    if (e.kernel == kernel && e.dev == dev) return e.blocks;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) != cudaSuccess)
-    return 0;
-  int sms = 0, per_sm = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileThreads, smem_bytes) != cudaSuccess) return 0;
-  const int blocks = std::min(std::min(sms * per_sm, kPassMaxBlocks), kCellBuildMaxBlocks);
-  cache.push_back({kernel, dev, blocks});
-  return blocks;
-}
 
 }  // namespace uph

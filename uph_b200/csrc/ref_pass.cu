@@ -455,40 +455,43 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
   }
 }
 
-// The REF rate pass: one persistent cooperative launch (tile_pass.cuh).
-// kBrute: the wall modes that act on every boundary particle within the
-// radius (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on
-// listed pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
+// The REF rate pass: one CTA per storage tile (tile_pass.cuh).  kBrute: the
+// wall modes that act on every boundary particle within the radius
+// (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on listed
+// pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
 template <bool kBrute, bool kKnn>
 __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                           PassStats st, const CellBuildArgs BA, int build_cells)
+                                                           PassStats st)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned my_pairs = 0;
   int my_nb = 0;  // largest in-radius count of this thread's particles
-  persistent_pass(P, BA, build_cells != 0, smem, st, my_pairs, my_nb,
-                  [&](int tile) { ref_tile<kBrute, kKnn>(P, S, G, tile, smem, my_pairs, my_nb); });
+  ref_tile<kBrute, kKnn>(P, S, G, blockIdx.x, smem, my_pairs, my_nb);
+  pass_stats(st, my_pairs, my_nb);
 }
 
 template <bool kBrute, bool kKnn>
-uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
-                      unsigned *err, cudaStream_t s)
+uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
+  static bool attr_set[64] = {};  // once per device
+  int dev = 0;
+  UPH_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    UPH_CUDA(cudaFuncSetAttribute(k_ref_pass<kBrute, kKnn>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)ref_smem<kKnn>()));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  return launch_persistent(k_ref_pass<kBrute, kKnn>, ref_smem<kKnn>(), ntiles, s, P, S, G, st,
-                           pass_build_args(P, S, G, err), build_cells ? 1 : 0);
+  k_ref_pass<kBrute, kKnn><<<ntiles, kTileThreads, ref_smem<kKnn>(), s>>>(P, S, G, st);
+  return UPH_OK;
 }
 
-uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
-                           unsigned *err, cudaStream_t s)
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
   if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
-  if (P.knn > 0)
-    return brute ? launch_ref<true, true>(P, S, G, st, build_cells, err, s)
-                 : launch_ref<false, true>(P, S, G, st, build_cells, err, s);
-  return brute ? launch_ref<true, false>(P, S, G, st, build_cells, err, s)
-               : launch_ref<false, false>(P, S, G, st, build_cells, err, s);
+  if (P.knn > 0) return brute ? launch_ref<true, true>(P, S, G, st, s) : launch_ref<false, true>(P, S, G, st, s);
+  return brute ? launch_ref<true, false>(P, S, G, st, s) : launch_ref<false, false>(P, S, G, st, s);
 }
 
 // The knn cap's cut of every fluid query: walk the stencil (the global cell

@@ -77,10 +77,9 @@ struct uph_sim {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   unsigned *d_err = nullptr;
-  // the rate pass's statistics, one entry per block of its last launch
+  // the rate pass's statistics, zeroed by the cell-list launch before it
   unsigned long long *d_niac = nullptr;
   int *d_max_nb = nullptr;
-  int *d_pass_nblocks = nullptr;
   int *d_perm = nullptr;  // scratch for uploads and reorders
   int itime = 0;
   int steps_since_reorder = 0;
@@ -336,16 +335,17 @@ __global__ void k_iota(int *p, int first, int count)
 // storage key instead of the row-major cell-list id.
 uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, int count, bool storage_order)
 {
-  uph_status r = launch_cell_build(s->P, x, y, first, count, s->G, s->d_err, storage_order, s->stream);
+  uph_status r = launch_cell_build(s->P, x, y, first, count, s->G, s->d_err, storage_order, nullptr, s->stream);
   s->launches += 1;
   return r;
 }
 
-// the cell list of all interacting particles, when the skin test asks for it
-uph_status build_cell_list(uph_sim *s)
+// the cell list of all interacting particles, when the skin test asks for
+// it; zeroes the pass statistics given
+uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr)
 {
   Timer t(s, KF_CELLS);
-  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, s->stream, true);
+  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, stats, s->stream, true);
   s->launches += 1;
   return r;
 }
@@ -404,20 +404,16 @@ uph_status rate_pass(uph_sim *s, bool refresh)
     launch_refresh_inverse(s->P, s->S, 0, s->P.nf, s->stream);
     s->launches++;
   }
-  const PassStats st{s->d_niac, s->d_max_nb, s->d_pass_nblocks};
-  // the pass rebuilds the cell list itself (when the skin test asks for it)
-  // unless the knn cut must read the list first
-  const bool fused = s->P.knn <= 0;
-  if (!fused) {
-    uph_status r = build_cell_list(s);
-    if (r != UPH_OK) return r;
+  const PassStats st{s->d_niac, s->d_max_nb};
+  uph_status r = build_cell_list(s, &st);
+  if (r != UPH_OK) return r;
+  if (s->P.knn > 0) {
     launch_knn_cut(s->P, s->S, s->G, s->stream);
     s->launches++;
   }
   Timer t(s, KF_PASS);
-  uph_status r = s->P.profile == UPH_PROFILE_REF
-                     ? launch_ref_pass(s->P, s->S, s->G, st, fused, s->d_err, s->stream)
-                     : launch_wcsph_pass(s->P, s->S, s->G, st, fused, s->d_err, s->stream);
+  r = s->P.profile == UPH_PROFILE_REF ? launch_ref_pass(s->P, s->S, s->G, st, s->stream)
+                                      : launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
   if (r != UPH_OK) return r;
   s->launches++;
   if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF) {
@@ -655,10 +651,8 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   double **tfl2[] = {&T.vmin, &T.acc, &T.acc_a, &T.fvel};
   for (double **q : tfl2) TRY(dalloc(s, q, 2 * (size_t)nf));
   TRY(dalloc(s, &s->d_err, 1));
-  TRY(dalloc(s, &s->d_niac, kPassMaxBlocks));
-  TRY(dalloc(s, &s->d_max_nb, kPassMaxBlocks));
-  TRY(dalloc(s, &s->d_pass_nblocks, 1));
-  TRY(cudaMemset(s->d_pass_nblocks, 0, sizeof(int)));
+  TRY(dalloc(s, &s->d_niac, 1));
+  TRY(dalloc(s, &s->d_max_nb, 1));
   TRY(dalloc(s, &s->d_perm, (size_t)n));
   TRY(dalloc(s, &s->d_itime, 1));
   TRY(dalloc(s, &s->d_wall_tab, 4 * (size_t)(p->n_moving > 0 ? p->n_moving : 1)));
@@ -1334,22 +1328,12 @@ extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
   k_stats<<<nb, 256, 0, s->stream>>>(s->P, s->S, s->d_partials, nb);
   s->launches++;
   std::vector<double> part(4 * (size_t)nb);
-  std::vector<unsigned long long> niac_b(kPassMaxBlocks);
-  std::vector<int> nb_b(kPassMaxBlocks);
-  int pass_blocks = 0;
-  UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaMemcpyAsync(&pass_blocks, s->d_pass_nblocks, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaMemcpyAsync(niac_b.data(), s->d_niac, sizeof(unsigned long long) * kPassMaxBlocks,
-                           cudaMemcpyDeviceToHost, s->stream));
-  UPH_CUDA(cudaMemcpyAsync(nb_b.data(), s->d_max_nb, sizeof(int) * kPassMaxBlocks, cudaMemcpyDeviceToHost,
-                           s->stream));
-  UPH_CUDA(cudaStreamSynchronize(s->stream));
   unsigned long long niac = 0;
   int mx = 0;
-  for (int b = 0; b < std::min(pass_blocks, kPassMaxBlocks); b++) {
-    niac += niac_b[b];
-    mx = std::max(mx, nb_b[b]);
-  }
+  UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(&niac, s->d_niac, sizeof niac, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
   for (int b = 0; b < nb; b++) {
     out->kinetic_energy += part[b];
     out->potential_energy += part[nb + b];

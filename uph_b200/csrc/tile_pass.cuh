@@ -18,7 +18,6 @@
 
 #include <algorithm>
 
-#include "cell_build.cuh"
 #include "pass_common.cuh"
 
 namespace uph {
@@ -275,113 +274,16 @@ __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cur
   return cnt;
 }
 
-// ---- the persistent frame of a rate pass ------------------------------------------
-// One cooperative launch per pass with as many blocks as are resident: when
-// build_cells is set and the cell list's rebuild flag is raised, the blocks
-// first build the list (cell_build.cuh) and meet at a grid barrier.  Then
-// block b runs tile b and takes further tiles from a ticket counter
-// (G.bar[2]) in index order, as the hardware's block scheduler would hand
-// them out; the ticket for the next tile is drawn while the current one
-// runs.  The last block to finish (G.bar[3]) resets both words for the next
-// pass.  `tile_body(tile)` runs one tile (all threads; it may return early
-// for an empty tile).  Statistics are reduced over the block and stored in
-// the block's own entry of `st`.
-template <typename TileBody>
-__device__ __forceinline__ void persistent_pass(const DevParams &P, const CellBuildArgs &BA, bool build_cells,
-                                                unsigned char *scratch, PassStats st, unsigned &my_pairs,
-                                                int &my_nb, TileBody tile_body)
+// A pass CTA's statistics: warp reductions, then one atomic per warp into
+// the counters the cell-list launch zeroed.
+__device__ __forceinline__ void pass_stats(const PassStats &st, unsigned my_pairs, int my_nb)
 {
-  __shared__ int s_wt[33];
-  __shared__ unsigned long long s_pairs[kTileThreads / 32];
-  __shared__ int s_nb[kTileThreads / 32];
-  // every block reads the flag before any block can clear it (phase 4 of
-  // the build, after its third grid barrier): the decision is uniform
-  if (build_cells && *(volatile unsigned *)P.rebuild != 0u) {
-    if (!cell_build_phases(BA, reinterpret_cast<int *>(scratch), s_wt)) return;
-    if (!cell_grid_barrier(BA.G.bar, BA.err)) return;
-  }
-  __shared__ int s_next;
-  unsigned *ticket = BA.G.bar + 2, *done = BA.G.bar + 3;
-  const int ntiles = P.ntx * (P.ncy / P.tile);
-  int tile = blockIdx.x;
-  while (tile < ntiles) {
-    __syncthreads();  // the last tile's shared memory and s_next are free again
-    if (threadIdx.x == 0) s_next = (int)gridDim.x + (int)atomicAdd(ticket, 1u);
-    tile_body(tile);
-    __syncthreads();
-    tile = s_next;
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(done, 1u) == gridDim.x - 1) {
-      atomicExch(ticket, 0u);
-      atomicExch(done, 0u);
-    }
-  }
   const unsigned wp = __reduce_add_sync(0xffffffffu, my_pairs);
   const int wn = (int)__reduce_max_sync(0xffffffffu, (unsigned)my_nb);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    s_pairs[warp] = wp;
-    s_nb[warp] = wn;
+  if ((threadIdx.x & 31) == 0) {
+    if (wp) atomicAdd(st.niac, (unsigned long long)wp);
+    if (wn) atomicMax(st.max_nb, wn);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long tp = 0;
-    int tn = 0;
-    for (int w = 0; w < kTileThreads / 32; w++) {
-      tp += s_pairs[w];
-      tn = max(tn, s_nb[w]);
-    }
-    st.niac[blockIdx.x] = tp;
-    st.max_nb[blockIdx.x] = tn;
-    if (blockIdx.x == 0) *st.nblocks = gridDim.x;
-  }
-}
-
-// The cooperative launch of a persistent pass: as many blocks as fit on the
-// device at once (at most the tiles, kPassMaxBlocks and the build's limit).
-// Resident blocks of `kernel` (with its shared memory set up) on device
-// `dev`, looked up once per kernel and device.
-int persistent_blocks(const void *kernel, int dev, size_t smem_bytes);
-
-template <typename Kernel, typename... Args>
-uph_status launch_persistent(Kernel kernel, size_t smem_bytes, int ntiles, cudaStream_t s, Args... args)
-{
-  int dev = 0;
-  UPH_CUDA(cudaGetDevice(&dev));
-  const int mb = persistent_blocks((const void *)kernel, dev, smem_bytes);
-  if (mb < 1) return fail(UPH_CUDA_ERROR, "a rate pass block does not fit on an SM");
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(std::max(1, std::min(mb, ntiles)));
-  cfg.blockDim = dim3(kTileThreads);
-  cfg.dynamicSmemBytes = smem_bytes;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  UPH_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
-  return UPH_OK;
-}
-
-// the build arguments of the cell list the passes use
-inline CellBuildArgs pass_build_args(const DevParams &P, const SlotArrays &S, const CellGrid &G, unsigned *err)
-{
-  CellBuildArgs A;
-  A.P = P;
-  A.x = S.x;
-  A.y = S.y;
-  A.first = 0;
-  A.count = P.n;
-  A.G = G;
-  A.err = err;
-  A.storage_order = 0;
-  A.rebuild = P.rebuild;
-  A.xbin = P.xbin;
-  A.ybin = P.ybin;
-  return A;
 }
 
 }  // namespace uph

@@ -146,7 +146,7 @@ struct WallTable {
   const double *base;
 };
 
-constexpr int kGridWords = 4;
+constexpr int kGridWords = 2;
 
 struct CellGrid {
   int ncell;
@@ -158,12 +158,19 @@ struct CellGrid {
   int *block_sums;
   int nblock_sums;
   // one-launch build (launch_cell_build): rank of each slot in its cell,
-  // per-block totals, the grid barrier's two words and the persistent rate
-  // pass's tile ticket and finish count; count and bar are all zero between
-  // launches
+  // per-block totals and the grid barrier's two words; count and bar are all
+  // zero between builds
   int *rank;       // [n]
   int *totals;     // [kCellBuildMaxBlocks + 1]
   unsigned *bar;   // [kGridWords]
+};
+
+// Statistics of a rate pass, zeroed by the cell-list launch before it: pairs
+// (i < j) counted from the i side, and the largest in-radius neighbour count
+// of a fluid particle.
+struct PassStats {
+  unsigned long long *niac;
+  int *max_nb;
 };
 
 std::string &last_error();
@@ -194,32 +201,23 @@ void launch_cell_sort_segments(const CellGrid &G, unsigned *err, cudaStream_t s)
 constexpr int kCellBuildThreads = 512;
 constexpr int kCellBuildMaxBlocks = 1024;
 // check_rebuild: build only when *P.rebuild is set (and then clear it and
-// record the binned positions); otherwise always build.
+// record the binned positions); otherwise always build.  stats, when given,
+// are zeroed for the rate pass that follows, whether or not the list is
+// rebuilt.
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
-                             CellGrid &G, unsigned *err, bool storage_order, cudaStream_t s,
-                             bool check_rebuild = false);
+                             CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats,
+                             cudaStream_t s, bool check_rebuild = false);
 
-// REF / WCSPH rate pass over the fluid slots
-// Statistics of a rate pass, one entry per block of its (persistent) grid,
-// so that nothing needs zeroing between passes: pairs (i < j) counted from
-// the i side, and the largest in-radius neighbour count of a fluid particle.
-constexpr int kPassMaxBlocks = 1024;
-struct PassStats {
-  unsigned long long *niac;  // [kPassMaxBlocks]
-  int *max_nb;               // [kPassMaxBlocks]
-  int *nblocks;              // the grid size of the last pass (one int)
-};
-// The rate passes run as one persistent cooperative launch; with
-// build_cells they first rebuild the cell list when *P.rebuild is set.
-uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
-                           unsigned *err, cudaStream_t s);
+// REF / WCSPH rate pass over the fluid slots: one CTA per storage tile
+// (tile_pass.cuh); the cell list must be current.
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
 // the knn cap's cut of every fluid query (P.kcut_*), from the cell list
 void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
 // stressType 2, after the rate pass: the shear stress of every listed
 // particle (P.str_*), then its divergence added to the corrector's dv/dt
 void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
 uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
-                             bool build_cells, unsigned *err, cudaStream_t s);
+                             cudaStream_t s);
 
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);

@@ -312,38 +312,42 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
   }
 }
 
-// The WCSPH rate pass: one persistent cooperative launch (tile_pass.cuh).
+// The WCSPH rate pass: one CTA per storage tile (tile_pass.cuh).
 template <bool kBrute, typename Real>
 __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                             PassStats st, const CellBuildArgs BA, int build_cells)
+                                                             PassStats st)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned my_pairs = 0;
   int my_nb = 0;  // largest in-radius count of this thread's particles
-  persistent_pass(P, BA, build_cells != 0, smem, st, my_pairs, my_nb,
-                  [&](int tile) { wc_tile<kBrute, Real>(P, S, G, tile, smem, my_pairs, my_nb); });
+  wc_tile<kBrute, Real>(P, S, G, blockIdx.x, smem, my_pairs, my_nb);
+  pass_stats(st, my_pairs, my_nb);
 }
 
 template <bool kBrute, typename Real>
-uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, bool build_cells,
-                     unsigned *err, cudaStream_t s)
+uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
 {
+  static bool attr_set[64] = {};  // once per device
+  int dev = 0;
+  UPH_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    UPH_CUDA(cudaFuncSetAttribute(k_wcsph_pass<kBrute, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wc_smem<Real>()));
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  return launch_persistent(k_wcsph_pass<kBrute, Real>, wc_smem<Real>(), ntiles, s, P, S, G, st,
-                           pass_build_args(P, S, G, err), build_cells ? 1 : 0);
+  k_wcsph_pass<kBrute, Real><<<ntiles, kTileThreads, wc_smem<Real>(), s>>>(P, S, G, st);
+  return UPH_OK;
 }
 
 uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
-                             bool build_cells, unsigned *err, cudaStream_t s)
+                             cudaStream_t s)
 {
   if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
-  const bool f32 = P.precision == UPH_PREC_FP32_PAIR;
-  if (f32)
-    return brute ? launch_wc<true, float>(P, S, G, st, build_cells, err, s)
-                 : launch_wc<false, float>(P, S, G, st, build_cells, err, s);
-  return brute ? launch_wc<true, double>(P, S, G, st, build_cells, err, s)
-               : launch_wc<false, double>(P, S, G, st, build_cells, err, s);
+  if (P.precision == UPH_PREC_FP32_PAIR)
+    return brute ? launch_wc<true, float>(P, S, G, st, s) : launch_wc<false, float>(P, S, G, st, s);
+  return brute ? launch_wc<true, double>(P, S, G, st, s) : launch_wc<false, double>(P, S, G, st, s);
 }
 
 }  // namespace uph
