@@ -239,7 +239,9 @@ def gpu_arm(args, rank, world, local_rank):
     achieved = pass_bytes / pass_avg_s / 1e9 if pass_avg_s > 0 else 0.0
     # DRAM read + write bytes of one launch from the committed ncu capture
     # (profiles/rate_pass_ref_fp64_hydrostatic500k.md)
+    # and its FP64-pipe activity, the compute roof this kernel is held by
     traffic = None
+    fp64_active = None
     tpath = os.path.join(ROOT, "profiles", "rate_pass_traffic.txt")
     if os.path.exists(tpath):
         with open(tpath) as f:
@@ -247,6 +249,8 @@ def gpu_arm(args, rank, world, local_rank):
                 parts = line.split()
                 if len(parts) == 2 and parts[0] == "ref_fp64_bytes_per_launch":
                     traffic = int(parts[1])
+                if len(parts) == 2 and parts[0] == "ref_fp64_pipe_active":
+                    fp64_active = float(parts[1])
 
     # --- e2e: every step through the C ABI with pinned host buffers:
     # upload the full state, one step, download the full state
@@ -332,7 +336,7 @@ def gpu_arm(args, rank, world, local_rank):
 
     return dict(value=value, ms=ms_max, launches=launches, clocks=clocks, ktimes=ktimes, stats=stats,
                 pass_avg_s=pass_avg_s, pass_bytes=pass_bytes, achieved=achieved, peak=peak, peak_kind=peak_kind,
-                traffic=traffic, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
+                traffic=traffic, fp64_active=fp64_active, e2e_value=e2e_value, h2d=h2d, d2h=d2h, k_e2e=k_e2e, variants=variants,
                 deck=deck, e2e_dropin=e2e_dropin)
 
 
@@ -671,7 +675,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
                      "frac": r["achieved"] / r["peak"], "traffic": r["traffic"],
                      "kernel": "rate pass (k_ref_pass)", "bytes_per_launch": r["pass_bytes"],
-                     "avg_launch_ms": r["pass_avg_s"] * 1e3, "peak_source": r["peak_kind"]},
+                     "avg_launch_ms": r["pass_avg_s"] * 1e3, "peak_source": r["peak_kind"],
+                     "fp64_pipe_active_ncu": r["fp64_active"]},
         "cpu_baseline": cpu,
         "e2e": {"value": r["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "steps": r["k_e2e"],

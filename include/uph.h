@@ -240,6 +240,20 @@ uph_status uph_sim_derivatives(uph_sim *sim, double t);
 uph_status uph_sim_pairs(uph_sim *sim, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
                          double *w, double *dwcdx, int64_t *niac);
 
+/* The virtual mirror particles of the last evaluation (virtualType 1, 3, 4,
+ * 5, 7, 8; derivatives.c:3194-4192), in the reference's order: the reference
+ * index of virtual particle k is n_fluid + n_solid + n_fixed + n_moving + k.
+ * position [count][2]; src: the reference index of the fluid particle it
+ * copies; rule: the mirror that made it (each appears once per type):
+ * 0 left wall (u flipped), 1 right wall (u), 2 bottom (v), 3 top (v),
+ * 4 bottom-left corner (u, v), 5 bottom-right corner (u, v), 6 the slope of
+ * virtualType 1 (velocities reflected in it).  *count is set even when it exceeds `cap` (then
+ * UPH_BAD_ARG and nothing is written when an array is given); all arrays may
+ * be NULL.  They are never in a pair (j < Nf + Ns + Nb - 1,
+ * derivatives.c:1081-1083): they are points of the knn-capped search only. */
+uph_status uph_sim_virtual(uph_sim *sim, int64_t cap, double *position, int32_t *src, int32_t *rule,
+                           int64_t *count);
+
 uph_status uph_sim_stats(uph_sim *sim, uph_stats *out);
 
 /* The reference's per-evaluation diagnostics, computed on the device at the

@@ -207,9 +207,9 @@ class RefRunInProcess:
         self.close()
 
     def counts(self) -> dict:
-        c = np.zeros(8, np.int32)
+        c = np.zeros(9, np.int32)
         self.lib.ref_counts(self.h, c.ctypes.data)
-        keys = ["n_fluid", "n_solid", "n_fixed", "n_moving", "n_boundary", "niac", "max_n", "itime"]
+        keys = ["n_fluid", "n_solid", "n_fixed", "n_moving", "n_boundary", "niac", "max_n", "itime", "n_virtual"]
         return dict(zip(keys, (int(v) for v in c)))
 
     def scalars(self) -> dict:

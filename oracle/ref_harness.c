@@ -300,9 +300,10 @@ int ref_step(ref_run *run, int nsteps)
 }
 
 /* counts: Nf, Ns, Nfixed, Nmoving, Nb, niac, MaxN, itime */
-void ref_counts(const ref_run *run, int out[8])
+void ref_counts(const ref_run *run, int out[9])
 {
   const System *s = run->sys;
+  out[8] = s->NumberOfVirtualParticles;
   out[0] = s->NumberOfFluidParticles;
   out[1] = s->NumberOfSolidParticles;
   out[2] = s->NumberOfFixedBoundaryParticles;

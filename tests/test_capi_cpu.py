@@ -175,7 +175,7 @@ def test_sim_create_without_device_fails_cleanly():
 def test_sim_create_rejects_unsupported_modes():
     deck = D.dam_break(dx=0.1)
     # stressType 2 exists for the REF profile only
-    for over, status in [({"virtual_type": 7}, 8), ({"stress_type": 2, "profile": 1}, 8), ({"flag_init_simul": 0}, 8),
+    for over, status in [({"stress_type": 2, "profile": 1}, 8), ({"flag_init_simul": 0}, 8),
                          ({"precision": 1}, 8), ({"domain_hi": None}, 1)]:
         d = deck.uph_params()
         d.update(over)

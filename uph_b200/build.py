@@ -35,6 +35,7 @@ CORE_SOURCES = [
     ("ref_pass.cu", []),
     ("wcsph_pass.cu", []),
     ("integrate.cu", ["--fmad=false"]),
+    ("virtual.cu", ["--fmad=false"]),
     ("sim.cu", []),
     ("search_noalloc.cu", []),
     ("tc_gemm.cu", ["@cutlass"]),

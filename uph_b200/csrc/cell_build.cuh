@@ -46,6 +46,8 @@ struct CellBuildArgs {
   unsigned *rebuild;  // non-null: skip unless set; clear it and record the binned positions
   double *xbin, *ybin;
   PassStats stats;    // non-null niac: zeroed for the rate pass that follows, built or not
+  int *step_counter;  // non-null: advanced by one, built or not
+  const int *dyn_count;  // non-null: the ids are [first, first + min(count, *dyn_count))
 };
 
 // Grid-wide barrier over co-resident blocks: arrive on bar[0]; the last
@@ -121,12 +123,13 @@ __device__ __forceinline__ bool cell_build_phases(const CellBuildArgs &A, int *s
 {
   const int nb = gridDim.x, b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
   const int stride = nb * nt;
+  const int count = A.dyn_count ? min(A.count, *A.dyn_count) : A.count;
   const int ncell = A.G.ncell;
   int *cnt = A.G.count, *start = A.G.start, *fill = A.G.fill, *list = A.G.list;
   int *cell_of = A.G.cell_of, *rank = A.G.rank;
 
   // 1. keys and histogram
-  for (int k = b * nt + t; k < A.count; k += stride) {
+  for (int k = b * nt + t; k < count; k += stride) {
     const int s = A.first + k;
     const double px = A.x[s], py = A.y[s];
     const int c = cell_of_position(A.P, px, py, A.err, A.storage_order != 0);
@@ -184,7 +187,7 @@ __device__ __forceinline__ bool cell_build_phases(const CellBuildArgs &A, int *s
   }
   for (int c = c0 + t; c < c1; c += nt) start[c] = fill[c] + s_off[b];
   if (b == nb - 1 && t == 0) start[ncell] = s_off[nb];
-  for (int k = b * nt + t; k < A.count; k += stride) {
+  for (int k = b * nt + t; k < count; k += stride) {
     const int s = A.first + k;
     const int c = cell_of[s];
     list[fill[c] + s_off[c / chunk] + rank[s]] = s;

@@ -184,9 +184,12 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
 {
   __shared__ int s_off[kCellBuildMaxBlocks + 1];
   __shared__ int s_wt[33];
-  if (blockIdx.x == 0 && threadIdx.x == 0 && A.stats.niac) {
-    *A.stats.niac = 0ull;
-    *A.stats.max_nb = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (A.stats.niac) {
+      *A.stats.niac = 0ull;
+      *A.stats.max_nb = 0;
+    }
+    if (A.step_counter) *A.step_counter += 1;
   }
   // the list from the last build is still complete: nothing to do (every
   // block reads the flag before any block can clear it, in phase 4)
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(kCellBuildThreads) k_cell_build(const CellBuil
 
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
                              CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats,
-                             cudaStream_t s, bool check_rebuild)
+                             cudaStream_t s, bool check_rebuild, int *step_counter, const int *dyn_count)
 {
   // co-resident blocks: the cooperative launch refuses a grid that does not fit
   static int max_blocks[64] = {};
@@ -227,6 +230,8 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
   A.xbin = P.xbin;
   A.ybin = P.ybin;
   A.stats = stats ? *stats : PassStats{nullptr, nullptr};
+  A.step_counter = step_counter;
+  A.dyn_count = dyn_count;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(kCellBuildThreads);

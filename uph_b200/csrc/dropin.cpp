@@ -150,6 +150,64 @@ void ensure_sim(const System *sys, int n)
   g.p = p;
 }
 
+// The virtual mirror particles (derivatives.c:3194-4192) as the reference
+// leaves them in the System: rows from Nf + Ns + Nb on, each a copy of its
+// fluid particle taken before this call's equation of state, with the
+// mirrored position (computed on the device) and velocities, itype 4.
+void write_virtual_rows(System *sys, int n)
+{
+  int64_t nv = 0;
+  uph_status s = uph_sim_virtual(g.sim, 0, nullptr, nullptr, nullptr, &nv);
+  if (s != UPH_OK) die("derivatives", s);
+  sys->NumberOfVirtualParticles = (int)nv;
+  if (nv == 0) return;
+  if (n + nv > sys->MaxNumberOfParticles) {
+    printf("derivatives: %lld virtual particles do not fit in MaxNumberOfParticles = %d\n", (long long)nv,
+           sys->MaxNumberOfParticles);
+    fflush(stdout);
+    exit(1);
+  }
+  std::vector<double> pos(2 * (size_t)nv);
+  std::vector<int32_t> src((size_t)nv), kind((size_t)nv);
+  s = uph_sim_virtual(g.sim, nv, pos.data(), src.data(), kind.data(), &nv);
+  if (s != UPH_OK) die("derivatives", s);
+  const double sl = sys->slope, denoms = 1 + sl * sl, nums = 1 - sl * sl;
+  for (int64_t k = 0; k < nv; k++) {
+    const int ii = n + (int)k, i = src[k];
+    sys->Position[ii][0] = pos[2 * k];
+    sys->Position[ii][1] = pos[2 * k + 1];
+    for (double **v : {sys->Velocity, sys->Velocity_xsph, sys->localVelocity}) {
+      const double vx = v[i][0], vy = v[i][1];
+      switch (kind[k]) {
+        case 0:  // left and right walls
+        case 1:
+          v[ii][0] = -vx;
+          v[ii][1] = vy;
+          break;
+        case 2:  // bottom and top
+        case 3:
+          v[ii][0] = vx;
+          v[ii][1] = -vy;
+          break;
+        case 4:  // corners
+        case 5:
+          v[ii][0] = -vx;
+          v[ii][1] = -vy;
+          break;
+        default:  // the slope
+          v[ii][0] = (nums * vx + 2.0 * sl * vy) / denoms;
+          v[ii][1] = (2.0 * sl * vx - nums * vy) / denoms;
+          break;
+      }
+    }
+    for (double *f : {sys->mass, sys->density, sys->Pressure, sys->Energy, sys->hsml, sys->normalizationFactor,
+                      sys->DynamicPressure, sys->localDensity, sys->localPressure, sys->vorticity,
+                      sys->thermalDiffusivity})
+      f[ii] = f[i];
+    sys->itype[ii] = 4;
+  }
+}
+
 }  // namespace
 
 extern "C" void derivatives(System *sys, double t)
@@ -207,6 +265,7 @@ extern "C" void derivatives(System *sys, double t)
   if (s != UPH_OK) die("derivatives", s);
   s = uph_sim_derivatives(g.sim, t);
   if (s != UPH_OK) die("derivatives", s);
+  write_virtual_rows(sys, n);
   uph_state out;
   memset(&out, 0, sizeof out);
   out.ddensitydt = sys->ddensitydt;

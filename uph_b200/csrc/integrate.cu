@@ -7,6 +7,8 @@
 // n + 1 run in one kernel (they touch the same per-particle state and the
 // predictor needs nothing the corrector does not already hold); the first
 // step of a call uses the stand-alone predictor.
+#include <algorithm>
+
 #include "uph_internal.cuh"
 
 namespace uph {
@@ -84,12 +86,75 @@ __device__ __forceinline__ void note_moved(const DevParams &P, int slot, double 
   if (!(x >= P.lo_x && y >= P.lo_y && x <= P.hi_x && y <= P.hi_y)) atomicOr(err, ERR_OUT_OF_DOMAIN);
 }
 
-__global__ void k_correct(const DevParams P, const SlotArrays S, int first_step, int predict_next, unsigned *err,
-                          int *d_itime)
+// Moving boundary particles (reference indices [m0, b1)), found through
+// their slot's reference index.
+//  - inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
+//    x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt;
+//  - inputbp.c:209-223 (movingBoundary 3, the lid): x = x0 + U t,
+//    u = ut = U, from each particle's base x0;
+//  - inputbp.c:224-243 (movingBoundary 2, the gate): y = y0 + U t and
+//    v = U while 0 < t < t_stop, else y = y0 + U t_stop and v = 0 (the
+//    reference leaves the gate's local velocity alone);
+//  - a WallTable shakes each particle about its own rest position with its
+//    own half stroke and frequency (one entry per particle, e.g. every wall
+//    of a sloshing tank moving rigidly).
+__device__ __forceinline__ void wall_move_one(const DevParams &P, const SlotArrays &S, const WallTable &W, int s,
+                                              double t, unsigned *err)
+{
+  const int o = S.orig[s];
+  if (o < P.m0 || o >= P.b1) return;
+  if (!W.enabled && P.moving_boundary == 3) {
+    const double U = P.lid_velocity;
+    const double x = U * t + W.base[o - P.m0];
+    S.x[s] = x;
+    S.u[s] = U;
+    S.ut[s] = U;
+    note_moved(P, s, x, S.y[s], err);
+    return;
+  }
+  if (!W.enabled && P.moving_boundary == 2) {
+    const double U = P.lid_velocity;
+    double y;
+    if (t > 0.0 && t < P.gate_stop) {
+      y = U * t + W.base[o - P.m0];
+      S.v[s] = U;
+    } else {
+      y = U * P.gate_stop + W.base[o - P.m0];
+      S.v[s] = 0.0;
+    }
+    S.y[s] = y;
+    note_moved(P, s, S.x[s], y, err);
+    return;
+  }
+  double x, u;
+  if (W.enabled) {
+    const int m = o - P.m0;
+    const double hs = W.hs[m], om = W.om[m];
+    x = W.x0[m] + hs * (1.0 - cos(om * t));
+    u = hs * om * sin(om * t);
+  } else {
+    x = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
+    u = 0.5 * P.stroke * P.omega * sin(P.omega * t);
+  }
+  S.x[s] = x;
+  S.u[s] = u;
+  S.ut[s] = u;
+  note_moved(P, s, x, S.y[s], err);
+}
+
+
+// The corrector of the fluid slots; with predict_next also the next step's
+// predictor, and with walls_next the next step's wall motion on the threads
+// past the fluid (its time from the device step counter, which the next
+// step's cell-list launch advances: (steps started + 1) dt).
+__global__ void k_correct(const DevParams P, const SlotArrays S, const WallTable W, int first_step, int predict_next,
+                          int walls_next, unsigned *err, const int *d_itime)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a == 0 && d_itime) *d_itime += 1;  // steps completed, read by the next step's wall motion
-  if (a >= P.nf) return;
+  if (a >= P.nf) {
+    if (walls_next && a < P.n) wall_move_one(P, S, W, a, (*d_itime + 1) * P.dt, err);
+    return;
+  }
   const double dt = P.dt;
   const double drho = S.drho[a], dp = S.dp[a], ax = S.ax[a], ay = S.ay[a];
   const double frho = S.frho[a], fp = S.fp[a], fu = P.eps * S.fu[a], fv = P.eps * S.fv[a];
@@ -139,11 +204,11 @@ __global__ void k_correct(const DevParams P, const SlotArrays S, int first_step,
   }
 }
 
-void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
-                    int *d_itime, cudaStream_t s)
+void launch_correct(const DevParams &P, const SlotArrays &S, const WallTable &W, int first_step, int predict_next,
+                    int walls_next, unsigned *err, const int *d_itime, cudaStream_t s)
 {
-  const int n = P.nf > 0 ? P.nf : 1;
-  k_correct<<<(n + 255) / 256, 256, 0, s>>>(P, S, first_step, predict_next, err, d_itime);
+  const int n = std::max(walls_next ? P.n : P.nf, 1);
+  k_correct<<<(n + 255) / 256, 256, 0, s>>>(P, S, W, first_step, predict_next, walls_next, err, d_itime);
 }
 
 // 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure; for
@@ -172,64 +237,14 @@ void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, 
   if (count > 0) k_refresh<<<(count + 255) / 256, 256, 0, s>>>(P, S, first, count);
 }
 
-// Moving boundary particles (reference indices [m0, b1)), found through
-// their slot's reference index.
-//  - inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
-//    x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt;
-//  - inputbp.c:209-223 (movingBoundary 3, the lid): x = x0 + U t,
-//    u = ut = U, from each particle's base x0;
-//  - inputbp.c:224-243 (movingBoundary 2, the gate): y = y0 + U t and
-//    v = U while 0 < t < t_stop, else y = y0 + U t_stop and v = 0 (the
-//    reference leaves the gate's local velocity alone);
-//  - a WallTable shakes each particle about its own rest position with its
-//    own half stroke and frequency (one entry per particle, e.g. every wall
-//    of a sloshing tank moving rigidly).
+// the walls at the step's evaluation time: (steps started + 1) dt from the
+// device step counter, else t_host
 __global__ void k_wall_motion(const DevParams P, const SlotArrays S, const WallTable W, double t_host,
                               const int *d_itime, unsigned *err)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = P.nf + k;
+  const int s = P.nf + blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.n) return;
-  const int o = S.orig[s];
-  if (o < P.m0 || o >= P.b1) return;
-  const double t = d_itime ? (*d_itime + 1) * P.dt : t_host;
-  if (!W.enabled && P.moving_boundary == 3) {
-    const double U = P.lid_velocity;
-    const double x = U * t + W.base[o - P.m0];
-    S.x[s] = x;
-    S.u[s] = U;
-    S.ut[s] = U;
-    note_moved(P, s, x, S.y[s], err);
-    return;
-  }
-  if (!W.enabled && P.moving_boundary == 2) {
-    const double U = P.lid_velocity;
-    double y;
-    if (t > 0.0 && t < P.gate_stop) {
-      y = U * t + W.base[o - P.m0];
-      S.v[s] = U;
-    } else {
-      y = U * P.gate_stop + W.base[o - P.m0];
-      S.v[s] = 0.0;
-    }
-    S.y[s] = y;
-    note_moved(P, s, S.x[s], y, err);
-    return;
-  }
-  double x, u;
-  if (W.enabled) {
-    const int m = o - P.m0;
-    const double hs = W.hs[m], om = W.om[m];
-    x = W.x0[m] + hs * (1.0 - cos(om * t));
-    u = hs * om * sin(om * t);
-  } else {
-    x = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
-    u = 0.5 * P.stroke * P.omega * sin(P.omega * t);
-  }
-  S.x[s] = x;
-  S.u[s] = u;
-  S.ut[s] = u;
-  note_moved(P, s, x, S.y[s], err);
+  wall_move_one(P, S, W, s, d_itime ? (*d_itime + 1) * P.dt : t_host, err);
 }
 
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,

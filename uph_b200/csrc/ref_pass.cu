@@ -499,7 +499,26 @@ uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGr
 // the in-radius points (DBL_EPSILON < r^2 < (h h) 4, the own point and
 // coincident points excluded, as in SearchNeighbors) in a sorted array, and
 // record the largest kept key if more than knn points were in radius.
-__global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotArrays S, const CellGrid G)
+// One in-radius candidate (r2, reference index) of a query: kept among the
+// K smallest keys so far (kd, kj sorted ascending, m of them).
+__device__ __forceinline__ void knn_offer(double r2cut, int K, double r2, int ob, double *kd, int *kj, int &m,
+                                          int &count)
+{
+  if (!(r2 < r2cut) || r2 <= DBL_EPSILON) return;
+  count++;
+  if (m == K && knn_key_le(kd[K - 1], kj[K - 1], r2, ob)) return;  // not among the K smallest
+  int i = m < K ? m++ : K - 1;  // the slot the new key may take
+  while (i > 0 && !knn_key_le(kd[i - 1], kj[i - 1], r2, ob)) {
+    kd[i] = kd[i - 1];
+    kj[i] = kj[i - 1];
+    i--;
+  }
+  kd[i] = r2;
+  kj[i] = ob;
+}
+
+__global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                 const VirtualPoints V)
 {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= P.nf) return;
@@ -508,25 +527,24 @@ __global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotAr
   int kj[kKnnMax];
   int m = 0, count = 0;
   const double xa = S.x[a], ya = S.y[a];
+  auto offer = [&](double r2, int ob) { knn_offer(P.r2cut, K, r2, ob, kd, kj, m, count); };
+  const int cell = G.cell_of[a];
   NeighbourCursor cur;
-  cur.init(P, G, G.cell_of[a]);
+  cur.init(P, G, cell);
   int pos;
   while (cur.next(pos)) {
     const int b = G.list[pos];
     if (b == a) continue;
-    const double r2 = exact_r2(xa - S.x[b], ya - S.y[b]);
-    if (!(r2 < P.r2cut) || r2 <= DBL_EPSILON) continue;
-    const int ob = S.orig[b];
-    count++;
-    if (m == K && knn_key_le(kd[K - 1], kj[K - 1], r2, ob)) continue;  // not among the K smallest
-    int i = m < K ? m++ : K - 1;  // the slot the new key may take
-    while (i > 0 && !knn_key_le(kd[i - 1], kj[i - 1], r2, ob)) {
-      kd[i] = kd[i - 1];
-      kj[i] = kj[i - 1];
-      i--;
+    offer(exact_r2(xa - S.x[b], ya - S.y[b]), S.orig[b]);
+  }
+  // the virtual mirror particles are points of the reference's search too
+  // (reference indices from Nf + Ns + Nb on), though never in a pair
+  if (V.grid.list) {
+    cur.init(P, V.grid, cell);
+    while (cur.next(pos)) {
+      const int v = V.grid.list[pos];
+      offer(exact_r2(xa - V.x[v], ya - V.y[v]), P.n + v);
     }
-    kd[i] = r2;
-    kj[i] = ob;
   }
   if (count > K) {
     P.kcut_d2[a] = kd[K - 1];
@@ -537,10 +555,11 @@ __global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotAr
   }
 }
 
-void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s)
+void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, const VirtualPoints &V,
+                    cudaStream_t s)
 {
   if (P.nf <= 0 || P.knn <= 0) return;
-  k_knn_cut<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G);
+  k_knn_cut<<<(P.nf + 127) / 128, 128, 0, s>>>(P, S, G, V);
 }
 
 // ---- stressType 2 (ClassicShearStress, derivatives.c:1686-1721, and

@@ -123,6 +123,11 @@ struct uph_sim {
   double *d_diag_part = nullptr;  // [kDiagRows][diag_blocks]
   unsigned *d_diag_done = nullptr;
   DevDiag *d_diag = nullptr;
+  // virtual mirror particles (virtual.cu): generated every evaluation when
+  // the virtualType has rules; their own cell list feeds the knn cut
+  VirtualBuf vb = {};
+  CellGrid gv = {};
+  double deriv_t = 0.0;  // the time of a uph_sim_derivatives call
 };
 
 namespace {
@@ -341,11 +346,12 @@ uph_status sort_range(uph_sim *s, const double *x, const double *y, int first, i
 }
 
 // the cell list of all interacting particles, when the skin test asks for
-// it; zeroes the pass statistics given
-uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr)
+// it; zeroes the pass statistics given and advances the step counter given
+uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr, int *step_counter = nullptr)
 {
   Timer t(s, KF_CELLS);
-  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, stats, s->stream, true);
+  uph_status r = launch_cell_build(s->P, s->S.x, s->S.y, 0, s->P.n, s->G, s->d_err, false, stats, s->stream, true,
+                                   step_counter);
   s->launches += 1;
   return r;
 }
@@ -397,7 +403,9 @@ uph_status check_error_word(uph_sim *s)
 
 // refresh: recompute 1/rho, 1/rhot (and the WCSPH pressure) first; a
 // predictor that ran since the last state change has done it already
-uph_status rate_pass(uph_sim *s, bool refresh)
+// step: a leapfrog step of uph_sim_step starts (the device step counter
+// advances)
+uph_status rate_pass(uph_sim *s, bool refresh, bool step = false)
 {
   if (refresh) {
     Timer t(s, KF_REFRESH);
@@ -405,10 +413,23 @@ uph_status rate_pass(uph_sim *s, bool refresh)
     s->launches++;
   }
   const PassStats st{s->d_niac, s->d_max_nb};
-  uph_status r = build_cell_list(s, &st);
+  uph_status r = build_cell_list(s, &st, step ? s->d_itime : nullptr);
   if (r != UPH_OK) return r;
+  VirtualPoints vp = {nullptr, nullptr, CellGrid{}};
+  if (s->P.nvrules > 0) {
+    Timer t(s, KF_CELLS);
+    launch_virtual(s->P, s->S, s->vb, s->deriv_t, step ? s->d_itime : nullptr, s->stream);
+    s->launches += 3;
+    if (s->P.knn > 0) {
+      r = launch_cell_build(s->P, s->vb.x, s->vb.y, 0, s->vb.cap, s->gv, s->d_err, false, nullptr, s->stream,
+                            false, nullptr, s->vb.count);
+      if (r != UPH_OK) return r;
+      s->launches++;
+      vp = VirtualPoints{s->vb.x, s->vb.y, s->gv};
+    }
+  }
   if (s->P.knn > 0) {
-    launch_knn_cut(s->P, s->S, s->G, s->stream);
+    launch_knn_cut(s->P, s->S, s->G, vp, s->stream);
     s->launches++;
   }
   Timer t(s, KF_PASS);
@@ -439,9 +460,6 @@ uph_status validate(const uph_params *p)
   if (p->dim != 2) return fail(UPH_UNSUPPORTED, "only dim = 2 exists in the reference");
   if (p->flag_init_simul != 1)
     return fail(UPH_UNSUPPORTED, "flagInitSimul != 1 (particle-packing initialisation) is not implemented");
-  const int vt = p->virtual_type;
-  if (vt == 1 || vt == 3 || vt == 4 || vt == 5 || vt == 7 || vt == 8)
-    return fail(UPH_UNSUPPORTED, "virtual mirror particles (virtualType 1,3,4,5,7,8) are not implemented");
   if (p->stress_type == 2 && p->profile != UPH_PROFILE_REF)
     return fail(UPH_UNSUPPORTED, "stressType 2 belongs to the REF profile");
   if (p->knn_cap < 0) return fail(UPH_BAD_ARG, "negative knn_cap");
@@ -466,8 +484,9 @@ cudaError_t alloc_grid(uph_sim *s)
   if (ncell > (1LL << 28)) return cudaErrorInvalidValue;
   G.ncell = (int)ncell;
   G.nblock_sums = scan_block_sums_needed((int)ncell);
+  s->gv.ncell = (int)ncell;
   if (ncell <= s->grid_capacity) return cudaSuccess;
-  for (int **p : {&G.count, &G.start, &G.fill, &G.block_sums}) {
+  for (int **p : {&G.count, &G.start, &G.fill, &G.block_sums, &s->gv.count, &s->gv.start, &s->gv.fill}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -478,6 +497,13 @@ cudaError_t alloc_grid(uph_sim *s)
   if ((e = cudaMalloc((void **)&G.block_sums, sizeof(int) * (G.nblock_sums + 1))) != cudaSuccess) return e;
   // the one-launch build keeps count all zero between builds
   if ((e = cudaMemset(G.count, 0, sizeof(int) * ncell)) != cudaSuccess) return e;
+  if (s->P.nvrules > 0) {
+    CellGrid &V = s->gv;
+    if ((e = cudaMalloc((void **)&V.count, sizeof(int) * ncell)) != cudaSuccess) return e;
+    if ((e = cudaMalloc((void **)&V.start, sizeof(int) * (ncell + 1))) != cudaSuccess) return e;
+    if ((e = cudaMalloc((void **)&V.fill, sizeof(int) * ncell)) != cudaSuccess) return e;
+    if ((e = cudaMemset(V.count, 0, sizeof(int) * ncell)) != cudaSuccess) return e;
+  }
   s->grid_capacity = ncell;
   return cudaSuccess;
 }
@@ -511,6 +537,65 @@ void set_grid_geometry(DevParams &P, int reach, int tile)
   P.ntx = (int)tiles_x;
   P.ncx = P.ntx * tile;
   P.ncy = (int)tiles_y * tile;
+}
+
+// The mirror rules of each virtualType, in the reference's loop order
+// (derivatives.c:3195-4189).  Type 2's loops are commented out in the
+// reference; other types have none.
+void set_virtual_rules(DevParams &P, const uph_params *p)
+{
+  const double L = p->flat_bottom_length, D = p->local_depth;
+  auto rule = [&](int kind, int pos, double a, double b) {
+    P.vrule[P.nvrules++] = VirtualRule{kind, pos, a, b};
+  };
+  P.nvrules = 0;
+  P.flat_bottom_length = L;
+  P.local_depth = D;
+  switch (p->virtual_type) {
+    case 1:  // waves on a slope (:3195-3320); slope 1/15 (System.c:309)
+      rule(VK_LEFT, VP_LEFT, 0.0, 0.0);
+      rule(VK_BOTTOM, VP_CONST, L, 0.0);
+      rule(VK_CORNER_L, VP_LEFT, 0.0, 0.0);
+      rule(VK_SLOPE, VP_CONST, L, 1.0 / 15.0);
+      break;
+    case 3:  // vortex spin-down (:3471-3625)
+      rule(VK_LEFT, VP_CONST, 0.0, 0.0);
+      rule(VK_BOTTOM, VP_CONST, L, 0.0);
+      rule(VK_TOP, VP_CONST, D, p->dx);
+      rule(VK_CORNER_L, VP_LEFT, 0.0, 0.0);
+      rule(VK_RIGHT, VP_CONST, L, 0.0);
+      break;
+    case 4:  // dam break with a gate (:3783-3906)
+    case 8:  // dam break (:3907-4031)
+      rule(VK_LEFT, VP_CONST, 0.0, 0.0);
+      rule(VK_BOTTOM, VP_CONST, L, 0.0);
+      rule(VK_CORNER_L, VP_LEFT, 0.0, 0.0);
+      rule(VK_RIGHT, VP_CONST, L, 0.0);
+      break;
+    case 5:  // sloshing tank (:3626-3782)
+      rule(VK_LEFT, VP_LEFT, 0.0, 0.0);
+      rule(VK_CORNER_L, VP_LEFT, 0.0, 0.0);
+      rule(VK_CORNER_R, VP_RIGHT, 0.0, 0.0);
+      rule(VK_RIGHT, VP_RIGHT, 0.0, 0.0);
+      break;
+    case 7:  // hydrostatic tank (:4032-4189)
+      rule(VK_LEFT, VP_CONST, 0.0, 0.0);
+      rule(VK_BOTTOM, VP_CONST, L, 0.0);
+      rule(VK_TOP, VP_CONST, D, 0.0);
+      rule(VK_CORNER_L, VP_LEFT, 0.0, 0.0);
+      rule(VK_RIGHT, VP_CONST, L, 0.0);
+      break;
+    default:
+      break;
+  }
+  // inputbp.c's if-else chain: the piston law moves the left boundary for
+  // movingBoundary 1 and, failing 1, 2 and 3, for the sloshing walls; the
+  // lid and gate leave it where it was (0: nothing else sets it); the
+  // remaining case sets 0
+  const int mb = p->moving_boundary;
+  const bool piston = mb == 1 && p->flag_init_simul == 1;
+  const bool lid_or_gate = (mb == 3 || mb == 2) && p->flag_init_simul == 1;
+  P.vleft_moves = piston || (!lid_or_gate && !piston && p->virtual_type == 5);
 }
 
 DevParams make_dev_params(const uph_params *p)
@@ -568,6 +653,16 @@ DevParams make_dev_params(const uph_params *p)
   P.lo_y = p->domain_lo[1];
   P.hi_x = p->domain_hi[0];
   P.hi_y = p->domain_hi[1];
+  set_virtual_rules(P, p);
+  if (P.nvrules > 0) {
+    // mirror images lie up to 4h beyond the fluid (the top rule's
+    // D + 2 |y - D|): the grid covers them too
+    const double pad = 8.0 * p->h;
+    P.lo_x -= pad;
+    P.lo_y -= pad;
+    P.hi_x += pad;
+    P.hi_y += pad;
+  }
   // cells of half the search radius: a 5 x 5 block holds 25 h^2 of candidates
   // against 36 h^2 for a 3 x 3 block of radius-wide cells.  A cell then holds
   // about ((1 + skin) h / dx)^2 particles of a lattice; the default tile (11
@@ -639,6 +734,26 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &G.totals, (size_t)kCellBuildMaxBlocks + 1));
   TRY(dalloc(s, &G.bar, kGridWords));
   TRY(cudaMemset(G.bar, 0, kGridWords * sizeof(unsigned)));
+  if (s->P.nvrules > 0) {
+    VirtualBuf &V = s->vb;
+    V.cap = s->P.nvrules * nf;
+    TRY(dalloc(s, &V.flags, (size_t)V.cap));
+    TRY(dalloc(s, &V.offs, (size_t)V.cap));
+    TRY(dalloc(s, &V.block_sums, (size_t)scan_block_sums_needed(V.cap) + 1));
+    TRY(dalloc(s, &V.count, 1));
+    TRY(cudaMemset(V.count, 0, sizeof(int)));
+    TRY(dalloc(s, &V.x, (size_t)V.cap));
+    TRY(dalloc(s, &V.y, (size_t)V.cap));
+    TRY(dalloc(s, &V.src, (size_t)V.cap));
+    TRY(dalloc(s, &V.rule, (size_t)V.cap));
+    CellGrid &Gv = s->gv;
+    TRY(dalloc(s, &Gv.list, (size_t)V.cap));
+    TRY(dalloc(s, &Gv.cell_of, (size_t)V.cap));
+    TRY(dalloc(s, &Gv.rank, (size_t)V.cap));
+    TRY(dalloc(s, &Gv.totals, (size_t)kCellBuildMaxBlocks + 1));
+    TRY(dalloc(s, &Gv.bar, kGridWords));
+    TRY(cudaMemset(Gv.bar, 0, kGridWords * sizeof(unsigned)));
+  }
   TRY(alloc_grid(s));
   Staging &T = s->T;
   double **tall[] = {&T.rho, &T.lrho, &T.p, &T.lp, &T.mass, &T.pressure, &T.tmp_x, &T.tmp_y};
@@ -693,7 +808,8 @@ extern "C" uph_status uph_sim_destroy(uph_sim *s)
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graph(s);
   for (void *p : s->allocations) cudaFree(p);
-  for (void *p : {(void *)s->G.count, (void *)s->G.start, (void *)s->G.fill, (void *)s->G.block_sums})
+  for (void *p : {(void *)s->G.count, (void *)s->G.start, (void *)s->G.fill, (void *)s->G.block_sums,
+                  (void *)s->gv.count, (void *)s->gv.start, (void *)s->gv.fill})
     if (p) cudaFree(p);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   for (cudaEvent_t e : s->ev_pool)
@@ -862,18 +978,21 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
       launch_predict(s->P, s->S, s->stream);
       s->launches++;
     }
-    if (moving) {
+    // the walls of steps after the first of this call moved inside the
+    // previous step's corrector
+    if (moving && k == 0) {
       Timer tm(s, KF_WALLS);
       launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->d_err, s->stream);
       s->launches++;
     }
-    uph_status r = rate_pass(s, first);
+    uph_status r = rate_pass(s, first, true);
     if (r != UPH_OK) return r;
     if (k == 0) s->restart = false;
     if (s->diag_enabled) launch_diagnostics(s);
     {
       Timer tm(s, KF_CORRECT);
-      launch_correct(s->P, s->S, first, k + 1 < nsteps, s->d_err, s->d_itime, s->stream);
+      const bool more = k + 1 < nsteps;
+      launch_correct(s->P, s->S, s->W, first, more, more && moving, s->d_err, s->d_itime, s->stream);
       s->launches++;
     }
     if (++s->steps_since_reorder >= s->reorder_interval) {
@@ -1012,10 +1131,42 @@ extern "C" uph_status uph_sim_derivatives(uph_sim *s, double t)
     launch_wall_motion(s->P, s->S, s->W, t, nullptr, s->d_err, s->stream);
     s->launches++;
   }
+  s->deriv_t = t;
   uph_status r = rate_pass(s, true);
   if (r != UPH_OK) return r;
   UPH_CUDA(cudaGetLastError());
   return check_error_word(s);
+}
+
+extern "C" uph_status uph_sim_virtual(uph_sim *s, int64_t cap, double *position, int32_t *src, int32_t *rule,
+                                      int64_t *count)
+{
+  if (!s || !count) return fail(UPH_BAD_ARG, "uph_sim_virtual: NULL argument");
+  *count = 0;
+  if (s->P.nvrules <= 0 || !s->have_rates) return UPH_OK;
+  int nv = 0;
+  UPH_CUDA(cudaMemcpyAsync(&nv, s->vb.count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  UPH_CUDA(cudaStreamSynchronize(s->stream));
+  *count = nv;
+  if (!position && !src && !rule) return UPH_OK;
+  if (cap < nv) return fail(UPH_BAD_ARG, "uph_sim_virtual: " + std::to_string(nv) + " virtual particles, capacity " +
+                                             std::to_string(cap));
+  if (nv > 0) {
+    if (position) {
+      std::vector<double> x(nv), y(nv);
+      UPH_CUDA(cudaMemcpyAsync(x.data(), s->vb.x, sizeof(double) * nv, cudaMemcpyDeviceToHost, s->stream));
+      UPH_CUDA(cudaMemcpyAsync(y.data(), s->vb.y, sizeof(double) * nv, cudaMemcpyDeviceToHost, s->stream));
+      UPH_CUDA(cudaStreamSynchronize(s->stream));
+      for (int k = 0; k < nv; k++) {
+        position[2 * k] = x[k];
+        position[2 * k + 1] = y[k];
+      }
+    }
+    if (src) UPH_CUDA(cudaMemcpyAsync(src, s->vb.src, sizeof(int) * nv, cudaMemcpyDeviceToHost, s->stream));
+    if (rule) UPH_CUDA(cudaMemcpyAsync(rule, s->vb.rule, sizeof(int) * nv, cudaMemcpyDeviceToHost, s->stream));
+    UPH_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return UPH_OK;
 }
 
 // ---- pair export ---------------------------------------------------------------
@@ -1126,7 +1277,10 @@ extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, in
   uph_status r = build_cell_list(s);
   if (r != UPH_OK) return r;
   if (s->P.knn > 0) {
-    launch_knn_cut(s->P, s->S, s->G, q);
+    // the virtual particles of the last evaluation, when the virtualType has them
+    VirtualPoints vp = {nullptr, nullptr, CellGrid{}};
+    if (s->P.nvrules > 0 && s->have_rates) vp = VirtualPoints{s->vb.x, s->vb.y, s->gv};
+    launch_knn_cut(s->P, s->S, s->G, vp, q);
     s->launches++;
   }
   int *cnt = nullptr, *off = nullptr, *bsum = nullptr;
@@ -1278,7 +1432,7 @@ __global__ void k_diagnostics(DevParams P, SlotArrays S, DiagProbes q, double *p
     if (n1) out->point_pressure = sh[2][0] / sh[3][0];
     out->point_neighbors_two = n2;
     out->point_pressure_two = n2 ? sh[5][0] / n2 : 0.0;
-    out->itime = d_itime ? *d_itime + 1 : 0;
+    out->itime = d_itime ? *d_itime : 0;  // the steps started, this one included
     *done = 0u;
   }
 }

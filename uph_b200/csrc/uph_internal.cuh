@@ -52,6 +52,28 @@ struct SlotArrays {
   double *pressure;                         // algebraic Tait (all slots)
 };
 
+// One mirror rule of the reference's virtual particles: which fluid
+// particles it copies (within 2h of a wall line, 3h of the slope) and where
+// it puts the copy.  Line positions given as a source: a constant, or the
+// left/right boundary position of the step's time.
+enum VirtualKind {
+  VK_LEFT,      // |x - X| < 2h: x' = X - |x - X|, u' = -u
+  VK_RIGHT,     // |x - X| < 2h: x' = X + |x - X|, u' = -u
+  VK_BOTTOM,    // y < 2h and x <= L: y' = -y, v' = -v
+  VK_TOP,       // |(y - D) - e| < 2h: y' = D + 2 |(y - D) - e|, v' = -v
+  VK_CORNER_L,  // |x - X| < 2h and y < 2h: x' = X - |x - X|, y' = -y, both flipped
+  VK_CORNER_R,  // |x - X| < 2h and y < 2h: x' = X + |x - X|, y' = -y, both flipped
+  VK_SLOPE      // distance to y = s (x - L) below 3h and x > L: reflected in that line
+};
+enum VirtualPos { VP_CONST, VP_LEFT, VP_RIGHT };
+struct VirtualRule {
+  int kind;
+  int pos;   // VirtualPos of X (VK_LEFT / RIGHT / CORNER_*)
+  double a;  // X for VP_CONST; L (BOTTOM, SLOPE); D (TOP)
+  double b;  // e (TOP); slope s (SLOPE)
+};
+constexpr int kMaxVirtualRules = 5;
+
 // Constants of one simulation as the kernels see them.
 struct DevParams {
   int nf, n;        // fluid slots, all slots
@@ -98,6 +120,12 @@ struct DevParams {
   // stressType 2: each particle's shear stress over its density squared,
   // sigma / rho^2 (xx, xy = yx, yy), indexed by slot
   double *str_xx, *str_xy, *str_yy;
+  // virtual mirror particles (derivatives.c:3194-4192; virtual.cu): the
+  // virtualType's mirror rules in the reference's order
+  int nvrules;
+  VirtualRule vrule[kMaxVirtualRules];
+  int vleft_moves;  // LeftBoundaryPosition follows the piston law (inputbp.c:194-207, 244-250)
+  double flat_bottom_length, local_depth;
   // Skin of the cell list: cells are (1 + kCellSkin) radius / reach wide, so
   // the list stays complete while no particle has moved more than `skin`
   // (per axis) from where the last build binned it (xbin, ybin by slot).
@@ -204,15 +232,40 @@ constexpr int kCellBuildMaxBlocks = 1024;
 // record the binned positions); otherwise always build.  stats, when given,
 // are zeroed for the rate pass that follows, whether or not the list is
 // rebuilt.
+// step_counter, when given, is advanced by one (a leapfrog step starts);
+// dyn_count, when given, lowers count to the device value it points to.
 uph_status launch_cell_build(const DevParams &P, const double *x, const double *y, int first, int count,
                              CellGrid &G, unsigned *err, bool storage_order, const PassStats *stats,
-                             cudaStream_t s, bool check_rebuild = false);
+                             cudaStream_t s, bool check_rebuild = false, int *step_counter = nullptr,
+                             const int *dyn_count = nullptr);
 
 // REF / WCSPH rate pass over the fluid slots: one CTA per storage tile
 // (tile_pass.cuh); the cell list must be current.
 uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
-// the knn cap's cut of every fluid query (P.kcut_*), from the cell list
-void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
+// The virtual mirror particles of one evaluation (virtual.cu), and their own
+// cell list on the simulation's grid; grid.list == nullptr: none.
+struct VirtualPoints {
+  const double *x, *y;  // [count], in the reference's order
+  CellGrid grid;
+};
+// the knn cap's cut of every fluid query (P.kcut_*), from the cell list and
+// the virtual points
+void launch_knn_cut(const DevParams &P, const SlotArrays &S, const CellGrid &G, const VirtualPoints &V,
+                    cudaStream_t s);
+// Scratch and results of the virtual particles: flags and offsets by
+// (rule, reference fluid index), positions, source fluid index and rule of
+// each virtual particle, and their count.
+struct VirtualBuf {
+  int cap;  // P.nvrules * nf
+  int *flags, *offs, *block_sums;
+  int *count;
+  double *x, *y;
+  int *src, *rule;  // reference fluid index copied; the VirtualKind of the rule
+};
+// Generates the virtual particles of the time (*d_itime) dt, or t_host when
+// d_itime is null (derivatives.c:3194-4192).
+void launch_virtual(const DevParams &P, const SlotArrays &S, const VirtualBuf &V, double t_host, const int *d_itime,
+                    cudaStream_t s);
 // stressType 2, after the rate pass: the shear stress of every listed
 // particle (P.str_*), then its divergence added to the corrector's dv/dt
 void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
@@ -221,11 +274,14 @@ uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const Cell
 
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);
-void launch_correct(const DevParams &P, const SlotArrays &S, int first_step, int predict_next, unsigned *err,
-                    int *d_itime, cudaStream_t s);
+// predict_next: the next step's predictor too; walls_next: the next step's
+// wall motion too (threads past the fluid)
+void launch_correct(const DevParams &P, const SlotArrays &S, const WallTable &W, int first_step, int predict_next,
+                    int walls_next, unsigned *err, const int *d_itime, cudaStream_t s);
 void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s);
-// t = (*d_itime + 1) dt when d_itime is given (the step being computed; the
-// counter lives on the device so CUDA-graph replays see the right time),
+// t = (*d_itime + 1) dt when d_itime is given: the counter holds the steps
+// started (the cell-list launch of each step of uph_sim_step advances it)
+// and lives on the device so CUDA-graph replays see the right time;
 // else t = t_host
 void launch_wall_motion(const DevParams &P, const SlotArrays &S, const WallTable &W, double t_host,
                         const int *d_itime, unsigned *err, cudaStream_t s);
