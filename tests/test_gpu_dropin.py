@@ -88,6 +88,11 @@ def _driver_decks():
     rng = np.random.default_rng(4)
     d.fluid[:, 2:4] = rng.uniform(-0.02, 0.02, size=(d.n_fluid, 2))
     yield "flume_nn21", d
+    # virtual mirror particles (virtualType 7) under a binding 40-nearest cap:
+    # out<k>.dat prints the mirror rows the drop-in writes back
+    t = D.hydrostatic_tank(width=0.4, depth=0.3, dx=0.02, layers=2, eta=0.0)
+    t.params.update(near_neighbor=91, virtual_type=7, flat_bottom_length=0.4, local_depth=0.3)
+    yield "tank_virtual7_nn91", t
 
 
 # output.c:46-60 columns: i x y u v density mass hsml p damGateFlag approxVorticity

@@ -129,6 +129,20 @@ class Simulation:
                                           w.ctypes.data, dw.ctypes.data, C.byref(n)), "uph_sim_pairs")
         return i, j, r2, w, dw
 
+    def virtual(self):
+        """(position [k][2], source fluid index [k], mirror kind [k]) of the
+        virtual mirror particles of the last evaluation (uph_sim_virtual)."""
+        n = C.c_int64(0)
+        _lib.check(self.lib.uph_sim_virtual(self.handle, 0, None, None, None, C.byref(n)), "uph_sim_virtual")
+        k = n.value
+        pos = np.zeros((k, 2))
+        src = np.zeros(k, np.int32)
+        kind = np.zeros(k, np.int32)
+        if k:
+            _lib.check(self.lib.uph_sim_virtual(self.handle, k, pos.ctypes.data, src.ctypes.data, kind.ctypes.data,
+                                                C.byref(n)), "uph_sim_virtual")
+        return pos, src, kind
+
     def stats(self) -> dict:
         s = UphStats()
         _lib.check(self.lib.uph_sim_stats(self.handle, C.byref(s)), "uph_sim_stats")
