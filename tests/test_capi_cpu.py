@@ -174,8 +174,9 @@ def test_sim_create_without_device_fails_cleanly():
 
 def test_sim_create_rejects_unsupported_modes():
     deck = D.dam_break(dx=0.1)
-    # stressType 2 exists for the REF profile only
-    for over, status in [({"stress_type": 2, "profile": 1}, 8), ({"flag_init_simul": 0}, 8),
+    # particle packing and stressType 2 exist for the REF profile only
+    for over, status in [({"stress_type": 2, "profile": 1}, 8), ({"flag_init_simul": 0, "profile": 1}, 8),
+                         ({"flag_init_simul": 2}, 8),
                          ({"precision": 1}, 8), ({"domain_hi": None}, 1)]:
         d = deck.uph_params()
         d.update(over)

@@ -93,6 +93,12 @@ def _driver_decks():
     t = D.hydrostatic_tank(width=0.4, depth=0.3, dx=0.02, layers=2, eta=0.0)
     t.params.update(near_neighbor=91, virtual_type=7, flat_bottom_length=0.4, local_depth=0.3)
     yield "tank_virtual7_nn91", t
+    # particle packing (flagInitSimul 0) on a disturbed lattice
+    k = D.dam_break(tank=(1.0, 1.0), column=(0.4, 0.6), dx=0.02, layers=2, hydrostatic=True, eta=0.0,
+                    near_neighbor=21)
+    k.fluid[:, 0:2] += np.random.default_rng(11).uniform(-0.002, 0.002, size=(k.n_fluid, 2))
+    k.params["flag_init_simul"] = 0
+    yield "dambreak_packing_nn21", k
 
 
 # output.c:46-60 columns: i x y u v density mass hsml p damGateFlag approxVorticity

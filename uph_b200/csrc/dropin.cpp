@@ -247,6 +247,11 @@ extern "C" void derivatives(System *sys, double t)
   sys->NumberOfVirtualParticles = 0;
   const int n = nf + ns + nb;
   check_uniform(sys, n);
+  if (sys->flagInitSimul == 0 && sys->NumberOfFrozenParticles > 0) {
+    printf("derivatives: frozen particles (FrozenParticle.dat) are not supported\n");
+    fflush(stdout);
+    exit(1);
+  }
   ensure_sim(sys, n);
 
   uph_state in;
@@ -278,6 +283,14 @@ extern "C" void derivatives(System *sys, double t)
   out.pressureFluctuation = sys->pressureFluctuation;
   out.velocityFluctuation = sys->velocityFluctuation[0];
   out.Pressure = sys->Pressure;
+  if (sys->flagInitSimul == 0) {
+    // particle packing resets the fluid's density and pressure
+    // (InitialDensityAndPressure, derivatives.c:3056-3066) and computes no
+    // equation of state
+    out.density = sys->density;
+    out.DynamicPressure = sys->DynamicPressure;
+    out.Pressure = nullptr;
+  }
   s = uph_sim_download(g.sim, &out);
   if (s != UPH_OK) die("derivatives", s);
   // LocalDensity/Pressure/VelocityFluctuation zero the boundary entries (derivatives.c:2062-2066, 2103-2106, 2140-2143)

@@ -680,6 +680,100 @@ void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const Cell
   }
 }
 
+// ---- particle-packing initialisation (flagInitSimul == 0) ------------------------
+// derivatives.c:4279-4288 in place of the physics: the kernel-sum gradient
+// of each fluid particle, g_i = V0 sum_pairs dwcdx (both sides, j's with the
+// sign flipped: CalculateGradientOfNormalizationFactor, :2977-3012); a
+// momentum term that every pair of the particle adds once more,
+// -(beta g_i + damp v_i) with beta = 2 g LocalDepth, damp = 0.02
+// sqrt(beta / V0), V0 = mass[0] / rho0 (InitializationMomentumEquation,
+// :3014-3054); then the hydrostatic reset rho = rho0, p = rho0 g (D - y)
+// (InitialDensityAndPressure, :3056-3066) and the selected wall forces as in
+// the physics pass.  The other rates stay zero (:3147-3157), and so do the
+// fluctuations, which the physics would have set.  CalculateNormalizationFactor
+// (:2948-2975) only accumulates into normalizationFactor, which no rate, state
+// field or printed column reads; it is not kept.
+template <bool kBrute, bool kKnn>
+__global__ void __launch_bounds__(128) k_packing_pass(const DevParams P, const SlotArrays S, const CellGrid G,
+                                                    PassStats st)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned my_pairs = 0;
+  int my_nb = 0;
+  if (a < P.nf) {
+    const int oa = S.orig[a];
+    const double xa = S.x[a], ya = S.y[a], ua = S.u[a], va = S.v[a], ma = S.m[a];
+    const int ita = S.itype[a];
+    const double cd = kKnn ? P.kcut_d2[a] : 0.0;
+    const int cj = kKnn ? P.kcut_j[a] : 0;
+    RefAcc A = {};
+    double gx = 0.0, gy = 0.0, bx = 0.0, by = 0.0;
+    int np = 0;
+    NeighbourCursor cur;
+    cur.init(P, G, G.cell_of[a]);
+    int k;
+    while (cur.next(k)) {
+      const int b = G.list[k];
+      if (b == a) continue;
+      const double dx = xa - S.x[b], dy = ya - S.y[b];
+      const double r2 = exact_r2(dx, dy);
+      if (!(r2 < P.r2cut)) continue;
+      const int ob = S.orig[b];
+      if (kBrute && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dx, dy, S.m[b], bx, by);
+      if (r2 <= DBL_EPSILON) continue;
+      my_nb++;
+      if (max(oa, ob) >= P.pb) continue;
+      const bool isI = ob > oa;
+      if constexpr (kKnn) {
+        if (!(isI ? knn_key_le(r2, ob, cd, cj) : knn_key_le(r2, oa, P.kcut_d2[b], P.kcut_j[b]))) continue;
+      }
+      my_pairs += isI;
+      const double F = ref_grad_factor(P, r2);
+      gx = fma(F, dx, gx);
+      gy = fma(F, dy, gy);
+      np++;
+      if (isI && ita == 1 && S.itype[b] >= 2) wall_pair_force(P, S.itype[b], r2, dx, dy, ua - S.u[b], va - S.v[b], ma, A);
+    }
+    const double V0 = *P.pack_mass0 / P.rho0;
+    const double beta = 2.0 * P.g * P.local_depth;
+    const double damp = 0.02 * sqrt(beta / V0);
+    const double npd = (double)np;
+    A.ax += bx - npd * (beta * (V0 * gx)) - npd * (damp * ua);
+    A.ay += by - npd * (beta * (V0 * gy)) - npd * (damp * va);
+    S.drho[a] = 0.0;
+    S.dp[a] = 0.0;
+    S.drho_a[a] = 0.0;
+    S.dp_a[a] = 0.0;
+    S.ax[a] = A.ax;
+    S.ay[a] = A.ay;
+    S.ax_a[a] = A.ax_a;
+    S.ay_a[a] = A.ay_a;
+    S.frho[a] = 0.0;
+    S.fp[a] = 0.0;
+    S.fu[a] = 0.0;
+    S.fv[a] = 0.0;
+    S.rho[a] = P.rho0;
+    S.p[a] = P.rho0 * P.g * (P.local_depth - ya);
+  }
+  pass_stats(st, my_pairs, my_nb);
+}
+
+uph_status launch_packing_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                               cudaStream_t s)
+{
+  if (P.nf <= 0) return UPH_OK;
+  const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
+  const int blocks = (P.nf + 127) / 128;
+  if (P.knn > 0) {
+    if (brute) k_packing_pass<true, true><<<blocks, 128, 0, s>>>(P, S, G, st);
+    else k_packing_pass<false, true><<<blocks, 128, 0, s>>>(P, S, G, st);
+  } else {
+    if (brute) k_packing_pass<true, false><<<blocks, 128, 0, s>>>(P, S, G, st);
+    else k_packing_pass<false, false><<<blocks, 128, 0, s>>>(P, S, G, st);
+  }
+  return UPH_OK;
+}
+
 __global__ void k_rcp_selftest(const double *__restrict__ x, double *__restrict__ y, int64_t n)
 {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)

@@ -433,11 +433,15 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false)
     s->launches++;
   }
   Timer t(s, KF_PASS);
-  r = s->P.profile == UPH_PROFILE_REF ? launch_ref_pass(s->P, s->S, s->G, st, s->stream)
-                                      : launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
+  if (s->P.profile != UPH_PROFILE_REF)
+    r = launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
+  else if (s->P.flag_init_simul == 0)
+    r = launch_packing_pass(s->P, s->S, s->G, st, s->stream);
+  else
+    r = launch_ref_pass(s->P, s->S, s->G, st, s->stream);
   if (r != UPH_OK) return r;
   s->launches++;
-  if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF) {
+  if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF && s->P.flag_init_simul == 1) {
     launch_viscous_two_step(s->P, s->S, s->G, s->stream);
     s->launches += 2;
   }
@@ -458,8 +462,10 @@ uph_status validate(const uph_params *p)
     return fail(UPH_UNSUPPORTED, "FP32 pair arithmetic is implemented for the WCSPH profile only");
   if (!(p->h > 0) || !(p->dx > 0)) return fail(UPH_BAD_ARG, "smoothing length and dx must be positive");
   if (p->dim != 2) return fail(UPH_UNSUPPORTED, "only dim = 2 exists in the reference");
-  if (p->flag_init_simul != 1)
-    return fail(UPH_UNSUPPORTED, "flagInitSimul != 1 (particle-packing initialisation) is not implemented");
+  if (p->flag_init_simul != 1 && p->flag_init_simul != 0)
+    return fail(UPH_UNSUPPORTED, "flagInitSimul must be 0 (particle packing) or 1");
+  if (p->flag_init_simul == 0 && p->profile != UPH_PROFILE_REF)
+    return fail(UPH_UNSUPPORTED, "particle packing (flagInitSimul 0) belongs to the REF profile");
   if (p->stress_type == 2 && p->profile != UPH_PROFILE_REF)
     return fail(UPH_UNSUPPORTED, "stressType 2 belongs to the REF profile");
   if (p->knn_cap < 0) return fail(UPH_BAD_ARG, "negative knn_cap");
@@ -726,6 +732,12 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
     TRY(dalloc(s, &s->P.str_xy, (size_t)n));
     TRY(dalloc(s, &s->P.str_yy, (size_t)n));
   }
+  {
+    double *m0 = nullptr;
+    TRY(dalloc(s, &m0, 1));
+    TRY(cudaMemset(m0, 0, sizeof(double)));
+    s->P.pack_mass0 = m0;
+  }
   TRY(dalloc(s, &s->P.xbin, (size_t)n));
   TRY(dalloc(s, &s->P.ybin, (size_t)n));
   TRY(dalloc(s, &s->P.rebuild, 1));
@@ -868,6 +880,9 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
   UPH_CUDA(h2d(T.p, st->DynamicPressure, (size_t)n, q));
   UPH_CUDA(h2d(T.lp, st->localPressure, (size_t)n, q));
   UPH_CUDA(h2d(T.mass, st->mass, (size_t)n, q));
+  // the packing pass's volume scale is the mass of reference particle 0
+  UPH_CUDA(cudaMemcpyAsync(const_cast<double *>(s->P.pack_mass0), st->mass, sizeof(double), cudaMemcpyHostToDevice,
+                           q));
   UPH_CUDA(h2d(T.itype, st->itype, (size_t)n, q));
   UPH_CUDA(h2d(T.pressure, st->Pressure, (size_t)n, q));
   UPH_CUDA(h2d(T.vmin, st->Velocity_min, 2 * (size_t)nf, q));

@@ -126,6 +126,9 @@ struct DevParams {
   VirtualRule vrule[kMaxVirtualRules];
   int vleft_moves;  // LeftBoundaryPosition follows the piston law (inputbp.c:194-207, 244-250)
   double flat_bottom_length, local_depth;
+  // particle packing (flag_init_simul == 0): mass of reference particle 0,
+  // the reference's volume scale mass[0] / rho0 (derivatives.c:2967)
+  const double *pack_mass0;
   // Skin of the cell list: cells are (1 + kCellSkin) radius / reach wide, so
   // the list stays complete while no particle has moved more than `skin`
   // (per axis) from where the last build binned it (xbin, ybin by slot).
@@ -242,6 +245,9 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
 // REF / WCSPH rate pass over the fluid slots: one CTA per storage tile
 // (tile_pass.cuh); the cell list must be current.
 uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+// the REF profile's particle-packing pass (flag_init_simul == 0) in its place
+uph_status launch_packing_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                               cudaStream_t s);
 // The virtual mirror particles of one evaluation (virtual.cu), and their own
 // cell list on the simulation's grid; grid.list == nullptr: none.
 struct VirtualPoints {
