@@ -252,20 +252,23 @@ def gpu_arm(args, rank, world, local_rank):
                 if len(parts) == 2 and parts[0] == "ref_fp64_pipe_active":
                     fp64_active = float(parts[1])
 
-    # --- e2e: every step through the C ABI with pinned host buffers:
-    # upload the full state, one step, download the full state
+    # --- e2e: every step through the C ABI with pinned host buffers: upload
+    # the state the step reads (sim.STEP_INPUT_FIELDS), one step, download
+    # the state it hands to the next step (sim.STEP_OUTPUT_FIELDS)
     from uph_b200._capi import empty_state
+    from uph_b200.sim import STEP_INPUT_FIELDS, STEP_OUTPUT_FIELDS
+
+    def pinned_like(a):
+        t = torch.empty(a.shape, dtype=torch.int32 if a.dtype == np.int32 else torch.float64, pin_memory=True)
+        return t.numpy()
+
     st_host = {}
     for name, a in deck.initial_state().items():
-        t = torch.empty(a.shape, dtype=torch.int32 if a.dtype == np.int32 else torch.float64, pin_memory=True)
-        arr = t.numpy()
-        arr[...] = a
-        st_host[name] = arr
-    out_host = {}
-    for name, a in empty_state(nf, n_all).items():
-        t = torch.empty(a.shape, dtype=torch.int32 if a.dtype == np.int32 else torch.float64, pin_memory=True)
-        out_host[name] = t.numpy()
-    h2d = sum(a.nbytes for a in st_host.values())
+        st_host[name] = pinned_like(a)
+        st_host[name][...] = a
+    out_host = {name: pinned_like(a) for name, a in empty_state(nf, n_all).items() if name in STEP_OUTPUT_FIELDS}
+    in_host = {name: (out_host[name] if name in out_host else st_host[name]) for name in STEP_INPUT_FIELDS}
+    h2d = sum(a.nbytes for a in in_host.values())
     d2h = sum(a.nbytes for a in out_host.values())
     k_e2e = max(1, min(args.steps, args.e2e_steps))
     sim.upload(st_host, 0)
@@ -276,7 +279,7 @@ def gpu_arm(args, rank, world, local_rank):
     t0 = time.perf_counter()
     itime = 1
     for _ in range(k_e2e):
-        sim.upload(out_host if itime > 1 else st_host, itime)
+        sim.upload(in_host, itime)
         sim.step(1)
         sim.download(out_host)
         itime += 1
@@ -680,8 +683,10 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": r["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "steps": r["k_e2e"],
-                "how": "per step: uph_sim_upload of the full state from pinned host memory, uph_sim_step(1), "
-                       "uph_sim_download of the full state"},
+                "how": "per step: uph_sim_upload from pinned host memory of the state a step reads (positions, "
+                       "velocities, density and pressure of every particle, mass, type, sponge, the fluid's "
+                       "predictor rates and fluctuations), uph_sim_step(1), uph_sim_download of the state it hands "
+                       "to the next step"},
         "e2e_dropin": dict(r["e2e_dropin"], how="per step: the host leapfrog of src/bin/sph.cc:90-168 "
                            "(libuph_driver.so) around derivatives(System*, t) of libuph_sph.so, the reference's own "
                            "entry point: the fields it reads copied in and its rates, fluctuations, Tait pressure and "

@@ -218,9 +218,11 @@ __global__ void k_gather_upload(SlotArrays S, Staging T, const int *__restrict__
   S.ut[s] = T.lvel[2 * o];
   S.vt[s] = T.lvel[2 * o + 1];
   S.rho[s] = T.rho[o];
-  S.rhot[s] = T.lrho[o];
   S.p[s] = T.p[o];
-  S.pt[s] = T.lp[o];
+  // walls and solids: localDensity = rho0 and localPressure = 0, as inputbp
+  // sets them before every derivatives() (inputbp.c:289-290)
+  S.rhot[s] = s < nf ? T.lrho[o] : rho0;
+  S.pt[s] = s < nf ? T.lp[o] : 0.0;
   S.m[s] = T.mass[o];
   S.itype[s] = T.itype[o];
   S.pressure[s] = T.pressure[o];

@@ -27,6 +27,18 @@ from ._capi import (PREC_FP64, PROFILE_REF, STATE_FIELDS, UphDiagnostics, UphPar
 from .deck import Deck
 
 
+# The fields a leapfrog step after the first reads from an upload, and so
+# the state one step hands to the next: positions, velocities, density and
+# pressure of every particle, mass, type and sponge (constant), and the
+# fluid's predictor rates and fluctuations.  The step derives the rest
+# (local and *_min fields from the predictor, the corrector rates and the
+# equation of state from the rate pass), so an upload may leave them NULL.
+STEP_INPUT_FIELDS = ["Position", "Velocity", "density", "DynamicPressure", "mass", "itype", "spongeFactor",
+                     "ddensitydt_approx", "dpdt_approx", "dvdt_approx", "densityFluctuation",
+                     "pressureFluctuation", "velocityFluctuation"]
+STEP_OUTPUT_FIELDS = [f for f in STEP_INPUT_FIELDS if f not in ("mass", "itype", "spongeFactor")]
+
+
 class Simulation:
     def __init__(self, params: dict):
         self.lib = _lib.lib()
