@@ -42,7 +42,7 @@ CORE_SOURCES = [
     ("node_chain.cu", ["@cutlass"]),
     ("surrogate.cu", []),
 ]
-DROPIN_SOURCES = [("dropin.cpp", [])]
+DROPIN_SOURCES = [("dropin.cpp", ["-Xcompiler", "-fopenmp"])]
 
 LIB = os.path.join(HERE, "libuph.so")
 LIB_SPH = os.path.join(HERE, "libuph_sph.so")
@@ -108,7 +108,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     dobjs = [_compile(s, f, verbose) for s, f in DROPIN_SOURCES]
     if _newer(LIB_SPH, dobjs + [LIB]):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB_SPH] + dobjs +
-             ["-L" + HERE, "-luph", "-Xlinker", "-rpath,$ORIGIN", "-lcudart"], verbose)
+             ["-L" + HERE, "-luph", "-Xlinker", "-rpath,$ORIGIN", "-lcudart", "-lgomp"], verbose)
     if _newer(LIB_DRIVER, [DRIVER_SRC, LIB_SPH] + _headers()):
         cuda = os.path.dirname(os.path.dirname(shutil.which(NVCC) or "/usr/local/cuda/bin/nvcc"))
         _run([CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-shared", "-I" + INCLUDE,

@@ -228,15 +228,21 @@ extern "C" uph_status uph_driver_step(System *sys, int32_t nsteps)
     const int itime = ++o->itime;
     const double t = itime * dt;
     if (itime != 1) {
-      // sph.cc:93-124
-      memcpy(rho_min, rho, sizeof(double) * nf);
-      memcpy(p_min, p, sizeof(double) * nf);
-      memcpy(rhot, rho, sizeof(double) * nf);
-      memcpy(pt, p, sizeof(double) * nf);
-      memcpy(sys->localVelocity[0], sys->Velocity[0], sizeof(double) * 2 * n);
-      memcpy(sys->Velocity_min[0], sys->Velocity[0], sizeof(double) * 2 * n);
+      // sph.cc:93-124; its copies (sph.cc:94-99) done inside the parallel
+      // loop, element by element: the walls' velocity copies first
+#pragma omp parallel for schedule(static)
+      for (int i = nf; i < n; i++)
+        for (int d = 0; d < 2; d++) {
+          sys->localVelocity[i][d] = sys->Velocity[i][d];
+          sys->Velocity_min[i][d] = sys->Velocity[i][d];
+        }
 #pragma omp parallel for schedule(static)
       for (int i = 0; i < nf; i++) {
+        rho_min[i] = rho[i];
+        p_min[i] = p[i];
+        rhot[i] = rho[i];
+        pt[i] = p[i];
+        for (int d = 0; d < 2; d++) sys->localVelocity[i][d] = sys->Velocity[i][d];
         rho[i] += 0.5 * dt * sys->ddensitydt_approx[i];
         rhot[i] = rhot[i] + 0.5 * dt * sys->ddensitydt_approx[i] + sys->densityFluctuation[i];
         p[i] += 0.5 * dt * sys->dpdt_approx[i];

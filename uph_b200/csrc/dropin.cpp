@@ -105,39 +105,51 @@ void params_from_system(const System *sys, uph_params *p)
 void check_uniform(const System *sys, int n)
 {
   const double h = sys->hsml[0], mu = sys->viscosity[0], k = sys->thermalDiffusivity[0];
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
   for (int i = 0; i < n; i++)
-    if (sys->hsml[i] != h || sys->viscosity[i] != mu || sys->thermalDiffusivity[i] != k) {
-      printf("derivatives: particle %d has its own hsml/viscosity/thermalDiffusivity; "
-             "the GPU path needs the uniform values input() assigns\n", i);
-      exit(1);
-    }
+    bad |= sys->hsml[i] != h || sys->viscosity[i] != mu || sys->thermalDiffusivity[i] != k;
+  if (bad)
+    for (int i = 0; i < n; i++)
+      if (sys->hsml[i] != h || sys->viscosity[i] != mu || sys->thermalDiffusivity[i] != k) {
+        printf("derivatives: particle %d has its own hsml/viscosity/thermalDiffusivity; "
+               "the GPU path needs the uniform values input() assigns\n", i);
+        exit(1);
+      }
   if (mu != sys->viscosity0 || k != sys->thermalDiffusivity0) {
     printf("derivatives: per-particle viscosity/thermalDiffusivity differ from viscosity0/thermalDiffusivity0\n");
     exit(1);
   }
 }
 
-void ensure_sim(const System *sys, int n)
+// The simulation for this System's parameters.  Its cell-grid domain is the
+// particles' bounding box with room to move; the box is only measured when
+// the simulation is made, or with `remeasure` after an upload found a
+// particle outside the domain.
+void ensure_sim(const System *sys, int n, bool remeasure)
 {
   uph_params p;
   params_from_system(sys, &p);
-  // cell-grid domain: the particles' bounding box with room to move
-  double lo[2] = {sys->Position[0][0], sys->Position[0][1]}, hi[2] = {lo[0], lo[1]};
-  for (int i = 1; i < n; i++)
-    for (int d = 0; d < 2; d++) {
-      lo[d] = fmin(lo[d], sys->Position[i][d]);
-      hi[d] = fmax(hi[d], sys->Position[i][d]);
-    }
-  bool inside = g.sim != nullptr;
-  if (inside) {
+  bool same = g.sim != nullptr;
+  if (same) {
     const uph_params &q = g.p;
-    inside = q.n_fluid == p.n_fluid && q.n_solid == p.n_solid && q.n_fixed == p.n_fixed &&
-             q.n_moving == p.n_moving && q.h == p.h && q.time_step == p.time_step &&
-             lo[0] >= q.domain_lo[0] && lo[1] >= q.domain_lo[1] && hi[0] <= q.domain_hi[0] &&
-             hi[1] <= q.domain_hi[1] && memcmp(&q.stroke, &p.stroke, offsetof(uph_params, domain_lo) -
-                                                                          offsetof(uph_params, stroke)) == 0;
+    same = q.n_fluid == p.n_fluid && q.n_solid == p.n_solid && q.n_fixed == p.n_fixed && q.n_moving == p.n_moving &&
+           q.h == p.h && q.time_step == p.time_step &&
+           memcmp(&q.stroke, &p.stroke, offsetof(uph_params, domain_lo) - offsetof(uph_params, stroke)) == 0;
   }
-  if (inside) return;
+  if (same && !remeasure) return;
+  double x0 = sys->Position[0][0], x1 = x0, y0 = sys->Position[0][1], y1 = y0;
+#pragma omp parallel for schedule(static) reduction(min : x0, y0) reduction(max : x1, y1)
+  for (int i = 1; i < n; i++) {
+    x0 = fmin(x0, sys->Position[i][0]);
+    x1 = fmax(x1, sys->Position[i][0]);
+    y0 = fmin(y0, sys->Position[i][1]);
+    y1 = fmax(y1, sys->Position[i][1]);
+  }
+  const double lo[2] = {x0, y0}, hi[2] = {x1, y1};
+  if (same && lo[0] >= g.p.domain_lo[0] && lo[1] >= g.p.domain_lo[1] && hi[0] <= g.p.domain_hi[0] &&
+      hi[1] <= g.p.domain_hi[1])
+    return;
   if (g.sim) uph_sim_destroy(g.sim);
   g.sim = nullptr;
   for (int d = 0; d < 2; d++) {
@@ -252,7 +264,7 @@ extern "C" void derivatives(System *sys, double t)
     fflush(stdout);
     exit(1);
   }
-  ensure_sim(sys, n);
+  ensure_sim(sys, n, false);
 
   uph_state in;
   memset(&in, 0, sizeof in);
@@ -267,6 +279,11 @@ extern "C" void derivatives(System *sys, double t)
   in.itype = sys->itype;
   in.spongeFactor = sys->spongeFactor;
   uph_status s = uph_sim_upload(g.sim, &in, 0);
+  if (s == UPH_OUT_OF_DOMAIN) {
+    // a particle left the cell grid made for an earlier call: measure again
+    ensure_sim(sys, n, true);
+    s = uph_sim_upload(g.sim, &in, 0);
+  }
   if (s != UPH_OK) die("derivatives", s);
   s = uph_sim_derivatives(g.sim, t);
   if (s != UPH_OK) die("derivatives", s);
@@ -314,11 +331,27 @@ extern "C" void derivatives(System *sys, double t)
     if (s != UPH_OK) die("derivatives", s);
   }
   sys->NumberOfInteractingParticles = (int)niac;
-  // TotalKineticEnergy, derivatives.c:2254-2264
+  // TotalKineticEnergy, derivatives.c:2254-2264: the reference's terms, summed
+  // in 64 fixed chunks and then the chunks in order, so the result does not
+  // depend on the thread count (it can differ from the serial sum in the
+  // last bits)
+  constexpr int kChunks = 64;
+  double ke_c[kChunks], pe_c[kChunks];
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < kChunks; c++) {
+    const int i0 = (int)((int64_t)nf * c / kChunks), i1 = (int)((int64_t)nf * (c + 1) / kChunks);
+    double ke = 0.0, pe = 0.0;
+    for (int i = i0; i < i1; i++) {
+      ke += 0.5 * sys->mass[i] * (sys->Velocity[i][0] * sys->Velocity[i][0] + sys->Velocity[i][1] * sys->Velocity[i][1]);
+      pe += sys->mass[i] * sys->Gravity * sys->Position[i][1];
+    }
+    ke_c[c] = ke;
+    pe_c[c] = pe;
+  }
   double ke = 0.0, pe = 0.0;
-  for (int i = 0; i < nf; i++) {
-    ke += 0.5 * sys->mass[i] * (sys->Velocity[i][0] * sys->Velocity[i][0] + sys->Velocity[i][1] * sys->Velocity[i][1]);
-    pe += sys->mass[i] * sys->Gravity * sys->Position[i][1];
+  for (int c = 0; c < kChunks; c++) {
+    ke += ke_c[c];
+    pe += pe_c[c];
   }
   sys->totalKineticEnergy = ke;
   sys->potentialEnergy = pe;

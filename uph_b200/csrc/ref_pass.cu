@@ -530,20 +530,40 @@ __global__ void __launch_bounds__(128) k_knn_cut(const DevParams P, const SlotAr
   auto offer = [&](double r2, int ob) { knn_offer(P.r2cut, K, r2, ob, kd, kj, m, count); };
   const int cell = G.cell_of[a];
   NeighbourCursor cur;
-  cur.init(P, G, cell);
   int pos;
+  // a first walk only counts the in-radius points: where there are at most
+  // K, nothing is cut and the sorted walk is not needed
+  int inradius = 0;
+  cur.init(P, G, cell);
   while (cur.next(pos)) {
     const int b = G.list[pos];
     if (b == a) continue;
-    offer(exact_r2(xa - S.x[b], ya - S.y[b]), S.orig[b]);
+    const double r2 = exact_r2(xa - S.x[b], ya - S.y[b]);
+    inradius += (r2 < P.r2cut && r2 > DBL_EPSILON) ? 1 : 0;
   }
-  // the virtual mirror particles are points of the reference's search too
-  // (reference indices from Nf + Ns + Nb on), though never in a pair
   if (V.grid.list) {
     cur.init(P, V.grid, cell);
     while (cur.next(pos)) {
       const int v = V.grid.list[pos];
-      offer(exact_r2(xa - V.x[v], ya - V.y[v]), P.n + v);
+      const double r2 = exact_r2(xa - V.x[v], ya - V.y[v]);
+      inradius += (r2 < P.r2cut && r2 > DBL_EPSILON) ? 1 : 0;
+    }
+  }
+  if (inradius > K) {
+    cur.init(P, G, cell);
+    while (cur.next(pos)) {
+      const int b = G.list[pos];
+      if (b == a) continue;
+      offer(exact_r2(xa - S.x[b], ya - S.y[b]), S.orig[b]);
+    }
+    // the virtual mirror particles are points of the reference's search too
+    // (reference indices from Nf + Ns + Nb on), though never in a pair
+    if (V.grid.list) {
+      cur.init(P, V.grid, cell);
+      while (cur.next(pos)) {
+        const int v = V.grid.list[pos];
+        offer(exact_r2(xa - V.x[v], ya - V.y[v]), P.n + v);
+      }
     }
   }
   if (count > K) {

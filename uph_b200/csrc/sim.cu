@@ -128,6 +128,13 @@ struct uph_sim {
   VirtualBuf vb = {};
   CellGrid gv = {};
   double deriv_t = 0.0;  // the time of a uph_sim_derivatives call
+  // pair export (uph_sim_pairs): counts and offsets by reference index, and
+  // the pair arrays, grown as needed and kept
+  int *pe_cnt = nullptr, *pe_off = nullptr, *pe_bsum = nullptr;
+  int32_t *pe_ip = nullptr, *pe_jp = nullptr;
+  double *pe_r2 = nullptr, *pe_w = nullptr, *pe_dw = nullptr;
+  int64_t pe_cap = 0;
+  bool kcut_fresh = false;  // the knn cut matches the current positions and cell list
 };
 
 namespace {
@@ -362,6 +369,7 @@ uph_status build_cell_list(uph_sim *s, const PassStats *stats = nullptr, int *st
 // slots changed outside the leapfrog)
 uph_status force_rebuild(uph_sim *s)
 {
+  s->kcut_fresh = false;
   UPH_CUDA(cudaMemsetAsync(s->P.rebuild, 1, sizeof(unsigned), s->stream));
   return UPH_OK;
 }
@@ -433,6 +441,7 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false)
   if (s->P.knn > 0) {
     launch_knn_cut(s->P, s->S, s->G, vp, s->stream);
     s->launches++;
+    s->kcut_fresh = true;
   }
   Timer t(s, KF_PASS);
   if (s->P.profile != UPH_PROFILE_REF)
@@ -823,7 +832,8 @@ extern "C" uph_status uph_sim_destroy(uph_sim *s)
   drop_graph(s);
   for (void *p : s->allocations) cudaFree(p);
   for (void *p : {(void *)s->G.count, (void *)s->G.start, (void *)s->G.fill, (void *)s->G.block_sums,
-                  (void *)s->gv.count, (void *)s->gv.start, (void *)s->gv.fill})
+                  (void *)s->gv.count, (void *)s->gv.start, (void *)s->gv.fill, (void *)s->pe_ip, (void *)s->pe_jp,
+                  (void *)s->pe_r2, (void *)s->pe_w, (void *)s->pe_dw})
     if (p) cudaFree(p);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   for (cudaEvent_t e : s->ev_pool)
@@ -1028,6 +1038,7 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
     uph_status r = reorder_fluid(s);
     if (r != UPH_OK) return r;
   }
+  s->kcut_fresh = false;  // the correctors moved the particles
   return UPH_OK;
 }
 
@@ -1214,6 +1225,32 @@ __global__ void k_pair_count(DevParams P, SlotArrays S, CellGrid G, int *__restr
   cnt_by_orig[oa] = cnt;
 }
 
+// the kernel values of a listed pair, as CalculateKernel exports them
+__device__ __forceinline__ void pair_kernel(const DevParams &P, double r2, double &W, double &F)
+{
+  const double r = sqrt(r2), q = r * P.inv_h;
+  if (P.profile == UPH_PROFILE_REF) {
+    const double q2 = q * q, t = 1.0 - 0.25 * q2, t2 = t * t, t4 = t2 * t2;
+    const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
+    const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
+    W = P.w_alpha * (t4 * t4) * pp;
+    F = P.dw_alpha * (t4 * t2 * t) * pp7 * P.inv_h2;
+  } else if (q < 1.0) {
+    W = P.cs_alpha * (1 - 1.5 * q * q + 0.75 * q * q * q);
+    F = P.cs_alpha * (-3 + 2.25 * q) * P.inv_h2;
+  } else {
+    const double t = 2 - q;
+    W = P.cs_alpha * 0.25 * t * t * t;
+    F = -P.cs_alpha * 0.75 * t * t / (P.h * r);
+  }
+}
+
+constexpr int kPairSortLocal = 128;  // partners a query orders in thread-local memory
+
+// The pairs whose i is the fluid particle in slot a, ordered by j, written
+// from off[i]: the partners are gathered as (j, slot) keys, ordered by j in
+// thread-local memory (more than kPairSortLocal: in place in the outputs),
+// then each pair's values written once.
 __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *__restrict__ off, int32_t *ip,
                              int32_t *jp, double *rij2, double *w, double *dw)
 {
@@ -1221,9 +1258,11 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
   if (a >= P.nf) return;
   const double xa = S.x[a], ya = S.y[a];
   const int oa = S.orig[a];
-  const int base = off[oa];
+  const int base = off[oa], total = off[oa + 1] - base;
   const double cd = P.knn > 0 ? P.kcut_d2[a] : 0.0;
   const int cj = P.knn > 0 ? P.kcut_j[a] : 0;
+  const bool local = total <= kPairSortLocal;
+  int kj[kPairSortLocal], kb[kPairSortLocal];
   int cnt = 0, k;
   NeighbourCursor cur;
   cur.init(P, G, G.cell_of[a]);
@@ -1235,22 +1274,20 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
     const double r2 = pr2(dx, dy);
     if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
     if (P.knn > 0 && !knn_key_le(r2, ob, cd, cj)) continue;
-    const double r = sqrt(r2), q = r * P.inv_h;
-    double W, F;
-    if (P.profile == UPH_PROFILE_REF) {
-      const double q2 = q * q, t = 1.0 - 0.25 * q2, t2 = t * t, t4 = t2 * t2;
-      const double pp = (((((305.0 * q2 - 628.0) * q2 + 1184.0) * q2 - 1984.0) * q2 + 2816.0) * q2 - 3072.0) * q2 + 2048.0;
-      const double pp7 = (((((305.0 * q2 - 1106.0) * q2 + 1912.0) * q2 - 2912.0) * q2 + 3712.0) * q2 - 3584.0) * q2 + 2048.0;
-      W = P.w_alpha * (t4 * t4) * pp;
-      F = P.dw_alpha * (t4 * t2 * t) * pp7 * P.inv_h2;
-    } else if (q < 1.0) {
-      W = P.cs_alpha * (1 - 1.5 * q * q + 0.75 * q * q * q);
-      F = P.cs_alpha * (-3 + 2.25 * q) * P.inv_h2;
-    } else {
-      const double t = 2 - q;
-      W = P.cs_alpha * 0.25 * t * t * t;
-      F = -P.cs_alpha * 0.75 * t * t / (P.h * r);
+    if (local) {
+      // insertion by j
+      int i = cnt++;
+      while (i > 0 && kj[i - 1] > ob) {
+        kj[i] = kj[i - 1];
+        kb[i] = kb[i - 1];
+        i--;
+      }
+      kj[i] = ob;
+      kb[i] = b;
+      continue;
     }
+    double W, F;
+    pair_kernel(P, r2, W, F);
     const int o = base + cnt++;
     if (ip) ip[o] = oa;
     if (jp) jp[o] = ob;
@@ -1261,7 +1298,25 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
       dw[2 * o + 1] = F * dy;
     }
   }
-  // order the segment by j (insertion sort; segments are short)
+  if (local) {
+    for (int e = 0; e < cnt; e++) {
+      const int b = kb[e], o = base + e;
+      const double dx = xa - S.x[b], dy = ya - S.y[b];
+      const double r2 = pr2(dx, dy);
+      double W, F;
+      pair_kernel(P, r2, W, F);
+      if (ip) ip[o] = oa;
+      if (jp) jp[o] = kj[e];
+      if (rij2) rij2[o] = r2;
+      if (w) w[o] = W;
+      if (dw) {
+        dw[2 * o] = F * dx;
+        dw[2 * o + 1] = F * dy;
+      }
+    }
+    return;
+  }
+  // order the segment by j (insertion sort in place)
   if (jp) {
     for (int i = base + 1; i < base + cnt; i++) {
       const int vj = jp[i];
@@ -1293,18 +1348,21 @@ extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, in
   // the cell list of the last evaluation is still valid unless a reorder moved slots since
   uph_status r = build_cell_list(s);
   if (r != UPH_OK) return r;
-  if (s->P.knn > 0) {
+  if (s->P.knn > 0 && !s->kcut_fresh) {
     // the virtual particles of the last evaluation, when the virtualType has them
     VirtualPoints vp = {nullptr, nullptr, CellGrid{}};
     if (s->P.nvrules > 0 && s->have_rates) vp = VirtualPoints{s->vb.x, s->vb.y, s->gv};
     launch_knn_cut(s->P, s->S, s->G, vp, q);
     s->launches++;
+    s->kcut_fresh = true;
   }
-  int *cnt = nullptr, *off = nullptr, *bsum = nullptr;
-  const int nb = scan_block_sums_needed(nf > 0 ? nf : 1);
-  UPH_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * (nf + 1), q));
-  UPH_CUDA(cudaMallocAsync((void **)&off, sizeof(int) * (nf + 1), q));
-  UPH_CUDA(cudaMallocAsync((void **)&bsum, sizeof(int) * nb, q));
+  if (!s->pe_cnt) {
+    const int nb = scan_block_sums_needed(nf > 0 ? nf : 1);
+    UPH_CUDA(dalloc(s, &s->pe_cnt, (size_t)nf + 1));
+    UPH_CUDA(dalloc(s, &s->pe_off, (size_t)nf + 1));
+    UPH_CUDA(dalloc(s, &s->pe_bsum, (size_t)nb));
+  }
+  int *cnt = s->pe_cnt, *off = s->pe_off, *bsum = s->pe_bsum;
   uph_status result = UPH_OK;
   int total = 0;
   if (nf > 0) {
@@ -1318,13 +1376,24 @@ extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, in
   if (total > cap) {
     result = fail(UPH_NEIGHBOR_OVERFLOW, "pair buffer too small: " + std::to_string(total) + " pairs");
   } else if (total > 0) {
-    int32_t *dip = nullptr, *djp = nullptr;
-    double *dr = nullptr, *dww = nullptr, *ddw = nullptr;
-    cudaMallocAsync((void **)&dip, sizeof(int32_t) * total, q);
-    cudaMallocAsync((void **)&djp, sizeof(int32_t) * total, q);
-    cudaMallocAsync((void **)&dr, sizeof(double) * total, q);
-    cudaMallocAsync((void **)&dww, sizeof(double) * total, q);
-    cudaMallocAsync((void **)&ddw, sizeof(double) * 2 * total, q);
+    if (total > s->pe_cap) {
+      // grow by a quarter beyond what is needed, so small growth reallocates rarely
+      UPH_CUDA(cudaStreamSynchronize(q));
+      for (void *p : {(void *)s->pe_ip, (void *)s->pe_jp, (void *)s->pe_r2, (void *)s->pe_w, (void *)s->pe_dw})
+        if (p) cudaFree(p);
+      s->pe_ip = s->pe_jp = nullptr;
+      s->pe_r2 = s->pe_w = s->pe_dw = nullptr;
+      s->pe_cap = 0;
+      const int64_t cap2 = (int64_t)total + total / 4 + 1024;
+      UPH_CUDA(cudaMalloc((void **)&s->pe_ip, sizeof(int32_t) * cap2));
+      UPH_CUDA(cudaMalloc((void **)&s->pe_jp, sizeof(int32_t) * cap2));
+      UPH_CUDA(cudaMalloc((void **)&s->pe_r2, sizeof(double) * cap2));
+      UPH_CUDA(cudaMalloc((void **)&s->pe_w, sizeof(double) * cap2));
+      UPH_CUDA(cudaMalloc((void **)&s->pe_dw, sizeof(double) * 2 * cap2));
+      s->pe_cap = cap2;
+    }
+    int32_t *dip = s->pe_ip, *djp = s->pe_jp;
+    double *dr = s->pe_r2, *dww = s->pe_w, *ddw = s->pe_dw;
     k_pair_write<<<(nf + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, off, dip, djp, dr, dww, ddw);
     s->launches++;
     if (i_pair) cudaMemcpyAsync(i_pair, dip, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, q);
@@ -1332,15 +1401,7 @@ extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, in
     if (rij2) cudaMemcpyAsync(rij2, dr, sizeof(double) * total, cudaMemcpyDeviceToHost, q);
     if (w) cudaMemcpyAsync(w, dww, sizeof(double) * total, cudaMemcpyDeviceToHost, q);
     if (dwcdx) cudaMemcpyAsync(dwcdx, ddw, sizeof(double) * 2 * total, cudaMemcpyDeviceToHost, q);
-    cudaFreeAsync(dip, q);
-    cudaFreeAsync(djp, q);
-    cudaFreeAsync(dr, q);
-    cudaFreeAsync(dww, q);
-    cudaFreeAsync(ddw, q);
   }
-  cudaFreeAsync(cnt, q);
-  cudaFreeAsync(off, q);
-  cudaFreeAsync(bsum, q);
   UPH_CUDA(cudaStreamSynchronize(q));
   UPH_CUDA(cudaGetLastError());
   return result;
