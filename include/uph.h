@@ -254,6 +254,13 @@ uph_status uph_sim_pairs(uph_sim *sim, int64_t cap, int32_t *i_pair, int32_t *j_
 uph_status uph_sim_virtual(uph_sim *sim, int64_t cap, double *position, int32_t *src, int32_t *rule,
                            int64_t *count);
 
+/* The reference's approxVorticity of every fluid particle ([n_fluid], by
+ * reference index) on the current state and pair set: each pair adds
+ * V_partner (dv_y dx - dv_x dy) w / (r^2 + 0.01 h^2) to both of its
+ * particles (ApproximateVortcity, derivatives.c:2840-2885).  A diagnostic
+ * printed in out<k>.dat; REF profile. */
+uph_status uph_sim_approx_vorticity(uph_sim *sim, double *vorticity);
+
 uph_status uph_sim_stats(uph_sim *sim, uph_stats *out);
 
 /* The reference's per-evaluation diagnostics, computed on the device at the

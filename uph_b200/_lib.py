@@ -36,6 +36,7 @@ SIGNATURES = {
     "uph_sim_derivatives": (C.c_int, [C.c_void_p, C.c_double]),
     "uph_sim_pairs": (C.c_int, [C.c_void_p, C.c_int64] + [C.c_void_p] * 5 + [C.POINTER(C.c_int64)]),
     "uph_sim_stats": (C.c_int, [C.c_void_p, C.POINTER(UphStats)]),
+    "uph_sim_approx_vorticity": (C.c_int, [C.c_void_p, C.c_void_p]),
     "uph_sim_virtual": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_int64)]),
     "uph_sim_set_diagnostics": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]),

@@ -331,6 +331,12 @@ extern "C" void derivatives(System *sys, double t)
     if (s != UPH_OK) die("derivatives", s);
   }
   sys->NumberOfInteractingParticles = (int)niac;
+  // ApproximateVortcity (derivatives.c:2840-2885), printed by output()
+  if (sys->flagInitSimul == 1 && sys->approxVorticity) {
+    s = uph_sim_approx_vorticity(g.sim, sys->approxVorticity);
+    if (s != UPH_OK) die("derivatives", s);
+    for (int i = nf; i < nf + nb; i++) sys->approxVorticity[i] = 0.0;  // derivatives.c:2843-2846
+  }
   // TotalKineticEnergy, derivatives.c:2254-2264: the reference's terms, summed
   // in 64 fixed chunks and then the chunks in order, so the result does not
   // depend on the thread count (it can differ from the serial sum in the

@@ -1337,7 +1337,65 @@ __global__ void k_pair_write(DevParams P, SlotArrays S, CellGrid G, const int *_
   }
 }
 
+// ApproximateVortcity (derivatives.c:2840-2885) for the fluid particle in
+// slot a: every pair adds V_partner (dv_y dx - dv_x dy) w / (r^2 + 0.01 h^2)
+// to both of its particles (the expression is the same from either side),
+// dx = x_i - x_j, dv = v_i - v_j, V = m / rho.  Written by reference index.
+__global__ void k_approx_vorticity(DevParams P, SlotArrays S, CellGrid G, double *__restrict__ out)
+{
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= P.nf) return;
+  const double xa = S.x[a], ya = S.y[a], ua = S.u[a], va = S.v[a];
+  const int oa = S.orig[a];
+  const double cd = P.knn > 0 ? P.kcut_d2[a] : 0.0;
+  const int cj = P.knn > 0 ? P.kcut_j[a] : 0;
+  double acc = 0.0;
+  int k;
+  NeighbourCursor cur;
+  cur.init(P, G, G.cell_of[a]);
+  while (cur.next(k)) {
+    const int b = G.list[k];
+    const int ob = S.orig[b];
+    if (b == a || max(oa, ob) >= P.pb) continue;
+    const double dx = xa - S.x[b], dy = ya - S.y[b];
+    const double r2 = pr2(dx, dy);
+    if (!(r2 < P.r2cut && r2 > DBL_EPSILON)) continue;
+    if (P.knn > 0 && !(ob > oa ? knn_key_le(r2, ob, cd, cj) : knn_key_le(r2, oa, P.kcut_d2[b], P.kcut_j[b])))
+      continue;
+    double W, F;
+    pair_kernel(P, r2, W, F);
+    const double aij = ((va - S.v[b]) * dx - (ua - S.u[b]) * dy) * W * (1.0 / (r2 + P.eta2));
+    acc += S.m[b] / S.rho[b] * aij;
+  }
+  out[oa] = acc;
+}
+
 }  // namespace
+
+extern "C" uph_status uph_sim_approx_vorticity(uph_sim *s, double *vorticity)
+{
+  if (!s || !vorticity) return fail(UPH_BAD_ARG, "uph_sim_approx_vorticity: NULL argument");
+  const int nf = s->P.nf;
+  if (nf <= 0) return UPH_OK;
+  if (s->P.profile != UPH_PROFILE_REF) return fail(UPH_UNSUPPORTED, "approxVorticity is a REF-profile diagnostic");
+  cudaStream_t q = s->stream;
+  uph_status r = build_cell_list(s);
+  if (r != UPH_OK) return r;
+  if (s->P.knn > 0 && !s->kcut_fresh) {
+    VirtualPoints vp = {nullptr, nullptr, CellGrid{}};
+    if (s->P.nvrules > 0 && s->have_rates) vp = VirtualPoints{s->vb.x, s->vb.y, s->gv};
+    launch_knn_cut(s->P, s->S, s->G, vp, q);
+    s->launches++;
+    s->kcut_fresh = true;
+  }
+  double *d = s->T.rho;  // staging, nf entries free until the next upload or download
+  k_approx_vorticity<<<(nf + 127) / 128, 128, 0, q>>>(s->P, s->S, s->G, d);
+  s->launches++;
+  UPH_CUDA(cudaMemcpyAsync(vorticity, d, sizeof(double) * nf, cudaMemcpyDeviceToHost, q));
+  UPH_CUDA(cudaStreamSynchronize(q));
+  UPH_CUDA(cudaGetLastError());
+  return UPH_OK;
+}
 
 extern "C" uph_status uph_sim_pairs(uph_sim *s, int64_t cap, int32_t *i_pair, int32_t *j_pair, double *rij2,
                                     double *w, double *dwcdx, int64_t *niac)
