@@ -27,12 +27,14 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
           "-ccbin", "g++"]
 
-# (source, extra flags).  The leapfrog is compiled without multiply-add
-# contraction so its arithmetic rounds exactly like the reference's.
+# (source, extra flags).  The leapfrog and the wall laws (leapfrog.cuh) are
+# compiled without multiply-add contraction so their arithmetic rounds
+# exactly like the reference's; the REF pass applies the leapfrog in its
+# epilogue, and its own pair arithmetic names every fused multiply-add.
 CORE_SOURCES = [
     ("host.cpp", []),
     ("celllist.cu", []),
-    ("ref_pass.cu", []),
+    ("ref_pass.cu", ["--fmad=false"]),
     ("wcsph_pass.cu", []),
     ("integrate.cu", ["--fmad=false"]),
     ("virtual.cu", ["--fmad=false"]),

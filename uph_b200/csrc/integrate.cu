@@ -9,7 +9,7 @@
 // step of a call uses the stand-alone predictor.
 #include <algorithm>
 
-#include "uph_internal.cuh"
+#include "leapfrog.cuh"
 
 namespace uph {
 
@@ -29,37 +29,33 @@ __device__ __forceinline__ void store_pair_operands(const SlotArrays &S, int a, 
 // sph.cc:93-125 (itime != 1) for one particle whose post-step state is
 // (rho, p, u, v): *_min <- current, local* <- current, then the half kick
 // with the predictor rates and the fluctuations of the last rate
-// evaluation.  Also refreshes 1/rho and 1/rhot for the next rate pass.
+// evaluation (leap_predict).  Also refreshes 1/rho and 1/rhot for the next
+// rate pass.
 __device__ __forceinline__ void predict_one(const DevParams &P, const SlotArrays &S, int a, double rho, double p,
                                             double u, double v)
 {
-  const double dt = P.dt;
-  const double drho_a = S.drho_a[a], dp_a = S.dp_a[a];
+  const LeapPred q = leap_predict(P.dt, P.eps, rho, p, u, v, S.drho_a[a], S.dp_a[a], S.ax_a[a], S.ay_a[a], S.frho[a],
+                                  S.fp[a], S.fu[a], S.fv[a]);
   S.rho_min[a] = rho;
   S.p_min[a] = p;
-  const double rn = rho + 0.5 * dt * drho_a;
-  const double rt = rho + 0.5 * dt * drho_a + S.frho[a];
-  double pn = p + 0.5 * dt * dp_a;
-  S.pt[a] = p + 0.5 * dt * dp_a + S.fp[a];
   S.u_min[a] = u;
   S.v_min[a] = v;
-  const double ax_a = S.ax_a[a], ay_a = S.ay_a[a];
-  const double un = u + 0.5 * dt * ax_a, vn = v + 0.5 * dt * ay_a;
-  S.u[a] = un;
-  S.v[a] = vn;
-  S.ut[a] = un + 0.5 * dt * ax_a + P.eps * S.fu[a];
-  S.vt[a] = vn + 0.5 * dt * ay_a + P.eps * S.fv[a];
+  S.u[a] = q.u;
+  S.v[a] = q.v;
+  S.ut[a] = q.ut;
+  S.vt[a] = q.vt;
+  S.pt[a] = q.pt;
+  double pn = q.p;
   if (P.profile == UPH_PROFILE_WCSPH) {
-    pn = tait(P, rn);
+    pn = tait(P, q.rho);
     S.pressure[a] = pn;
   }
-  S.rho[a] = rn;
-  S.rhot[a] = rt;
+  S.rho[a] = q.rho;
+  S.rhot[a] = q.rt;
   S.p[a] = pn;
-  const double ir = 1.0 / rn;
-  S.inv_rho[a] = ir;
-  S.inv_rhot[a] = 1.0 / rt;
-  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pn, ir, rn);
+  S.inv_rho[a] = q.ir;
+  S.inv_rhot[a] = q.irt;
+  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pn, q.ir, q.rho);
 }
 
 __global__ void k_predict(const DevParams P, const SlotArrays S)
@@ -77,72 +73,6 @@ void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s)
 // sph.cc:137-168: the corrector with the rates just evaluated, then the
 // drift x += dt v.  With predict_next the predictor of the following step
 // runs right after.  Flags non-finite results.
-// A particle now at (x, y): raise the cell list's rebuild flag if it left
-// its skin since the last build, and report it if it left the domain (the
-// build, which also checks, may not run this step).
-__device__ __forceinline__ void note_moved(const DevParams &P, int slot, double x, double y, unsigned *err)
-{
-  if (P.rebuild && (fabs(x - P.xbin[slot]) > P.skin || fabs(y - P.ybin[slot]) > P.skin)) atomicOr(P.rebuild, 1u);
-  if (!(x >= P.lo_x && y >= P.lo_y && x <= P.hi_x && y <= P.hi_y)) atomicOr(err, ERR_OUT_OF_DOMAIN);
-}
-
-// Moving boundary particles (reference indices [m0, b1)), found through
-// their slot's reference index.
-//  - inputbp.c:194-207 (movingBoundary 1): the piston's particles all sit at
-//    x = S/2 (1 - cos wt) with u = ut = S w / 2 sin wt;
-//  - inputbp.c:209-223 (movingBoundary 3, the lid): x = x0 + U t,
-//    u = ut = U, from each particle's base x0;
-//  - inputbp.c:224-243 (movingBoundary 2, the gate): y = y0 + U t and
-//    v = U while 0 < t < t_stop, else y = y0 + U t_stop and v = 0 (the
-//    reference leaves the gate's local velocity alone);
-//  - a WallTable shakes each particle about its own rest position with its
-//    own half stroke and frequency (one entry per particle, e.g. every wall
-//    of a sloshing tank moving rigidly).
-__device__ __forceinline__ void wall_move_one(const DevParams &P, const SlotArrays &S, const WallTable &W, int s,
-                                              double t, unsigned *err)
-{
-  const int o = S.orig[s];
-  if (o < P.m0 || o >= P.b1) return;
-  if (!W.enabled && P.moving_boundary == 3) {
-    const double U = P.lid_velocity;
-    const double x = U * t + W.base[o - P.m0];
-    S.x[s] = x;
-    S.u[s] = U;
-    S.ut[s] = U;
-    note_moved(P, s, x, S.y[s], err);
-    return;
-  }
-  if (!W.enabled && P.moving_boundary == 2) {
-    const double U = P.lid_velocity;
-    double y;
-    if (t > 0.0 && t < P.gate_stop) {
-      y = U * t + W.base[o - P.m0];
-      S.v[s] = U;
-    } else {
-      y = U * P.gate_stop + W.base[o - P.m0];
-      S.v[s] = 0.0;
-    }
-    S.y[s] = y;
-    note_moved(P, s, S.x[s], y, err);
-    return;
-  }
-  double x, u;
-  if (W.enabled) {
-    const int m = o - P.m0;
-    const double hs = W.hs[m], om = W.om[m];
-    x = W.x0[m] + hs * (1.0 - cos(om * t));
-    u = hs * om * sin(om * t);
-  } else {
-    x = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
-    u = 0.5 * P.stroke * P.omega * sin(P.omega * t);
-  }
-  S.x[s] = x;
-  S.u[s] = u;
-  S.ut[s] = u;
-  note_moved(P, s, x, S.y[s], err);
-}
-
-
 // The corrector of the fluid slots; with predict_next also the next step's
 // predictor, and with walls_next the next step's wall motion on the threads
 // past the fluid (its time from the device step counter, which the next
@@ -155,36 +85,16 @@ __global__ void k_correct(const DevParams P, const SlotArrays S, const WallTable
     if (walls_next && a < P.n) wall_move_one(P, S, W, a, (*d_itime + 1) * P.dt, err);
     return;
   }
-  const double dt = P.dt;
-  const double drho = S.drho[a], dp = S.dp[a], ax = S.ax[a], ay = S.ay[a];
-  const double frho = S.frho[a], fp = S.fp[a], fu = P.eps * S.fu[a], fv = P.eps * S.fv[a];
-  double rho, p, u, v, rt, pt, ut, vt;
-  if (first_step) {
-    const double rho0 = S.rho[a], p0 = S.p[a], u0 = S.u[a], v0 = S.v[a];
-    rt = rho0 + 0.5 * dt * drho + frho;
-    rho = rho0 + 0.5 * dt * drho;
-    pt = p0 + 0.5 * dt * dp + fp;
-    p = p0 + 0.5 * dt * dp;
-    ut = u0 + 0.5 * dt * ax + fu;
-    vt = v0 + 0.5 * dt * ay + fv;
-    u = u0 + 0.5 * dt * ax;
-    v = v0 + 0.5 * dt * ay;
-  } else {
-    const double rmin = S.rho_min[a], pmin = S.p_min[a], umin = S.u_min[a], vmin = S.v_min[a];
-    rt = rmin + dt * drho + frho;
-    rho = rmin + dt * drho;
-    pt = pmin + dt * dp + fp;
-    p = pmin + dt * dp;
-    ut = umin + dt * ax + fu;
-    vt = vmin + dt * ay + fv;
-    u = umin + dt * ax;
-    v = vmin + dt * ay;
-  }
+  const LeapRates R = {S.drho[a], S.dp[a], S.ax[a], S.ay[a], S.frho[a], S.fp[a], S.fu[a], S.fv[a]};
+  const LeapState c = first_step ? leap_correct(P.dt, P.eps, true, S.rho[a], S.p[a], S.u[a], S.v[a], R)
+                                 : leap_correct(P.dt, P.eps, false, S.rho_min[a], S.p_min[a], S.u_min[a], S.v_min[a], R);
+  const double rho = c.rho, u = c.u, v = c.v, rt = c.rt, pt = c.pt, ut = c.ut, vt = c.vt;
+  double p = c.p;
   if (P.profile == UPH_PROFILE_WCSPH) {
     p = tait(P, rho);
     S.pressure[a] = p;
   }
-  const double x = S.x[a] + dt * u, y = S.y[a] + dt * v;
+  const double x = leap_drift(P.dt, S.x[a], u), y = leap_drift(P.dt, S.y[a], v);
   S.x[a] = x;
   S.y[a] = y;
   if (!isfinite(rho) || !isfinite(p) || !isfinite(x) || !isfinite(y) || !isfinite(u) || !isfinite(v))

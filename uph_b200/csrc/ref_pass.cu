@@ -56,6 +56,7 @@
 // the expensive loop.
 #include <limits.h>
 
+#include "leapfrog.cuh"
 #include "tile_pass.cuh"
 
 namespace uph {
@@ -287,6 +288,97 @@ __device__ __forceinline__ void ref_epilogue(const DevParams &P, const SlotArray
   S.pressure[a] = P.B * (pow(o.r.rho / P.rho0, P.gamma) - 1.0);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// The epilogue of a pass that applies the step (StepOut): the same rates as
+// ref_epilogue, then the corrector with them, the drift and, with
+// predict_next, the next step's predictor (sph.cc:93-168, leapfrog.cuh),
+// all written to slot a of the other buffer.  The rates and the algebraic
+// pressure are stored only by the last step of a call (no predictor
+// follows): inside a call nothing reads them before that step writes them
+// again, and the step's own predictor has used them already.  The
+// particle's constants (mass, type, reference index, sponge factor) are the
+// same in both buffers and are not written.  S is only read here, at the
+// particle's own slot.
+__device__ __forceinline__ void ref_step_epilogue(const DevParams &P, const SlotArrays &S, const StepOut &F, int a,
+                                                  const RefOwn &o, RefAcc &A, double bx, double by)
+{
+  const SlotArrays &D = F.D;
+  A.ax += bx;
+  A.ay += by;
+  if (P.gravity_flag == 1) {
+    A.ay -= P.g;
+    A.ay_a -= P.g;
+  }
+  if (P.moving_boundary == 1 && P.wave_absorption == 1) A.ax -= S.sponge[a] * o.r.u;
+  if (!F.predict_next) {
+    D.drho[a] = A.drho;
+    D.dp[a] = A.dp;
+    D.ax[a] = A.ax;
+    D.ay[a] = A.ay;
+    D.drho_a[a] = A.drho_a;
+    D.dp_a[a] = A.dp_a;
+    D.ax_a[a] = A.ax_a;
+    D.ay_a[a] = A.ay_a;
+    D.frho[a] = A.frho;
+    D.fp[a] = A.fp;
+    D.fu[a] = A.fu;
+    D.fv[a] = A.fv;
+    D.pressure[a] = P.B * (pow(o.r.rho / P.rho0, P.gamma) - 1.0);
+  }
+  const LeapRates R = {A.drho, A.dp, A.ax, A.ay, A.frho, A.fp, A.fu, A.fv};
+  // the *_min state: the corrector's base after the first step, and carried
+  // over unchanged when no predictor follows
+  double rmin = 0.0, pmin = 0.0, umin = 0.0, vmin = 0.0;
+  if (!F.first_step || !F.predict_next) {
+    rmin = S.rho_min[a];
+    pmin = S.p_min[a];
+    umin = S.u_min[a];
+    vmin = S.v_min[a];
+  }
+  const LeapState c = F.first_step ? leap_correct(P.dt, P.eps, true, o.r.rho, o.r.p, o.r.u, o.r.v, R)
+                                   : leap_correct(P.dt, P.eps, false, rmin, pmin, umin, vmin, R);
+  const double x = leap_drift(P.dt, o.r.x, c.u), y = leap_drift(P.dt, o.r.y, c.v);
+  D.x[a] = x;
+  D.y[a] = y;
+  if (!isfinite(c.rho) || !isfinite(c.p) || !isfinite(x) || !isfinite(y) || !isfinite(c.u) || !isfinite(c.v))
+    atomicOr(F.err, ERR_NAN);
+  note_moved(P, a, x, y, F.err);
+  if (F.predict_next) {
+    const LeapPred q = leap_predict(P.dt, P.eps, c.rho, c.p, c.u, c.v, A.drho_a, A.dp_a, A.ax_a, A.ay_a, A.frho,
+                                    A.fp, A.fu, A.fv);
+    D.rho_min[a] = c.rho;
+    D.p_min[a] = c.p;
+    D.u_min[a] = c.u;
+    D.v_min[a] = c.v;
+    D.u[a] = q.u;
+    D.v[a] = q.v;
+    D.ut[a] = q.ut;
+    D.vt[a] = q.vt;
+    D.rho[a] = q.rho;
+    D.rhot[a] = q.rt;
+    D.p[a] = q.p;
+    D.pt[a] = q.pt;
+    D.inv_rho[a] = q.ir;
+    D.inv_rhot[a] = q.irt;
+  } else {
+    D.rho_min[a] = rmin;
+    D.p_min[a] = pmin;
+    D.u_min[a] = umin;
+    D.v_min[a] = vmin;
+    D.u[a] = c.u;
+    D.v[a] = c.v;
+    D.ut[a] = c.ut;
+    D.vt[a] = c.vt;
+    D.rho[a] = c.rho;
+    D.rhot[a] = c.rt;
+    D.p[a] = c.p;
+    D.pt[a] = c.pt;
+    D.inv_rho[a] = __ddiv_rn(1.0, c.rho);
+    D.inv_rhot[a] = __ddiv_rn(1.0, c.rt);
+  }
+}
+
 // ---- the two partner sources ---------------------------------------------------------
 // Staged: records in shared memory, list entries are record indices.
 struct StagedSrc {
@@ -369,8 +461,9 @@ static_assert(sizeof(RefRec) * 560 >= sizeof(unsigned) * kTileChunk * kTileThrea
 // phase 2 runs the FP64 pair arithmetic over the lists, so the lanes of a
 // warp stay converged in the expensive loop.
 template <bool kBrute, bool kKnn>
-__device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G, int tile,
-                                         unsigned char *smem, unsigned &my_pairs, int &my_nb)
+__device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G,
+                                         const StepOut &F, int tile, unsigned char *smem, unsigned &my_pairs,
+                                         int &my_nb)
 {
   constexpr int kCap = ref_rec_cap<kKnn>();
   TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
@@ -408,6 +501,17 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
         a = G.list[pos];
       }
       const bool active = k < ncore && a < P.nf;
+      // the epilogue's reads of the particle's own *_min state and sponge
+      // factor: fetched into L2 now, while the pair loop runs
+      if (F.enabled && active) {
+        if (!F.first_step || !F.predict_next) {
+          prefetch_l2(S.rho_min + a);
+          prefetch_l2(S.p_min + a);
+          prefetch_l2(S.u_min + a);
+          prefetch_l2(S.v_min + a);
+        }
+        if (P.moving_boundary == 1 && P.wave_absorption == 1) prefetch_l2(S.sponge + a);
+      }
       const RefOwn o = make_own(P, rec[active ? kr : 0]);
       StagedCursor cur;
       const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
@@ -422,7 +526,12 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
       int nb = 0;
       ref_particle<kBrute, kKnn, true>(P, src, cur, active, kr, o, ft, s_nb16, A, bx, by, my_pairs, nb, cd, cj);
       my_nb = max(my_nb, nb);
-      if (active) ref_epilogue(P, S, a, o, A, bx, by);
+      if (active) {
+        if (F.enabled)
+          ref_step_epilogue(P, S, F, a, o, A, bx, by);
+        else
+          ref_epilogue(P, S, a, o, A, bx, by);
+      }
     }
   } else {
     // a crowded tile: the same walk over the cell list in global memory
@@ -450,7 +559,12 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
       int nb = 0;
       ref_particle<kBrute, kKnn, false>(P, src, cur, active, as, o, ft, s_nb32, A, bx, by, my_pairs, nb, cd, cj);
       my_nb = max(my_nb, nb);
-      if (active) ref_epilogue(P, S, a, o, A, bx, by);
+      if (active) {
+        if (F.enabled)
+          ref_step_epilogue(P, S, F, a, o, A, bx, by);
+        else
+          ref_epilogue(P, S, a, o, A, bx, by);
+      }
     }
   }
 }
@@ -459,19 +573,28 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
 // wall modes that act on every boundary particle within the radius
 // (LeonnardJonesBoundaryForces, MonaghanBoundaryForce) rather than on listed
 // pairs.  kKnn: the reference's k-nearest cap (DevParams::knn).
+// With F.enabled the pass also applies the step (StepOut): the wall motion
+// goes first, grid-strided over the wall slots of F.D, which no CTA of this
+// pass reads.
 template <bool kBrute, bool kKnn>
 __global__ void __launch_bounds__(kTileThreads, 2) k_ref_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                           PassStats st)
+                                                           PassStats st, const StepOut F)
 {
   extern __shared__ __align__(16) unsigned char smem[];
+  if (F.enabled && F.walls) {
+    const double t = (*F.d_itime + (F.walls == 2 ? 1 : 0)) * P.dt;
+    for (int w = P.nf + blockIdx.x * kTileThreads + threadIdx.x; w < P.n; w += gridDim.x * kTileThreads)
+      wall_move_one(P, F.D, F.W, w, t, F.err);
+  }
   unsigned my_pairs = 0;
   int my_nb = 0;  // largest in-radius count of this thread's particles
-  ref_tile<kBrute, kKnn>(P, S, G, blockIdx.x, smem, my_pairs, my_nb);
+  ref_tile<kBrute, kKnn>(P, S, G, F, blockIdx.x, smem, my_pairs, my_nb);
   pass_stats(st, my_pairs, my_nb);
 }
 
 template <bool kBrute, bool kKnn>
-uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, const StepOut &F,
+                      cudaStream_t s)
 {
   static bool attr_set[64] = {};  // once per device
   int dev = 0;
@@ -482,16 +605,18 @@ uph_status launch_ref(const DevParams &P, const SlotArrays &S, const CellGrid &G
     if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  k_ref_pass<kBrute, kKnn><<<ntiles, kTileThreads, ref_smem<kKnn>(), s>>>(P, S, G, st);
+  k_ref_pass<kBrute, kKnn><<<ntiles, kTileThreads, ref_smem<kKnn>(), s>>>(P, S, G, st, F);
   return UPH_OK;
 }
 
-uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                           const StepOut &F, cudaStream_t s)
 {
   if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
-  if (P.knn > 0) return brute ? launch_ref<true, true>(P, S, G, st, s) : launch_ref<false, true>(P, S, G, st, s);
-  return brute ? launch_ref<true, false>(P, S, G, st, s) : launch_ref<false, false>(P, S, G, st, s);
+  if (P.knn > 0)
+    return brute ? launch_ref<true, true>(P, S, G, st, F, s) : launch_ref<false, true>(P, S, G, st, F, s);
+  return brute ? launch_ref<true, false>(P, S, G, st, F, s) : launch_ref<false, false>(P, S, G, st, F, s);
 }
 
 // The knn cap's cut of every fluid query: walk the stencil (the global cell

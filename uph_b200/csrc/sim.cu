@@ -116,6 +116,8 @@ struct uph_sim {
   // next step starts the leapfrog afresh with the first-step half kick
   bool restart = false;
   int64_t serial = 0;  // distinct for every simulation this process creates
+  // the REF pass applies the leapfrog step (uph_sim_set_fused_step)
+  bool fused_step = true;
   // per-evaluation diagnostics (off by default)
   bool diag_enabled = false;
   DiagProbes diag_probes = {0, 0, 0, 0};
@@ -313,6 +315,19 @@ __global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ pe
   }
 }
 
+// The wall slots of S copied into D, the other buffer, so that a pass that
+// writes its post-step state into D (StepOut) finds the walls' fields there.
+__global__ void k_copy_walls(SlotArrays D, SlotArrays S, int nf, int n)
+{
+  const int s = nf + blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  D.x[s] = S.x[s]; D.y[s] = S.y[s]; D.u[s] = S.u[s]; D.v[s] = S.v[s];
+  D.ut[s] = S.ut[s]; D.vt[s] = S.vt[s]; D.rho[s] = S.rho[s]; D.rhot[s] = S.rhot[s];
+  D.p[s] = S.p[s]; D.pt[s] = S.pt[s]; D.m[s] = S.m[s]; D.inv_rho[s] = S.inv_rho[s];
+  D.inv_rhot[s] = S.inv_rhot[s]; D.pressure[s] = S.pressure[s]; D.itype[s] = S.itype[s]; D.orig[s] = S.orig[s];
+  D.pk[s] = S.pk[s];
+}
+
 bool p_lid_or_gate(const DevParams &P)
 {
   return (P.moving_boundary == 2 || P.moving_boundary == 3) && P.flag_init_simul == 1;
@@ -374,6 +389,20 @@ uph_status force_rebuild(uph_sim *s)
   return UPH_OK;
 }
 
+// The particle constants (mass, type, reference index, sponge factor) of S
+// copied into S2: a pass that applies the step (StepOut) writes its
+// post-step state into S2 without them.
+uph_status sync_constants(uph_sim *s)
+{
+  const size_t n = s->P.n, nf = s->P.nf;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  UPH_CUDA(cudaMemcpyAsync(s->S2.m, s->S.m, sizeof(double) * n, k, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(s->S2.itype, s->S.itype, sizeof(int32_t) * n, k, s->stream));
+  UPH_CUDA(cudaMemcpyAsync(s->S2.orig, s->S.orig, sizeof(int32_t) * n, k, s->stream));
+  if (nf > 0) UPH_CUDA(cudaMemcpyAsync(s->S2.sponge, s->S.sponge, sizeof(double) * nf, k, s->stream));
+  return UPH_OK;
+}
+
 uph_status reorder_fluid(uph_sim *s)
 {
   Timer t(s, KF_REORDER);
@@ -388,6 +417,8 @@ uph_status reorder_fluid(uph_sim *s)
   s->S = s->S2;
   s->S2 = tmp;
   s->steps_since_reorder = 0;
+  uph_status r2 = sync_constants(s);
+  if (r2 != UPH_OK) return r2;
   return force_rebuild(s);
 }
 
@@ -415,7 +446,9 @@ uph_status check_error_word(uph_sim *s)
 // predictor that ran since the last state change has done it already
 // step: a leapfrog step of uph_sim_step starts (the device step counter
 // advances)
-uph_status rate_pass(uph_sim *s, bool refresh, bool step = false)
+// F: the REF pass applies the step too (StepOut), writing the post-step
+// state into F->D; null: the pass writes the rates into s->S
+uph_status rate_pass(uph_sim *s, bool refresh, bool step = false, const StepOut *F = nullptr)
 {
   if (refresh) {
     Timer t(s, KF_REFRESH);
@@ -449,7 +482,7 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false)
   else if (s->P.flag_init_simul == 0)
     r = launch_packing_pass(s->P, s->S, s->G, st, s->stream);
   else
-    r = launch_ref_pass(s->P, s->S, s->G, st, s->stream);
+    r = launch_ref_pass(s->P, s->S, s->G, st, F ? *F : StepOut{}, s->stream);
   if (r != UPH_OK) return r;
   s->launches++;
   if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF && s->P.flag_init_simul == 1) {
@@ -931,6 +964,12 @@ extern "C" uph_status uph_sim_upload(uph_sim *s, const uph_state *st, int32_t it
     k_wall_base<<<(nw + 255) / 256, 256, 0, q>>>(s->P, s->S, const_cast<double *>(s->W.base), itime * s->P.dt);
     s->launches++;
   }
+  if (n > nf) {
+    k_copy_walls<<<(n - nf + 255) / 256, 256, 0, q>>>(s->S2, s->S, nf, n);
+    s->launches++;
+  }
+  r = sync_constants(s);
+  if (r != UPH_OK) return r;
   s->launches += 3;
   s->itime = itime;
   UPH_CUDA(cudaMemcpyAsync(s->d_itime, &s->itime, sizeof(int), cudaMemcpyHostToDevice, q));
@@ -985,16 +1024,21 @@ bool walls_move(const uph_sim *s)
   return s->hp.n_moving > 0 && (s->W.enabled || ((mb == 1 || mb == 2 || mb == 3) && s->P.flag_init_simul == 1));
 }
 
-// Enqueues `nsteps` leapfrog steps on the sim's stream.  With `capturing`
-// the sequence is being recorded into a CUDA graph: no host synchronisation,
-// no profiling events, and an even number of storage re-sorts so the graph
-// ends on the buffer it started on.
+// Enqueues `nsteps` leapfrog steps on the sim's stream.  Where the REF pass
+// applies the step (StepOut) each step is the list launch and the pass, and
+// the two state buffers swap; else the pass and the corrector.  With
+// `capturing` the sequence is being recorded into a CUDA graph: no host
+// synchronisation, no profiling events, and an even number of buffer swaps
+// (one more storage re-sort where needed) so the graph ends on the buffer it
+// started on.
 void launch_diagnostics(uph_sim *s);
 
 uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
 {
   const bool moving = walls_move(s);
-  int swaps = 0;
+  const bool fuse = s->fused_step && s->P.profile == UPH_PROFILE_REF && s->P.precision == UPH_PREC_FP64 &&
+                    s->P.flag_init_simul == 1 && s->P.stress_type != 2 && !s->diag_enabled;
+  int swaps = 0;  // buffer swaps: fused steps and storage re-sorts
   for (int k = 0; k < nsteps; k++) {
     const int itime = ++s->itime;
     const bool first = itime == 1 || (k == 0 && s->restart);
@@ -1012,13 +1056,24 @@ uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
       launch_wall_motion(s->P, s->S, s->W, 0.0, s->d_itime, s->d_err, s->stream);
       s->launches++;
     }
-    uph_status r = rate_pass(s, first, true);
-    if (r != UPH_OK) return r;
-    if (k == 0) s->restart = false;
-    if (s->diag_enabled) launch_diagnostics(s);
-    {
+    const bool more = k + 1 < nsteps;
+    uph_status r;
+    if (fuse) {
+      // the pass writes the post-step state into the other buffer
+      const StepOut F{s->S2, s->W, s->d_err, s->d_itime, 1, first ? 1 : 0, more ? 1 : 0, moving ? (more ? 2 : 1) : 0};
+      r = rate_pass(s, first, true, &F);
+      if (r != UPH_OK) return r;
+      const SlotArrays tmp = s->S;
+      s->S = s->S2;
+      s->S2 = tmp;
+      swaps++;
+      if (k == 0) s->restart = false;
+    } else {
+      r = rate_pass(s, first, true);
+      if (r != UPH_OK) return r;
+      if (k == 0) s->restart = false;
+      if (s->diag_enabled) launch_diagnostics(s);
       Timer tm(s, KF_CORRECT);
-      const bool more = k + 1 < nsteps;
       launch_correct(s->P, s->S, s->W, first, more, more && moving, s->d_err, s->d_itime, s->stream);
       s->launches++;
     }
@@ -1069,6 +1124,8 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
       uph_status r = enqueue_steps(s, nsteps, true);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+      // replaying leaves the re-sort counter where the recording left it
+      const int since_after = s->steps_since_reorder;
       // the recording ran nothing: restore the host-side counters
       s->itime = itime0;
       s->steps_since_reorder = since0;
@@ -1082,15 +1139,7 @@ extern "C" uph_status uph_sim_step(uph_sim *s, int32_t nsteps)
       s->graph = g;
       UPH_CUDA(cudaGraphInstantiate(&s->graph_exec, g, 0));
       s->graph_buffer = buffer0;
-      s->graph_since_after = 0;
-      // replaying leaves the re-sort counter where the recording left it
-      int since = 0, swaps = 0;
-      for (int k = 0; k < nsteps; k++)
-        if (++since >= s->reorder_interval) {
-          since = 0;
-          swaps++;
-        }
-      s->graph_since_after = (swaps & 1) ? 0 : since;
+      s->graph_since_after = since_after;
     }
     UPH_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
     s->itime += nsteps;
@@ -1112,6 +1161,14 @@ extern "C" uph_status uph_sim_set_graph(uph_sim *s, int32_t steps_per_graph)
   if (steps_per_graph < 0) return fail(UPH_BAD_ARG, "negative graph length");
   drop_graph(s);
   s->graph_steps = steps_per_graph;
+  return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_set_fused_step(uph_sim *s, int32_t enable)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  drop_graph(s);
+  s->fused_step = enable != 0;
   return UPH_OK;
 }
 

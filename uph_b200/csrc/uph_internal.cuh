@@ -242,9 +242,29 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
                              cudaStream_t s, bool check_rebuild = false, int *step_counter = nullptr,
                              const int *dyn_count = nullptr);
 
+// A leapfrog step applied by the REF pass itself.  The pass reads the state
+// of S (staged in shared memory, so other tiles' particles must not change
+// under it) and writes each fluid particle's post-step state -- corrected,
+// with the next step's predictor when predict_next, and with the rates and
+// the algebraic pressure when not -- into D, the simulation's other buffer;
+// the caller then swaps the two.  D must hold the same particle constants
+// (mass, type, reference index, sponge factor) as S, and the walls' fields;
+// where walls move the pass also moves D's walls: walls == 1
+// to this step's time, *d_itime dt (where S's walls are), walls == 2 to the
+// next step's, (*d_itime + 1) dt.  enabled == 0: the pass writes only the
+// rates, into S.
+struct StepOut {
+  SlotArrays D;
+  WallTable W;
+  unsigned *err;
+  const int *d_itime;
+  int enabled, first_step, predict_next, walls;
+};
+
 // REF / WCSPH rate pass over the fluid slots: one CTA per storage tile
 // (tile_pass.cuh); the cell list must be current.
-uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s);
+uph_status launch_ref_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
+                           const StepOut &F, cudaStream_t s);
 // the REF profile's particle-packing pass (flag_init_simul == 0) in its place
 uph_status launch_packing_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
                                cudaStream_t s);
