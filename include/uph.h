@@ -198,14 +198,15 @@ uph_status uph_sim_step(uph_sim *sim, int32_t nsteps);
  * counterpart; its loop is sph.cc:90-168.) */
 uph_status uph_sim_set_graph(uph_sim *sim, int32_t steps_per_graph);
 
-/* Whether the REF rate pass applies the leapfrog step in its epilogue
+/* Whether the rate pass applies the leapfrog step in its epilogue
  * (default 1): the pass then writes each fluid particle's corrected state
  * and the next step's predictor into the simulation's second state buffer,
  * which becomes the current one, and no separate corrector launch runs.
  * The state is bit-identical either way (0 runs the pass and the corrector
- * as two launches).  Applies to the REF profile with flagInitSimul 1 and
- * stressType 1 while diagnostics are off; elsewhere the corrector always
- * runs separately.  (The reference's corrector is sph.cc:137-168.) */
+ * as two launches).  Applies to the WCSPH profile, and to the REF profile
+ * with flagInitSimul 1 and stressType 1, while diagnostics are off;
+ * elsewhere the corrector always runs separately.  (The reference's
+ * corrector is sph.cc:137-168.) */
 uph_status uph_sim_set_fused_step(uph_sim *sim, int32_t enable);
 
 /* Execution tuning (no counterpart in the reference): cell width = search

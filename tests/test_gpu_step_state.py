@@ -43,16 +43,22 @@ def test_step_fields_round_trip_matches_full_state():
 
 
 def _fused_cases():
+    from uph_b200._capi import PREC_FP32_PAIR, PREC_FP64, PROFILE_REF, PROFILE_WCSPH
+
+    flume = D.wave_flume(length=1.5, depth=0.2, dx=0.02, layers=2, amplitude=0.02, period=1.2)
     # piston flume: moving walls, the sponge layer; graph replays and
-    # frequent storage re-sorts in between
-    yield "flume_piston", D.wave_flume(length=1.5, depth=0.2, dx=0.02, layers=2, amplitude=0.02, period=1.2), 0
+    # frequent storage re-sorts in between; both profiles and precisions
+    yield "flume_piston_ref", flume, PROFILE_REF, PREC_FP64, 0
+    yield "flume_piston_wcsph_fp64", flume, PROFILE_WCSPH, PREC_FP64, 0
+    yield "flume_piston_wcsph_fp32", flume, PROFILE_WCSPH, PREC_FP32_PAIR, 0
     # the lid of a driven cavity (movingBoundary 3) under the 40-nearest cap
-    yield "lid_cavity_knn40", D.lid_cavity(size=0.3, dx=0.015, layers=2), 40
+    yield "lid_cavity_ref_knn40", D.lid_cavity(size=0.3, dx=0.015, layers=2), PROFILE_REF, PREC_FP64, 40
 
 
-@pytest.mark.parametrize("case,deck,knn", list(_fused_cases()), ids=lambda v: v if isinstance(v, str) else "")
-def test_fused_step_matches_separate_corrector(case, deck, knn):
-    """The REF pass that applies the leapfrog step in its epilogue (writing
+@pytest.mark.parametrize("case,deck,profile,precision,knn", list(_fused_cases()),
+                         ids=lambda v: v if isinstance(v, str) else "")
+def test_fused_step_matches_separate_corrector(case, deck, profile, precision, knn):
+    """The rate pass that applies the leapfrog step in its epilogue (writing
     the other state buffer) leaves every field bit-identical to the pass
     followed by the stand-alone corrector, through multi-step calls, graph
     replays, storage re-sorts and downloads in between."""
@@ -62,7 +68,7 @@ def test_fused_step_matches_separate_corrector(case, deck, knn):
     nf, n = deck.n_fluid, deck.n_all
     runs = []
     for fused in (False, True):
-        with Simulation.from_deck(deck, knn_cap=knn) as s:
+        with Simulation.from_deck(deck, profile=profile, precision=precision, knn_cap=knn) as s:
             s.set_fused_step(fused)
             s.set_tuning(2, 8, 3)
             states = []

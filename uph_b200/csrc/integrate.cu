@@ -13,19 +13,6 @@
 
 namespace uph {
 
-// WCSPH pressure is the algebraic Tait law of the density (derivatives.c:1674-1682)
-__device__ __forceinline__ double tait(const DevParams &P, double rho)
-{
-  return P.B * (pow(rho / P.rho0, P.gamma) - 1.0);
-}
-
-// the FP32-pair pass's per-particle operands, rounded once from FP64
-__device__ __forceinline__ void store_pair_operands(const SlotArrays &S, int a, double m, double p, double inv_rho,
-                                                    double rho)
-{
-  S.pk[a] = make_float4((float)m, (float)(p * inv_rho * inv_rho), (float)rho, 0.0f);
-}
-
 // sph.cc:93-125 (itime != 1) for one particle whose post-step state is
 // (rho, p, u, v): *_min <- current, local* <- current, then the half kick
 // with the predictor rates and the fluctuations of the last rate
@@ -55,7 +42,6 @@ __device__ __forceinline__ void predict_one(const DevParams &P, const SlotArrays
   S.p[a] = pn;
   S.inv_rho[a] = q.ir;
   S.inv_rhot[a] = q.irt;
-  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pn, q.ir, q.rho);
 }
 
 __global__ void k_predict(const DevParams P, const SlotArrays S)
@@ -121,8 +107,7 @@ void launch_correct(const DevParams &P, const SlotArrays &S, const WallTable &W,
   k_correct<<<(n + 255) / 256, 256, 0, s>>>(P, S, W, first_step, predict_next, walls_next, err, d_itime);
 }
 
-// 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure; for
-// FP32 pair arithmetic the packed operands.
+// 1/rho and 1/rhot for the rate pass; for WCSPH also the Tait pressure.
 // Needed where no predictor ran: a fresh upload and the first step.
 __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int count)
 {
@@ -139,7 +124,6 @@ __global__ void k_refresh(const DevParams P, const SlotArrays S, int first, int 
     S.p[a] = pr;
     S.pressure[a] = pr;
   }
-  if (P.precision == UPH_PREC_FP32_PAIR) store_pair_operands(S, a, S.m[a], pr, ir, rho);
 }
 
 void launch_refresh_inverse(const DevParams &P, const SlotArrays &S, int first, int count, cudaStream_t s)

@@ -1,14 +1,15 @@
 // The leapfrog corrector and predictor of src/bin/sph.cc:90-168 for one
-// fluid particle, and the wall laws of inputbp.c:194-243, shared by the
-// stand-alone corrector (integrate.cu) and the REF rate pass that applies
-// the step in its epilogue (ref_pass.cu).
+// fluid particle, the WCSPH profile's algebraic Tait pressure and the wall
+// laws of inputbp.c:194-243, shared by the stand-alone corrector
+// (integrate.cu) and the rate passes that apply the step in their epilogue
+// (ref_pass.cu, wcsph_pass.cu).
 //
-// The leapfrog is written with explicitly rounded intrinsics (__dadd_rn,
-// __dmul_rn, __ddiv_rn) in the reference's evaluation order, so its results
-// are the same bits whatever the including file's multiply-add contraction
-// setting, and equal to the reference's own (compiled without contraction)
-// whenever the rates are.  The wall laws are plain expressions: every file
-// that includes this header is compiled with --fmad=false.
+// Every sum and product is an explicitly rounded intrinsic (__dadd_rn,
+// __dsub_rn, __dmul_rn, __ddiv_rn) in the reference's evaluation order, so
+// the results are the same bits whatever the including file's multiply-add
+// contraction setting, and equal to the reference's own (compiled without
+// contraction) whenever the rates are.  (cos, sin and pow return the same
+// bits with and without contraction.)
 #pragma once
 
 #include "uph_internal.cuh"
@@ -109,7 +110,7 @@ __device__ __forceinline__ void wall_move_one(const DevParams &P, const SlotArra
   if (o < P.m0 || o >= P.b1) return;
   if (!W.enabled && P.moving_boundary == 3) {
     const double U = P.lid_velocity;
-    const double x = U * t + W.base[o - P.m0];
+    const double x = __dadd_rn(__dmul_rn(U, t), W.base[o - P.m0]);
     S.x[s] = x;
     S.u[s] = U;
     S.ut[s] = U;
@@ -120,10 +121,10 @@ __device__ __forceinline__ void wall_move_one(const DevParams &P, const SlotArra
     const double U = P.lid_velocity;
     double y;
     if (t > 0.0 && t < P.gate_stop) {
-      y = U * t + W.base[o - P.m0];
+      y = __dadd_rn(__dmul_rn(U, t), W.base[o - P.m0]);
       S.v[s] = U;
     } else {
-      y = U * P.gate_stop + W.base[o - P.m0];
+      y = __dadd_rn(__dmul_rn(U, P.gate_stop), W.base[o - P.m0]);
       S.v[s] = 0.0;
     }
     S.y[s] = y;
@@ -132,18 +133,29 @@ __device__ __forceinline__ void wall_move_one(const DevParams &P, const SlotArra
   }
   double x, u;
   if (W.enabled) {
+    // x0 + hs (1 - cos wt), hs w sin wt
     const int m = o - P.m0;
     const double hs = W.hs[m], om = W.om[m];
-    x = W.x0[m] + hs * (1.0 - cos(om * t));
-    u = hs * om * sin(om * t);
+    const double ph = __dmul_rn(om, t);
+    x = __dadd_rn(W.x0[m], __dmul_rn(hs, __dsub_rn(1.0, cos(ph))));
+    u = __dmul_rn(__dmul_rn(hs, om), sin(ph));
   } else {
-    x = 0.5 * P.stroke * (1.0 - cos(P.omega * t));
-    u = 0.5 * P.stroke * P.omega * sin(P.omega * t);
+    // S/2 (1 - cos wt), S/2 w sin wt
+    const double hs = __dmul_rn(0.5, P.stroke);
+    const double ph = __dmul_rn(P.omega, t);
+    x = __dmul_rn(hs, __dsub_rn(1.0, cos(ph)));
+    u = __dmul_rn(__dmul_rn(hs, P.omega), sin(ph));
   }
   S.x[s] = x;
   S.u[s] = u;
   S.ut[s] = u;
   note_moved(P, s, x, S.y[s], err);
+}
+
+// WCSPH pressure is the algebraic Tait law of the density (derivatives.c:1674-1682)
+__device__ __forceinline__ double tait(const DevParams &P, double rho)
+{
+  return __dmul_rn(P.B, __dsub_rn(pow(__ddiv_rn(rho, P.rho0), P.gamma), 1.0));
 }
 
 }  // namespace uph

@@ -288,8 +288,6 @@ __device__ __forceinline__ void ref_epilogue(const DevParams &P, const SlotArray
   S.pressure[a] = P.B * (pow(o.r.rho / P.rho0, P.gamma) - 1.0);
 }
 
-__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 // The epilogue of a pass that applies the step (StepOut): the same rates as
 // ref_epilogue, then the corrector with them, the drift and, with
 // predict_next, the next step's predictor (sph.cc:93-168, leapfrog.cuh),

@@ -160,7 +160,6 @@ cudaError_t alloc_slots(uph_sim *s, SlotArrays &A, int n, int nf)
     if ((e = dalloc(s, p, (size_t)n)) != cudaSuccess) return e;
   if ((e = dalloc(s, &A.itype, (size_t)n)) != cudaSuccess) return e;
   if ((e = dalloc(s, &A.orig, (size_t)n)) != cudaSuccess) return e;
-  if ((e = dalloc(s, &A.pk, (size_t)n)) != cudaSuccess) return e;
   double **fl[] = {&A.rho_min, &A.p_min, &A.u_min, &A.v_min, &A.sponge, &A.drho, &A.dp, &A.ax, &A.ay,
                    &A.drho_a, &A.dp_a, &A.ax_a, &A.ay_a, &A.frho, &A.fp, &A.fu, &A.fv};
   for (double **p : fl)
@@ -306,7 +305,6 @@ __global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ pe
   D.ut[s] = S.ut[o]; D.vt[s] = S.vt[o]; D.rho[s] = S.rho[o]; D.rhot[s] = S.rhot[o];
   D.p[s] = S.p[o]; D.pt[s] = S.pt[o]; D.m[s] = S.m[o]; D.inv_rho[s] = S.inv_rho[o];
   D.inv_rhot[s] = S.inv_rhot[o]; D.pressure[s] = S.pressure[o]; D.itype[s] = S.itype[o]; D.orig[s] = S.orig[o];
-  D.pk[s] = S.pk[o];
   if (s < nf) {
     D.rho_min[s] = S.rho_min[o]; D.p_min[s] = S.p_min[o]; D.u_min[s] = S.u_min[o]; D.v_min[s] = S.v_min[o];
     D.sponge[s] = S.sponge[o]; D.drho[s] = S.drho[o]; D.dp[s] = S.dp[o]; D.ax[s] = S.ax[o]; D.ay[s] = S.ay[o];
@@ -325,7 +323,6 @@ __global__ void k_copy_walls(SlotArrays D, SlotArrays S, int nf, int n)
   D.ut[s] = S.ut[s]; D.vt[s] = S.vt[s]; D.rho[s] = S.rho[s]; D.rhot[s] = S.rhot[s];
   D.p[s] = S.p[s]; D.pt[s] = S.pt[s]; D.m[s] = S.m[s]; D.inv_rho[s] = S.inv_rho[s];
   D.inv_rhot[s] = S.inv_rhot[s]; D.pressure[s] = S.pressure[s]; D.itype[s] = S.itype[s]; D.orig[s] = S.orig[s];
-  D.pk[s] = S.pk[s];
 }
 
 bool p_lid_or_gate(const DevParams &P)
@@ -446,7 +443,7 @@ uph_status check_error_word(uph_sim *s)
 // predictor that ran since the last state change has done it already
 // step: a leapfrog step of uph_sim_step starts (the device step counter
 // advances)
-// F: the REF pass applies the step too (StepOut), writing the post-step
+// F: the rate pass applies the step too (StepOut), writing the post-step
 // state into F->D; null: the pass writes the rates into s->S
 uph_status rate_pass(uph_sim *s, bool refresh, bool step = false, const StepOut *F = nullptr)
 {
@@ -478,7 +475,7 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false, const StepOut 
   }
   Timer t(s, KF_PASS);
   if (s->P.profile != UPH_PROFILE_REF)
-    r = launch_wcsph_pass(s->P, s->S, s->G, st, s->stream);
+    r = launch_wcsph_pass(s->P, s->S, s->G, st, F ? *F : StepOut{}, s->stream);
   else if (s->P.flag_init_simul == 0)
     r = launch_packing_pass(s->P, s->S, s->G, st, s->stream);
   else
@@ -1024,7 +1021,7 @@ bool walls_move(const uph_sim *s)
   return s->hp.n_moving > 0 && (s->W.enabled || ((mb == 1 || mb == 2 || mb == 3) && s->P.flag_init_simul == 1));
 }
 
-// Enqueues `nsteps` leapfrog steps on the sim's stream.  Where the REF pass
+// Enqueues `nsteps` leapfrog steps on the sim's stream.  Where the rate pass
 // applies the step (StepOut) each step is the list launch and the pass, and
 // the two state buffers swap; else the pass and the corrector.  With
 // `capturing` the sequence is being recorded into a CUDA graph: no host
@@ -1036,8 +1033,9 @@ void launch_diagnostics(uph_sim *s);
 uph_status enqueue_steps(uph_sim *s, int nsteps, bool capturing)
 {
   const bool moving = walls_move(s);
-  const bool fuse = s->fused_step && s->P.profile == UPH_PROFILE_REF && s->P.precision == UPH_PREC_FP64 &&
-                    s->P.flag_init_simul == 1 && s->P.stress_type != 2 && !s->diag_enabled;
+  const bool fuse = s->fused_step && !s->diag_enabled &&
+                    (s->P.profile == UPH_PROFILE_WCSPH ||
+                     (s->P.flag_init_simul == 1 && s->P.stress_type != 2 && s->P.precision == UPH_PREC_FP64));
   int swaps = 0;  // buffer swaps: fused steps and storage re-sorts
   for (int k = 0; k < nsteps; k++) {
     const int itime = ++s->itime;

@@ -11,7 +11,8 @@ namespace uph {
 
 struct SimView {
   DevParams P;
-  SlotArrays S;   // current storage buffers (they swap at every re-sort)
+  SlotArrays S;   // current storage buffers (they swap at every re-sort and
+                  // every step whose rate pass applies the leapfrog)
   WallTable W;
   cudaStream_t stream;
   unsigned *err;

@@ -29,6 +29,9 @@ constexpr int kTileTabMax = (kTileRowsMax + 1) * kTileRowsMax;
 constexpr unsigned short kRoleI16 = 0x8000u;  // list-entry flag: this particle is the pair's i
 
 // one CTA's tile and block, in shared memory
+// a global line fetched into L2 ahead of its use
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 struct TileBlock {
   int bx0, by0, W, H;          // block: first cell (x, y) and size in cells
   int ncore;                   // particles (of any kind) in the core cells

@@ -40,7 +40,6 @@ struct SlotArrays {
   double *m;              // mass
   double *inv_rho;        // 1 / density (refreshed before every rate evaluation)
   double *inv_rhot;       // 1 / localDensity
-  float4 *pk;             // FP32 pair operands {m, p / rho^2, rho, 0}, refreshed with inv_rho
   int32_t *itype;
   int32_t *orig;          // reference index of the particle in this slot
   // fluid-only (first nf slots)
@@ -242,7 +241,7 @@ uph_status launch_cell_build(const DevParams &P, const double *x, const double *
                              cudaStream_t s, bool check_rebuild = false, int *step_counter = nullptr,
                              const int *dyn_count = nullptr);
 
-// A leapfrog step applied by the REF pass itself.  The pass reads the state
+// A leapfrog step applied by the rate pass itself.  The pass reads the state
 // of S (staged in shared memory, so other tiles' particles must not change
 // under it) and writes each fluid particle's post-step state -- corrected,
 // with the next step's predictor when predict_next, and with the rates and
@@ -296,7 +295,7 @@ void launch_virtual(const DevParams &P, const SlotArrays &S, const VirtualBuf &V
 // particle (P.str_*), then its divergence added to the corrector's dv/dt
 void launch_viscous_two_step(const DevParams &P, const SlotArrays &S, const CellGrid &G, cudaStream_t s);
 uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
-                             cudaStream_t s);
+                             const StepOut &F, cudaStream_t s);
 
 // leapfrog
 void launch_predict(const DevParams &P, const SlotArrays &S, cudaStream_t s);

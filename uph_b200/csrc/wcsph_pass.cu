@@ -11,15 +11,15 @@
 // modes), in FP64.
 //
 // Real = double: everything in FP64.  Real = float: the pair arithmetic and
-// the per-particle sums run in FP32 from FP64 differences of positions and
-// velocities (taken before rounding, so small separations keep their
-// precision); the pair test itself stays the exact FP64 predicate so both
-// precisions see the same pairs.  The partner's m, p / rho^2 and rho come
-// from one packed FP32 load (SlotArrays::pk, rounded once from FP64 where
-// 1/rho is refreshed) instead of four FP64 loads.
+// the per-particle sums run in FP32 on the staged records' FP32 operands --
+// positions relative to the CTA's block origin (so small separations keep
+// their precision), velocities, m, p / rho^2 and rho, each rounded once from
+// FP64 when the record is staged; the pair test itself stays the exact FP64
+// predicate so both precisions see the same pairs.
 //
 // Execution as in the REF pass: a cheap listing phase (distance test only)
 // per thread into shared memory, then the pair arithmetic over the lists.
+#include "leapfrog.cuh"
 #include "tile_pass.cuh"
 
 namespace uph {
@@ -210,13 +210,23 @@ __device__ __forceinline__ void wc_particle(const DevParams &P, const Src &src, 
   }
 }
 
+// dv/dt with the wall forces, gravity and the sponge layer
+template <typename Real>
+__device__ __forceinline__ void wc_accel(const DevParams &P, const SlotArrays &S, int a, const WcRec<Real> &o, Real ax,
+                                         Real ay, const WcAcc &W, double &axd, double &ayd)
+{
+  axd = (double)ax + W.wx;
+  ayd = (double)ay + W.wy;
+  if (P.gravity_flag == 1) ayd -= P.g;
+  if (P.moving_boundary == 1 && P.wave_absorption == 1) axd -= S.sponge[a] * o.u;
+}
+
 template <typename Real>
 __device__ __forceinline__ void wc_epilogue(const DevParams &P, const SlotArrays &S, int a, const WcRec<Real> &o,
                                             Real drho, Real ax, Real ay, const WcAcc &W)
 {
-  double axd = (double)ax + W.wx, ayd = (double)ay + W.wy;
-  if (P.gravity_flag == 1) ayd -= P.g;
-  if (P.moving_boundary == 1 && P.wave_absorption == 1) axd -= S.sponge[a] * o.u;
+  double axd, ayd;
+  wc_accel(P, S, a, o, ax, ay, W, axd, ayd);
   S.drho[a] = (double)drho;
   S.dp[a] = 0.0;
   S.ax[a] = axd;
@@ -231,6 +241,88 @@ __device__ __forceinline__ void wc_epilogue(const DevParams &P, const SlotArrays
   S.fv[a] = 0.0;
 }
 
+// The epilogue of a pass that applies the step (StepOut), as the stand-alone
+// corrector does it for WCSPH (integrate.cu): the corrector with the rates
+// just summed (no predictor rates or fluctuations of their own: the same
+// rates, zeros), the Tait pressure of the corrected density, the drift and,
+// with predict_next, the next step's predictor, written to slot a of the
+// other buffer.  Rates and the algebraic pressure are stored only by the
+// last step of a call, and the particle's constants not at all (see the REF
+// pass's ref_step_epilogue).
+template <typename Real>
+__device__ __forceinline__ void wc_step_epilogue(const DevParams &P, const SlotArrays &S, const StepOut &F, int a,
+                                                 const WcRec<Real> &o, Real drho, Real ax, Real ay, const WcAcc &W)
+{
+  const SlotArrays &D = F.D;
+  double axd, ayd;
+  wc_accel(P, S, a, o, ax, ay, W, axd, ayd);
+  const double drhod = (double)drho;
+  if (!F.predict_next) {
+    D.drho[a] = drhod;
+    D.dp[a] = 0.0;
+    D.ax[a] = axd;
+    D.ay[a] = ayd;
+    D.drho_a[a] = drhod;
+    D.dp_a[a] = 0.0;
+    D.ax_a[a] = axd;
+    D.ay_a[a] = ayd;
+    D.frho[a] = 0.0;
+    D.fp[a] = 0.0;
+    D.fu[a] = 0.0;
+    D.fv[a] = 0.0;
+  }
+  const LeapRates R = {drhod, 0.0, axd, ayd, 0.0, 0.0, 0.0, 0.0};
+  double rmin = 0.0, pmin = 0.0, umin = 0.0, vmin = 0.0;
+  if (!F.first_step || !F.predict_next) {
+    rmin = S.rho_min[a];
+    pmin = S.p_min[a];
+    umin = S.u_min[a];
+    vmin = S.v_min[a];
+  }
+  const LeapState c = F.first_step ? leap_correct(P.dt, P.eps, true, S.rho[a], S.p[a], o.u, o.v, R)
+                                   : leap_correct(P.dt, P.eps, false, rmin, pmin, umin, vmin, R);
+  const double p = tait(P, c.rho);
+  const double x = leap_drift(P.dt, o.x, c.u), y = leap_drift(P.dt, o.y, c.v);
+  D.x[a] = x;
+  D.y[a] = y;
+  if (!isfinite(c.rho) || !isfinite(p) || !isfinite(x) || !isfinite(y) || !isfinite(c.u) || !isfinite(c.v))
+    atomicOr(F.err, ERR_NAN);
+  note_moved(P, a, x, y, F.err);
+  if (F.predict_next) {
+    const LeapPred q = leap_predict(P.dt, P.eps, c.rho, p, c.u, c.v, drhod, 0.0, axd, ayd, 0.0, 0.0, 0.0, 0.0);
+    D.rho_min[a] = c.rho;
+    D.p_min[a] = p;
+    D.u_min[a] = c.u;
+    D.v_min[a] = c.v;
+    D.u[a] = q.u;
+    D.v[a] = q.v;
+    D.ut[a] = q.ut;
+    D.vt[a] = q.vt;
+    D.pt[a] = q.pt;
+    D.rho[a] = q.rho;
+    D.rhot[a] = q.rt;
+    D.p[a] = tait(P, q.rho);
+    D.inv_rho[a] = q.ir;
+    D.inv_rhot[a] = q.irt;
+  } else {
+    D.rho_min[a] = rmin;
+    D.p_min[a] = pmin;
+    D.u_min[a] = umin;
+    D.v_min[a] = vmin;
+    D.u[a] = c.u;
+    D.v[a] = c.v;
+    D.ut[a] = c.ut;
+    D.vt[a] = c.vt;
+    D.pt[a] = c.pt;
+    D.rho[a] = c.rho;
+    D.rhot[a] = c.rt;
+    D.p[a] = p;
+    D.pressure[a] = p;
+    D.inv_rho[a] = __ddiv_rn(1.0, c.rho);
+    D.inv_rhot[a] = __ddiv_rn(1.0, c.rt);
+  }
+}
+
 constexpr int kWcRecCap = 640;
 constexpr size_t kWcListBytes = sizeof(unsigned short) * kTileChunk * kTileThreads;
 template <typename Real>
@@ -243,8 +335,8 @@ static_assert(sizeof(WcRec<float>) * kWcRecCap >= sizeof(unsigned) * kTileChunk 
 
 // One tile of the WCSPH pass, as the REF pass's (tile_pass.cuh).
 template <bool kBrute, typename Real>
-__device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G, int tile,
-                                        unsigned char *smem, unsigned &my_pairs, int &my_nb)
+__device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S, const CellGrid &G, const StepOut &F,
+                                        int tile, unsigned char *smem, unsigned &my_pairs, int &my_nb)
 {
   TileBlock &B = *reinterpret_cast<TileBlock *>(smem);
   unsigned short *s_nb16 = reinterpret_cast<unsigned short *>(smem + sizeof(TileBlock));
@@ -272,6 +364,14 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
         a = G.list[pos];
       }
       const bool active = k < ncore && a < P.nf;
+      // the epilogue's reads of the particle's own *_min state: fetched into
+      // L2 now, while the pair loop runs
+      if (F.enabled && active && (!F.first_step || !F.predict_next)) {
+        prefetch_l2(S.rho_min + a);
+        prefetch_l2(S.p_min + a);
+        prefetch_l2(S.u_min + a);
+        prefetch_l2(S.v_min + a);
+      }
       const WcRec<Real> o = rec[active ? kr : 0];
       StagedCursor cur;
       const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
@@ -283,7 +383,12 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       int nb = 0;
       wc_particle<kBrute, true, Real>(P, src, cur, active, kr, o, ft, s_nb16, drho, ax, ay, W, my_pairs, nb);
       my_nb = max(my_nb, nb);
-      if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
+      if (active) {
+        if (F.enabled)
+          wc_step_epilogue<Real>(P, S, F, a, o, drho, ax, ay, W);
+        else
+          wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
+      }
     }
   } else {
     unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
@@ -307,25 +412,38 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       int nb = 0;
       wc_particle<kBrute, false, Real>(P, src, cur, active, as, o, ft, s_nb32, drho, ax, ay, W, my_pairs, nb);
       my_nb = max(my_nb, nb);
-      if (active) wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
+      if (active) {
+        if (F.enabled)
+          wc_step_epilogue<Real>(P, S, F, a, o, drho, ax, ay, W);
+        else
+          wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
+      }
     }
   }
 }
 
 // The WCSPH rate pass: one CTA per storage tile (tile_pass.cuh).
+// With F.enabled the pass also applies the step (StepOut), wall motion first
+// as in the REF pass.
 template <bool kBrute, typename Real>
 __global__ void __launch_bounds__(kTileThreads, 3) k_wcsph_pass(const DevParams P, const SlotArrays S, const CellGrid G,
-                                                             PassStats st)
+                                                             PassStats st, const StepOut F)
 {
   extern __shared__ __align__(16) unsigned char smem[];
+  if (F.enabled && F.walls) {
+    const double t = (*F.d_itime + (F.walls == 2 ? 1 : 0)) * P.dt;
+    for (int w = P.nf + blockIdx.x * kTileThreads + threadIdx.x; w < P.n; w += gridDim.x * kTileThreads)
+      wall_move_one(P, F.D, F.W, w, t, F.err);
+  }
   unsigned my_pairs = 0;
   int my_nb = 0;  // largest in-radius count of this thread's particles
-  wc_tile<kBrute, Real>(P, S, G, blockIdx.x, smem, my_pairs, my_nb);
+  wc_tile<kBrute, Real>(P, S, G, F, blockIdx.x, smem, my_pairs, my_nb);
   pass_stats(st, my_pairs, my_nb);
 }
 
 template <bool kBrute, typename Real>
-uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, cudaStream_t s)
+uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st, const StepOut &F,
+                     cudaStream_t s)
 {
   static bool attr_set[64] = {};  // once per device
   int dev = 0;
@@ -336,18 +454,18 @@ uph_status launch_wc(const DevParams &P, const SlotArrays &S, const CellGrid &G,
     if (dev >= 0 && dev < 64) attr_set[dev] = true;
   }
   const int ntiles = P.ntx * (P.ncy / P.tile);
-  k_wcsph_pass<kBrute, Real><<<ntiles, kTileThreads, wc_smem<Real>(), s>>>(P, S, G, st);
+  k_wcsph_pass<kBrute, Real><<<ntiles, kTileThreads, wc_smem<Real>(), s>>>(P, S, G, st, F);
   return UPH_OK;
 }
 
 uph_status launch_wcsph_pass(const DevParams &P, const SlotArrays &S, const CellGrid &G, PassStats st,
-                             cudaStream_t s)
+                             const StepOut &F, cudaStream_t s)
 {
   if (P.nf <= 0) return UPH_OK;
   const bool brute = P.boundary_force != 3 && P.boundary_force != 4 && P.boundary_force != 5;
   if (P.precision == UPH_PREC_FP32_PAIR)
-    return brute ? launch_wc<true, float>(P, S, G, st, s) : launch_wc<false, float>(P, S, G, st, s);
-  return brute ? launch_wc<true, double>(P, S, G, st, s) : launch_wc<false, double>(P, S, G, st, s);
+    return brute ? launch_wc<true, float>(P, S, G, st, F, s) : launch_wc<false, float>(P, S, G, st, F, s);
+  return brute ? launch_wc<true, double>(P, S, G, st, F, s) : launch_wc<false, double>(P, S, G, st, F, s);
 }
 
 }  // namespace uph

@@ -101,7 +101,7 @@ class Simulation:
         _lib.check(self.lib.uph_sim_set_graph(self.handle, steps_per_graph), "uph_sim_set_graph")
 
     def set_fused_step(self, enable: bool) -> None:
-        """Whether the REF rate pass applies the leapfrog step itself (default on)."""
+        """Whether the rate pass applies the leapfrog step itself (default on)."""
         _lib.check(self.lib.uph_sim_set_fused_step(self.handle, 1 if enable else 0), "uph_sim_set_fused_step")
 
     def set_tuning(self, reach: int, tile: int, reorder_interval: int) -> None:
