@@ -41,13 +41,16 @@ UNIT = "particle-steps/s"
 WORKLOAD = ("hydrostatic tank 2.0 x 1.0 m, dx=0.002 m (500,000 fluid particles) + 3 wall layers, h=1.3dx, "
             "rho0=1000, gamma=7, c0=10*sqrt(2g), dt=0.2h/c0; REF (drop-in) physics, FP64")
 
-# Algorithmic bytes of one rate pass (the dominant kernel): every
-# interacting particle's 13 FP64 fields (x y u v ut vt rho rhot p pt m
-# 1/rho 1/rhot) + orig index + itype + its cell-list entry read once
-# (120 B), every fluid particle's 12 rates + Tait pressure written once and
-# its sponge factor read (112 B).  Neighbour re-reads are served on chip.
+# Algorithmic bytes of one rate pass (the dominant kernel), which applies
+# the leapfrog step in its epilogue: every interacting particle's 13 FP64
+# fields (x y u v ut vt rho rhot p pt m 1/rho 1/rhot) + orig index + itype +
+# its cell-list entry read once (120 B); every fluid particle's *_min state
+# read (4 x 8 B) and its post-step state written once (x y, the four *_min,
+# u v ut vt rho rhot p pt 1/rho 1/rhot: 16 x 8 B), 160 B.  (The rates and
+# the Tait pressure are written by a call's last step only.)  Neighbour
+# re-reads are served on chip.
 PASS_BYTES_PER_SLOT = 13 * 8 + 4 + 4 + 8
-PASS_BYTES_PER_FLUID = 13 * 8 + 8
+PASS_BYTES_PER_FLUID = 4 * 8 + 16 * 8
 
 
 def load_peaks():
