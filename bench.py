@@ -51,6 +51,9 @@ WORKLOAD = ("hydrostatic tank 2.0 x 1.0 m, dx=0.002 m (500,000 fluid particles) 
 # re-reads are served on chip.
 PASS_BYTES_PER_SLOT = 13 * 8 + 4 + 4 + 8
 PASS_BYTES_PER_FLUID = 4 * 8 + 16 * 8
+# with --separate-corrector the pass writes the 12 rates + Tait pressure and
+# reads the sponge factor instead (112 B); the corrector is its own launch
+PASS_BYTES_PER_FLUID_RATES = 13 * 8 + 8
 
 
 def load_peaks():
@@ -220,6 +223,7 @@ def gpu_arm(args, rank, world, local_rank):
 
     # --- headline: REF profile, FP64
     sim = Simulation.from_deck(deck, profile=PROFILE_REF)
+    sim.set_fused_step(not args.separate_corrector)
     sim.set_stream(stream.cuda_stream)
     sim.step(args.warmup)
     sim.profile(True)
@@ -237,7 +241,8 @@ def gpu_arm(args, rank, world, local_rank):
 
     pass_ms, pass_n = ktimes.get("rate_pass", (0.0, 0))
     pass_avg_s = pass_ms / max(pass_n, 1) / 1e3
-    pass_bytes = n_all * PASS_BYTES_PER_SLOT + nf * PASS_BYTES_PER_FLUID
+    pass_bytes = n_all * PASS_BYTES_PER_SLOT + nf * (PASS_BYTES_PER_FLUID_RATES if args.separate_corrector
+                                                     else PASS_BYTES_PER_FLUID)
     peak, peak_kind = load_peaks()
     achieved = pass_bytes / pass_avg_s / 1e9 if pass_avg_s > 0 else 0.0
     # DRAM read + write bytes of one launch from the committed ncu capture
@@ -246,7 +251,8 @@ def gpu_arm(args, rank, world, local_rank):
     traffic = None
     fp64_active = None
     tpath = os.path.join(ROOT, "profiles", "rate_pass_traffic.txt")
-    if os.path.exists(tpath):
+    # the capture is of the pass that applies the step
+    if os.path.exists(tpath) and not args.separate_corrector:
         with open(tpath) as f:
             for line in f:
                 parts = line.split()
@@ -320,6 +326,7 @@ def gpu_arm(args, rank, world, local_rank):
     finals = {}
     for label, prof, prec in [("wcsph_fp64", PROFILE_WCSPH, 0), ("wcsph_fp32_pair", PROFILE_WCSPH, PREC_FP32_PAIR)]:
         v = Simulation.from_deck(deck, profile=prof, precision=prec)
+        v.set_fused_step(not args.separate_corrector)
         v.set_stream(stream.cuda_stream)
         v.step(args.warmup)
         v.profile(True)
@@ -620,6 +627,9 @@ def main():
     ap.add_argument("--no-dambreak", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-dropin-e2e", action="store_true")
+    ap.add_argument("--separate-corrector", action="store_true",
+                    help="run the leapfrog corrector as its own launch after each rate pass "
+                         "(uph_sim_set_fused_step(0)) instead of in the pass's epilogue")
     ap.add_argument("--sur-steps", type=int, default=2000, help="wave-flume surrogate configuration: SPH steps")
     ap.add_argument("--sur-warm", type=float, default=1.0, help="wave-flume warm-up from rest (s)")
     ap.add_argument("--sur-length", type=float, default=10.0, help="wave-flume length (m); 10 m is the workload")
@@ -677,6 +687,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_fluid": r["deck"].n_fluid, "n_particles": r["deck"].n_all,
                    "l2": "state 0.2 GB per GPU > 126 MB L2; no flush between steps",
+                   "leapfrog": "separate corrector launch" if args.separate_corrector
+                               else "in the rate pass's epilogue",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
                      "frac": r["achieved"] / r["peak"], "traffic": r["traffic"],
