@@ -477,25 +477,48 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
   // the origin of the block: the listing's FP32 positions are relative to it
   const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
   if (staged) {
-    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
-      const int slot = G.list[tile_record_pos(B, k)];
-      const RefRec r = load_ref_rec(P, S, slot);
+    // two records per thread at a time, every load issued before the first
+    // store, so the staging waits for two rounds of loads (the slots, then
+    // their fields) instead of two per record
+    auto put = [&](int k, const RefRec &r, double cd, int cj) {
       rec[k] = r;
       s_posf[k] = make_float2((float)(r.x - ox), (float)(r.y - oy));
       if constexpr (kKnn) {
-        // only fluid queries have a cut; other records are never a pair's i
-        // seen from a fluid particle that is its j
-        s_cd[k] = slot < P.nf ? P.kcut_d2[slot] : 0.0;
-        s_cj[k] = slot < P.nf ? P.kcut_j[slot] : 0;
+        s_cd[k] = cd;
+        s_cj[k] = cj;
       }
+    };
+    for (int k0 = threadIdx.x; k0 < B.nrec; k0 += 2 * kTileThreads) {
+      const int k1 = k0 + kTileThreads;
+      const bool two = k1 < B.nrec;
+      const int s0 = G.list[tile_record_pos(B, k0)];
+      const int s1 = two ? G.list[tile_record_pos(B, k1)] : s0;
+      const RefRec r0 = load_ref_rec(P, S, s0);
+      const RefRec r1 = load_ref_rec(P, S, s1);
+      // only fluid queries have a cut; other records are never a pair's i
+      // seen from a fluid particle that is its j
+      double cd0 = 0.0, cd1 = 0.0;
+      int cj0 = 0, cj1 = 0;
+      if constexpr (kKnn) {
+        if (s0 < P.nf) {
+          cd0 = P.kcut_d2[s0];
+          cj0 = P.kcut_j[s0];
+        }
+        if (s1 < P.nf) {
+          cd1 = P.kcut_d2[s1];
+          cj1 = P.kcut_j[s1];
+        }
+      }
+      put(k0, r0, cd0, cj0);
+      if (two) put(k1, r1, cd1, cj1);
     }
     __syncthreads();
     const StagedSrc src{rec, s_posf, s_cd, s_cj};
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
-      int kr = 0, pos = 0, a = 0;
+      int kr = 0, pos = 0, a = 0, cx = B.bx0, cy = B.by0;
       if (k < ncore) {
-        tile_core(B, k, kr, pos);
+        tile_core_cell(B, k, kr, pos, cx, cy);
         a = G.list[pos];
       }
       const bool active = k < ncore && a < P.nf;
@@ -512,8 +535,7 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
       }
       const RefOwn o = make_own(P, rec[active ? kr : 0]);
       StagedCursor cur;
-      const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
-      cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
+      cur.c.init(B, P.reach, active ? cx : B.bx0, active ? cy : B.by0);
       double cd = 0.0;
       int cj = 0;
       if (kKnn && active) src.cut(kr, cd, cj);

@@ -43,7 +43,11 @@ struct TileBlock {
   int tab[kTileTabMax];        // record index of block cell (r, c): tab[r (W + 1) + c]
 };
 
-// Fills B for tile `tile_id` (all threads; ends with a barrier).
+// Fills B for tile `tile_id` (all threads; ends with a barrier).  One round
+// of global loads: the cell-list start of every block cell and of the cell
+// after each block row (which also give the core rows' ranges, the tile's
+// columns lying inside the block), kept in tab; the row scans and the
+// record indices then come from shared memory.
 __device__ __forceinline__ void tile_setup(const DevParams &P, const CellGrid &G, int tile_id, TileBlock &B)
 {
   const int T = P.tile, R = P.reach;
@@ -52,17 +56,24 @@ __device__ __forceinline__ void tile_setup(const DevParams &P, const CellGrid &G
   const int bx0 = max(cx0 - R, 0), bx1 = min(cx0 + T - 1 + R, P.ncx - 1);
   const int by0 = max(cy0 - R, 0), by1 = min(cy0 + T - 1 + R, P.ncy - 1);
   const int W = bx1 - bx0 + 1, H = by1 - by0 + 1;
+  for (int e = threadIdx.x; e < (W + 1) * H; e += blockDim.x) {
+    const int r = e / (W + 1), c = e % (W + 1);
+    B.tab[e] = G.start[(by0 + r) * P.ncx + bx0 + c];
+  }
+  __syncthreads();
   if (threadIdx.x < 32) {
     const int r = threadIdx.x;
     int len = 0, clen = 0, gsr = 0, cs0r = 0;
     if (r < H) {
-      const int row = (by0 + r) * P.ncx;
-      gsr = G.start[row + bx0];
-      len = G.start[row + bx1 + 1] - gsr;
+      const int *row = B.tab + r * (W + 1);
+      gsr = row[0];
+      len = row[W] - gsr;
       const int cr = by0 + r - cy0;
       if (cr >= 0 && cr < T) {
-        cs0r = G.start[row + cx0];
-        clen = G.start[row + cx0 + T] - cs0r;
+        // the tile's columns cx0 .. cx0 + T - 1 lie inside the block (ncx is
+        // a multiple of T), so their starts and the one after are in tab
+        cs0r = row[cx0 - bx0];
+        clen = row[cx0 + T - bx0] - cs0r;
       }
     }
     int il = len, ic = clen;
@@ -91,9 +102,10 @@ __device__ __forceinline__ void tile_setup(const DevParams &P, const CellGrid &G
     }
   }
   __syncthreads();
+  // list positions -> record indices of the block
   for (int e = threadIdx.x; e < (W + 1) * H; e += blockDim.x) {
-    const int r = e / (W + 1), c = e % (W + 1);
-    B.tab[e] = B.roff[r] + (G.start[(by0 + r) * P.ncx + bx0 + c] - B.gs[r]);
+    const int r = e / (W + 1);
+    B.tab[e] = B.roff[r] + (B.tab[e] - B.gs[r]);
   }
   __syncthreads();
 }
@@ -115,6 +127,23 @@ __device__ __forceinline__ void tile_core(const TileBlock &B, int k, int &rec, i
   pos = B.cs0[r] + (k - B.coff[r]);
   const int br = r;  // core rows are block rows with the same index
   rec = B.roff[br] + (pos - B.gs[br]);
+}
+
+// The same, with the grid cell (cx, cy) the particle is listed in: the
+// block cell of its row whose record range holds rec (the largest column
+// whose first record is <= rec), from tab, without a global load.
+__device__ __forceinline__ void tile_core_cell(const TileBlock &B, int k, int &rec, int &pos, int &cx, int &cy)
+{
+  const int r = tile_row_of(B.coff, k);
+  pos = B.cs0[r] + (k - B.coff[r]);
+  rec = B.roff[r] + (pos - B.gs[r]);
+  const int *row = B.tab + r * (B.W + 1);
+  int c = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    if (c + step < B.W && row[c + step] <= rec) c += step;
+  cx = B.bx0 + c;
+  cy = B.by0 + r;
 }
 
 // cell-list position of record k of the block

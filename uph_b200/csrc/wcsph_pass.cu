@@ -349,18 +349,29 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
   // the origin of the block: FP32 positions are taken relative to it
   const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
   if (staged) {
-    for (int k = threadIdx.x; k < B.nrec; k += kTileThreads) {
-      const WcRec<Real> r = load_wc_rec<Real>(S, G.list[tile_record_pos(B, k)], ox, oy);
-      rec[k] = r;
-      s_posf[k] = make_float2((float)(r.x - ox), (float)(r.y - oy));
+    // two records per thread at a time, every load issued before the first
+    // store (two rounds of loads: the slots, then their fields)
+    for (int k0 = threadIdx.x; k0 < B.nrec; k0 += 2 * kTileThreads) {
+      const int k1 = k0 + kTileThreads;
+      const bool two = k1 < B.nrec;
+      const int s0 = G.list[tile_record_pos(B, k0)];
+      const int s1 = two ? G.list[tile_record_pos(B, k1)] : s0;
+      const WcRec<Real> r0 = load_wc_rec<Real>(S, s0, ox, oy);
+      const WcRec<Real> r1 = load_wc_rec<Real>(S, s1, ox, oy);
+      rec[k0] = r0;
+      s_posf[k0] = make_float2((float)(r0.x - ox), (float)(r0.y - oy));
+      if (two) {
+        rec[k1] = r1;
+        s_posf[k1] = make_float2((float)(r1.x - ox), (float)(r1.y - oy));
+      }
     }
     __syncthreads();
     const WcStagedSrc<Real> src{rec, s_posf};
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
-      int kr = 0, pos = 0, a = 0;
+      int kr = 0, pos = 0, a = 0, cx = B.bx0, cy = B.by0;
       if (k < ncore) {
-        tile_core(B, k, kr, pos);
+        tile_core_cell(B, k, kr, pos, cx, cy);
         a = G.list[pos];
       }
       const bool active = k < ncore && a < P.nf;
@@ -374,8 +385,7 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       }
       const WcRec<Real> o = rec[active ? kr : 0];
       StagedCursor cur;
-      const int cell = active ? G.cell_of[a] : B.by0 * P.ncx + B.bx0;
-      cur.c.init(B, P.reach, cell % P.ncx, cell / P.ncx);
+      cur.c.init(B, P.reach, active ? cx : B.bx0, active ? cy : B.by0);
       const float2 of = s_posf[active ? kr : 0];
       const F32Test ft = make_f32_test(P, B, of.x, of.y);
       Real drho = 0, ax = 0, ay = 0;
