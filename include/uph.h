@@ -209,6 +209,16 @@ uph_status uph_sim_set_graph(uph_sim *sim, int32_t steps_per_graph);
  * corrector is sph.cc:137-168.) */
 uph_status uph_sim_set_fused_step(uph_sim *sim, int32_t enable);
 
+/* Whether the rate passes keep a candidate list per fluid particle between
+ * cell-list builds (default 1): at a build's first pass each particle lists
+ * the records of its tile's block within the search radius plus twice the
+ * largest displacement before the next build (up to 24 of them), and the
+ * passes until the next build test only those instead of walking the cell
+ * stencil.  The pairs, their order and so the results are bit-identical
+ * either way.  (The reference rebuilds its kd-tree search every call,
+ * Search.cc:5-44.) */
+uph_status uph_sim_set_candidate_lists(uph_sim *sim, int32_t enable);
+
 /* Execution tuning (no counterpart in the reference): cell width = search
  * radius / reach (reach 1-3), particle-storage tile edge in cells (power of
  * two <= 32) and the storage re-sort interval in steps.  Defaults 2, 8, 16. */

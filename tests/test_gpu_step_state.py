@@ -60,16 +60,19 @@ def _fused_cases():
 def test_fused_step_matches_separate_corrector(case, deck, profile, precision, knn):
     """The rate pass that applies the leapfrog step in its epilogue (writing
     the other state buffer) leaves every field bit-identical to the pass
-    followed by the stand-alone corrector, through multi-step calls, graph
-    replays, storage re-sorts and downloads in between."""
+    followed by the stand-alone corrector, and the passes' per-particle
+    candidate lists leave it bit-identical to walking the cell stencil at
+    every pass, through multi-step calls, graph replays, storage re-sorts and
+    downloads in between."""
     from uph_b200._capi import empty_state
     from uph_b200.sim import Simulation
 
     nf, n = deck.n_fluid, deck.n_all
     runs = []
-    for fused in (False, True):
+    for fused, lists in ((False, True), (True, True), (True, False)):
         with Simulation.from_deck(deck, profile=profile, precision=precision, knn_cap=knn) as s:
             s.set_fused_step(fused)
+            s.set_candidate_lists(lists)
             s.set_tuning(2, 8, 3)
             states = []
             for k, nsteps in enumerate([1, 4, 4, 3, 4, 1, 4]):
@@ -80,8 +83,9 @@ def test_fused_step_matches_separate_corrector(case, deck, profile, precision, k
                 s.download(out)
                 states.append(out)
             runs.append(states)
-    for k, (a, b) in enumerate(zip(*runs)):
-        for f in a:
-            assert np.array_equal(a[f], b[f], equal_nan=True), (k, f)
+    for other in runs[1:]:
+        for k, (a, b) in enumerate(zip(runs[0], other)):
+            for f in a:
+                assert np.array_equal(a[f], b[f], equal_nan=True), (k, f)
     last = runs[1][-1]
     assert np.abs(last["Velocity"][:nf]).max() > 0

@@ -30,6 +30,7 @@ SIGNATURES = {
     "uph_sim_step": (C.c_int, [C.c_void_p, C.c_int32]),
     "uph_sim_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "uph_sim_set_fused_step": (C.c_int, [C.c_void_p, C.c_int32]),
+    "uph_sim_set_candidate_lists": (C.c_int, [C.c_void_p, C.c_int32]),
     "uph_sim_set_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "uph_sim_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32 * 3), C.POINTER(C.c_double)]),
     "uph_sim_set_wall_motion": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -195,7 +195,10 @@ __device__ __forceinline__ bool cell_build_phases(const CellBuildArgs &A, int *s
   if (!cell_grid_barrier(A.G.bar, A.err)) return false;
 
   // 4. per-cell sort by slot
-  if (A.rebuild && b == 0 && t == 0) *A.rebuild = 0u;
+  if (b == 0 && t == 0) {
+    if (A.rebuild) *A.rebuild = 0u;
+    if (A.G.gen) *A.G.gen += 1u;  // the passes' candidate lists are stale
+  }
   for (int c = b * nt + t; c < ncell; c += stride) {
     const int a0 = start[c], a1 = start[c + 1];
     if (a1 - a0 > kMaxCellOccupancy) {

@@ -411,17 +411,31 @@ struct GlobalSrc {
   }
 };
 // Phase 1 and 2 for one own particle until its stencil is exhausted.
+// nshort >= 0: the own particle's candidate list, nshort entries, is in its
+// column of s_nb (kF32 only); else the stencil is walked, appending to
+// vl_out (if not null) as tile_list does.
 template <bool kBrute, bool kKnn, bool kF32, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ void ref_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
                                              const RefOwn &o, const F32Test &ft, Entry *s_nb, RefAcc &A, double &bx,
-                                             double &by, unsigned &my_pairs, int &my_nb, double cd, int cj)
+                                             double &by, unsigned &my_pairs, int &my_nb, double cd, int cj,
+                                             int nshort, unsigned short *vl_out, int &vl_cnt)
 {
   constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
   const int col = threadIdx.x;
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
-    const int cnt = tile_list<kBrute, kTileChunk, kKnn, kF32>(P, src, cur, more, self, o.r.orig, o.r.x, o.r.y, ft,
-                                                              s_nb, col, my_pairs, my_nb, bx, by, cd, cj);
+    int cnt = 0;
+    if (kF32 && nshort >= 0) {
+      if constexpr (kF32) {
+        if (more)
+          cnt = tile_list_short<kBrute, kKnn>(P, src, nshort, self, o.r.orig, o.r.x, o.r.y, ft, s_nb, col, my_pairs,
+                                              my_nb, bx, by, cd, cj);
+      }
+      more = false;
+    } else {
+      cnt = tile_list<kBrute, kTileChunk, kKnn, kF32>(P, src, cur, more, self, o.r.orig, o.r.x, o.r.y, ft, s_nb, col,
+                                                      my_pairs, my_nb, bx, by, cd, cj, vl_out, vl_cnt);
+    }
     __syncwarp();
     for (int e = 0; e < cnt; e++) {
       const Entry ent = s_nb[e * kTileThreads + col];
@@ -514,6 +528,10 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
     }
     __syncthreads();
     const StagedSrc src{rec, s_posf, s_cd, s_cj};
+    // this tile's candidate lists are current if written since the last
+    // build (G.vl null: the lists are off, every particle walks the stencil)
+    const unsigned gen = G.vl ? *G.gen : 0u;
+    const bool vl_use = G.vl && G.tile_gen[tile] == gen;
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0, cx = B.bx0, cy = B.by0;
@@ -541,10 +559,15 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
       if (kKnn && active) src.cut(kr, cd, cj);
       const float2 of = s_posf[active ? kr : 0];
       const F32Test ft = make_f32_test(P, B, of.x, of.y);
+      int nshort = -1, vl_cnt = 0;
+      unsigned short *vl_out = nullptr;
+      if (active && G.vl) nshort = load_candidates(G, a, vl_use, s_nb16, threadIdx.x, vl_out);
       RefAcc A = {};
       double bx = 0.0, by = 0.0;
       int nb = 0;
-      ref_particle<kBrute, kKnn, true>(P, src, cur, active, kr, o, ft, s_nb16, A, bx, by, my_pairs, nb, cd, cj);
+      ref_particle<kBrute, kKnn, true>(P, src, cur, active, kr, o, ft, s_nb16, A, bx, by, my_pairs, nb, cd, cj, nshort,
+                                       vl_out, vl_cnt);
+      if (vl_out) G.vl_n[a] = vl_cnt <= kVlMax ? (unsigned char)vl_cnt : kVlOverflow;
       my_nb = max(my_nb, nb);
       if (active) {
         if (F.enabled)
@@ -553,6 +576,7 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
           ref_epilogue(P, S, a, o, A, bx, by);
       }
     }
+    if (G.vl && !vl_use && threadIdx.x == 0) G.tile_gen[tile] = gen;
   } else {
     // a crowded tile: the same walk over the cell list in global memory
     unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
@@ -577,7 +601,9 @@ __device__ __forceinline__ void ref_tile(const DevParams &P, const SlotArrays &S
       RefAcc A = {};
       double bx = 0.0, by = 0.0;
       int nb = 0;
-      ref_particle<kBrute, kKnn, false>(P, src, cur, active, as, o, ft, s_nb32, A, bx, by, my_pairs, nb, cd, cj);
+      int vl_none = 0;
+      ref_particle<kBrute, kKnn, false>(P, src, cur, active, as, o, ft, s_nb32, A, bx, by, my_pairs, nb, cd, cj, -1,
+                                        nullptr, vl_none);
       my_nb = max(my_nb, nb);
       if (active) {
         if (F.enabled)

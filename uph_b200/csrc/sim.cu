@@ -112,12 +112,16 @@ struct uph_sim {
   // tuning: storage re-sort interval and the grid arrays' capacity in cells
   int reorder_interval = kReorderInterval;
   long long grid_capacity = 0;
+  long long tile_gen_capacity = 0;
   // the fluid state was replaced from outside (the learned surrogate): the
   // next step starts the leapfrog afresh with the first-step half kick
   bool restart = false;
   int64_t serial = 0;  // distinct for every simulation this process creates
   // the REF pass applies the leapfrog step (uph_sim_set_fused_step)
   bool fused_step = true;
+  // the tiled passes keep per-particle candidate lists between cell-list
+  // builds (uph_sim_set_candidate_lists)
+  bool cand_lists = true;
   // per-evaluation diagnostics (off by default)
   bool diag_enabled = false;
   DiagProbes diag_probes = {0, 0, 0, 0};
@@ -474,12 +478,18 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false, const StepOut 
     s->kcut_fresh = true;
   }
   Timer t(s, KF_PASS);
+  // the tiled passes' candidate lists (uph_sim_set_candidate_lists)
+  CellGrid gp = s->G;
+  if (!s->cand_lists) {
+    gp.vl = nullptr;
+    gp.vl_n = nullptr;
+  }
   if (s->P.profile != UPH_PROFILE_REF)
-    r = launch_wcsph_pass(s->P, s->S, s->G, st, F ? *F : StepOut{}, s->stream);
+    r = launch_wcsph_pass(s->P, s->S, gp, st, F ? *F : StepOut{}, s->stream);
   else if (s->P.flag_init_simul == 0)
     r = launch_packing_pass(s->P, s->S, s->G, st, s->stream);
   else
-    r = launch_ref_pass(s->P, s->S, s->G, st, F ? *F : StepOut{}, s->stream);
+    r = launch_ref_pass(s->P, s->S, gp, st, F ? *F : StepOut{}, s->stream);
   if (r != UPH_OK) return r;
   s->launches++;
   if (s->P.stress_type == 2 && s->P.profile == UPH_PROFILE_REF && s->P.flag_init_simul == 1) {
@@ -532,6 +542,19 @@ cudaError_t alloc_grid(uph_sim *s)
   G.ncell = (int)ncell;
   G.nblock_sums = scan_block_sums_needed((int)ncell);
   s->gv.ncell = (int)ncell;
+  // the tiles' candidate-list generations: none matches any build's
+  const long long ntiles = (long long)s->P.ntx * (s->P.ncy / s->P.tile);
+  if (ntiles > s->tile_gen_capacity) {
+    if (G.tile_gen) cudaFree(G.tile_gen);
+    G.tile_gen = nullptr;
+    cudaError_t e = cudaMalloc((void **)&G.tile_gen, sizeof(unsigned) * ntiles);
+    if (e != cudaSuccess) return e;
+    s->tile_gen_capacity = ntiles;
+  }
+  if (ntiles > 0) {
+    cudaError_t e = cudaMemset(G.tile_gen, 0xff, sizeof(unsigned) * ntiles);
+    if (e != cudaSuccess) return e;
+  }
   if (ncell <= s->grid_capacity) return cudaSuccess;
   for (int **p : {&G.count, &G.start, &G.fill, &G.block_sums, &s->gv.count, &s->gv.start, &s->gv.fill}) {
     if (*p) cudaFree(*p);
@@ -783,6 +806,10 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
   TRY(dalloc(s, &s->P.ybin, (size_t)n));
   TRY(dalloc(s, &s->P.rebuild, 1));
   TRY(cudaMemset(s->P.rebuild, 1, sizeof(unsigned)));
+  TRY(dalloc(s, &G.gen, 1));
+  TRY(cudaMemset(G.gen, 0, sizeof(unsigned)));
+  TRY(dalloc(s, &G.vl, (size_t)nf * kVlMax));
+  TRY(dalloc(s, &G.vl_n, (size_t)nf));
   TRY(dalloc(s, &G.rank, (size_t)n));
   TRY(dalloc(s, &G.totals, (size_t)kCellBuildMaxBlocks + 1));
   TRY(dalloc(s, &G.bar, kGridWords));
@@ -862,6 +889,7 @@ extern "C" uph_status uph_sim_destroy(uph_sim *s)
   drop_graph(s);
   for (void *p : s->allocations) cudaFree(p);
   for (void *p : {(void *)s->G.count, (void *)s->G.start, (void *)s->G.fill, (void *)s->G.block_sums,
+                  (void *)s->G.tile_gen,
                   (void *)s->gv.count, (void *)s->gv.start, (void *)s->gv.fill, (void *)s->pe_ip, (void *)s->pe_jp,
                   (void *)s->pe_r2, (void *)s->pe_w, (void *)s->pe_dw})
     if (p) cudaFree(p);
@@ -1168,6 +1196,15 @@ extern "C" uph_status uph_sim_set_fused_step(uph_sim *s, int32_t enable)
   drop_graph(s);
   s->fused_step = enable != 0;
   return UPH_OK;
+}
+
+extern "C" uph_status uph_sim_set_candidate_lists(uph_sim *s, int32_t enable)
+{
+  if (!s) return fail(UPH_BAD_ARG, "NULL sim");
+  drop_graph(s);
+  s->cand_lists = enable != 0;
+  // lists written before a switch off are not trusted after a switch back on
+  return force_rebuild(s);
 }
 
 extern "C" uph_status uph_sim_set_wall_motion(uph_sim *s, const double *x0, const double *half_stroke,

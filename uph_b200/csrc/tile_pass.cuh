@@ -217,6 +217,7 @@ struct F32Test {
   float xa, ya;  // own position relative to the origin
   float lo, hi;  // r2cut (1 -+ band): surely inside below lo, surely outside above hi
   float tiny;    // below this, r^2 may be at the DBL_EPSILON coincidence test: exact
+  float vl;      // the candidate lists' radius squared (1 + band)
 };
 
 __device__ __forceinline__ F32Test make_f32_test(const DevParams &P, const TileBlock &B, float xa, float ya)
@@ -224,8 +225,11 @@ __device__ __forceinline__ F32Test make_f32_test(const DevParams &P, const TileB
   const double R = sqrt(P.r2cut);
   const double E = (double)max(B.W, B.H) * P.cell;
   const double band = 32.0 * (E / R) * 0x1p-23 + 0x1p-20;
+  // between two builds a particle moves at most the skin along each axis,
+  // so a pair's distance shrinks by at most 2 sqrt(2) skin
+  const double Rl = R + 2.0 * 1.4142135623730951 * P.skin;
   return F32Test{xa, ya, (float)(P.r2cut * (1.0 - band)), (float)(P.r2cut * (1.0 + band)),
-                 (float)(P.r2cut * 1e-3)};
+                 (float)(P.r2cut * 1e-3), (float)(Rl * Rl * (1.0 + band))};
 }
 
 // Phase 1 of a rate pass: lists up to kChunk in-radius partners of the own
@@ -241,13 +245,101 @@ __device__ __forceinline__ F32Test make_f32_test(const DevParams &P, const TileB
 // kKnn: the reference's k-nearest cap (DevParams::knn): a pair is kept iff
 // the partner is among query i's kept points -- the own particle's cut
 // (cd, cj) when it is i, the partner's (src.cut(b)) when the partner is i.
+// The own particle's (slot a) candidate list for its listing.  use (the
+// tile's lists are current) and no overflow: the entries are copied into
+// column col of s_nb and their count returned.  Else -1: the stencil is
+// walked, and vl_out points at the particle's list to write meanwhile (null
+// when the lists are current but this one overflowed).
+static_assert(kVlMax == 24 && kVlMax <= kTileChunk, "a candidate list is three 16-byte words and fits a column");
+__device__ __forceinline__ int load_candidates(const CellGrid &G, int a, bool use, unsigned short *s_nb, int col,
+                                               unsigned short *&vl_out)
+{
+  vl_out = nullptr;
+  if (!use) {
+    vl_out = G.vl + (size_t)a * kVlMax;
+    return -1;
+  }
+  const uint4 *w = reinterpret_cast<const uint4 *>(G.vl + (size_t)a * kVlMax);
+  const uint4 w0 = w[0], w1 = w[1], w2 = w[2];
+  const int n = G.vl_n[a];
+  if (n == kVlOverflow) return -1;
+  const unsigned v[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+#pragma unroll
+  for (int q = 0; q < 12; q++) {
+    if (2 * q < n) s_nb[(2 * q) * kTileThreads + col] = (unsigned short)(v[q] & 0xffffu);
+    if (2 * q + 1 < n) s_nb[(2 * q + 1) * kTileThreads + col] = (unsigned short)(v[q] >> 16);
+  }
+  return n;
+}
+
+// One batch of kB candidates b[] (the own index `self` for none) of the
+// listing: the FP32 pre-test (kF32), the exact predicate and the pair
+// filters; each listed partner goes to row cnt of column col of s_nb.
+// vl_out (may be null): candidates within the list radius are appended to
+// the own particle's candidate list, vl_cnt counting them past kVlMax too.
+template <bool kBrute, bool kKnn, bool kF32, int kB, typename Src, typename Entry>
+__device__ __forceinline__ void list_batch(const DevParams &P, const Src &src, int (&b)[kB], int self, int oa,
+                                           double xa, double ya, const F32Test &ft, Entry *s_nb, int col, int &cnt,
+                                           unsigned &my_pairs, int &my_nb, double &bx, double &by, double cd, int cj,
+                                           unsigned short *vl_out, int &vl_cnt)
+{
+  constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
+  bool sure[kB];  // FP32 says: surely inside and not coincident
+  if constexpr (kF32) {
+    float2 f[kB];
+#pragma unroll
+    for (int u = 0; u < kB; u++) f[u] = src.xyf(b[u]);
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      const float dxf = ft.xa - f[u].x, dyf = ft.ya - f[u].y;
+      const float r2f = fmaf(dxf, dxf, dyf * dyf);
+      if (vl_out && b[u] != self && r2f < ft.vl) {
+        if (vl_cnt < kVlMax) vl_out[vl_cnt] = (unsigned short)b[u];
+        vl_cnt++;
+      }
+      if (r2f > ft.hi) b[u] = self;  // surely outside: drop
+      sure[u] = r2f < ft.lo && r2f > ft.tiny;
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < kB; u++) sure[u] = false;
+  }
+#pragma unroll
+  for (int u = 0; u < kB; u++) {
+    if (b[u] == self) continue;
+    double r2 = 0.0, dxa = 0.0, dya = 0.0;
+    const bool exact = !sure[u] || kBrute || kKnn;
+    if (exact) {
+      const double2 q = src.xy(b[u]);
+      dxa = xa - q.x;
+      dya = ya - q.y;
+      r2 = exact_r2(dxa, dya);
+      if (!(r2 < P.r2cut)) continue;
+    }
+    const int ob = src.orig(b[u]);
+    if (kBrute && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, src.mass(b[u]), bx, by);
+    if (exact && r2 <= DBL_EPSILON) continue;
+    my_nb++;
+    if (max(oa, ob) >= P.pb) continue;
+    const bool isI = ob > oa;
+    if constexpr (kKnn) {
+      double pd;
+      int pj;
+      if (!isI) src.cut(b[u], pd, pj);
+      if (!(isI ? knn_key_le(r2, ob, cd, cj) : knn_key_le(r2, oa, pd, pj))) continue;
+    }
+    my_pairs += isI;
+    s_nb[cnt++ * kTileThreads + col] = (Entry)b[u] | (isI ? kRole : (Entry)0);
+  }
+}
+
 template <bool kBrute, int kChunk, bool kKnn, bool kF32, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cursor &cur, bool &more, int self,
                                         int oa, double xa, double ya, const F32Test &ft, Entry *s_nb, int col,
-                                        unsigned &my_pairs, int &my_nb, double &bx, double &by, double cd, int cj)
+                                        unsigned &my_pairs, int &my_nb, double &bx, double &by, double cd, int cj,
+                                        unsigned short *vl_out, int &vl_cnt)
 {
   constexpr int kB = 4;
-  constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
   int cnt = 0;
   while (more && cnt <= kChunk - kB) {
     int pos;
@@ -259,49 +351,31 @@ __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cur
     int b[kB];
 #pragma unroll
     for (int u = 0; u < kB; u++) b[u] = (u < n) ? cur.at(pos + u) : self;
-    bool sure[kB];  // FP32 says: surely inside and not coincident
-    if constexpr (kF32) {
-      float2 f[kB];
+    list_batch<kBrute, kKnn, kF32, kB>(P, src, b, self, oa, xa, ya, ft, s_nb, col, cnt, my_pairs, my_nb, bx, by, cd,
+                                       cj, vl_out, vl_cnt);
+  }
+  return cnt;
+}
+
+// The listing from the own particle's candidate list, which the caller has
+// copied into rows 0 .. nshort - 1 of column col of s_nb: filtered in place
+// (a listed partner is written at a row not above the one it was read
+// from), in the list's order, which is the stencil walk's.  nshort <=
+// kVlMax <= the rows of s_nb.
+template <bool kBrute, bool kKnn, typename Src, typename Entry>
+__device__ __forceinline__ int tile_list_short(const DevParams &P, const Src &src, int nshort, int self, int oa,
+                                              double xa, double ya, const F32Test &ft, Entry *s_nb, int col,
+                                              unsigned &my_pairs, int &my_nb, double &bx, double &by, double cd,
+                                              int cj)
+{
+  constexpr int kB = 4;
+  int cnt = 0, none = 0;
+  for (int j = 0; j < nshort; j += kB) {
+    int b[kB];
 #pragma unroll
-      for (int u = 0; u < kB; u++) f[u] = src.xyf(b[u]);
-#pragma unroll
-      for (int u = 0; u < kB; u++) {
-        const float dxf = ft.xa - f[u].x, dyf = ft.ya - f[u].y;
-        const float r2f = fmaf(dxf, dxf, dyf * dyf);
-        if (r2f > ft.hi) b[u] = self;  // surely outside: drop
-        sure[u] = r2f < ft.lo && r2f > ft.tiny;
-      }
-    } else {
-#pragma unroll
-      for (int u = 0; u < kB; u++) sure[u] = false;
-    }
-#pragma unroll
-    for (int u = 0; u < kB; u++) {
-      if (b[u] == self) continue;
-      double r2 = 0.0, dxa = 0.0, dya = 0.0;
-      const bool exact = !sure[u] || kBrute || kKnn;
-      if (exact) {
-        const double2 q = src.xy(b[u]);
-        dxa = xa - q.x;
-        dya = ya - q.y;
-        r2 = exact_r2(dxa, dya);
-        if (!(r2 < P.r2cut)) continue;
-      }
-      const int ob = src.orig(b[u]);
-      if (kBrute && ob >= P.b0 && ob < P.b1) brute_wall_force(P, r2, dxa, dya, src.mass(b[u]), bx, by);
-      if (exact && r2 <= DBL_EPSILON) continue;
-      my_nb++;
-      if (max(oa, ob) >= P.pb) continue;
-      const bool isI = ob > oa;
-      if constexpr (kKnn) {
-        double pd;
-        int pj;
-        if (!isI) src.cut(b[u], pd, pj);
-        if (!(isI ? knn_key_le(r2, ob, cd, cj) : knn_key_le(r2, oa, pd, pj))) continue;
-      }
-      my_pairs += isI;
-      s_nb[cnt++ * kTileThreads + col] = (Entry)b[u] | (isI ? kRole : (Entry)0);
-    }
+    for (int u = 0; u < kB; u++) b[u] = (j + u < nshort) ? (int)s_nb[(j + u) * kTileThreads + col] : self;
+    list_batch<kBrute, kKnn, true, kB>(P, src, b, self, oa, xa, ya, ft, s_nb, col, cnt, my_pairs, my_nb, bx, by, cd,
+                                       cj, nullptr, none);
   }
   return cnt;
 }

@@ -193,7 +193,20 @@ struct CellGrid {
   int *rank;       // [n]
   int *totals;     // [kCellBuildMaxBlocks + 1]
   unsigned *bar;   // [kGridWords]
+  // The tiled passes' candidate lists (the simulation's main grid only; null
+  // on other grids).  gen counts the builds that rebuilt the list.  A tile
+  // whose tile_gen equals gen has, for each of its fluid particles (by
+  // slot), vl_n candidates in vl[slot * kVlMax ...]: the records of its
+  // block within the list radius (the search radius plus twice the largest
+  // displacement a rebuild allows), in the stencil walk's order, or vl_n ==
+  // kVlOverflow when there were more than kVlMax.
+  unsigned *gen;           // [1]
+  unsigned *tile_gen;      // [number of tiles]
+  unsigned short *vl;      // [nf * kVlMax]
+  unsigned char *vl_n;     // [nf]
 };
+constexpr int kVlMax = 24;
+constexpr unsigned char kVlOverflow = 255;
 
 // Statistics of a rate pass, zeroed by the cell-list launch before it: pairs
 // (i < j) counted from the i side, and the largest in-radius neighbour count

@@ -189,17 +189,30 @@ __device__ __forceinline__ void wc_pair(const DevParams &P, const WcRec<Real> &a
   }
 }
 
+// nshort, vl_out, vl_cnt: the candidate lists, as in the REF pass's
+// ref_particle
 template <bool kBrute, bool kF32, typename Real, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ void wc_particle(const DevParams &P, const Src &src, Cursor &cur, bool active, int self,
                                             const WcRec<Real> &o, const F32Test &ft, Entry *s_nb, Real &drho,
-                                            Real &ax, Real &ay, WcAcc &W, unsigned &my_pairs, int &my_nb)
+                                            Real &ax, Real &ay, WcAcc &W, unsigned &my_pairs, int &my_nb, int nshort,
+                                            unsigned short *vl_out, int &vl_cnt)
 {
   constexpr Entry kRole = sizeof(Entry) == 2 ? (Entry)kRoleI16 : (Entry)kRoleI;
   const int col = threadIdx.x;
   bool more = active;
   while (__any_sync(0xffffffffu, more)) {
-    const int cnt = tile_list<kBrute, kTileChunk, false, kF32>(P, src, cur, more, self, o.orig, o.x, o.y, ft, s_nb,
-                                                               col, my_pairs, my_nb, W.wx, W.wy, 0.0, 0);
+    int cnt = 0;
+    if (kF32 && nshort >= 0) {
+      if constexpr (kF32) {
+        if (more)
+          cnt = tile_list_short<kBrute, false>(P, src, nshort, self, o.orig, o.x, o.y, ft, s_nb, col, my_pairs, my_nb,
+                                               W.wx, W.wy, 0.0, 0);
+      }
+      more = false;
+    } else {
+      cnt = tile_list<kBrute, kTileChunk, false, kF32>(P, src, cur, more, self, o.orig, o.x, o.y, ft, s_nb, col,
+                                                       my_pairs, my_nb, W.wx, W.wy, 0.0, 0, vl_out, vl_cnt);
+    }
     __syncwarp();
     for (int e = 0; e < cnt; e++) {
       const Entry ent = s_nb[e * kTileThreads + col];
@@ -367,6 +380,10 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
     }
     __syncthreads();
     const WcStagedSrc<Real> src{rec, s_posf};
+    // this tile's candidate lists are current if written since the last
+    // build (G.vl null: the lists are off, every particle walks the stencil)
+    const unsigned gen = G.vl ? *G.gen : 0u;
+    const bool vl_use = G.vl && G.tile_gen[tile] == gen;
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0, cx = B.bx0, cy = B.by0;
@@ -391,7 +408,12 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       Real drho = 0, ax = 0, ay = 0;
       WcAcc W = {0.0, 0.0};
       int nb = 0;
-      wc_particle<kBrute, true, Real>(P, src, cur, active, kr, o, ft, s_nb16, drho, ax, ay, W, my_pairs, nb);
+      int nshort = -1, vl_cnt = 0;
+      unsigned short *vl_out = nullptr;
+      if (active && G.vl) nshort = load_candidates(G, a, vl_use, s_nb16, threadIdx.x, vl_out);
+      wc_particle<kBrute, true, Real>(P, src, cur, active, kr, o, ft, s_nb16, drho, ax, ay, W, my_pairs, nb, nshort,
+                                      vl_out, vl_cnt);
+      if (vl_out) G.vl_n[a] = vl_cnt <= kVlMax ? (unsigned char)vl_cnt : kVlOverflow;
       my_nb = max(my_nb, nb);
       if (active) {
         if (F.enabled)
@@ -400,6 +422,7 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
           wc_epilogue<Real>(P, S, a, o, drho, ax, ay, W);
       }
     }
+    if (G.vl && !vl_use && threadIdx.x == 0) G.tile_gen[tile] = gen;
   } else {
     unsigned *s_nb32 = reinterpret_cast<unsigned *>(rec);
     const WcGlobalSrc<Real> src{S, ox, oy};
@@ -420,7 +443,9 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       Real drho = 0, ax = 0, ay = 0;
       WcAcc W = {0.0, 0.0};
       int nb = 0;
-      wc_particle<kBrute, false, Real>(P, src, cur, active, as, o, ft, s_nb32, drho, ax, ay, W, my_pairs, nb);
+      int vl_none = 0;
+      wc_particle<kBrute, false, Real>(P, src, cur, active, as, o, ft, s_nb32, drho, ax, ay, W, my_pairs, nb, -1,
+                                       nullptr, vl_none);
       my_nb = max(my_nb, nb);
       if (active) {
         if (F.enabled)

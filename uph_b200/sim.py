@@ -104,6 +104,11 @@ class Simulation:
         """Whether the rate pass applies the leapfrog step itself (default on)."""
         _lib.check(self.lib.uph_sim_set_fused_step(self.handle, 1 if enable else 0), "uph_sim_set_fused_step")
 
+    def set_candidate_lists(self, enable: bool) -> None:
+        """Whether the rate passes keep per-particle candidate lists between cell-list builds (default on)."""
+        _lib.check(self.lib.uph_sim_set_candidate_lists(self.handle, 1 if enable else 0),
+                   "uph_sim_set_candidate_lists")
+
     def set_tuning(self, reach: int, tile: int, reorder_interval: int) -> None:
         _lib.check(self.lib.uph_sim_set_tuning(self.handle, reach, tile, reorder_interval), "uph_sim_set_tuning")
 
