@@ -45,12 +45,14 @@ WORKLOAD = ("hydrostatic tank 2.0 x 1.0 m, dx=0.002 m (500,000 fluid particles) 
 # the leapfrog step in its epilogue: every interacting particle's 13 FP64
 # fields (x y u v ut vt rho rhot p pt m 1/rho 1/rhot) + orig index + itype +
 # its cell-list entry read once (120 B); every fluid particle's *_min state
-# read (4 x 8 B) and its post-step state written once (x y, the four *_min,
-# u v ut vt rho rhot p pt 1/rho 1/rhot: 16 x 8 B), 160 B.  (The rates and
-# the Tait pressure are written by a call's last step only.)  Neighbour
-# re-reads are served on chip.
+# read (4 x 8 B), its candidate list read (24 record indices of 2 B and a
+# 1 B count) and its post-step state written once (x y, the four *_min,
+# u v ut vt rho rhot p pt 1/rho 1/rhot: 16 x 8 B), 209 B.  (The rates and
+# the Tait pressure are written by a call's last step only; the first pass
+# after a cell-list build writes the candidate lists instead of reading
+# them.)  Neighbour re-reads are served on chip.
 PASS_BYTES_PER_SLOT = 13 * 8 + 4 + 4 + 8
-PASS_BYTES_PER_FLUID = 4 * 8 + 16 * 8
+PASS_BYTES_PER_FLUID = 4 * 8 + 24 * 2 + 1 + 16 * 8
 # with --separate-corrector the pass writes the 12 rates + Tait pressure and
 # reads the sponge factor instead (112 B); the corrector is its own launch
 PASS_BYTES_PER_FLUID_RATES = 13 * 8 + 8

@@ -478,9 +478,11 @@ uph_status rate_pass(uph_sim *s, bool refresh, bool step = false, const StepOut 
     s->kcut_fresh = true;
   }
   Timer t(s, KF_PASS);
-  // the tiled passes' candidate lists (uph_sim_set_candidate_lists)
+  // the tiled passes' candidate lists (uph_sim_set_candidate_lists), for
+  // the steps of uph_sim_step: a lone evaluation (uph_sim_derivatives, after
+  // an upload that rebuilt the list) would only write lists nobody reads
   CellGrid gp = s->G;
-  if (!s->cand_lists) {
+  if (!s->cand_lists || !step) {
     gp.vl = nullptr;
     gp.vl_n = nullptr;
   }
