@@ -362,6 +362,10 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
   // the origin of the block: FP32 positions are taken relative to it
   const double ox = P.lo_x + B.bx0 * P.cell, oy = P.lo_y + B.by0 * P.cell;
   if (staged) {
+    // this tile's candidate lists are current if written since the last
+    // build (G.vl null: the lists are off, every particle walks the stencil)
+    const unsigned gen = G.vl ? *G.gen : 0u;
+    const bool vl_use = G.vl && G.tile_gen[tile] == gen;
     // two records per thread at a time, every load issued before the first
     // store (two rounds of loads: the slots, then their fields)
     for (int k0 = threadIdx.x; k0 < B.nrec; k0 += 2 * kTileThreads) {
@@ -369,6 +373,18 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
       const bool two = k1 < B.nrec;
       const int s0 = G.list[tile_record_pos(B, k0)];
       const int s1 = two ? G.list[tile_record_pos(B, k1)] : s0;
+      // the candidate lists the core's fluid particles will read after the
+      // staging: fetched into L2 meanwhile (the halo's too, for their tiles)
+      if (vl_use) {
+        if (s0 < P.nf) {
+          prefetch_l2(G.vl + (size_t)s0 * kVlMax);
+          prefetch_l2(G.vl_n + s0);
+        }
+        if (two && s1 < P.nf) {
+          prefetch_l2(G.vl + (size_t)s1 * kVlMax);
+          prefetch_l2(G.vl_n + s1);
+        }
+      }
       const WcRec<Real> r0 = load_wc_rec<Real>(S, s0, ox, oy);
       const WcRec<Real> r1 = load_wc_rec<Real>(S, s1, ox, oy);
       rec[k0] = r0;
@@ -380,10 +396,6 @@ __device__ __forceinline__ void wc_tile(const DevParams &P, const SlotArrays &S,
     }
     __syncthreads();
     const WcStagedSrc<Real> src{rec, s_posf};
-    // this tile's candidate lists are current if written since the last
-    // build (G.vl null: the lists are off, every particle walks the stencil)
-    const unsigned gen = G.vl ? *G.gen : 0u;
-    const bool vl_use = G.vl && G.tile_gen[tile] == gen;
     for (int base = 0; base < ncore; base += kTileThreads) {
       const int k = base + threadIdx.x;
       int kr = 0, pos = 0, a = 0, cx = B.bx0, cy = B.by0;
