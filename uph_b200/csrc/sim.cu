@@ -557,7 +557,11 @@ cudaError_t alloc_grid(uph_sim *s)
     cudaError_t e = cudaMemset(G.tile_gen, 0xff, sizeof(unsigned) * ntiles);
     if (e != cudaSuccess) return e;
   }
-  if (ncell <= s->grid_capacity) return cudaSuccess;
+  // cudaMemset runs on the legacy default stream, which the simulation's
+  // non-blocking stream does not wait for: the memsets here must have
+  // completed before the caller's next launch (a list build that started on
+  // stale counts would scatter out of range)
+  if (ncell <= s->grid_capacity) return cudaDeviceSynchronize();
   for (int **p : {&G.count, &G.start, &G.fill, &G.block_sums, &s->gv.count, &s->gv.start, &s->gv.fill}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
@@ -577,7 +581,7 @@ cudaError_t alloc_grid(uph_sim *s)
     if ((e = cudaMemset(V.count, 0, sizeof(int) * ncell)) != cudaSuccess) return e;
   }
   s->grid_capacity = ncell;
-  return cudaSuccess;
+  return cudaDeviceSynchronize();
 }
 
 // Cell width radius / reach; cells per axis rounded up to whole tiles.  A
@@ -872,6 +876,9 @@ extern "C" uph_status uph_sim_create(const uph_params *p, uph_sim **out)
     static std::atomic<int64_t> created{0};
     s->serial = ++created;
   }
+  // the memsets above ran on the legacy default stream, which the
+  // non-blocking stream does not wait for
+  TRY(cudaDeviceSynchronize());
   TRY(cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), s->stream));
   TRY(cudaMemsetAsync(s->d_diag_done, 0, sizeof(unsigned), s->stream));
   TRY(cudaMemsetAsync(s->d_diag, 0, sizeof(DevDiag), s->stream));
