@@ -232,19 +232,6 @@ __device__ __forceinline__ F32Test make_f32_test(const DevParams &P, const TileB
                  (float)(P.r2cut * 1e-3), (float)(Rl * Rl * (1.0 + band))};
 }
 
-// Phase 1 of a rate pass: lists up to kChunk in-radius partners of the own
-// particle (index `self` in the source) into column `col` of s_nb (row
-// stride kTileThreads), four candidates at a time, each entry the partner's
-// index with the role flag set when the own particle is the pair's i.  A
-// partner is in-radius and in the reference's pair list exactly as in
-// list_partners (pass_common.cuh): the decision is always the exact FP64
-// predicate; with kF32 the FP32 pre-test (F32Test) settles the candidates
-// far from the cut-off and the FP64 r^2 is computed only near it.  The
-// brute-force wall modes see every in-radius boundary candidate.  The source
-// gives xy(k), xyf(k) (kF32), orig(k), mass(k).
-// kKnn: the reference's k-nearest cap (DevParams::knn): a pair is kept iff
-// the partner is among query i's kept points -- the own particle's cut
-// (cd, cj) when it is i, the partner's (src.cut(b)) when the partner is i.
 // The own particle's (slot a) candidate list for its listing.  use (the
 // tile's lists are current) and no overflow: the entries are copied into
 // column col of s_nb and their count returned.  Else -1: the stencil is
@@ -333,6 +320,20 @@ __device__ __forceinline__ void list_batch(const DevParams &P, const Src &src, i
   }
 }
 
+// Phase 1 of a rate pass: lists up to kChunk in-radius partners of the own
+// particle (index `self` in the source) into column `col` of s_nb (row
+// stride kTileThreads), four candidates at a time, each entry the partner's
+// index with the role flag set when the own particle is the pair's i.  A
+// partner is in-radius and in the reference's pair list exactly as in
+// list_partners (pass_common.cuh): the decision is always the exact FP64
+// predicate; with kF32 the FP32 pre-test (F32Test) settles the candidates
+// far from the cut-off and the FP64 r^2 is computed only near it.  The
+// brute-force wall modes see every in-radius boundary candidate.  The source
+// gives xy(k), xyf(k) (kF32), orig(k), mass(k).
+// kKnn: the reference's k-nearest cap (DevParams::knn): a pair is kept iff
+// the partner is among query i's kept points -- the own particle's cut
+// (cd, cj) when it is i, the partner's (src.cut(b)) when the partner is i.
+// vl_out, vl_cnt: the candidate list written meanwhile (list_batch).
 template <bool kBrute, int kChunk, bool kKnn, bool kF32, typename Src, typename Cursor, typename Entry>
 __device__ __forceinline__ int tile_list(const DevParams &P, const Src &src, Cursor &cur, bool &more, int self,
                                         int oa, double xa, double ya, const F32Test &ft, Entry *s_nb, int col,
