@@ -53,6 +53,10 @@ def _fused_cases():
     yield "flume_piston_wcsph_fp32", flume, PROFILE_WCSPH, PREC_FP32_PAIR, 0
     # the lid of a driven cavity (movingBoundary 3) under the 40-nearest cap
     yield "lid_cavity_ref_knn40", D.lid_cavity(size=0.3, dx=0.015, layers=2), PROFILE_REF, PREC_FP64, 40
+    # h = 1.5 dx: about 28 partners in radius, so the bulk's candidate lists
+    # overflow (those particles walk the stencil) while the surface's fit
+    yield "dambreak_ref_h15_overflow", D.dam_break(tank=(0.6, 0.5), column=(0.2, 0.3), dx=0.01, eta=1.5), \
+        PROFILE_REF, PREC_FP64, 0
 
 
 @pytest.mark.parametrize("case,deck,profile,precision,knn", list(_fused_cases()),
