@@ -80,7 +80,7 @@ struct uph_sim {
   // the rate pass's statistics, zeroed by the cell-list launch before it
   unsigned long long *d_niac = nullptr;
   int *d_max_nb = nullptr;
-  int *d_perm = nullptr;  // scratch for uploads and reorders
+  int *d_perm = nullptr;  // scratch for uploads
   int itime = 0;
   int steps_since_reorder = 0;
   bool have_rates = false;
@@ -300,11 +300,13 @@ __global__ void k_scatter_download(SlotArrays S, Staging T, int n, int nf)
 }
 
 // D <- S through perm[new slot] = old slot, for slots [0, count)
+// D's slot s takes S's slot perm[s] for the fluid (s < nf) and slot s for
+// the rest (walls keep their order)
 __global__ void k_reorder(SlotArrays D, SlotArrays S, const int *__restrict__ perm, int count, int nf)
 {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= count) return;
-  const int o = perm[s];
+  const int o = s < nf ? perm[s] : s;
   D.x[s] = S.x[o]; D.y[s] = S.y[o]; D.u[s] = S.u[o]; D.v[s] = S.v[o];
   D.ut[s] = S.ut[o]; D.vt[s] = S.vt[o]; D.rho[s] = S.rho[o]; D.rhot[s] = S.rhot[o];
   D.p[s] = S.p[o]; D.pt[s] = S.pt[o]; D.m[s] = S.m[o]; D.inv_rho[s] = S.inv_rho[o];
@@ -352,12 +354,6 @@ __global__ void k_wall_base(DevParams P, SlotArrays S, double *base, double t0)
   else
     b = S.y[s] - (t0 <= 0.0 ? 0.0 : U * fmin(t0, P.gate_stop));
   base[o - P.m0] = b;
-}
-
-__global__ void k_iota(int *p, int first, int count)
-{
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < count) p[first + k] = first + k;
 }
 
 // counting sort of ids [first, first+count) by cell, result: G.list[0, count)
@@ -410,10 +406,9 @@ uph_status reorder_fluid(uph_sim *s)
   const int nf = s->P.nf, n = s->P.n;
   uph_status r = sort_range(s, s->S.x, s->S.y, 0, nf, true);
   if (r != UPH_OK) return r;
-  UPH_CUDA(cudaMemcpyAsync(s->d_perm, s->G.list, sizeof(int) * nf, cudaMemcpyDeviceToDevice, s->stream));
-  if (n > nf) k_iota<<<(n - nf + 255) / 256, 256, 0, s->stream>>>(s->d_perm, nf, n - nf);
-  k_reorder<<<(n + 255) / 256, 256, 0, s->stream>>>(s->S2, s->S, s->d_perm, n, nf);
-  s->launches += 2;
+  // the fluid's new order is the list the sort left in G.list[0, nf)
+  k_reorder<<<(n + 255) / 256, 256, 0, s->stream>>>(s->S2, s->S, s->G.list, n, nf);
+  s->launches += 1;
   SlotArrays tmp = s->S;
   s->S = s->S2;
   s->S2 = tmp;
