@@ -234,9 +234,11 @@ def gpu_arm(args, rank, world, local_rank):
         uuid = "GPU-" + str(uuid) if uuid else None
     except Exception:
         uuid = None
+    builds0 = sim.stats()["list_builds"]
     ms, launches, clocks = timed_steps(sim, args.steps, ClockSampler(uuid) if rank == 0 else None)
     ktimes = sim.kernel_times()
     stats = sim.stats()
+    stats["list_builds_per_step"] = (stats["list_builds"] - builds0) / args.steps
     sim.profile(False)
     ms_max = max_over_ranks(ms)
     value = whole_job_rate(nf * args.steps, ms_max / 1e3, world)
@@ -712,7 +714,8 @@ def main():
         "clocks": r["clocks"],
         "kernel_ms": kt,
         "variants": r["variants"],
-        "stats": {"niac": r["stats"]["niac"], "max_neighbors": r["stats"]["max_neighbors"]},
+        "stats": {"niac": r["stats"]["niac"], "max_neighbors": r["stats"]["max_neighbors"],
+                  "list_builds_per_step": r["stats"]["list_builds_per_step"]},
     }
     print(json.dumps(line), flush=True)
 

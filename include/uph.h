@@ -152,6 +152,9 @@ typedef struct uph_stats {
   double potential_energy; /* sum m g y over fluid */
   double total_mass;       /* sum m over fluid */
   double max_abs_density_error; /* max |rho - rho0| / rho0 over fluid */
+  int64_t list_builds;     /* cell-list builds that re-binned the particles since the simulation was made
+                              (a step rebuilds when a particle moved more than the skin; uploads and storage
+                              re-sorts sort too) */
 } uph_stats;
 
 typedef struct uph_sim uph_sim;

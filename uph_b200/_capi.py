@@ -110,7 +110,7 @@ class UphStats(C.Structure):
     _fields_ = [
         ("niac", C.c_int64), ("max_neighbors", i32), ("itime", i32),
         ("kinetic_energy", f64), ("potential_energy", f64), ("total_mass", f64),
-        ("max_abs_density_error", f64),
+        ("max_abs_density_error", f64), ("list_builds", C.c_int64),
     ]
 
 

@@ -1719,6 +1719,8 @@ extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
   UPH_CUDA(cudaMemcpyAsync(part.data(), s->d_partials, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s->stream));
   UPH_CUDA(cudaMemcpyAsync(&niac, s->d_niac, sizeof niac, cudaMemcpyDeviceToHost, s->stream));
   UPH_CUDA(cudaMemcpyAsync(&mx, s->d_max_nb, sizeof mx, cudaMemcpyDeviceToHost, s->stream));
+  unsigned builds = 0;
+  UPH_CUDA(cudaMemcpyAsync(&builds, s->G.gen, sizeof builds, cudaMemcpyDeviceToHost, s->stream));
   UPH_CUDA(cudaStreamSynchronize(s->stream));
   for (int b = 0; b < nb; b++) {
     out->kinetic_energy += part[b];
@@ -1729,6 +1731,7 @@ extern "C" uph_status uph_sim_stats(uph_sim *s, uph_stats *out)
   out->niac = s->have_rates ? (int64_t)niac : 0;
   out->max_neighbors = s->have_rates ? mx : 0;
   out->itime = s->itime;
+  out->list_builds = builds;
   return UPH_OK;
 }
 
