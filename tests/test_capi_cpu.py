@@ -185,3 +185,29 @@ def test_sim_create_rejects_unsupported_modes():
         p = UphParams.from_dict(d)
         h = C.c_void_p()
         assert _lib.lib().uph_sim_create(C.byref(p), C.byref(h)) == status, over
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+def test_python_structs_match_the_c_header():
+    """The ctypes mirrors of include/uph.h's structs have the header's size
+    and field offsets (a mismatch would let the library write past a Python
+    buffer)."""
+    from uph_b200._capi import UphDiagnostics, UphStats
+    checks = [("uph_stats", UphStats), ("uph_params", UphParams), ("uph_diagnostics", UphDiagnostics)]
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"uph.h\"\nint main(void){\n"
+    for cname, cls in checks:
+        src += f'printf("%zu\\n", sizeof({cname}));\n'
+        for field, _ in cls._fields_:
+            src += f'printf("%zu\\n", offsetof({cname}, {field}));\n'
+    src += "return 0;}\n"
+    with tempfile.TemporaryDirectory() as tmp:
+        c = os.path.join(tmp, "s.c")
+        open(c, "w").write(src)
+        exe = os.path.join(tmp, "s")
+        subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for _, cls in checks:
+        want.append(C.sizeof(cls))
+        want += [getattr(cls, field).offset for field, _ in cls._fields_]
+    assert got == want
