@@ -317,12 +317,19 @@ extern "C" void derivatives(System *sys, double t)
     sys->velocityFluctuation[i][0] = 0.0;
     sys->velocityFluctuation[i][1] = 0.0;
   }
+  // the pair count, and TotalKineticEnergy (derivatives.c:2254-2264): the
+  // reference's terms over the fluid, reduced on the device from the state
+  // this call uploaded (a fixed grid of partial sums, so the result does not
+  // depend on anything but the state; it can differ from the serial sum in
+  // the last bits)
+  uph_stats st;
+  s = uph_sim_stats(g.sim, &st);
+  if (s != UPH_OK) die("derivatives", s);
+  sys->totalKineticEnergy = st.kinetic_energy;
+  sys->potentialEnergy = st.potential_energy;
   // pair list (CalculateKernel's outputs, derivatives.c:1076-1105)
   int64_t niac = 0;
   if (g.pair_export == 0) {
-    uph_stats st;
-    s = uph_sim_stats(g.sim, &st);
-    if (s != UPH_OK) die("derivatives", s);
     niac = st.niac;
   } else {
     const bool all = g.pair_export >= 2;
@@ -337,30 +344,6 @@ extern "C" void derivatives(System *sys, double t)
     if (s != UPH_OK) die("derivatives", s);
     for (int i = nf; i < nf + nb; i++) sys->approxVorticity[i] = 0.0;  // derivatives.c:2843-2846
   }
-  // TotalKineticEnergy, derivatives.c:2254-2264: the reference's terms, summed
-  // in 64 fixed chunks and then the chunks in order, so the result does not
-  // depend on the thread count (it can differ from the serial sum in the
-  // last bits)
-  constexpr int kChunks = 64;
-  double ke_c[kChunks], pe_c[kChunks];
-#pragma omp parallel for schedule(static)
-  for (int c = 0; c < kChunks; c++) {
-    const int i0 = (int)((int64_t)nf * c / kChunks), i1 = (int)((int64_t)nf * (c + 1) / kChunks);
-    double ke = 0.0, pe = 0.0;
-    for (int i = i0; i < i1; i++) {
-      ke += 0.5 * sys->mass[i] * (sys->Velocity[i][0] * sys->Velocity[i][0] + sys->Velocity[i][1] * sys->Velocity[i][1]);
-      pe += sys->mass[i] * sys->Gravity * sys->Position[i][1];
-    }
-    ke_c[c] = ke;
-    pe_c[c] = pe;
-  }
-  double ke = 0.0, pe = 0.0;
-  for (int c = 0; c < kChunks; c++) {
-    ke += ke_c[c];
-    pe += pe_c[c];
-  }
-  sys->totalKineticEnergy = ke;
-  sys->potentialEnergy = pe;
 }
 
 extern "C" int SearchNeighbors(const double **Position, int *i_pair, int *j_pair, double *rij2,
